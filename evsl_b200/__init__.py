@@ -1,0 +1,335 @@
+"""evsl_b200 -- B200-native polynomial-filtered spectrum slicing (EVSL API).
+
+The product is the C-ABI shared library ``libevsl_b200.so`` built from
+``evsl_b200/csrc`` (C99 host keeping EVSL's API + CUDA sm_100a kernels).  This
+module is a thin ctypes binding of that library, mirroring the reference's
+entry points (EVSLStart, SetAMatrix, find_pol, ChebLanNr, ChebLanTr, kpmdos,
+spslicer, ChebAv) with numpy arrays for host data.  It contains no numerical
+code of its own: every call goes through the library, and importing fails
+loudly if the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["Library", "PolParams", "DeviceBuffer", "EvslError", "library_path", "load"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def library_path() -> str:
+    return os.path.join(_HERE, "libevsl_b200.so")
+
+
+class EvslError(RuntimeError):
+    """A non-zero return code from the library."""
+
+
+class PolParams(C.Structure):
+    """polparams, same layout as the reference (INC/struct.h:68-98)."""
+
+    _fields_ = [
+        ("max_deg", C.c_int),
+        ("min_deg", C.c_int),
+        ("damping", C.c_int),
+        ("thresh_ext", C.c_double),
+        ("thresh_int", C.c_double),
+        ("intvtol", C.c_double),
+        ("type", C.c_int),
+        ("mu", C.POINTER(C.c_double)),
+        ("cc", C.c_double),
+        ("dd", C.c_double),
+        ("gam", C.c_double),
+        ("bar", C.c_double),
+        ("deg", C.c_int),
+    ]
+
+    def as_dict(self):
+        mu = np.ctypeslib.as_array(self.mu, (self.deg + 1,)).copy() if self.mu else None
+        return dict(type=self.type, deg=self.deg, cc=self.cc, dd=self.dd, gam=self.gam, bar=self.bar, mu=mu)
+
+
+class CsrMat(C.Structure):
+    """csrMat, same layout as the reference CUDA build (INC/struct.h:29-42)."""
+
+    _fields_ = [
+        ("owndata", C.c_int),
+        ("nrows", C.c_int),
+        ("ncols", C.c_int),
+        ("nnz", C.c_int),
+        ("ia", C.POINTER(C.c_int)),
+        ("ja", C.POINTER(C.c_int)),
+        ("a", C.POINTER(C.c_double)),
+        ("descr", C.c_void_p),
+        ("dBuffer", C.c_char_p),
+    ]
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+_LIB = None
+
+
+def load():
+    """Load libevsl_b200.so (raises if it is missing)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `make -C evsl_b200/csrc` "
+                          "(or __graft_entry__.build())")
+    lib = C.CDLL(path, mode=C.RTLD_LOCAL)
+    sig = {
+        "EVSLStart": ([], C.c_int),
+        "EVSLFinish": ([], C.c_int),
+        "SetAMatrix": ([C.POINTER(CsrMat)], C.c_int),
+        "SetAMatrix_device_csr": ([C.POINTER(CsrMat)], C.c_int),
+        "SetAMatvec": ([C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+        "set_pol_def": ([C.POINTER(PolParams)], None),
+        "find_pol": ([_dp, C.POINTER(PolParams)], C.c_int),
+        "free_pol": ([C.POINTER(PolParams)], None),
+        "ChebAv": ([C.POINTER(PolParams), C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+        "ChebLanNr": ([_dp, C.c_int, C.c_double, C.c_void_p, C.POINTER(PolParams), _ip,
+                       C.POINTER(_dp), C.POINTER(C.c_void_p), C.POINTER(_dp), C.c_void_p], C.c_int),
+        "ChebLanTr": ([C.c_int, C.c_int, _dp, C.c_int, C.c_double, C.c_void_p, C.POINTER(PolParams), _ip,
+                       C.POINTER(_dp), C.POINTER(C.c_void_p), C.POINTER(_dp), C.c_void_p], C.c_int),
+        "kpmdos": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp], C.c_int),
+        "spslicer": ([_dp, _dp, C.c_int, _dp, C.c_int, C.c_int], C.c_int),
+        "dampcf": ([C.c_int, C.c_int, _dp], C.c_int),
+        "_evsl_Malloc_device": ([C.c_size_t], C.c_void_p),
+        "_evsl_Free_device": ([C.c_void_p], None),
+        "_evsl_Free": ([C.c_void_p], None),
+        "evsl_memcpy_host_to_device": ([C.c_void_p, C.c_void_p, C.c_size_t], None),
+        "evsl_memcpy_device_to_host": ([C.c_void_p, C.c_void_p, C.c_size_t], None),
+        "rand_double_device": ([C.c_int, C.c_void_p], None),
+        "evslx_last_error": ([], C.c_char_p),
+        "evslx_set_seed": ([C.c_uint64], C.c_int),
+        "evslx_get_draw": ([], C.c_uint64),
+        "evslx_kpmdos_probes": ([C.c_int, C.c_int, C.c_int, _dp, C.c_void_p, _dp, _dp], C.c_int),
+        "evslx_set_spmv_kernel": ([C.c_int], C.c_int),
+        "evslx_get_spmv_kernel": ([], C.c_int),
+        "evslx_matvec": ([C.c_void_p, C.c_void_p], C.c_int),
+        "evslx_problem_info": ([_ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
+        "evslx_launch_count": ([], C.c_uint64),
+        "evslx_last_kpm_seconds": ([], C.c_double),
+        "evsl_timer": ([], C.c_double),
+        "StatsReset": ([], None),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = lib
+    return lib
+
+
+class DeviceBuffer:
+    """A block of device memory owned by the library allocator."""
+
+    def __init__(self, lib, nbytes, ptr=None, owned=True):
+        self.lib = lib
+        self.nbytes = int(nbytes)
+        self.ptr = ptr if ptr is not None else lib._evsl_Malloc_device(max(self.nbytes, 1))
+        if not self.ptr:
+            raise EvslError(f"device allocation of {nbytes} bytes failed")
+        self.owned = owned
+
+    @classmethod
+    def from_host(cls, lib, arr):
+        arr = np.ascontiguousarray(arr)
+        buf = cls(lib, arr.nbytes)
+        lib.evsl_memcpy_host_to_device(buf.ptr, arr.ctypes.data, arr.nbytes)
+        return buf
+
+    def to_host(self, dtype=np.float64, shape=None):
+        out = np.empty(self.nbytes // np.dtype(dtype).itemsize, dtype=dtype)
+        self.lib.evsl_memcpy_device_to_host(out.ctypes.data, self.ptr, out.nbytes)
+        return out if shape is None else out.reshape(shape)
+
+    def free(self):
+        if self.owned and self.ptr:
+            self.lib._evsl_Free_device(self.ptr)
+        self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Library:
+    """One EVSL session (EVSLStart ... EVSLFinish) on the current GPU."""
+
+    def __init__(self):
+        self.lib = load()
+        self._check(self.lib.EVSLStart(), "EVSLStart")
+        self.n = 0
+        self._csr = None
+        self._keep = None
+
+    # -- errors ------------------------------------------------------------
+    def last_error(self) -> str:
+        return (self.lib.evslx_last_error() or b"").decode(errors="replace")
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise EvslError(f"{what} returned {rc}: {self.last_error()}")
+
+    def finish(self):
+        self._check(self.lib.EVSLFinish(), "EVSLFinish")
+
+    # -- matrix ------------------------------------------------------------
+    def set_csr(self, ia, ja, a):
+        """SetAMatrix with a host CSR (uploaded to the device once)."""
+        ia = np.ascontiguousarray(ia, dtype=np.int32)
+        ja = np.ascontiguousarray(ja, dtype=np.int32)
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        n = len(ia) - 1
+        m = CsrMat(owndata=0, nrows=n, ncols=n, nnz=int(ia[-1]), ia=_i(ia), ja=_i(ja), a=_d(a))
+        self._keep = (ia, ja, a, m)
+        self._check(self.lib.SetAMatrix(C.byref(m)), "SetAMatrix")
+        self.n = n
+
+    def set_csr_device(self, ia, ja, a):
+        """SetAMatrix_device_csr with the CSR copied to device buffers first."""
+        ia = np.ascontiguousarray(ia, dtype=np.int32)
+        ja = np.ascontiguousarray(ja, dtype=np.int32)
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        n = len(ia) - 1
+        bufs = [DeviceBuffer.from_host(self.lib, x) for x in (ia, ja, a)]
+        m = CsrMat(owndata=0, nrows=n, ncols=n, nnz=int(ia[-1]), ia=C.cast(bufs[0].ptr, _ip),
+                   ja=C.cast(bufs[1].ptr, _ip), a=C.cast(bufs[2].ptr, _dp))
+        self._keep = (bufs, m)
+        self._check(self.lib.SetAMatrix_device_csr(C.byref(m)), "SetAMatrix_device_csr")
+        self.n = n
+
+    def set_spmv_kernel(self, which):
+        self._check(self.lib.evslx_set_spmv_kernel(which), "evslx_set_spmv_kernel")
+
+    def problem_info(self):
+        n = C.c_int()
+        nnz = C.c_longlong()
+        st = C.c_longlong()
+        self.lib.evslx_problem_info(C.byref(n), C.byref(nnz), C.byref(st))
+        return n.value, nnz.value, st.value
+
+    def matvec(self, x):
+        dx = DeviceBuffer.from_host(self.lib, np.asarray(x, dtype=np.float64))
+        dy = DeviceBuffer(self.lib, dx.nbytes)
+        self._check(self.lib.evslx_matvec(dx.ptr, dy.ptr), "evslx_matvec")
+        return dy.to_host()
+
+    # -- filter --------------------------------------------------------------
+    def find_pol(self, intv, *, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=None, deg=0):
+        pol = PolParams()
+        self.lib.set_pol_def(C.byref(pol))
+        pol.damping = damping
+        pol.thresh_int = thresh_int
+        pol.thresh_ext = thresh_ext
+        if max_deg is not None:
+            pol.max_deg = max_deg
+        pol.deg = deg
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        rc = self.lib.find_pol(_d(iv), C.byref(pol))
+        if rc != 0:
+            raise EvslError(f"find_pol returned {rc}")
+        return pol
+
+    def free_pol(self, pol):
+        self.lib.free_pol(C.byref(pol))
+
+    def chebav(self, pol, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        dv = DeviceBuffer.from_host(self.lib, v)
+        dy = DeviceBuffer(self.lib, v.nbytes)
+        dw = DeviceBuffer(self.lib, 3 * v.nbytes)
+        self._check(self.lib.ChebAv(C.byref(pol), dv.ptr, dy.ptr, dw.ptr), "ChebAv")
+        return dy.to_host()
+
+    # -- DOS / slicing -----------------------------------------------------
+    def set_seed(self, seed):
+        self.lib.evslx_set_seed(seed)
+
+    def kpmdos(self, Mdeg, damping, nvec, intv):
+        mu = np.zeros(Mdeg + 1)
+        ec = C.c_double()
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        self._check(self.lib.kpmdos(Mdeg, damping, nvec, _d(iv), _d(mu), C.byref(ec)), "kpmdos")
+        return mu, ec.value
+
+    def kpmdos_probes(self, Mdeg, damping, probes, intv):
+        """kpmdos with explicit probe vectors (nvec x n host array)."""
+        probes = np.ascontiguousarray(np.atleast_2d(probes), dtype=np.float64)
+        dp = DeviceBuffer.from_host(self.lib, probes)  # row p = probe p = column p of n x nvec
+        mu = np.zeros(Mdeg + 1)
+        ec = C.c_double()
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        self._check(self.lib.evslx_kpmdos_probes(Mdeg, damping, probes.shape[0], _d(iv), dp.ptr, _d(mu),
+                                                 C.byref(ec)), "evslx_kpmdos_probes")
+        return mu, ec.value
+
+    def spslicer(self, mu, intv, n_int, npts):
+        sli = np.zeros(n_int + 1)
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        rc = self.lib.spslicer(_d(sli), _d(mu), len(mu) - 1, _d(iv), n_int, npts)
+        return rc, sli
+
+    # -- Lanczos -------------------------------------------------------------
+    def _outputs(self, m, lam, W, res, want_vectors):
+        n = self.n
+        if m > 0:
+            lam_h = np.ctypeslib.as_array(lam, (m,)).copy()
+            res_h = np.ctypeslib.as_array(res, (m,)).copy()
+            Y = None
+            if want_vectors:
+                Y = np.empty((m, n))
+                self.lib.evsl_memcpy_device_to_host(Y.ctypes.data, W, Y.nbytes)
+        else:
+            lam_h, res_h, Y = np.zeros(0), np.zeros(0), (np.zeros((0, n)) if want_vectors else None)
+        for p in (lam, res):
+            if p:
+                self.lib._evsl_Free(C.cast(p, C.c_void_p))
+        if W:
+            self.lib._evsl_Free_device(W)
+        return lam_h, Y, res_h
+
+    def cheblan_nr(self, intv, maxit, tol, vinit, pol, want_vectors=True):
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        dv = DeviceBuffer.from_host(self.lib, np.asarray(vinit, dtype=np.float64))
+        nev = C.c_int()
+        lam, res = _dp(), _dp()
+        W = C.c_void_p()
+        rc = self.lib.ChebLanNr(_d(iv), maxit, tol, dv.ptr, C.byref(pol), C.byref(nev), C.byref(lam),
+                                C.byref(W), C.byref(res), None)
+        self._check(rc, "ChebLanNr")
+        return self._outputs(nev.value, lam, W.value, res, want_vectors)
+
+    def cheblan_tr(self, lanm, nev, intv, maxit, tol, vinit, pol, want_vectors=True):
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        dv = DeviceBuffer.from_host(self.lib, np.asarray(vinit, dtype=np.float64))
+        nev2 = C.c_int()
+        lam, res = _dp(), _dp()
+        W = C.c_void_p()
+        rc = self.lib.ChebLanTr(lanm, nev, _d(iv), maxit, tol, dv.ptr, C.byref(pol), C.byref(nev2), C.byref(lam),
+                                C.byref(W), C.byref(res), None)
+        self._check(rc, "ChebLanTr")
+        return self._outputs(nev2.value, lam, W.value, res, want_vectors)
+
+    def launch_count(self):
+        return int(self.lib.evslx_launch_count())

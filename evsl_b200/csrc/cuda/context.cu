@@ -1,0 +1,207 @@
+// Library context: stream, scratch for reductions, memory and error helpers.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <atomic>
+
+#include "common.cuh"
+
+namespace evslcu {
+
+namespace {
+struct Context {
+  bool ready = false;
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  double *partials = nullptr;
+  unsigned int *counters = nullptr;
+  double *scalars = nullptr;
+};
+Context g_ctx;
+char g_err[512] = "";
+std::atomic<uint64_t> g_launches{0};
+}  // namespace
+
+cudaStream_t stream() { return g_ctx.stream; }
+double *partials() { return g_ctx.partials; }
+unsigned int *counters() { return g_ctx.counters; }
+double *dev_scratch_scalars() { return g_ctx.scalars; }
+int sm_count() { return g_ctx.sms; }
+void count_launch(uint64_t k) { g_launches += k; }
+
+int fail(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int check_launch(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e));
+  return 0;
+}
+
+}  // namespace evslcu
+
+using namespace evslcu;
+
+extern "C" {
+
+int evslcu_initialized(void) { return g_ctx.ready ? 1 : 0; }
+
+const char *evslcu_errstr(void) { return g_err; }
+
+void evslcu_set_error(int code, const char *msg) { fail(code, "%s", msg ? msg : ""); }
+
+uint64_t evslcu_launch_count(void) { return g_launches.load(); }
+
+int evslcu_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int evslcu_init(void) {
+  if (g_ctx.ready) return 0;
+  if (evslcu_device_count() < 1) return fail(EVSLCU_ERR_NODEV, "no CUDA device is visible");
+  EVSLCU_CUDA(cudaGetDevice(&g_ctx.device));
+  cudaDeviceProp prop;
+  EVSLCU_CUDA(cudaGetDeviceProperties(&prop, g_ctx.device));
+  if (prop.major < 10)
+    return fail(EVSLCU_ERR_NODEV, "device %s is sm_%d%d; this library is built for sm_100a", prop.name,
+                prop.major, prop.minor);
+  g_ctx.sms = prop.multiProcessorCount;
+  // Blocking w.r.t. the legacy default stream, so user matvec callbacks that
+  // launch on stream 0 are ordered with the library's work.
+  EVSLCU_CUDA(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamDefault));
+  EVSLCU_CUDA(cudaMalloc(&g_ctx.partials, sizeof(double) * (size_t)kMaxPartials * 2));
+  EVSLCU_CUDA(cudaMalloc(&g_ctx.counters, sizeof(unsigned int) * kNumCounters));
+  EVSLCU_CUDA(cudaMemset(g_ctx.counters, 0, sizeof(unsigned int) * kNumCounters));
+  EVSLCU_CUDA(cudaMalloc(&g_ctx.scalars, sizeof(double) * 64));
+  EVSLCU_CUDA(cudaMemset(g_ctx.scalars, 0, sizeof(double) * 64));
+  g_ctx.ready = true;
+  return 0;
+}
+
+int evslcu_finish(void) {
+  if (!g_ctx.ready) return 0;
+  cudaStreamSynchronize(g_ctx.stream);
+  cudaFree(g_ctx.partials);
+  cudaFree(g_ctx.counters);
+  cudaFree(g_ctx.scalars);
+  cudaStreamDestroy(g_ctx.stream);
+  g_ctx = Context();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "pending CUDA error at finish: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+int evslcu_sync(void) {
+  if (!g_ctx.ready) return fail(EVSLCU_ERR_STATE, "library not started (EVSLStart)");
+  EVSLCU_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return 0;
+}
+
+int evslcu_device_name(int dev, char *buf, int len, int *sm, size_t *mem) {
+  cudaDeviceProp prop;
+  EVSLCU_CUDA(cudaGetDeviceProperties(&prop, dev));
+  if (buf && len > 0) snprintf(buf, (size_t)len, "%s", prop.name);
+  if (sm) *sm = prop.multiProcessorCount;
+  if (mem) *mem = prop.totalGlobalMem;
+  return 0;
+}
+
+int evslcu_last_cuda_error(char *buf, int len) {
+  cudaError_t e = cudaGetLastError();
+  if (buf && len > 0) snprintf(buf, (size_t)len, "%s", e == cudaSuccess ? "" : cudaGetErrorString(e));
+  return e == cudaSuccess ? 0 : EVSLCU_ERR_CUDA;
+}
+
+void *evslcu_malloc(size_t nbytes) {
+  void *p = nullptr;
+  if (nbytes == 0) nbytes = 1;
+  cudaError_t e = cudaMalloc(&p, nbytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fail(EVSLCU_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", nbytes, cudaGetErrorString(e));
+    return nullptr;
+  }
+  return p;
+}
+
+int evslcu_free(void *p) {
+  if (!p) return 0;
+  // Memory may still be in use by queued work on the library stream.
+  if (g_ctx.ready) cudaStreamSynchronize(g_ctx.stream);
+  EVSLCU_CUDA(cudaFree(p));
+  return 0;
+}
+
+int evslcu_h2d(void *dst, const void *src, size_t nbytes) {
+  if (!nbytes) return 0;
+  EVSLCU_CUDA(cudaMemcpyAsync(dst, src, nbytes, cudaMemcpyHostToDevice, g_ctx.stream));
+  EVSLCU_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return 0;
+}
+
+int evslcu_h2d_async(void *dst, const void *src, size_t nbytes) {
+  if (!nbytes) return 0;
+  EVSLCU_CUDA(cudaMemcpyAsync(dst, src, nbytes, cudaMemcpyHostToDevice, g_ctx.stream));
+  return 0;
+}
+
+int evslcu_d2h(void *dst, const void *src, size_t nbytes) {
+  if (!nbytes) return 0;
+  EVSLCU_CUDA(cudaMemcpyAsync(dst, src, nbytes, cudaMemcpyDeviceToHost, g_ctx.stream));
+  EVSLCU_CUDA(cudaStreamSynchronize(g_ctx.stream));
+  return 0;
+}
+
+int evslcu_d2d(void *dst, const void *src, size_t nbytes) {
+  if (!nbytes) return 0;
+  EVSLCU_CUDA(cudaMemcpyAsync(dst, src, nbytes, cudaMemcpyDeviceToDevice, g_ctx.stream));
+  return 0;
+}
+
+int evslcu_memset(void *p, int v, size_t nbytes) {
+  if (!nbytes) return 0;
+  EVSLCU_CUDA(cudaMemsetAsync(p, v, nbytes, g_ctx.stream));
+  return 0;
+}
+
+int evslcu_get_scalars(const double *dev, double *host, int count) {
+  return evslcu_d2h(host, dev, sizeof(double) * (size_t)count);
+}
+
+struct evslcu_timer {
+  cudaEvent_t a, b;
+};
+
+evslcu_timer *evslcu_timer_start(void) {
+  evslcu_timer *t = new evslcu_timer;
+  cudaEventCreate(&t->a);
+  cudaEventCreate(&t->b);
+  cudaEventRecord(t->a, g_ctx.stream);
+  return t;
+}
+
+double evslcu_timer_stop(evslcu_timer *t) {
+  if (!t) return 0.0;
+  float ms = 0.f;
+  cudaEventRecord(t->b, g_ctx.stream);
+  cudaEventSynchronize(t->b);
+  cudaEventElapsedTime(&ms, t->a, t->b);
+  cudaEventDestroy(t->a);
+  cudaEventDestroy(t->b);
+  delete t;
+  return 1e-3 * (double)ms;
+}
+
+}  // extern "C"

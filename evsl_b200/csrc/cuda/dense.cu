@@ -1,0 +1,441 @@
+// Dense FP64 kernels: level-1 operations with device-resident scalars,
+// classical Gram-Schmidt with the DGKS test, GEMV/GEMM and the batched Ritz
+// pair evaluation.
+//
+// Reductions are deterministic: every block writes one partial in a fixed
+// thread order and the last block to finish sums the partials in index order.
+// Element-wise updates use explicitly rounded multiply/add so they match the
+// reference CPU build's daxpy/dscal/dgemv('N') arithmetic element for element
+// (SRC/blas/daxpy.c, dscal.c, dgemv.c); only dot products and norms are summed
+// in a different (tree) order.
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+
+using namespace evslcu;
+
+namespace {
+
+constexpr double kEta = 0.70710678118654752440;  // 1/sqrt(2), SRC/misc_la.c:226
+
+__global__ void k_dot(int n, const double *x, const double *y, double *part, unsigned int *ctr, double *out,
+                      int sqrt_result) {
+  __shared__ double sh[kThreads / 32];
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += x[i] * y[i];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+  if (last_block(ctr)) {
+    double t = reduce_partials(part, gridDim.x, ctr, sh);
+    if (threadIdx.x == 0) *out = sqrt_result ? sqrt(t) : t;
+  }
+}
+
+__global__ void k_axpy_ds(int n, const double *coef, double sign, const double *x, double *y) {
+  const double c = sign * (*coef);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = __dadd_rn(y[i], __dmul_rn(c, x[i]));
+}
+
+__global__ void k_axpy(int n, double a, const double *x, double *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = __dadd_rn(y[i], __dmul_rn(a, x[i]));
+}
+
+__global__ void k_scal_inv_ds(int n, const double *s, double *x) {
+  const double t = 1.0 / (*s);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = __dmul_rn(t, x[i]);
+}
+
+__global__ void k_scal(int n, double a, double *x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = __dmul_rn(a, x[i]);
+}
+
+// ---------------------------------------------------------------------------
+// Gram-Schmidt building blocks.  State slots: [0] old norm, [1] new norm,
+// [2] done flag (1.0 once the DGKS test has passed).
+// ---------------------------------------------------------------------------
+constexpr int kGemvTRows = 1024;   // rows per chunk of the transposed product
+constexpr int kGemvTCols = 32;     // columns per block
+constexpr int kGemvNChunk = 2048;  // h values staged in shared memory at once
+
+// part[chunk * k + j] = sum over the chunk's rows of Q[r, j] * v[r]
+__global__ void __launch_bounds__(kThreads)
+    k_gemvT_partial(int n, int k, const double *__restrict__ Q, long long ld, const double *__restrict__ v,
+                    double *__restrict__ part, const double *state) {
+  if (state && state[2] != 0.0) return;
+  __shared__ double sv[kGemvTRows];
+  const int r0 = blockIdx.x * kGemvTRows;
+  const int rows = min(kGemvTRows, n - r0);
+  for (int i = threadIdx.x; i < kGemvTRows; i += blockDim.x) sv[i] = (i < rows) ? v[r0 + i] : 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int jj = warp; jj < kGemvTCols; jj += kThreads / 32) {
+    const int j = blockIdx.y * kGemvTCols + jj;
+    if (j >= k) break;
+    const double *q = Q + (long long)j * ld + r0;
+    double acc = 0.0;
+#pragma unroll 8
+    for (int i = lane; i < rows; i += 32) acc += __ldg(q + i) * sv[i];
+    acc = warp_sum(acc);
+    if (lane == 0) part[(long long)blockIdx.x * k + j] = acc;
+  }
+}
+
+// h[j] = alpha * sum_chunks part[chunk*k + j] (+ beta * h[j] when beta != 0)
+__global__ void k_gemvT_reduce(int nchunks, int k, const double *part, double alpha, double beta, double *h,
+                               const double *state) {
+  if (state && state[2] != 0.0) return;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= k) return;
+  double s = 0.0;
+  for (int c = 0; c < nchunks; ++c) s += part[(long long)c * k + j];
+  h[j] = (beta == 0.0) ? alpha * s : __dadd_rn(__dmul_rn(beta, h[j]), alpha * s);
+}
+
+// v[r] <- v[r] + sum_j (alpha*h[j]) * Q[r, j], summed over j in order as the
+// reference dgemv('N') does.  With `state`, also computes ||v|| and applies
+// the DGKS decision of SRC/misc_la.c:246-250.
+__global__ void __launch_bounds__(kThreads)
+    k_gemvN(int n, int k, const double *__restrict__ Q, long long ld, const double *__restrict__ h, double alpha,
+            double *v, double *part, unsigned int *ctr, double *state) {
+  if (state && state[2] != 0.0) return;
+  __shared__ double sh_h[kGemvNChunk];
+  __shared__ double sh[kThreads / 32];
+  double nsum = 0.0;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+    const long long r = base + threadIdx.x;
+    double z = (r < n) ? v[r] : 0.0;
+    for (int j0 = 0; j0 < k; j0 += kGemvNChunk) {
+      const int cnt = min(kGemvNChunk, k - j0);
+      __syncthreads();
+      for (int j = threadIdx.x; j < cnt; j += blockDim.x) sh_h[j] = alpha * h[j0 + j];
+      __syncthreads();
+      if (r < n) {
+        const double *q = Q + (long long)j0 * ld + r;
+#pragma unroll 8
+        for (int j = 0; j < cnt; ++j) z = __dadd_rn(z, __dmul_rn(sh_h[j], __ldg(q + (long long)j * ld)));
+      }
+    }
+    if (r < n) {
+      v[r] = z;
+      nsum += z * z;
+    }
+  }
+  if (state) {
+    nsum = block_sum(nsum, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = nsum;
+    if (last_block(ctr)) {
+      double t = reduce_partials(part, gridDim.x, ctr, sh);
+      if (threadIdx.x == 0) {
+        const double nw = sqrt(t);
+        state[1] = nw;
+        if (nw > kEta * state[0])
+          state[2] = 1.0;
+        else
+          state[0] = nw;
+      }
+    }
+  }
+}
+
+__global__ void k_cgs_init(double *state, const double *nrm) {
+  state[0] = *nrm;
+  state[1] = 0.0;
+  state[2] = 0.0;
+}
+
+__global__ void k_copy_scalar(const double *src, double *dst) { *dst = *src; }
+
+// y = beta*y for the transposed GEMV when alpha == 0 etc. (rarely used)
+__global__ void k_scale_vec(int n, double beta, double *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = (beta == 0.0) ? 0.0 : __dmul_rn(beta, y[i]);
+}
+
+// ---------------------------------------------------------------------------
+// GEMM: C = alpha op(A) op(B) + beta C, column-major, 64x64 tiles, 4x4 per
+// thread, FP64 FMA.
+// ---------------------------------------------------------------------------
+constexpr int BM = 64, BN = 64, BK = 16;
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256)
+    k_dgemm(int m, int n, int k, double alpha, const double *__restrict__ A, long long lda,
+            const double *__restrict__ B, long long ldb, double beta, double *C, long long ldc) {
+  __shared__ double sA[BK][BM + 1];
+  __shared__ double sB[BK][BN + 1];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < k; k0 += BK) {
+    for (int i = threadIdx.x; i < BM * BK; i += 256) {
+      const int mm = i % BM, kk = i / BM;
+      const int gm = m0 + mm, gk = k0 + kk;
+      double val = 0.0;
+      if (gm < m && gk < k) val = TA ? A[(long long)gm * lda + gk] : A[(long long)gk * lda + gm];
+      sA[kk][mm] = val;
+    }
+    for (int i = threadIdx.x; i < BN * BK; i += 256) {
+      const int kk = i % BK, nn = i / BK;
+      const int gk = k0 + kk, gn = n0 + nn;
+      double val = 0.0;
+      if (gk < k && gn < n) val = TB ? B[(long long)gk * ldb + gn] : B[(long long)gn * ldb + gk];
+      sB[kk][nn] = val;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = sA[kk][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = sB[kk][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gm = m0 + tx + 16 * i, gn = n0 + ty + 16 * j;
+      if (gm < m && gn < n) {
+        double *c = C + (long long)gn * ldc + gm;
+        *c = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*c);
+      }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Batched column operations for Ritz pairs.  Grid (gx, m); part[c*gx + b].
+// ---------------------------------------------------------------------------
+// mode 0: out_c = sqrt(sum U_c^2)
+// mode 1: out_c = sum U_c * W_c
+// mode 2: out_c = sqrt(sum (W_c - lam_c U_c)^2), with the reference's rounding
+__global__ void k_colred(int n, int m, int mode, const double *U, const double *W, const double *lam,
+                         double *part, unsigned int *ctr, double *out) {
+  __shared__ double sh[kThreads / 32];
+  const int c = blockIdx.y;
+  const double *u = U + (long long)c * n;
+  const double *w = W ? W + (long long)c * n : nullptr;
+  const double nl = (mode == 2) ? -lam[c] : 0.0;
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (mode == 0)
+      s += u[i] * u[i];
+    else if (mode == 1)
+      s += w[i] * u[i];
+    else {
+      const double r = __dadd_rn(w[i], __dmul_rn(nl, u[i]));
+      s += r * r;
+    }
+  }
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) part[(long long)c * gridDim.x + blockIdx.x] = s;
+  if (last_block(ctr)) {
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+      double t = 0.0;
+      for (int b = 0; b < (int)gridDim.x; ++b) t += __ldcg(part + (long long)q * gridDim.x + b);
+      out[q] = (mode == 1) ? t : sqrt(t);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *ctr = 0u;
+  }
+}
+
+// U_c *= 1/norm_c
+__global__ void k_colscale_inv(int n, const double *nrm, double *U) {
+  const int c = blockIdx.y;
+  const double t = 1.0 / nrm[c];
+  double *u = U + (long long)c * n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) u[i] = __dmul_rn(t, u[i]);
+}
+
+int colred(int n, int m, int mode, const double *U, const double *W, const double *lam, double *out) {
+  const int gx = std::max(1, std::min(grid_for(n), std::max(1, 2048 / std::max(1, m))));
+  double *part = (double *)evslcu_malloc(sizeof(double) * (size_t)gx * m);
+  if (!part) return EVSLCU_ERR_NOMEM;
+  dim3 g(gx, m);
+  k_colred<<<g, kThreads, 0, stream()>>>(n, m, mode, U, W, lam, part, counters() + CTR_COL, out);
+  count_launch();
+  int rc = check_launch("k_colred");
+  int rc2 = evslcu_free(part);
+  return rc ? rc : rc2;
+}
+
+}  // namespace
+
+extern "C" {
+
+int evslcu_dot(int n, const double *x, const double *y, double *out_dev) {
+  k_dot<<<grid_for(n, kThreads, 1024), kThreads, 0, stream()>>>(n, x, y, partials(), counters() + CTR_DOT, out_dev,
+                                                                 0);
+  EVSLCU_LAUNCH_CHECK("k_dot");
+  return 0;
+}
+
+int evslcu_nrm2(int n, const double *x, double *out_dev) {
+  k_dot<<<grid_for(n, kThreads, 1024), kThreads, 0, stream()>>>(n, x, x, partials(), counters() + CTR_NRM, out_dev,
+                                                                 1);
+  EVSLCU_LAUNCH_CHECK("k_nrm2");
+  return 0;
+}
+
+int evslcu_axpy_ds(int n, const double *coef_dev, double sign, const double *x, double *y) {
+  k_axpy_ds<<<grid_for(n), kThreads, 0, stream()>>>(n, coef_dev, sign, x, y);
+  EVSLCU_LAUNCH_CHECK("k_axpy_ds");
+  return 0;
+}
+
+int evslcu_axpy(int n, double a, const double *x, double *y) {
+  k_axpy<<<grid_for(n), kThreads, 0, stream()>>>(n, a, x, y);
+  EVSLCU_LAUNCH_CHECK("k_axpy");
+  return 0;
+}
+
+int evslcu_scal_inv_ds(int n, const double *s_dev, double *x) {
+  k_scal_inv_ds<<<grid_for(n), kThreads, 0, stream()>>>(n, s_dev, x);
+  EVSLCU_LAUNCH_CHECK("k_scal_inv_ds");
+  return 0;
+}
+
+int evslcu_scal(int n, double a, double *x) {
+  k_scal<<<grid_for(n), kThreads, 0, stream()>>>(n, a, x);
+  EVSLCU_LAUNCH_CHECK("k_scal");
+  return 0;
+}
+
+int evslcu_copy(int n, const double *x, double *y) { return evslcu_d2d(y, x, sizeof(double) * (size_t)n); }
+
+size_t evslcu_cgs_work_size(int n, int k) {
+  const size_t nchunks = ((size_t)n + kGemvTRows - 1) / kGemvTRows;
+  return nchunks * (size_t)std::max(k, 1) + (size_t)std::max(k, 1) + 8;
+}
+
+int evslcu_cgs_dgks(int n, int k, int imax, const double *Q, long long ldq, double *v, double *nrm_out_dev,
+                    double *work) {
+  if (k < 1 || n < 1) return fail(EVSLCU_ERR_ARG, "cgs: bad sizes n=%d k=%d", n, k);
+  const int nchunks = (n + kGemvTRows - 1) / kGemvTRows;
+  double *part = work;
+  double *h = work + (size_t)nchunks * k;
+  double *state = h + k;
+  double *nrm0 = state + 4;
+  cudaStream_t st = stream();
+  int rc;
+  if ((rc = evslcu_nrm2(n, v, nrm0))) return rc;
+  k_cgs_init<<<1, 1, 0, st>>>(state, nrm0);
+  EVSLCU_LAUNCH_CHECK("k_cgs_init");
+  const dim3 gT(nchunks, (k + kGemvTCols - 1) / kGemvTCols);
+  const int gN = grid_for(n, kThreads, kMaxPartials);
+  for (int pass = 0; pass < imax; ++pass) {
+    k_gemvT_partial<<<gT, kThreads, 0, st>>>(n, k, Q, ldq, v, part, state);
+    EVSLCU_LAUNCH_CHECK("k_gemvT_partial");
+    k_gemvT_reduce<<<(k + 255) / 256, 256, 0, st>>>(nchunks, k, part, 1.0, 0.0, h, state);
+    EVSLCU_LAUNCH_CHECK("k_gemvT_reduce");
+    k_gemvN<<<gN, kThreads, 0, st>>>(n, k, Q, ldq, h, -1.0, v, partials(), counters() + CTR_CGS, state);
+    EVSLCU_LAUNCH_CHECK("k_gemvN");
+  }
+  if (nrm_out_dev) {
+    k_copy_scalar<<<1, 1, 0, st>>>(state + 1, nrm_out_dev);
+    EVSLCU_LAUNCH_CHECK("k_copy_scalar");
+  }
+  return 0;
+}
+
+int evslcu_dgemv(char trans, int m, int n, double alpha, const double *A, long long lda, const double *x,
+                 double beta, double *y) {
+  cudaStream_t st = stream();
+  const bool T = (trans == 'T' || trans == 't');
+  if (m <= 0 || n <= 0) return 0;
+  if (T) {
+    // y (n) = alpha A^T x + beta y; A is m x n
+    const int nchunks = (m + kGemvTRows - 1) / kGemvTRows;
+    double *part = (double *)evslcu_malloc(sizeof(double) * (size_t)nchunks * n);
+    if (!part) return EVSLCU_ERR_NOMEM;
+    const dim3 gT(nchunks, (n + kGemvTCols - 1) / kGemvTCols);
+    k_gemvT_partial<<<gT, kThreads, 0, st>>>(m, n, A, lda, x, part, nullptr);
+    count_launch();
+    int rc = check_launch("k_gemvT_partial");
+    if (!rc) {
+      k_gemvT_reduce<<<(n + 255) / 256, 256, 0, st>>>(nchunks, n, part, alpha, beta, y, nullptr);
+      count_launch();
+      rc = check_launch("k_gemvT_reduce");
+    }
+    evslcu_free(part);
+    return rc;
+  }
+  // y (m) = beta y + alpha A x
+  if (beta != 1.0) {
+    k_scale_vec<<<grid_for(m), kThreads, 0, st>>>(m, beta, y);
+    EVSLCU_LAUNCH_CHECK("k_scale_vec");
+  }
+  k_gemvN<<<grid_for(m, kThreads, kMaxPartials), kThreads, 0, st>>>(m, n, A, lda, x, alpha, y, nullptr, nullptr,
+                                                                      nullptr);
+  EVSLCU_LAUNCH_CHECK("k_gemvN");
+  return 0;
+}
+
+int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const double *A, long long lda,
+                 const double *B, long long ldb, double beta, double *C, long long ldc) {
+  if (m <= 0 || n <= 0) return 0;
+  const bool TA = (ta == 'T' || ta == 't'), TB = (tb == 'T' || tb == 't');
+  dim3 g((m + BM - 1) / BM, (n + BN - 1) / BN);
+  cudaStream_t st = stream();
+  if (!TA && !TB)
+    k_dgemm<false, false><<<g, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  else if (TA && !TB)
+    k_dgemm<true, false><<<g, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  else if (!TA && TB)
+    k_dgemm<false, true><<<g, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  else
+    k_dgemm<true, true><<<g, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  EVSLCU_LAUNCH_CHECK("k_dgemm");
+  return 0;
+}
+
+int evslcu_ritz_eval(const evslcu_op *op, int n, int m, double *U, double *W, double *norm, double *lam,
+                     double *res) {
+  if (m <= 0) return 0;
+  double *d = (double *)evslcu_malloc(sizeof(double) * 3 * (size_t)m);
+  if (!d) return EVSLCU_ERR_NOMEM;
+  double *dn = d, *dl = d + m, *dr = d + 2 * m;
+  int rc = colred(n, m, 0, U, nullptr, nullptr, dn);
+  if (!rc) {
+    dim3 g(std::min(grid_for(n), 1024), m);
+    k_colscale_inv<<<g, kThreads, 0, stream()>>>(n, dn, U);
+    count_launch();
+    rc = check_launch("k_colscale_inv");
+  }
+  for (int c = 0; !rc && c < m; ++c) {
+    if (op->A) {
+      rc = evslcu_spmv(op->A, U + (size_t)c * n, W + (size_t)c * n);
+    } else {
+      cudaError_t e = cudaStreamSynchronize(stream());
+      if (e != cudaSuccess) rc = fail(EVSLCU_ERR_CUDA, "sync before matvec: %s", cudaGetErrorString(e));
+      if (!rc) op->func(U + (size_t)c * n, W + (size_t)c * n, op->data);
+    }
+  }
+  if (!rc) rc = colred(n, m, 1, U, W, nullptr, dl);
+  if (!rc) rc = colred(n, m, 2, U, W, dl, dr);
+  if (!rc) rc = evslcu_d2h(norm, dn, sizeof(double) * m);
+  if (!rc) rc = evslcu_d2h(lam, dl, sizeof(double) * m);
+  if (!rc) rc = evslcu_d2h(res, dr, sizeof(double) * m);
+  evslcu_free(d);
+  return rc;
+}
+
+int evslcu_gather_cols(int n, int cnt, const int *idx, const double *src, double *dst) {
+  for (int j = 0; j < cnt; ++j) {
+    if (idx[j] == j && src == dst) continue;
+    int rc = evslcu_d2d(dst + (size_t)j * n, src + (size_t)idx[j] * n, sizeof(double) * (size_t)n);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,613 @@
+// Sparse operator, fused Chebyshev filter steps, KPM block moments and the
+// device random-vector generator.
+//
+// Filter kernels (reference ChebAv, SRC/chebpoly.c:519-598, and its CUDA
+// update kernel SRC/evsl_cuda.cu:175-191):
+//   * one thread per row; the row's products are summed left to right with
+//     explicitly rounded multiply and add (no FMA contraction), which is the
+//     arithmetic of the reference CPU build's CSR matvec (SRC/spmat.c:257-298);
+//   * the Chebyshev update w = t*(A vk - cc vk) - vkm1, y += mu_k w is applied
+//     in the reference's operation order (daxpy, dscal, daxpy, daxpy;
+//     SRC/chebpoly.c:575-582) in the epilogue, so the filtered vector equals
+//     the reference CPU result bit for bit;
+//   * matrix storage is SELL-32 (chunks of 32 rows, column-major inside the
+//     chunk, padded with zeros) so every warp load is coalesced; the plain
+//     CSR thread-per-row kernel is kept as an alternative.
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+
+using namespace evslcu;
+
+struct evslcu_mat {
+  int n = 0;
+  long long nnz = 0;
+  // CSR on device
+  const int *ia = nullptr;
+  const int *ja = nullptr;
+  const double *a = nullptr;
+  bool own_csr = false;
+  // SELL-32 on device
+  int nchunks = 0;
+  long long padded = 0;
+  long long *cptr = nullptr;  // nchunks+1 element offsets
+  int *cw = nullptr;          // chunk widths
+  int *scol = nullptr;
+  double *sval = nullptr;
+  int kernel = 0;  // 0 SELL-32, 1 CSR
+};
+
+namespace {
+
+struct SellView {
+  int n;
+  const long long *__restrict__ cptr;
+  const int *__restrict__ cw;
+  const int *__restrict__ col;
+  const double *__restrict__ val;
+};
+
+struct CsrView {
+  int n;
+  const int *__restrict__ ia;
+  const int *__restrict__ ja;
+  const double *__restrict__ a;
+};
+
+__device__ __forceinline__ double row_dot(const SellView &A, int r, const double *__restrict__ x) {
+  const int c = r >> 5;
+  long long p = A.cptr[c] + (r & 31);
+  const int w = A.cw[c];
+  double acc = 0.0;
+#pragma unroll 4
+  for (int j = 0; j < w; ++j, p += 32) acc = __dadd_rn(acc, __dmul_rn(__ldg(A.val + p), __ldg(x + __ldg(A.col + p))));
+  return acc;
+}
+
+__device__ __forceinline__ double row_dot(const CsrView &A, int r, const double *__restrict__ x) {
+  const int b = A.ia[r], e = A.ia[r + 1];
+  double acc = 0.0;
+#pragma unroll 4
+  for (int j = b; j < e; ++j) acc = __dadd_rn(acc, __dmul_rn(__ldg(A.a + j), __ldg(x + __ldg(A.ja + j))));
+  return acc;
+}
+
+template <class M>
+__global__ void __launch_bounds__(kThreads) k_spmv(M A, const double *__restrict__ x, double *__restrict__ y) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) y[r] = row_dot(A, r, x);
+}
+
+// One Chebyshev degree step k (FIRST: k == 1; EPI: k == deg, Lanczos epilogue).
+//   out may alias vkm1 (each thread reads vkm1[r] before writing out[r]).
+template <class M, bool FIRST, bool EPI>
+__global__ void __launch_bounds__(kThreads)
+    k_cheb(M A, const double *__restrict__ vk, const double *vkm1, double *out, double *__restrict__ y, double t,
+           double ncc, double s, double mu0, const double *__restrict__ zold, double nbeta,
+           const double *__restrict__ dotv, double *part, unsigned int *ctr, double *dot_out) {
+  __shared__ double sh[kThreads / 32];
+  double dsum = 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) {
+    const double acc = row_dot(A, r, vk);
+    const double x = vk[r];
+    // vkp1 = A vk; vkp1 += (-cc) vk; vkp1 *= t; vkp1 += (-1) vkm1
+    double w = __dmul_rn(t, __dadd_rn(acc, __dmul_rn(ncc, x)));
+    if (!FIRST) w = __dadd_rn(w, -vkm1[r]);
+    out[r] = w;
+    // k == 1: y = mu0 * v (v == vk); then y += mu_k * w
+    double yv = FIRST ? __dmul_rn(mu0, x) : y[r];
+    yv = __dadd_rn(yv, __dmul_rn(s, w));
+    if (EPI) {
+      if (zold) yv = __dadd_rn(yv, __dmul_rn(nbeta, zold[r]));
+      if (dotv) dsum += dotv[r] * yv;
+    }
+    y[r] = yv;
+  }
+  if (EPI && dot_out) {
+    double b = block_sum(dsum, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = b;
+    if (last_block(ctr)) {
+      double tot = reduce_partials(part, gridDim.x, ctr, sh);
+      if (threadIdx.x == 0) *dot_out = tot;
+    }
+  }
+}
+
+// Stand-alone update for a user matvec (SRC/evsl_cuda.cu:175-184 semantics,
+// CPU-build operation order).
+__global__ void k_cheb_update(int n, int k, double t, double s, double ncc, double *vkp1, const double *vk,
+                              const double *vkm1, double *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double w = __dmul_rn(t, __dadd_rn(vkp1[i], __dmul_rn(ncc, vk[i])));
+    if (k > 1) w = __dadd_rn(w, -vkm1[i]);
+    vkp1[i] = w;
+    y[i] = __dadd_rn(y[i], __dmul_rn(s, w));
+  }
+}
+
+__global__ void k_scale_copy(int n, double a, const double *x, double *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = __dmul_rn(a, x[i]);
+}
+
+// Lanczos epilogue when the last step could not be fused (user matvec).
+__global__ void k_lan_epi(int n, const double *zold, double nbeta, const double *dotv, double *y, double *part,
+                          unsigned int *ctr, double *dot_out) {
+  __shared__ double sh[kThreads / 32];
+  double dsum = 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    double yv = y[r];
+    if (zold) yv = __dadd_rn(yv, __dmul_rn(nbeta, zold[r]));
+    y[r] = yv;
+    if (dotv) dsum += dotv[r] * yv;
+  }
+  if (dot_out) {
+    double b = block_sum(dsum, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = b;
+    if (last_block(ctr)) {
+      double tot = reduce_partials(part, gridDim.x, ctr, sh);
+      if (threadIdx.x == 0) *dot_out = tot;
+    }
+  }
+}
+
+SellView sell_view(const evslcu_mat *A) { return SellView{A->n, A->cptr, A->cw, A->scol, A->sval}; }
+CsrView csr_view(const evslcu_mat *A) { return CsrView{A->n, A->ia, A->ja, A->a}; }
+
+template <class M>
+int launch_cheb_step(const M &view, int n, bool first, bool epi, const double *vk, const double *vkm1, double *out,
+                     double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *e) {
+  const int grid = grid_for(n);
+  cudaStream_t st = stream();
+  const double *zold = (epi && e) ? e->zold : nullptr;
+  const double nbeta = (epi && e) ? e->nbeta : 0.0;
+  const double *dotv = (epi && e) ? e->dotv : nullptr;
+  double *dout = (epi && e) ? e->dot_out : nullptr;
+  unsigned int *ctr = counters() + CTR_CHEB;
+  if (first && epi)
+    k_cheb<M, true, true><<<grid, kThreads, 0, st>>>(view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
+                                                     partials(), ctr, dout);
+  else if (first)
+    k_cheb<M, true, false><<<grid, kThreads, 0, st>>>(view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
+                                                      partials(), ctr, dout);
+  else if (epi)
+    k_cheb<M, false, true><<<grid, kThreads, 0, st>>>(view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
+                                                      partials(), ctr, dout);
+  else
+    k_cheb<M, false, false><<<grid, kThreads, 0, st>>>(view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
+                                                       partials(), ctr, dout);
+  EVSLCU_LAUNCH_CHECK("k_cheb");
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// KPM block moments: warp per row, lane = probe; vectors interleaved [n][B].
+// ---------------------------------------------------------------------------
+template <int G, bool FIRST>
+__global__ void __launch_bounds__(kThreads)
+    k_kpm(CsrView A, int B, const double *__restrict__ vk, const double *vkm1, double *out, double scal, double nctr,
+          const double *__restrict__ v0, double *part, unsigned int *ctr, double *dots_row) {
+  __shared__ double sh[kThreads / 32][G * 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps_total = gridDim.x * (kThreads / 32);
+  double dsum[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) dsum[g] = 0.0;
+  for (int r = blockIdx.x * (kThreads / 32) + warp; r < A.n; r += nwarps_total) {
+    const int b = A.ia[r], e = A.ia[r + 1];
+    double acc[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) acc[g] = 0.0;
+    for (int j = b; j < e; ++j) {
+      const double aj = __ldg(A.a + j);
+      const long long cj = (long long)__ldg(A.ja + j) * B;
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const int p = lane + 32 * g;
+        if (p < B) acc[g] = __dadd_rn(acc[g], __dmul_rn(aj, __ldg(vk + cj + p)));
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const int p = lane + 32 * g;
+      if (p < B) {
+        const long long idx = (long long)r * B + p;
+        double w = __dmul_rn(scal, __dadd_rn(acc[g], __dmul_rn(nctr, vk[idx])));
+        if (!FIRST) w = __dadd_rn(w, -vkm1[idx]);
+        out[idx] = w;
+        dsum[g] += w * v0[idx];
+      }
+    }
+  }
+#pragma unroll
+  for (int g = 0; g < G; ++g) sh[warp][lane + 32 * g] = dsum[g];
+  __syncthreads();
+  for (int p = threadIdx.x; p < B; p += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) s += sh[w][p];
+    part[(long long)blockIdx.x * B + p] = s;
+  }
+  if (last_block(ctr)) {
+    for (int p = threadIdx.x; p < B; p += blockDim.x) {
+      double s = 0.0;
+      for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(part + (long long)b * B + p);
+      dots_row[p] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *ctr = 0u;
+  }
+}
+
+// Column sums of squares of a column-major n x B block: part[blk*B + p].
+__global__ void k_colsq_partial(int n, int B, const double *X, double *part, unsigned int *ctr, double *nrm) {
+  __shared__ double sh[kThreads / 32];
+  const int p = blockIdx.y;
+  double s = 0.0;
+  const double *x = X + (long long)p * n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += x[i] * x[i];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) part[(long long)p * gridDim.x + blockIdx.x] = s;
+  if (last_block(ctr)) {
+    for (int q = threadIdx.x; q < B; q += blockDim.x) {
+      double t = 0.0;
+      for (int b = 0; b < (int)gridDim.x; ++b) t += __ldcg(part + (long long)q * gridDim.x + b);
+      nrm[q] = sqrt(t);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *ctr = 0u;
+  }
+}
+
+// v0[r*B + p] = (1/nrm_p) * probes[p*n + r]   (t = 1/||v||; dscal(t))
+__global__ void k_interleave_scaled(int n, int B, const double *probes, const double *nrm, double *v0) {
+  const long long total = (long long)n * B;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / B), p = (int)(i % B);
+    const double t = 1.0 / nrm[p];
+    v0[i] = __dmul_rn(t, probes[(long long)p * n + r]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Random vectors
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ULL;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double uniform_pm1(uint64_t seed, uint64_t draw, uint64_t i) {
+  const uint64_t key = seed * 0x9E3779B97F4A7C15ULL + (draw << 32) + i;
+  const double u = (double)(mix64(key) >> 11) * (1.0 / 9007199254740992.0);
+  return 2.0 * u - 1.0;
+}
+
+__global__ void k_rand_pm1(int n, int count, uint64_t seed, uint64_t draw, double *v) {
+  const long long total = (long long)n * count;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const long long d = i / n, r = i % n;
+    v[i] = uniform_pm1(seed, draw + (uint64_t)d, (uint64_t)r);
+  }
+}
+
+__global__ void k_randn(int n, uint64_t seed, uint64_t draw, double *v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double u1 = 0.5 * (uniform_pm1(seed, draw, 2 * (uint64_t)i) + 1.0);
+    double u2 = 0.5 * (uniform_pm1(seed, draw, 2 * (uint64_t)i + 1) + 1.0);
+    if (u1 < 1e-300) u1 = 1e-300;
+    v[i] = sqrt(-2.0 * log(u1)) * cos(2.0 * 3.14159265358979323846 * u2);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+evslcu_mat *evslcu_mat_create(int n, int nnz, const int *ia, const int *ja, const double *a, int on_device) {
+  if (!evslcu_initialized()) {
+    fail(EVSLCU_ERR_STATE, "library not started (EVSLStart)");
+    return nullptr;
+  }
+  if (n <= 0 || nnz < 0 || !ia || (nnz > 0 && (!ja || !a))) {
+    fail(EVSLCU_ERR_ARG, "invalid CSR matrix (n=%d nnz=%d)", n, nnz);
+    return nullptr;
+  }
+  // Host copies of the CSR arrays for building SELL-32.
+  std::vector<int> hia(n + 1), hja;
+  std::vector<double> ha;
+  const int *pia = ia, *pja = ja;
+  const double *pa = a;
+  if (on_device) {
+    if (evslcu_d2h(hia.data(), ia, sizeof(int) * (n + 1))) return nullptr;
+    nnz = hia[n];
+    hja.resize(nnz);
+    ha.resize(nnz);
+    if (nnz && (evslcu_d2h(hja.data(), ja, sizeof(int) * (size_t)nnz) ||
+                evslcu_d2h(ha.data(), a, sizeof(double) * (size_t)nnz)))
+      return nullptr;
+    pia = hia.data();
+    pja = hja.data();
+    pa = ha.data();
+  }
+  if (pia[0] != 0 || pia[n] != nnz) {
+    fail(EVSLCU_ERR_ARG, "CSR row pointer must start at 0 and end at nnz (%d vs %d)", pia[n], nnz);
+    return nullptr;
+  }
+  for (int r = 0; r < n; ++r) {
+    if (pia[r + 1] < pia[r]) {
+      fail(EVSLCU_ERR_ARG, "CSR row pointer decreases at row %d", r);
+      return nullptr;
+    }
+  }
+  for (long long j = 0; j < nnz; ++j) {
+    if (pja[j] < 0 || pja[j] >= n) {
+      fail(EVSLCU_ERR_ARG, "CSR column index %d at position %lld is outside [0, %d)", pja[j], j, n);
+      return nullptr;
+    }
+  }
+  evslcu_mat *M = new evslcu_mat;
+  M->n = n;
+  M->nnz = nnz;
+  if (on_device) {
+    M->ia = ia;
+    M->ja = ja;
+    M->a = a;
+    M->own_csr = false;
+  } else {
+    int *dia = (int *)evslcu_malloc(sizeof(int) * (n + 1));
+    int *dja = (int *)evslcu_malloc(sizeof(int) * (size_t)std::max(nnz, 1));
+    double *da = (double *)evslcu_malloc(sizeof(double) * (size_t)std::max(nnz, 1));
+    if (!dia || !dja || !da || evslcu_h2d(dia, ia, sizeof(int) * (n + 1)) ||
+        evslcu_h2d(dja, ja, sizeof(int) * (size_t)nnz) || evslcu_h2d(da, a, sizeof(double) * (size_t)nnz)) {
+      evslcu_free(dia);
+      evslcu_free(dja);
+      evslcu_free(da);
+      delete M;
+      return nullptr;
+    }
+    M->ia = dia;
+    M->ja = dja;
+    M->a = da;
+    M->own_csr = true;
+  }
+  // SELL-32: chunk c holds rows 32c..32c+31; entry j of lane l at cptr[c] + 32 j + l.
+  const int nch = (n + 31) / 32;
+  std::vector<long long> cptr(nch + 1, 0);
+  std::vector<int> cw(nch, 0);
+  for (int c = 0; c < nch; ++c) {
+    int w = 0;
+    for (int r = 32 * c; r < std::min(n, 32 * c + 32); ++r) w = std::max(w, pia[r + 1] - pia[r]);
+    cw[c] = w;
+    cptr[c + 1] = cptr[c] + 32LL * w;
+  }
+  const long long padded = cptr[nch];
+  std::vector<int> scol((size_t)std::max(padded, 1LL), 0);
+  std::vector<double> sval((size_t)std::max(padded, 1LL), 0.0);
+  for (int c = 0; c < nch; ++c) {
+    for (int l = 0; l < 32; ++l) {
+      const int r = 32 * c + l;
+      const int len = (r < n) ? pia[r + 1] - pia[r] : 0;
+      for (int j = 0; j < cw[c]; ++j) {
+        const long long p = cptr[c] + 32LL * j + l;
+        if (j < len) {
+          scol[p] = pja[pia[r] + j];
+          sval[p] = pa[pia[r] + j];
+        } else {
+          scol[p] = (r < n) ? r : 0;  // padding: 0 * x[r] adds nothing
+          sval[p] = 0.0;
+        }
+      }
+    }
+  }
+  M->nchunks = nch;
+  M->padded = padded;
+  M->cptr = (long long *)evslcu_malloc(sizeof(long long) * (nch + 1));
+  M->cw = (int *)evslcu_malloc(sizeof(int) * nch);
+  M->scol = (int *)evslcu_malloc(sizeof(int) * (size_t)std::max(padded, 1LL));
+  M->sval = (double *)evslcu_malloc(sizeof(double) * (size_t)std::max(padded, 1LL));
+  if (!M->cptr || !M->cw || !M->scol || !M->sval || evslcu_h2d(M->cptr, cptr.data(), sizeof(long long) * (nch + 1)) ||
+      evslcu_h2d(M->cw, cw.data(), sizeof(int) * nch) ||
+      evslcu_h2d(M->scol, scol.data(), sizeof(int) * (size_t)padded) ||
+      evslcu_h2d(M->sval, sval.data(), sizeof(double) * (size_t)padded)) {
+    evslcu_mat_destroy(M);
+    return nullptr;
+  }
+  M->kernel = 0;
+  return M;
+}
+
+void evslcu_mat_destroy(evslcu_mat *M) {
+  if (!M) return;
+  if (M->own_csr) {
+    evslcu_free((void *)M->ia);
+    evslcu_free((void *)M->ja);
+    evslcu_free((void *)M->a);
+  }
+  evslcu_free(M->cptr);
+  evslcu_free(M->cw);
+  evslcu_free(M->scol);
+  evslcu_free(M->sval);
+  delete M;
+}
+
+int evslcu_mat_n(const evslcu_mat *A) { return A ? A->n : 0; }
+long long evslcu_mat_nnz(const evslcu_mat *A) { return A ? A->nnz : 0; }
+long long evslcu_mat_padded_nnz(const evslcu_mat *A) { return A ? A->padded : 0; }
+
+int evslcu_mat_set_kernel(evslcu_mat *A, int which) {
+  if (!A || which < 0 || which > 1) return fail(EVSLCU_ERR_ARG, "invalid kernel choice %d", which);
+  A->kernel = which;
+  return 0;
+}
+
+int evslcu_mat_get_kernel(const evslcu_mat *A) { return A ? A->kernel : -1; }
+
+int evslcu_spmv(const evslcu_mat *A, const double *x, double *y) {
+  if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
+  const int grid = grid_for(A->n);
+  if (A->kernel == 0)
+    k_spmv<SellView><<<grid, kThreads, 0, stream()>>>(sell_view(A), x, y);
+  else
+    k_spmv<CsrView><<<grid, kThreads, 0, stream()>>>(csr_view(A), x, y);
+  EVSLCU_LAUNCH_CHECK("k_spmv");
+  return 0;
+}
+
+int evslcu_cheb_update(int n, int k, double t, double s, double cc, double *vkp1, const double *vk,
+                       const double *vkm1, double *y) {
+  k_cheb_update<<<grid_for(n), kThreads, 0, stream()>>>(n, k, t, s, -cc, vkp1, vk, vkm1, y);
+  EVSLCU_LAUNCH_CHECK("k_cheb_update");
+  return 0;
+}
+
+int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, double dd, const double *v, double *y,
+                  double *work, const evslcu_cheb_epi *epi) {
+  if (!op || !mu || deg < 0 || !v || !y || !work) return fail(EVSLCU_ERR_ARG, "evslcu_chebav: bad arguments");
+  const int n = op->n;
+  const double t1 = 1.0 / dd, t2 = 2.0 / dd, ncc = -cc;
+  double *W[2] = {work, work + n};
+  if (deg == 0) {
+    k_scale_copy<<<grid_for(n), kThreads, 0, stream()>>>(n, mu[0], v, y);
+    EVSLCU_LAUNCH_CHECK("k_scale_copy");
+    if (epi) {
+      k_lan_epi<<<grid_for(n), kThreads, 0, stream()>>>(n, epi->zold, epi->nbeta, epi->dotv, y, partials(),
+                                                        counters() + CTR_CHEB, epi->dot_out);
+      EVSLCU_LAUNCH_CHECK("k_lan_epi");
+    }
+    return 0;
+  }
+  if (op->A) {
+    const evslcu_mat *A = op->A;
+    for (int k = 1; k <= deg; ++k) {
+      const double t = (k == 1) ? t1 : t2;
+      const double *vk = (k == 1) ? v : W[(k - 2) % 2];
+      const double *vkm1 = (k == 1) ? nullptr : ((k == 2) ? v : W[(k - 1) % 2]);
+      double *out = W[(k - 1) % 2];
+      const bool last = (k == deg);
+      int rc;
+      if (A->kernel == 0)
+        rc = launch_cheb_step(sell_view(A), n, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
+      else
+        rc = launch_cheb_step(csr_view(A), n, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
+      if (rc) return rc;
+    }
+    return 0;
+  }
+  // User matvec (SetAMatvec): the reference's three-vector rotation
+  // (SRC/chebpoly.c:532-589) with the callback computing vkp1 = A vk.  The
+  // callback must enqueue on the legacy default stream (which orders with the
+  // library stream) or finish its work before returning.
+  if (!op->func) return fail(EVSLCU_ERR_STATE, "no matrix or matvec registered");
+  double *vk = work, *vkp1 = work + n, *vkm1 = work + 2 * (size_t)n;
+  if (evslcu_d2d(vk, v, sizeof(double) * n)) return EVSLCU_ERR_CUDA;
+  k_scale_copy<<<grid_for(n), kThreads, 0, stream()>>>(n, mu[0], v, y);
+  EVSLCU_LAUNCH_CHECK("k_scale_copy");
+  for (int k = 1; k <= deg; ++k) {
+    const double t = (k == 1) ? t1 : t2;
+    cudaError_t e = cudaStreamSynchronize(stream());
+    if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "sync before matvec: %s", cudaGetErrorString(e));
+    op->func(vk, vkp1, op->data);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "user matvec failed: %s", cudaGetErrorString(e));
+    k_cheb_update<<<grid_for(n), kThreads, 0, stream()>>>(n, k, t, mu[k], ncc, vkp1, vk, vkm1, y);
+    EVSLCU_LAUNCH_CHECK("k_cheb_update");
+    double *tmp = vkm1;
+    vkm1 = vk;
+    vk = vkp1;
+    vkp1 = tmp;
+  }
+  if (epi) {
+    k_lan_epi<<<grid_for(n), kThreads, 0, stream()>>>(n, epi->zold, epi->nbeta, epi->dotv, y, partials(),
+                                                      counters() + CTR_CHEB, epi->dot_out);
+    EVSLCU_LAUNCH_CHECK("k_lan_epi");
+  }
+  return 0;
+}
+
+int evslcu_kpm_dots(const evslcu_op *op, int n, int Mdeg, int nvec, const double *probes, double ctr, double wid,
+                    double *dots) {
+  if (!op || !op->A) return fail(EVSLCU_ERR_STATE, "KPM needs a registered CSR matrix");
+  if (nvec < 1 || nvec > 128 || Mdeg < 1 || n < 1) return fail(EVSLCU_ERR_ARG, "kpm: bad sizes");
+  const int B = nvec;
+  const size_t blk = (size_t)n * B;
+  double *buf = (double *)evslcu_malloc(sizeof(double) * blk * 3);
+  double *ddots = (double *)evslcu_malloc(sizeof(double) * (size_t)Mdeg * B);
+  double *nrm = (double *)evslcu_malloc(sizeof(double) * B);
+  const int rows_per_block = kThreads / 32;
+  int grid = (int)std::min<long long>(((long long)n + rows_per_block - 1) / rows_per_block, 4096);
+  double *part = (double *)evslcu_malloc(sizeof(double) * (size_t)std::max(grid * B, 512 * B));
+  if (!buf || !ddots || !nrm || !part) {
+    evslcu_free(buf);
+    evslcu_free(ddots);
+    evslcu_free(nrm);
+    evslcu_free(part);
+    return EVSLCU_ERR_NOMEM;
+  }
+  double *V0 = buf, *W0 = buf + blk, *W1 = buf + 2 * blk;
+  int rc = 0;
+  {
+    dim3 g(std::min(grid_for(n), 512), B);
+    k_colsq_partial<<<g, kThreads, 0, stream()>>>(n, B, probes, part, counters() + CTR_COL, nrm);
+    count_launch();
+    if ((rc = check_launch("k_colsq_partial"))) goto done;
+    k_interleave_scaled<<<grid_for(blk), kThreads, 0, stream()>>>(n, B, probes, nrm, V0);
+    count_launch();
+    if ((rc = check_launch("k_interleave_scaled"))) goto done;
+  }
+  {
+    const CsrView A = csr_view(op->A);
+    const double nctr = -ctr;
+    unsigned int *c = counters() + CTR_KPM;
+    double *W[2] = {W0, W1};
+    for (int k = 0; k < Mdeg; ++k) {
+      const double scal = (k == 0 ? 1.0 : 2.0) / wid;
+      const double *vk = (k == 0) ? V0 : W[(k - 1) % 2];
+      const double *vkm1 = (k == 0) ? nullptr : ((k == 1) ? V0 : W[k % 2]);
+      double *out = W[k % 2];
+      double *drow = ddots + (size_t)k * B;
+      if (B <= 32) {
+        if (k == 0)
+          k_kpm<1, true><<<grid, kThreads, 0, stream()>>>(A, B, vk, vkm1, out, scal, nctr, V0, part, c, drow);
+        else
+          k_kpm<1, false><<<grid, kThreads, 0, stream()>>>(A, B, vk, vkm1, out, scal, nctr, V0, part, c, drow);
+      } else if (B <= 64) {
+        if (k == 0)
+          k_kpm<2, true><<<grid, kThreads, 0, stream()>>>(A, B, vk, vkm1, out, scal, nctr, V0, part, c, drow);
+        else
+          k_kpm<2, false><<<grid, kThreads, 0, stream()>>>(A, B, vk, vkm1, out, scal, nctr, V0, part, c, drow);
+      } else {
+        if (k == 0)
+          k_kpm<4, true><<<grid, kThreads, 0, stream()>>>(A, B, vk, vkm1, out, scal, nctr, V0, part, c, drow);
+        else
+          k_kpm<4, false><<<grid, kThreads, 0, stream()>>>(A, B, vk, vkm1, out, scal, nctr, V0, part, c, drow);
+      }
+      count_launch();
+      if ((rc = check_launch("k_kpm"))) goto done;
+    }
+  }
+  rc = evslcu_d2h(dots, ddots, sizeof(double) * (size_t)Mdeg * B);
+done:
+  evslcu_free(buf);
+  evslcu_free(ddots);
+  evslcu_free(nrm);
+  evslcu_free(part);
+  return rc;
+}
+
+int evslcu_rand_pm1(int n, int count, uint64_t seed, uint64_t draw, double *v) {
+  k_rand_pm1<<<grid_for((long long)n * count), kThreads, 0, stream()>>>(n, count, seed, draw, v);
+  EVSLCU_LAUNCH_CHECK("k_rand_pm1");
+  return 0;
+}
+
+int evslcu_randn(int n, uint64_t seed, uint64_t draw, double *v) {
+  k_randn<<<grid_for(n), kThreads, 0, stream()>>>(n, seed, draw, v);
+  EVSLCU_LAUNCH_CHECK("k_randn");
+  return 0;
+}
+
+}  // extern "C"

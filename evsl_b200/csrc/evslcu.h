@@ -1,0 +1,183 @@
+/*
+ * evslcu.h -- the thin C ABI between the C host (the EVSL API in the host sources)
+ * and the CUDA sm_100a back end (the .cu sources).
+ *
+ * Conventions
+ *   - Every device pointer is plain device memory; vectors are contiguous
+ *     doubles, blocks of vectors are column-major with a leading dimension.
+ *   - All work is enqueued on the library's stream (evslcu_stream()) and is
+ *     asynchronous unless the function says it returns a host value.
+ *   - Scalars that one kernel produces and a later kernel consumes stay in
+ *     device memory ("device scalars"); the host reads them only where the
+ *     algorithm needs a host decision.
+ *   - Functions return 0 on success and a negative EVSLCU_ERR_* code on
+ *     failure; evslcu_errstr() describes the last failure.
+ *   - The FP64 filter kernels reproduce the reference CPU build's arithmetic
+ *     bit for bit: each row of y = A x is summed left to right without fused
+ *     multiply-add, and the Chebyshev update applies the same sequence of
+ *     rounded axpy/scal operations (SRC/chebpoly.c:575-582).
+ */
+#ifndef EVSL_B200_EVSLCU_H
+#define EVSL_B200_EVSLCU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  EVSLCU_OK = 0,
+  EVSLCU_ERR_CUDA = -100,
+  EVSLCU_ERR_ARG = -101,
+  EVSLCU_ERR_NOMEM = -102,
+  EVSLCU_ERR_NODEV = -103,
+  EVSLCU_ERR_STATE = -104,
+  EVSLCU_ERR_TIMEOUT = -105
+};
+
+/* ---- context ------------------------------------------------------------ */
+int evslcu_init(void);
+int evslcu_finish(void);
+int evslcu_initialized(void);
+const char *evslcu_errstr(void);
+void evslcu_set_error(int code, const char *msg);
+int evslcu_sync(void);                 /* wait for the library stream */
+int evslcu_device_count(void);
+int evslcu_device_name(int dev, char *buf, int len, int *sm_count, size_t *mem_bytes);
+int evslcu_last_cuda_error(char *buf, int len);
+/* Number of kernels this library has launched since evslcu_init. */
+uint64_t evslcu_launch_count(void);
+
+/* ---- memory ------------------------------------------------------------- */
+void *evslcu_malloc(size_t nbytes);
+int evslcu_free(void *p);
+int evslcu_h2d(void *dst, const void *src, size_t nbytes);  /* synchronous */
+int evslcu_d2h(void *dst, const void *src, size_t nbytes);  /* synchronous */
+int evslcu_d2d(void *dst, const void *src, size_t nbytes);  /* async */
+int evslcu_memset(void *p, int v, size_t nbytes);           /* async */
+int evslcu_h2d_async(void *dst, const void *src, size_t nbytes);
+
+/* ---- timing (CUDA events on the library stream) ------------------------- */
+typedef struct evslcu_timer evslcu_timer;
+evslcu_timer *evslcu_timer_start(void);
+double evslcu_timer_stop(evslcu_timer *t); /* seconds; synchronises on the stop event */
+
+/* ---- prepared sparse matrix --------------------------------------------- */
+typedef struct evslcu_mat evslcu_mat;
+/* Build the device operator from a CSR matrix (0-based, rows sorted).  When
+ * on_device is non-zero the arrays are device pointers (borrowed); otherwise
+ * host arrays that are uploaded.  The SELL-32 copy used by the filter is
+ * built once here. */
+evslcu_mat *evslcu_mat_create(int n, int nnz, const int *ia, const int *ja, const double *a,
+                              int on_device);
+void evslcu_mat_destroy(evslcu_mat *A);
+int evslcu_mat_n(const evslcu_mat *A);
+long long evslcu_mat_nnz(const evslcu_mat *A);
+long long evslcu_mat_padded_nnz(const evslcu_mat *A);
+/* Kernel choice for the filter: 0 = SELL-32 thread-per-row, 1 = CSR thread-per-row. */
+int evslcu_mat_set_kernel(evslcu_mat *A, int which);
+int evslcu_mat_get_kernel(const evslcu_mat *A);
+/* y = A x, rows summed left to right. */
+int evslcu_spmv(const evslcu_mat *A, const double *x, double *y);
+
+/* User matvec callback (SetAMatvec): y = A x on device vectors. */
+typedef void (*evslcu_mvfunc)(double *x, double *y, void *data);
+
+/* Operator used by the filter: a prepared matrix, or a user callback. */
+typedef struct {
+  const evslcu_mat *A;
+  evslcu_mvfunc func;
+  void *data;
+  int n;
+} evslcu_op;
+
+/* Optional fused epilogue of the last Chebyshev step used by Lanczos:
+ *   y <- y + nbeta * zold        (when zold != NULL; SRC/cheblanNr.c:197-200)
+ *   *dot_out <- v . y            (device scalar; SRC/cheblanNr.c:202) */
+typedef struct {
+  const double *zold;
+  double nbeta;
+  const double *dotv;
+  double *dot_out;
+} evslcu_cheb_epi;
+
+/* y = p((A - cc I)/dd) v with p = sum_k mu[k] T_k (SRC/chebpoly.c:519-598).
+ * mu is a HOST array of deg+1 coefficients.  work holds 3n doubles (only 2n
+ * are touched when a prepared matrix is registered). */
+int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, double dd,
+                  const double *v, double *y, double *work, const evslcu_cheb_epi *epi);
+
+/* One fused Chebyshev update on device vectors (SRC/evsl_cuda.cu:175-191):
+ *   w = t*(vkp1 - cc*vk) - (k>1 ? vkm1 : 0); vkp1 = w; y += s*w. */
+int evslcu_cheb_update(int n, int k, double t, double s, double cc, double *vkp1,
+                       const double *vk, const double *vkm1, double *y);
+
+/* ---- level-1 with device scalars ---------------------------------------- */
+/* out = x . y  (device scalar, deterministic fixed-order reduction) */
+int evslcu_dot(int n, const double *x, const double *y, double *out_dev);
+/* out = ||x||_2 (device scalar) */
+int evslcu_nrm2(int n, const double *x, double *out_dev);
+/* y <- y + sign * (*coef_dev) * x */
+int evslcu_axpy_ds(int n, const double *coef_dev, double sign, const double *x, double *y);
+/* y <- y + a * x (host scalar) */
+int evslcu_axpy(int n, double a, const double *x, double *y);
+/* x <- (1 / *s_dev) * x */
+int evslcu_scal_inv_ds(int n, const double *s_dev, double *x);
+/* x <- a * x (host scalar) */
+int evslcu_scal(int n, double a, double *x);
+int evslcu_copy(int n, const double *x, double *y);
+/* read back device scalars (synchronous) */
+int evslcu_get_scalars(const double *dev, double *host, int count);
+
+/* ---- Gram-Schmidt (SRC/misc_la.c:221-261) -------------------------------- */
+/* Classical GS of v against the k columns of Q (ld = ldq) with the DGKS test,
+ * at most imax passes; the pass decisions are taken on the device.  When
+ * nrm_out_dev is not NULL the final norm of v is stored there.  work must
+ * hold evslcu_cgs_work_size(n, k) doubles. */
+size_t evslcu_cgs_work_size(int n, int k);
+int evslcu_cgs_dgks(int n, int k, int imax, const double *Q, long long ldq, double *v,
+                    double *nrm_out_dev, double *work);
+
+/* ---- dense kernels -------------------------------------------------------- */
+/* y = alpha * op(A) x + beta * y, column-major A (m x n); trans 'N' or 'T'. */
+int evslcu_dgemv(char trans, int m, int n, double alpha, const double *A, long long lda,
+                 const double *x, double beta, double *y);
+/* C = alpha * op(A) op(B) + beta * C, column-major; op = 'N' or 'T'. */
+int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const double *A,
+                 long long lda, const double *B, long long ldb, double beta, double *C,
+                 long long ldc);
+
+/* ---- Ritz pairs (SRC/cheblanNr.c:336-399, SRC/cheblanTr.c:545-632) -------- */
+/* For the m columns of U (n x m, ld = n):
+ *   norm_c = ||U_c||; U_c *= 1/norm_c; W_c = A U_c; lam_c = U_c . W_c;
+ *   res_c = || W_c - lam_c U_c ||.
+ * Host arrays norm, lam, res receive m values each (synchronous).  W needs
+ * n*m doubles of scratch. */
+int evslcu_ritz_eval(const evslcu_op *op, int n, int m, double *U, double *W, double *norm,
+                     double *lam, double *res);
+/* Gather columns: dst[:, j] = src[:, idx[j]] for j < cnt (idx host array). */
+int evslcu_gather_cols(int n, int cnt, const int *idx, const double *src, double *dst);
+
+/* ---- KPM block moments (SRC/spslice.c:76-130) ----------------------------- */
+/* Runs the damped-Chebyshev moment recurrence for nvec probe vectors at once.
+ * probes: device, column-major n x nvec (each column is normalised inside, as
+ * the reference does).  dots (HOST, Mdeg x nvec, row k = degree k+1): the raw
+ * products (T_{k+1}(A~) v_m) . v_m.  ctr/wid map the spectrum to [-1,1]. */
+int evslcu_kpm_dots(const evslcu_op *op, int n, int Mdeg, int nvec, const double *probes,
+                    double ctr, double wid, double *dots);
+
+/* ---- random vectors ------------------------------------------------------- */
+/* Counter-based uniform [-1,1) generator: value i of draw d under seed s is
+ * mix64(s*0x9E3779B97F4A7C15 + (d<<32) + i) mapped to [-1,1), where mix64 is
+ * the SplitMix64 output function.  Writes `count` draws starting at `draw`
+ * into columns of v (ld = n). */
+int evslcu_rand_pm1(int n, int count, uint64_t seed, uint64_t draw, double *v);
+int evslcu_randn(int n, uint64_t seed, uint64_t draw, double *v);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,68 @@
+/*
+ * evslx.h -- extensions of libevsl_b200 beyond the reference EVSL API.
+ *
+ * None of these exist in the reference; each says which reference behaviour
+ * it exposes or replaces.  All functions return 0 on success and a negative
+ * code on failure (evslx_last_error() then describes it), instead of the
+ * reference's assert()/exit() on library failures.
+ */
+#ifndef EVSL_B200_EVSLX_H
+#define EVSL_B200_EVSLX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes (the reference returns 0 / -1 / 2 from the solvers and calls
+ * assert or exit elsewhere; those paths return these codes here). */
+#define EVSLX_ERR_CUDA (-100)
+#define EVSLX_ERR_ARG (-101)
+#define EVSLX_ERR_NOMEM (-102)
+#define EVSLX_ERR_NODEV (-103)
+#define EVSLX_ERR_STATE (-104)
+#define EVSLX_ERR_UNSUPPORTED (-106)
+#define EVSLX_ERR_NUMERIC (-107)
+
+/* Text of the last error raised by the library. */
+const char *evslx_last_error(void);
+
+/* Seed of the device random-vector generator used by rand_double_device and
+ * therefore by kpmdos probes and lucky-breakdown restarts (the reference uses
+ * unseeded libc rand(), SRC/vect.c:14-20).  Resets the draw counter. */
+int evslx_set_seed(uint64_t seed);
+/* Current draw counter (each rand_double_device call consumes one draw). */
+uint64_t evslx_get_draw(void);
+
+/* kpmdos (SRC/spslice.c:29) with caller-supplied probe vectors instead of
+ * vectors drawn inside: probes is DEVICE memory, column-major n x nvec; each
+ * column is normalised inside exactly as the reference normalises its draws.
+ * All nvec probes run as one block recurrence (one pass over A per degree). */
+int evslx_kpmdos_probes(int Mdeg, int damping, int nvec, double *intv, const double *probes,
+                        double *mu, double *ecnt);
+
+/* Filter SpMV kernel for the registered matrix: 0 = SELL-32 (default),
+ * 1 = CSR one thread per row.  Both give identical (bitwise) results. */
+int evslx_set_spmv_kernel(int which);
+int evslx_get_spmv_kernel(void);
+
+/* y = A x for the registered matrix on device vectors (rows summed left to
+ * right, like the reference CPU matvec SRC/spmat.c:257-298). */
+int evslx_matvec(const double *x, double *y);
+
+/* Size of the registered problem and of the stored matrix. */
+int evslx_problem_info(int *n, long long *nnz, long long *stored_nnz);
+
+/* Number of GPU kernels the library has launched since EVSLStart. */
+uint64_t evslx_launch_count(void);
+
+/* Device time (seconds, CUDA events) of the last kpmdos moment recurrence. */
+double evslx_last_kpm_seconds(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

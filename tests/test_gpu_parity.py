@@ -1,0 +1,206 @@
+"""GPU parity tests: the CUDA sm_100a library through its C ABI against the
+oracle (numpy restatement + golden fixtures from the reference build).
+
+Tolerances (written per test):
+  * SpMV and ChebAv (the FP64 filter): bitwise equal to the reference CPU
+    arithmetic;
+  * KPM moments: normwise ||mu - mu_ref||_inf <= 1e-12 ||mu_ref||_inf (only
+    the summation order of the dot products differs); counts to 1e-10;
+  * eigenvalues: within 1e-10 x (spectral width) of the reference's, counts
+    exact against the analytic Laplacian spectrum, residuals < tol.
+"""
+import numpy as np
+import pytest
+
+from oracle import evsl_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _lap(lib, nx, ny, nz):
+    ia, ja, a = O.lap_csr(nx, ny, nz)
+    lib.set_csr(ia, ja, a)
+    return ia, ja, a
+
+
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_spmv_bitwise(gpu_lib, kernel):
+    for dims in ((37, 23, 1), (17, 13, 11)):
+        ia, ja, a = _lap(gpu_lib, *dims)
+        gpu_lib.set_spmv_kernel(kernel)
+        x = np.random.default_rng(5).standard_normal(len(ia) - 1)
+        assert np.array_equal(gpu_lib.matvec(x), O.csr_matvec(ia, ja, a, x))
+    gpu_lib.set_spmv_kernel(0)
+
+
+def test_spmv_irregular_rows(gpu_lib):
+    # rows of very different lengths (1 .. 70 entries), unsorted input order irrelevant
+    rng = np.random.default_rng(11)
+    n = 1000
+    rows, cols = [], []
+    for r in range(n):
+        k = 1 + (r * 37) % 70
+        c = np.unique(np.concatenate([[r], rng.integers(0, n, k)]))
+        rows += [r] * len(c)
+        cols += list(c)
+    rows, cols = np.array(rows), np.array(cols)
+    vals = rng.standard_normal(len(rows))
+    ia = np.zeros(n + 1, dtype=np.int32)
+    np.add.at(ia, rows + 1, 1)
+    ia = np.cumsum(ia).astype(np.int32)
+    gpu_lib.set_csr(ia, cols.astype(np.int32), vals)
+    x = rng.standard_normal(n)
+    for kernel in (0, 1):
+        gpu_lib.set_spmv_kernel(kernel)
+        assert np.array_equal(gpu_lib.matvec(x), O.csr_matvec(ia, cols, vals, x))
+    gpu_lib.set_spmv_kernel(0)
+
+
+def test_chebav_matches_reference_golden(gpu_lib, golden):
+    _lap(gpu_lib, 20, 20, 1)
+    pol = gpu_lib.find_pol([0.6, 1.2, 0.0, 8.0])
+    y = gpu_lib.chebav(pol, golden["chebav_v"])
+    assert np.array_equal(y, golden["chebav_y"])
+    gpu_lib.free_pol(pol)
+
+
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_chebav_bitwise_config_sizes(gpu_lib, kernel):
+    # config-1 matrix and filter; and a 3-D case with a degree ~100 filter
+    for dims, iv in (((100, 100, 1), [0.6, 0.9, 0.0, 8.0]), ((24, 24, 24), [0.6, 0.69331, 0.0, 12.0])):
+        ia, ja, a = _lap(gpu_lib, *dims)
+        gpu_lib.set_spmv_kernel(kernel)
+        pol = gpu_lib.find_pol(iv, max_deg=3000)
+        v = O.seeded_normal(len(ia) - 1, 42)
+        y = gpu_lib.chebav(pol, v)
+        y_ref = O.cheb_av(O.find_pol(iv, max_deg=3000), ia, ja, a, v)
+        assert np.array_equal(y, y_ref), (dims, np.max(np.abs(y - y_ref)))
+        gpu_lib.free_pol(pol)
+    gpu_lib.set_spmv_kernel(0)
+
+
+def test_kpmdos_probes_match_reference(gpu_lib, golden):
+    _lap(gpu_lib, 20, 20, 1)
+    probes = O.seeded_rademacher(6, 400, 7)
+    mu, ec = gpu_lib.kpmdos_probes(40, 1, probes, [0.6, 1.2, 0.0, 8.0])
+    ref = golden["kpm20_mu"]
+    assert np.max(np.abs(mu - ref)) <= 1e-12 * np.max(np.abs(ref))
+    assert abs(ec - golden["kpm20_ecnt"][0]) <= 1e-10 * abs(golden["kpm20_ecnt"][0])
+    _lap(gpu_lib, 8, 8, 8)
+    probes = O.seeded_rademacher(5, 512, 9)
+    mu, ec = gpu_lib.kpmdos_probes(60, 1, probes, [0.6, 2.0, 0.0, 12.0])
+    ref = golden["kpm8_mu"]
+    assert np.max(np.abs(mu - ref)) <= 1e-12 * np.max(np.abs(ref))
+    rc, sli = gpu_lib.spslicer(mu, [0.6, 2.0, 0.0, 12.0], 5, int(10 * ec))
+    assert rc == 0 and np.max(np.abs(sli - golden["sli8"])) <= 1e-12
+
+
+def test_kpmdos_many_probes_and_device_rng(gpu_lib):
+    # 70 probes (two probe groups) drawn by the library's generator, against
+    # the restatement fed the same vectors
+    ia, ja, a = _lap(gpu_lib, 15, 11, 3)
+    n = len(ia) - 1
+    gpu_lib.set_seed(2024)
+    mu, ec = gpu_lib.kpmdos(30, 1, 70, [1.0, 3.0, 0.0, 12.0])
+    probes = np.stack([O.library_uniform(2024, d, n) for d in range(70)])
+    mu_ref, ec_ref = O.kpmdos(30, 1, probes, [1.0, 3.0, 0.0, 12.0], ia, ja, a)
+    assert np.max(np.abs(mu - mu_ref)) <= 1e-12 * np.max(np.abs(mu_ref))
+    assert abs(ec - ec_ref) <= 1e-10 * abs(ec_ref)
+
+
+def test_cheblan_nr_small_matches_reference(gpu_lib, golden):
+    _lap(gpu_lib, 20, 20, 1)
+    pol = gpu_lib.find_pol([0.6, 1.2, 0.0, 8.0])
+    lam, Y, res = gpu_lib.cheblan_nr([0.6, 1.2, 0.0, 8.0], 400, 1e-8, golden["chebav_v"], pol)
+    ref = golden["nr20_lam"]
+    assert len(lam) == len(ref) == len(O.exeiglap3(20, 20, 1, 0.6, 1.2))
+    assert np.max(np.abs(np.sort(lam) - ref)) <= 1e-10 * 8.0
+    assert np.all(res < 1e-8)
+    # eigenvectors: unit norm, mutually orthogonal, A y = lam y
+    ia, ja, a = O.lap_csr(20, 20, 1)
+    G = Y @ Y.T
+    assert np.max(np.abs(G - np.eye(len(lam)))) < 1e-8
+    for i in range(len(lam)):
+        r = O.csr_matvec(ia, ja, a, Y[i]) - lam[i] * Y[i]
+        assert np.linalg.norm(r) < 1e-8
+    gpu_lib.free_pol(pol)
+
+
+def test_cheblan_nr_config1(gpu_lib, golden):
+    """Config 1: 2-D 100x100 Laplacian, [0.6, 0.9], thresholds 0.8/0.2,
+    tol 1e-8, maxit 2000, seeded normal start vector: 260 eigenpairs."""
+    _lap(gpu_lib, 100, 100, 1)
+    iv = [0.6, 0.9, 0.0, 8.0]
+    pol = gpu_lib.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+    v = O.seeded_normal(10000, int(golden["cfg1_vinit_seed"][0]))
+    lam, Y, res = gpu_lib.cheblan_nr(iv, 2000, 1e-8, v, pol, want_vectors=True)
+    exact = O.exeiglap3(100, 100, 1, 0.6, 0.9)
+    assert len(lam) == 260 == len(exact)
+    lam = np.sort(lam)
+    assert np.max(np.abs(lam - golden["cfg1_lam"])) <= 1e-10 * 8.0
+    assert np.max(np.abs(lam - exact)) <= 1e-10 * 8.0
+    assert np.all(res < 1e-8)
+    G = Y @ Y.T
+    assert np.max(np.abs(G - np.eye(260))) < 1e-6
+    gpu_lib.free_pol(pol)
+
+
+def test_cheblan_tr_small_matches_reference(gpu_lib, golden):
+    _lap(gpu_lib, 20, 20, 1)
+    pol = gpu_lib.find_pol([0.6, 1.2, 0.0, 8.0])
+    lam, Y, res = gpu_lib.cheblan_tr(100, 30, [0.6, 1.2, 0.0, 8.0], 300, 1e-8, golden["chebav_v"], pol)
+    ref = golden["tr20_lam"]
+    assert len(lam) == len(ref) == len(O.exeiglap3(20, 20, 1, 0.6, 1.2))
+    assert np.max(np.abs(np.sort(lam) - ref)) <= 1e-10 * 8.0
+    assert np.all(res < 1e-8)
+    gpu_lib.free_pol(pol)
+
+
+def test_cheblan_tr_config1_sized(gpu_lib):
+    _lap(gpu_lib, 100, 100, 1)
+    iv = [0.6, 0.9, 0.0, 8.0]
+    pol = gpu_lib.find_pol(iv, max_deg=3000)
+    v = O.seeded_normal(10000, 1234)
+    lam, Y, res = gpu_lib.cheblan_tr(1100, 270, iv, 3300, 1e-8, v, pol, want_vectors=False)
+    exact = O.exeiglap3(100, 100, 1, 0.6, 0.9)
+    assert len(lam) == len(exact)
+    assert np.max(np.abs(np.sort(lam) - exact)) <= 1e-10 * 8.0
+    assert np.all(res < 1e-8)
+    gpu_lib.free_pol(pol)
+
+
+def test_interval_edge_cases(gpu_lib):
+    _lap(gpu_lib, 20, 20, 1)
+    pol = gpu_lib.find_pol([0.6, 1.2, 0.0, 8.0])
+    v = O.seeded_normal(400, 1)
+    # interval outside the spectrum bounds: no eigenpairs, return code 0
+    lam, Y, res = gpu_lib.cheblan_nr([9.0, 10.0, 0.0, 8.0], 100, 1e-8, v, pol)
+    assert len(lam) == 0
+    lam, Y, res = gpu_lib.cheblan_tr(60, 10, [9.0, 10.0, 0.0, 8.0], 100, 1e-8, v, pol)
+    assert len(lam) == 0
+    # an interval with no eigenvalues inside the spectrum: nothing accepted
+    gap = [0.30, 0.3005, 0.0, 8.0]
+    assert len(O.exeiglap3(20, 20, 1, gap[0], gap[1])) == 0
+    p2 = gpu_lib.find_pol(gap, max_deg=3000)
+    lam, Y, res = gpu_lib.cheblan_nr(gap, 200, 1e-8, v, p2)
+    assert len(lam) == 0
+    gpu_lib.free_pol(p2)
+    # end intervals (left and right filters)
+    for iv in ([0.0, 0.3, 0.0, 8.0], [7.5, 8.0, 0.0, 8.0]):
+        p3 = gpu_lib.find_pol(iv)
+        lam, Y, res = gpu_lib.cheblan_nr(iv, 400, 1e-8, v, p3)
+        assert len(lam) == len(O.exeiglap3(20, 20, 1, iv[0], iv[1]))
+        gpu_lib.free_pol(p3)
+    gpu_lib.free_pol(pol)
+
+
+def test_tiny_problem(gpu_lib):
+    # n = 6: Lanczos runs out of dimensions (maxit clipped to n)
+    ia, ja, a = _lap(gpu_lib, 3, 2, 1)
+    iv = [1.0, 5.0, 0.0, 8.0]
+    pol = gpu_lib.find_pol(iv)
+    lam, Y, res = gpu_lib.cheblan_nr(iv, 100, 1e-8, O.seeded_normal(6, 2), pol)
+    ex = O.exeiglap3(3, 2, 1, iv[0], iv[1])
+    assert len(lam) == len(ex)
+    assert np.max(np.abs(np.sort(lam) - ex)) < 1e-10
+    gpu_lib.free_pol(pol)
