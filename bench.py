@@ -1,0 +1,483 @@
+#!/usr/bin/env python
+"""Benchmark of the spectrum-slicing hot path on B200.
+
+Workload (default, "lap3d-slice"): one polynomial-filtered Lanczos slice solve
+(ChebLanNr, FP64, tol 1e-8) on the 3-D 7-point Dirichlet Laplacian 100^3
+(n = 1,000,000, nnz = 6,940,000, spectrum bounds [0, 12]) -- the config-2
+matrix -- over an interval that holds 100 eigenvalues just above 0.6, with
+both end points at midpoints of gaps of the analytic spectrum (the
+serving-size slice request of the mixed request stream).  The filter is
+designed by find_pol with damping 2, thresholds 0.8 / 0.2, max degree 3000.
+One step = one complete slice solve; every step checks the eigenvalue count
+against the analytic spectrum and the residuals against tol.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (launched by torch.distributed.run): every rank solves its own slice of
+the same matrix (independent units, no data-path collective, weak scaling);
+rank 0 prints the aggregate.  --impl reference times the reference EVSL CPU
+build (oracle/_ref) on the same request with all host threads.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = NZ = 100
+LMIN, LMAX = 0.0, 12.0
+COUNT = 100
+TOL = 1e-8
+MAXIT = 2000
+SEED = 1234
+METRIC = "eigenpairs/sec + p50/p99 slice latency at resid<=1e-8; filter SpMV GB/s vs HBM"
+UNIT = "eigenpairs/s"
+# Lanczos dimension of this request, as the GPU arm measures it (used only to
+# scale the CPU sample to a whole request; the recurrence is the same).
+REQUEST_LANCZOS_STEPS = None
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--count", type=int, default=COUNT)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter"], default="lap3d-slice",
+                   help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark)")
+    return p.parse_args()
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def slice_interval(ev, rank, count):
+    from evsl_b200 import workloads as W
+
+    lo = 0.6 + 0.01 * rank  # every rank gets its own slice
+    a, b, cnt = W.gap_interval(ev, lo, count)
+    return [a, b, LMIN, LMAX], cnt
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sms, maxs, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                maxs = max(maxs, float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sms:
+            return None
+        loaded = [s for s in sms if s > 0.5 * maxs] or sms
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": maxs, "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def measured_peak_hbm():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split()
+        if len(f) >= 3 and not line.startswith("#") and f[0] == "lap3d-slice" and f[1] == kernel:
+            return float(f[2])
+    return None
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    import evsl_b200
+    from evsl_b200 import workloads as W
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    lib = evsl_b200.Library()
+    ia, ja, a = W.laplacian_csr(NX, NY, NZ)
+    ev = W.laplacian_eigenvalues(NX, NY, NZ)
+    lib.set_csr(ia, ja, a)
+    intv, expected = slice_interval(ev, rank, args.count)
+    exact = ev[(ev >= intv[0]) & (ev <= intv[1])]
+    pol = lib.find_pol(intv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+    rng = np.random.default_rng(SEED + rank)
+    v0 = rng.standard_normal(NX * NY * NZ)
+    v0 /= np.linalg.norm(v0)
+    dv = evsl_b200.DeviceBuffer.from_host(lib.lib, v0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    lstream = torch.cuda.ExternalStream(lib.stream_handle())
+    import ctypes as C
+
+    def solve_device():
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        nev = C.c_int()
+        lam, res = C.POINTER(C.c_double)(), C.POINTER(C.c_double)()
+        Wp = C.c_void_p()
+        rc = lib.lib.ChebLanNr(iv.ctypes.data_as(C.POINTER(C.c_double)), MAXIT, TOL, dv.ptr, C.byref(pol),
+                               C.byref(nev), C.byref(lam), C.byref(Wp), C.byref(res), None)
+        if rc != 0:
+            raise RuntimeError(f"ChebLanNr returned {rc}: {lib.last_error()}")
+        m = nev.value
+        lam_h = np.ctypeslib.as_array(lam, (m,)).copy() if m else np.zeros(0)
+        res_h = np.ctypeslib.as_array(res, (m,)).copy() if m else np.zeros(0)
+        lib.lib._evsl_Free(C.cast(lam, C.c_void_p))
+        lib.lib._evsl_Free(C.cast(res, C.c_void_p))
+        return lam_h, res_h, Wp.value
+
+    def check(lam, res):
+        ok = len(lam) == len(exact)
+        err = float(np.max(np.abs(np.sort(lam) - exact))) if ok and len(lam) else float("inf")
+        return {"count": int(len(lam)), "exact": int(len(exact)), "max_res": float(np.max(res)) if len(res) else 0.0,
+                "max_err": err, "ok": bool(ok and err <= 1e-10 * (LMAX - LMIN) and (len(res) == 0 or res.max() < TOL))}
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up
+    for _ in range(args.warmup):
+        lam, res, Wp = solve_device()
+        lib.lib._evsl_Free_device(Wp)
+    kdim, cand = lib.last_solve_info()
+    # timed region: device-resident inputs
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    lib.filter_profile(True)
+    launches0 = lib.launch_count()
+    ev_start = torch.cuda.Event(enable_timing=True)
+    ev_end = torch.cuda.Event(enable_timing=True)
+    lat = []
+    found = 0
+    checks = []
+    ev_start.record(lstream)
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lstream)
+        lam, res, Wp = solve_device()
+        e1.record(lstream)
+        e1.synchronize()
+        lat.append(e0.elapsed_time(e1))
+        lib.lib._evsl_Free_device(Wp)
+        found += len(lam)
+        checks.append(check(lam, res))
+    ev_end.record(lstream)
+    ev_end.synchronize()
+    launches = lib.launch_count() - launches0
+    f_sec, f_bytes, f_launch, f_calls = lib.filter_stats()
+    lib.filter_profile(False)
+    clocks = sampler.stop()
+    t_dev = sum(lat) / 1e3  # seconds of device time in the solves (flushes excluded)
+    barrier()
+
+    # e2e through the C ABI with host buffers: vinit H2D and eigenpairs D2H each step
+    pinned_in = torch.from_numpy(v0).pin_memory()
+    pinned_out = torch.empty((len(exact) + 16, NX * NY * NZ), dtype=torch.float64).pin_memory()
+    e2e_times, e2e_found, h2d, d2h = [], 0, 0, 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lib.lib.evsl_memcpy_host_to_device(dv.ptr, pinned_in.data_ptr(), v0.nbytes)
+        lam, res, Wp = solve_device()
+        m = len(lam)
+        if m and m <= pinned_out.shape[0]:
+            lib.lib.evsl_memcpy_device_to_host(pinned_out.data_ptr(), Wp, m * NX * NY * NZ * 8)
+        lib.lib._evsl_Free_device(Wp)
+        e2e_times.append(time.perf_counter() - t0)
+        e2e_found += m
+        h2d = v0.nbytes
+        d2h = m * NX * NY * NZ * 8 + 2 * m * 8
+
+    # aggregate over ranks
+    stats = torch.tensor([t_dev, float(found), sum(e2e_times), float(e2e_found)], dtype=torch.float64,
+                         device="cuda")
+    if dist is not None:
+        tmax = stats.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = stats.clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        t_all, found_all, e2e_t, e2e_f = tmax[0].item(), tsum[1].item(), tmax[2].item(), tsum[3].item()
+    else:
+        t_all, found_all, e2e_t, e2e_f = t_dev, float(found), sum(e2e_times), float(e2e_found)
+
+    result = None
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        achieved = f_bytes / f_sec / 1e9 if f_sec > 0 else 0.0
+        traffic = profiled_traffic("k_cheb")
+        result = {
+            "metric": METRIC,
+            "value": found_all / t_all,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_all / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (3-D Dirichlet Laplacian, seeded start vector)",
+            "config": {
+                "workload": "lap3d-slice: ChebLanNr FP64 tol 1e-8 on the 3-D 7-point Laplacian 100^3 "
+                            "(n=1e6, nnz=6.94e6, bounds [0,12]), one slice of %d eigenvalues above 0.6 per rank "
+                            "(end points at spectral gap midpoints), find_pol damping 2, thresholds 0.8/0.2, "
+                            "max_deg 3000, maxit %d" % (args.count, MAXIT),
+                "interval": intv[:2],
+                "filter_degree": int(pol.deg),
+                "lanczos_steps": int(kdim),
+                "parallelism": f"replicas x{world} (independent slices)",
+                "l2": "256 MB buffer written between steps; per-step working set (A + basis) > L2",
+            },
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "per_step": lat},
+            "check": checks[-1],
+            "all_steps_ok": all(c["ok"] for c in checks),
+            "roofline": {
+                "kernel": "k_cheb (fused FP64 SELL-32 SpMV + Chebyshev step)",
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peak,
+                "peak_kind": peak_kind,
+                "unit": "GB/s",
+                "frac": achieved / peak if peak else None,
+                "traffic": traffic,
+                "algorithmic_bytes_per_launch": f_bytes / f_launch if f_launch else None,
+                "avg_launch_us": 1e6 * f_sec / f_launch if f_launch else None,
+                "launches": f_launch,
+                "share_of_step": f_sec / t_dev if t_dev else None,
+            },
+            "e2e": {"value": e2e_f / e2e_t if e2e_t else None, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(pol.deg, kdim, intv, found / args.steps, v0, nthreads=1)
+    lib.free_pol(pol)
+    dv.free()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+
+
+# ---------------------------------------------------------------------------
+# reference CPU build (oracle/_ref): the CPU baseline and the reference arm
+# ---------------------------------------------------------------------------
+SAMPLE_DEG = 96
+
+
+def _ref_setup():
+    from oracle import evsl_oracle as O
+
+    R = O.RefLib()
+    ia, ja, a = R.lap_csr(NX, NY, NZ)  # the reference's own generator
+    R.set_csr(ia, ja, a)
+    return R, (ia, ja, a)
+
+
+def cpu_baseline(deg, kdim, intv, pairs_per_request, v0, nthreads=1):
+    """Reference ChebAv on the same matrix and filter, truncated to SAMPLE_DEG
+    degrees, run by `nthreads` concurrent threads; scaled to the request:
+    request time = (kdim + 1) filter applications of degree `deg` (the
+    filter is >97% of a request's cost at this size)."""
+    try:
+        R, keep = _ref_setup()
+    except Exception as e:
+        return {"value": None, "unit": UNIT, "cores": nthreads, "kind": "reference", "sample": f"unavailable: {e}"}
+    rc, rpol = R.find_pol(intv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+    wall = R.chebav_multi(rpol, SAMPLE_DEG, v0, nthreads)
+    per_degree = wall / SAMPLE_DEG  # per thread
+    request_s = (kdim + 1) * rpol.deg * per_degree
+    R.free_pol(rpol)
+    return {"value": nthreads * pairs_per_request / request_s, "unit": UNIT, "cores": nthreads, "kind": "reference",
+            "sample": f"{nthreads} thread(s) x reference ChebAv truncated to {SAMPLE_DEG} of {deg} degrees on the "
+                      f"same matrix and filter ({wall:.2f} s); request = ({kdim}+1) x degree-{deg} filter "
+                      f"applications, extrapolated"}
+
+
+def run_reference(args):
+    rank, world, local = rank_info()
+    if rank != 0:
+        return
+    from evsl_b200 import workloads as W
+
+    nthreads = os.cpu_count() or 1
+    ev = W.laplacian_eigenvalues(NX, NY, NZ)
+    intv, expected = slice_interval(ev, 0, args.count)
+    try:
+        R, keep = _ref_setup()
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build missing: {e}"}))
+        return
+    rc, rpol = R.find_pol(intv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+    rng = np.random.default_rng(SEED)
+    v0 = rng.standard_normal(NX * NY * NZ)
+    v0 /= np.linalg.norm(v0)
+    kdim = REQUEST_LANCZOS_STEPS or int(os.environ.get("EVSL_BENCH_KDIM", "0")) or 330
+    for _ in range(args.warmup):
+        R.chebav_multi(rpol, SAMPLE_DEG, v0, nthreads)
+    walls = [R.chebav_multi(rpol, SAMPLE_DEG, v0, nthreads) for _ in range(args.steps)]
+    per_degree = statistics.median(walls) / SAMPLE_DEG
+    request_s = (kdim + 1) * rpol.deg * per_degree
+    value = nthreads * expected / request_s
+    out = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * request_s,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (3-D Dirichlet Laplacian, seeded start vector)",
+        "config": {"workload": "lap3d-slice (same request as the GPU arm)", "interval": intv[:2],
+                   "filter_degree": int(rpol.deg), "lanczos_steps": kdim,
+                   "parallelism": f"{nthreads} concurrent requests (one per host thread)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                         "sample": f"{nthreads} threads x reference ChebAv truncated to {SAMPLE_DEG} of "
+                                   f"{rpol.deg} degrees per step; request = ({kdim}+1) filter applications"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    R.free_pol(rpol)
+    print(json.dumps(out))
+
+
+def run_filter(args):
+    """The dominant kernel alone: W + K applications of the request's filter
+    p(A)v (ChebAv, degree ~1440) on the 3-D Laplacian 100^3."""
+    import ctypes as C
+
+    import torch
+
+    import evsl_b200
+    from evsl_b200 import workloads as W
+
+    lib = evsl_b200.Library()
+    ia, ja, a = W.laplacian_csr(NX, NY, NZ)
+    ev = W.laplacian_eigenvalues(NX, NY, NZ)
+    lib.set_csr(ia, ja, a)
+    intv, _ = slice_interval(ev, 0, args.count)
+    pol = lib.find_pol(intv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+    n = NX * NY * NZ
+    v0 = np.random.default_rng(SEED).standard_normal(n)
+    dv = evsl_b200.DeviceBuffer.from_host(lib.lib, v0)
+    dy = evsl_b200.DeviceBuffer(lib.lib, 8 * n)
+    dw = evsl_b200.DeviceBuffer(lib.lib, 24 * n)
+    for _ in range(args.warmup):
+        lib._check(lib.lib.ChebAv(C.byref(pol), dv.ptr, dy.ptr, dw.ptr), "ChebAv")
+    lib.filter_profile(True)
+    sampler = ClockSampler(rank_info()[2])
+    sampler.start()
+    for _ in range(args.steps):
+        lib._check(lib.lib.ChebAv(C.byref(pol), dv.ptr, dy.ptr, dw.ptr), "ChebAv")
+    sec, byt, launches, calls = lib.filter_stats()
+    clocks = sampler.stop()
+    peak, kind = measured_peak_hbm()
+    gbs = byt / sec / 1e9
+    print(json.dumps({"metric": "filter SpMV GB/s", "value": gbs, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+                      "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": "lap3d-filter: ChebAv degree %d on the 3-D Laplacian 100^3" % pol.deg},
+                      "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "peak_kind": kind, "unit": "GB/s",
+                                   "frac": gbs / peak, "traffic": profiled_traffic("k_cheb"),
+                                   "avg_launch_us": 1e6 * sec / launches},
+                      "gpu_launches": launches, "clocks": clocks}))
+    lib.free_pol(pol)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    elif args.workload == "lap3d-filter":
+        run_filter(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

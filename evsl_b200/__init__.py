@@ -127,7 +127,11 @@ def load():
         "evslx_launch_count": ([], C.c_uint64),
         "evslx_last_kpm_seconds": ([], C.c_double),
         "evsl_timer": ([], C.c_double),
+        "evslx_stream": ([], C.c_void_p),
+        "evslx_filter_profile": ([C.c_int], C.c_int),
+        "evslx_filter_stats": ([_dp, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
         "StatsReset": ([], None),
+        "evslx_last_solve_info": ([_ip, _ip], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -333,3 +337,24 @@ class Library:
 
     def launch_count(self):
         return int(self.lib.evslx_launch_count())
+
+    def last_solve_info(self):
+        """(Lanczos dimension, Ritz candidates) of the last Lanczos solve."""
+        k, c = C.c_int(), C.c_int()
+        self.lib.evslx_last_solve_info(C.byref(k), C.byref(c))
+        return k.value, c.value
+
+    def stream_handle(self):
+        """cudaStream_t of the library (for recording CUDA events on it)."""
+        return int(self.lib.evslx_stream() or 0)
+
+    def filter_profile(self, enable=True):
+        self._check(self.lib.evslx_filter_profile(1 if enable else 0), "evslx_filter_profile")
+
+    def filter_stats(self):
+        """(device seconds, algorithmic bytes, kernel launches, filter calls)."""
+        sec, byt = C.c_double(), C.c_double()
+        la, ca = C.c_uint64(), C.c_uint64()
+        self._check(self.lib.evslx_filter_stats(C.byref(sec), C.byref(byt), C.byref(la), C.byref(ca)),
+                    "evslx_filter_stats")
+        return sec.value, byt.value, int(la.value), int(ca.value)

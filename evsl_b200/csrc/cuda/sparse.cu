@@ -43,6 +43,48 @@ struct evslcu_mat {
 
 namespace {
 
+// Optional timing of filter applications: CUDA events around the degree
+// kernels of each evslcu_chebav call, with the call's algorithmic bytes.
+struct FilterProf {
+  bool on = false;
+  struct Rec {
+    cudaEvent_t a, b;
+    double bytes;
+    int launches;
+  };
+  std::vector<Rec> pending;
+  std::vector<cudaEvent_t> pool;
+  double seconds = 0.0, bytes = 0.0;
+  uint64_t launches = 0, calls = 0;
+};
+FilterProf g_prof;
+
+cudaEvent_t prof_event() {
+  if (!g_prof.pool.empty()) {
+    cudaEvent_t e = g_prof.pool.back();
+    g_prof.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void prof_resolve() {
+  for (auto &r : g_prof.pending) {
+    float ms = 0.f;
+    cudaEventSynchronize(r.b);
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    g_prof.seconds += 1e-3 * ms;
+    g_prof.bytes += r.bytes;
+    g_prof.launches += (uint64_t)r.launches;
+    g_prof.calls += 1;
+    g_prof.pool.push_back(r.a);
+    g_prof.pool.push_back(r.b);
+  }
+  g_prof.pending.clear();
+}
+
 struct SellView {
   int n;
   const long long *__restrict__ cptr;
@@ -482,6 +524,11 @@ int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, dou
   }
   if (op->A) {
     const evslcu_mat *A = op->A;
+    cudaEvent_t ev_a = nullptr;
+    if (g_prof.on) {
+      ev_a = prof_event();
+      cudaEventRecord(ev_a, stream());
+    }
     for (int k = 1; k <= deg; ++k) {
       const double t = (k == 1) ? t1 : t2;
       const double *vk = (k == 1) ? v : W[(k - 2) % 2];
@@ -494,6 +541,21 @@ int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, dou
       else
         rc = launch_cheb_step(csr_view(A), n, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
       if (rc) return rc;
+    }
+    if (g_prof.on) {
+      // algorithmic bytes: A once per degree (8-byte value + 4-byte column per
+      // nonzero, 4-byte row pointer per row) plus the vectors each kernel
+      // touches: k = 1 reads v, writes w and y; k > 1 reads vk, vkm1, y and
+      // writes w, y; the Lanczos epilogue adds zold and v reads.
+      const double abytes = 12.0 * (double)A->nnz + 4.0 * ((double)n + 1.0);
+      double b = 0.0;
+      for (int k = 1; k <= deg; ++k) {
+        b += abytes + 8.0 * (double)n * ((k == 1) ? 3.0 : 5.0);
+        if (k == deg && epi) b += 8.0 * (double)n * ((epi->zold ? 1.0 : 0.0) + (epi->dotv ? 1.0 : 0.0));
+      }
+      cudaEvent_t ev_b = prof_event();
+      cudaEventRecord(ev_b, stream());
+      g_prof.pending.push_back({ev_a, ev_b, b, deg});
     }
     return 0;
   }
@@ -609,5 +671,24 @@ int evslcu_randn(int n, uint64_t seed, uint64_t draw, double *v) {
   EVSLCU_LAUNCH_CHECK("k_randn");
   return 0;
 }
+
+int evslcu_filter_profile(int enable) {
+  prof_resolve();
+  g_prof.on = enable != 0;
+  g_prof.seconds = g_prof.bytes = 0.0;
+  g_prof.launches = g_prof.calls = 0;
+  return 0;
+}
+
+int evslcu_filter_stats(double *seconds, double *bytes, uint64_t *launches, uint64_t *calls) {
+  prof_resolve();
+  if (seconds) *seconds = g_prof.seconds;
+  if (bytes) *bytes = g_prof.bytes;
+  if (launches) *launches = g_prof.launches;
+  if (calls) *calls = g_prof.calls;
+  return 0;
+}
+
+void *evslcu_stream_handle(void) { return (void *)stream(); }
 
 }  // extern "C"

@@ -168,6 +168,15 @@ int evslcu_gather_cols(int n, int cnt, const int *idx, const double *src, double
 int evslcu_kpm_dots(const evslcu_op *op, int n, int Mdeg, int nvec, const double *probes,
                     double ctr, double wid, double *dots);
 
+/* ---- filter timing ---------------------------------------------------------- */
+/* When enabled, every filter application with a prepared matrix is bracketed
+ * by CUDA events on the library stream; stats return the summed device time,
+ * the algorithmic bytes (A once per degree + vectors touched), the number of
+ * degree kernels and of filter calls since the last enable. */
+int evslcu_filter_profile(int enable);
+int evslcu_filter_stats(double *seconds, double *bytes, uint64_t *launches, uint64_t *calls);
+void *evslcu_stream_handle(void);
+
 /* ---- random vectors ------------------------------------------------------- */
 /* Counter-based uniform [-1,1) generator: value i of draw d under seed s is
  * mix64(s*0x9E3779B97F4A7C15 + (d<<32) + i) mapped to [-1,1), where mix64 is

@@ -146,6 +146,7 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
     sel = (int *)malloc(sizeof(int) * (size_t)(kdim > 0 ? kdim : 1));
     for (int i = 0; i < count; i++)
       if (EvalT[i] >= bar) sel[msel++] = i;
+    evslh.last_candidates = msel;
     double *wsel = (double *)malloc(sizeof(double) * (size_t)(msel > 0 ? msel : 1));
     for (int j = 0; j < msel; j++) wsel[j] = EvalT[sel[j]];
     EvecT = (double *)malloc(sizeof(double) * (size_t)kdim * (size_t)(msel > 0 ? msel : 1));
@@ -199,6 +200,7 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
     }
     tt_ritz = evsl_timer() - tr;
   }
+  evslh.last_kdim = kdim;
   *nevOut = nev;
   *lamo = Lam;
   *reso = res;

@@ -299,6 +299,7 @@ int ChebLanTr(int lanm, int nev, double *intv, int maxit, double tol, double *vi
   }
   if ((rc = evslcu_sync())) goto cuda_fail;
   if (do_print) fprintf(fstats, "     Number of evals found = %d\n--------------------------------------------------\n", lock);
+  evslh.last_kdim = it;
   *nev2 = lock;
   *vals = Lam;
   *resW = res;

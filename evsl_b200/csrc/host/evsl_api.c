@@ -507,3 +507,17 @@ int evsl_rand_device(int n, int count, double *v) {
   evslh.draw += (uint64_t)count;
   return from_cu(rc);
 }
+
+void *evslx_stream(void) { return evslcu_stream_handle(); }
+
+int evslx_filter_profile(int enable) { return from_cu(evslcu_filter_profile(enable)); }
+
+int evslx_filter_stats(double *seconds, double *bytes, uint64_t *launches, uint64_t *calls) {
+  return from_cu(evslcu_filter_stats(seconds, bytes, launches, calls));
+}
+
+int evslx_last_solve_info(int *lanczos_steps, int *candidates) {
+  if (lanczos_steps) *lanczos_steps = evslh.last_kdim;
+  if (candidates) *candidates = evslh.last_candidates;
+  return 0;
+}

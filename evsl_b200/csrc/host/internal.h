@@ -30,6 +30,8 @@ typedef struct {
   uint64_t draw;             /* next draw index of the device RNG */
   int kernel;                /* filter kernel choice, -1 = library default */
   double last_kpm_seconds;   /* device time of the last kpmdos moment loop */
+  int last_kdim;             /* Lanczos dimension of the last ChebLanNr/ChebLanTr */
+  int last_candidates;       /* Ritz values >= bar examined at the end */
   double last_filter_seconds;
 } evsl_host_state;
 

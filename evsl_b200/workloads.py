@@ -1,0 +1,69 @@
+"""Synthetic workloads of the spectrum-slicing path (host-side generators).
+
+Dirichlet Laplacians on nx x ny x nz grids: 5-point (2-D, diagonal 4) or
+7-point (3-D, diagonal 6) stencils with off-diagonals -1, x fastest, rows
+sorted by column -- the matrices the reference's Laplacian drivers build
+(TESTS/COMMON/lapl.c:13-65) -- and their analytic spectrum
+4 (sin^2(i pi/(2(nx+1))) + sin^2(j pi/(2(ny+1))) + sin^2(k pi/(2(nz+1)))).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def laplacian_csr(nx: int, ny: int, nz: int):
+    """(ia, ja, a) of the Dirichlet Laplacian, int32 indices, float64 values."""
+    n = nx * ny * nz
+    idx = np.arange(n, dtype=np.int64)
+    k = idx // (nx * ny)
+    i = (idx - k * nx * ny) // nx
+    j = idx - k * nx * ny - i * nx
+    # neighbour offsets in increasing column order: -nx*ny, -nx, -1, 0, +1, +nx, +nx*ny
+    offs = [(-nx * ny, k > 0), (-nx, i > 0), (-1, j > 0), (0, None), (1, j < nx - 1), (nx, i < ny - 1),
+            (nx * ny, k < nz - 1)]
+    diag = 6.0 if nz > 1 else 4.0
+    counts = np.ones(n, dtype=np.int64)
+    for off, mask in offs:
+        if mask is not None:
+            counts += mask
+    ia = np.zeros(n + 1, dtype=np.int64)
+    ia[1:] = np.cumsum(counts)
+    ja = np.empty(ia[-1], dtype=np.int32)
+    a = np.empty(ia[-1], dtype=np.float64)
+    pos = ia[:-1].copy()
+    for off, mask in offs:
+        rows = idx if mask is None else idx[mask]
+        p = pos[rows]
+        ja[p] = (rows + off).astype(np.int32)
+        a[p] = diag if off == 0 else -1.0
+        pos[rows] += 1
+    return ia.astype(np.int32), ja, a
+
+
+def laplacian_eigenvalues(nx: int, ny: int, nz: int) -> np.ndarray:
+    """All eigenvalues of the Dirichlet Laplacian, ascending."""
+    tx = np.sin(np.arange(1, nx + 1) * (0.5 * np.pi / (nx + 1.0))) ** 2
+    ty = np.sin(np.arange(1, ny + 1) * (0.5 * np.pi / (ny + 1.0))) ** 2
+    tz = np.sin(np.arange(1, nz + 1) * (0.5 * np.pi / (nz + 1.0))) ** 2 if nz > 1 else np.zeros(1)
+    ev = 4.0 * (tx[:, None, None] + ty[None, :, None] + tz[None, None, :])
+    return np.sort(ev.ravel())
+
+
+def count_in(ev: np.ndarray, a: float, b: float) -> int:
+    """Eigenvalues in [a, b] with the reference's 10*DBL_EPSILON slack."""
+    s = 10 * np.finfo(np.float64).eps
+    return int(np.count_nonzero((ev >= a - s) & (ev <= b + s)))
+
+
+def gap_interval(ev: np.ndarray, lo: float, count: int):
+    """An interval holding exactly `count` distinct-position eigenvalues
+    starting at the first eigenvalue above `lo`, with both end points at the
+    midpoints of the gaps around it (so counts are robust to rounding)."""
+    i0 = int(np.searchsorted(ev, lo))
+    i1 = i0 + count
+    # move the ends off clusters of equal eigenvalues
+    while i1 < len(ev) and ev[i1] - ev[i1 - 1] < 1e-10:
+        i1 += 1
+    a = 0.5 * (ev[i0 - 1] + ev[i0]) if i0 > 0 else ev[0] - 1e-3
+    b = 0.5 * (ev[i1 - 1] + ev[i1]) if i1 < len(ev) else ev[-1] + 1e-3
+    return float(a), float(b), i1 - i0

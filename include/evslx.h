@@ -61,6 +61,22 @@ uint64_t evslx_launch_count(void);
 /* Device time (seconds, CUDA events) of the last kpmdos moment recurrence. */
 double evslx_last_kpm_seconds(void);
 
+/* Size of the last ChebLanNr solve: Lanczos dimension kdim and the number of
+ * Ritz values >= bar examined (for ChebLanTr: total Lanczos steps). */
+int evslx_last_solve_info(int *lanczos_steps, int *candidates);
+
+/* The CUDA stream (cudaStream_t) all library work is queued on; callers can
+ * record their own events on it. */
+void *evslx_stream(void);
+
+/* Filter instrumentation: when enabled, each filter application p(A)v with a
+ * registered CSR matrix is bracketed by CUDA events.  evslx_filter_stats
+ * returns the device seconds spent in the filter kernels, their algorithmic
+ * bytes (12 bytes per nonzero + 4 per row for A at every degree, plus 8 bytes
+ * per vector element read or written), the kernel count and the call count. */
+int evslx_filter_profile(int enable);
+int evslx_filter_stats(double *seconds, double *bytes, uint64_t *launches, uint64_t *calls);
+
 #ifdef __cplusplus
 }
 #endif

@@ -117,6 +117,8 @@ class RefLib:
                                               _ip, _ip, _dp, _dp, _dp, C.c_int]
             lib.evslref_slices_nr.restype = C.c_double
             lib._evsl_Free.argtypes = [C.c_void_p]
+            lib.evslref_chebav_multi.argtypes = [C.POINTER(PolParams), C.c_int, _dp, C.c_int]
+            lib.evslref_chebav_multi.restype = C.c_double
             lib.EVSLStart()
             RefLib._lib = lib
         self.lib = RefLib._lib
@@ -250,6 +252,12 @@ class RefLib:
             if p:
                 self.lib._evsl_Free(C.cast(p, C.c_void_p))
         return out
+
+    def chebav_multi(self, pol, deg, v, nthreads):
+        """Wall seconds of `nthreads` concurrent reference ChebAv calls
+        truncated to `deg` degrees (CPU baseline sampler)."""
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        return self.lib.evslref_chebav_multi(C.byref(pol), deg, _dptr(v), nthreads)
 
     def slices_nr(self, sli, lmin, lmax, maxit, tol, vinit, *, damping=2, thresh_int=0.8,
                   thresh_ext=0.2, max_deg=10000, nthreads=0, evcap=4096):

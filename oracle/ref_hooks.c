@@ -217,3 +217,32 @@ double evslref_slices_nr(int nslices, const double *sli, double lmin, double lma
   clock_gettime(CLOCK_MONOTONIC, &t1);
   return (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
 }
+
+/* CPU baseline sampler: run `nthreads` independent reference ChebAv calls
+ * (SRC/chebpoly.c:519) concurrently, one per OpenMP thread, each on its own
+ * copy of v and its own workspace, with the filter truncated to `deg`
+ * degrees (the per-degree cost of ChebAv is constant).  This is the
+ * reference's own concurrency pattern (independent solves per thread,
+ * TESTS/PLanR/MMPLanR_omp.c:183).  Returns the wall seconds of the region. */
+double evslref_chebav_multi(polparams *pol, int deg, const double *v, int nthreads) {
+  const int n = g_A.nrows;
+  polparams p = *pol;
+  if (deg > 0 && deg < p.deg) p.deg = deg;
+  if (nthreads < 1) nthreads = 1;
+  struct timespec t0, t1;
+  clock_gettime(CLOCK_MONOTONIC, &t0);
+#pragma omp parallel num_threads(nthreads)
+  {
+    double *x = (double *)malloc((size_t)n * sizeof(double));
+    double *y = (double *)malloc((size_t)n * sizeof(double));
+    double *w = (double *)malloc(3 * (size_t)n * sizeof(double));
+    memcpy(x, v, (size_t)n * sizeof(double));
+    polparams q = p;
+    ChebAv(&q, x, y, w);
+    free(x);
+    free(y);
+    free(w);
+  }
+  clock_gettime(CLOCK_MONOTONIC, &t1);
+  return (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
+}
