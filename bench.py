@@ -135,14 +135,14 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(kernel):
+def profiled_traffic(kernel, workload="lap3d-slice"):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
         f = line.split()
-        if len(f) >= 3 and not line.startswith("#") and f[0] == "lap3d-slice" and f[1] == kernel:
+        if len(f) >= 3 and not line.startswith("#") and f[0] == workload and f[1] == kernel:
             return float(f[2])
     return None
 
@@ -463,7 +463,7 @@ def run_filter(args):
                       "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                       "config": {"workload": "lap3d-filter: ChebAv degree %d on the 3-D Laplacian 100^3" % pol.deg},
                       "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "peak_kind": kind, "unit": "GB/s",
-                                   "frac": gbs / peak, "traffic": profiled_traffic("k_cheb"),
+                                   "frac": gbs / peak, "traffic": profiled_traffic("k_cheb", "lap3d-filter"),
                                    "avg_launch_us": 1e6 * sec / launches},
                       "gpu_launches": launches, "clocks": clocks}))
     lib.free_pol(pol)
