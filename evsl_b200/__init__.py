@@ -132,6 +132,9 @@ def load():
         "evslx_filter_stats": ([_dp, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
         "StatsReset": ([], None),
         "evslx_last_solve_info": ([_ip, _ip], C.c_int),
+        "evslx_set_filter_persistent": ([C.c_int], C.c_int),
+        "evslx_set_matrix_compression": ([C.c_int], C.c_int),
+        "evslx_matrix_storage": ([_ip, _ip], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -221,6 +224,17 @@ class Library:
         self._keep = (bufs, m)
         self._check(self.lib.SetAMatrix_device_csr(C.byref(m)), "SetAMatrix_device_csr")
         self.n = n
+
+    def set_filter_persistent(self, on):
+        self._check(self.lib.evslx_set_filter_persistent(1 if on else 0), "evslx_set_filter_persistent")
+
+    def set_matrix_compression(self, on):
+        self._check(self.lib.evslx_set_matrix_compression(1 if on else 0), "evslx_set_matrix_compression")
+
+    def matrix_storage(self):
+        vb, ib = C.c_int(), C.c_int()
+        self._check(self.lib.evslx_matrix_storage(C.byref(vb), C.byref(ib)), "evslx_matrix_storage")
+        return vb.value, ib.value
 
     def set_spmv_kernel(self, which):
         self._check(self.lib.evslx_set_spmv_kernel(which), "evslx_set_spmv_kernel")

@@ -24,6 +24,7 @@ double *partials();
 unsigned int *counters();  // kNumCounters counters, all zero between kernels
 double *dev_scratch_scalars();  // 64 doubles of device scalar scratch
 constexpr int kNumCounters = 16;
+// Slots 8-10 hold the filter grid barrier (count, generation) and its error flag.
 enum CounterId { CTR_DOT = 0, CTR_NRM = 1, CTR_CHEB = 2, CTR_CGS = 3, CTR_KPM = 4, CTR_COL = 5 };
 
 constexpr int kThreads = 256;

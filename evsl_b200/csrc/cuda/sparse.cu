@@ -17,110 +17,18 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
-#include "common.cuh"
+#include "sparse_types.cuh"
 
 using namespace evslcu;
 
-struct evslcu_mat {
-  int n = 0;
-  long long nnz = 0;
-  // CSR on device
-  const int *ia = nullptr;
-  const int *ja = nullptr;
-  const double *a = nullptr;
-  bool own_csr = false;
-  // SELL-32 on device
-  int nchunks = 0;
-  long long padded = 0;
-  long long *cptr = nullptr;  // nchunks+1 element offsets
-  int *cw = nullptr;          // chunk widths
-  int *scol = nullptr;
-  double *sval = nullptr;
-  int kernel = 0;  // 0 SELL-32, 1 CSR
-};
-
 namespace {
-
-// Optional timing of filter applications: CUDA events around the degree
-// kernels of each evslcu_chebav call, with the call's algorithmic bytes.
-struct FilterProf {
-  bool on = false;
-  struct Rec {
-    cudaEvent_t a, b;
-    double bytes;
-    int launches;
-  };
-  std::vector<Rec> pending;
-  std::vector<cudaEvent_t> pool;
-  double seconds = 0.0, bytes = 0.0;
-  uint64_t launches = 0, calls = 0;
-};
-FilterProf g_prof;
-
-cudaEvent_t prof_event() {
-  if (!g_prof.pool.empty()) {
-    cudaEvent_t e = g_prof.pool.back();
-    g_prof.pool.pop_back();
-    return e;
-  }
-  cudaEvent_t e;
-  cudaEventCreate(&e);
-  return e;
-}
-
-void prof_resolve() {
-  for (auto &r : g_prof.pending) {
-    float ms = 0.f;
-    cudaEventSynchronize(r.b);
-    cudaEventElapsedTime(&ms, r.a, r.b);
-    g_prof.seconds += 1e-3 * ms;
-    g_prof.bytes += r.bytes;
-    g_prof.launches += (uint64_t)r.launches;
-    g_prof.calls += 1;
-    g_prof.pool.push_back(r.a);
-    g_prof.pool.push_back(r.b);
-  }
-  g_prof.pending.clear();
-}
-
-struct SellView {
-  int n;
-  const long long *__restrict__ cptr;
-  const int *__restrict__ cw;
-  const int *__restrict__ col;
-  const double *__restrict__ val;
-};
-
-struct CsrView {
-  int n;
-  const int *__restrict__ ia;
-  const int *__restrict__ ja;
-  const double *__restrict__ a;
-};
-
-__device__ __forceinline__ double row_dot(const SellView &A, int r, const double *__restrict__ x) {
-  const int c = r >> 5;
-  long long p = A.cptr[c] + (r & 31);
-  const int w = A.cw[c];
-  double acc = 0.0;
-#pragma unroll 4
-  for (int j = 0; j < w; ++j, p += 32) acc = __dadd_rn(acc, __dmul_rn(__ldg(A.val + p), __ldg(x + __ldg(A.col + p))));
-  return acc;
-}
-
-__device__ __forceinline__ double row_dot(const CsrView &A, int r, const double *__restrict__ x) {
-  const int b = A.ia[r], e = A.ia[r + 1];
-  double acc = 0.0;
-#pragma unroll 4
-  for (int j = b; j < e; ++j) acc = __dadd_rn(acc, __dmul_rn(__ldg(A.a + j), __ldg(x + __ldg(A.ja + j))));
-  return acc;
-}
 
 template <class M>
 __global__ void __launch_bounds__(kThreads) k_spmv(M A, const double *__restrict__ x, double *__restrict__ y) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) y[r] = row_dot(A, r, x);
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) y[r] = row_dot<false>(A, r, x);
 }
 
 // One Chebyshev degree step k (FIRST: k == 1; EPI: k == deg, Lanczos epilogue).
@@ -133,7 +41,7 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ double sh[kThreads / 32];
   double dsum = 0.0;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) {
-    const double acc = row_dot(A, r, vk);
+    const double acc = row_dot<false>(A, r, vk);
     const double x = vk[r];
     // vkp1 = A vk; vkp1 += (-cc) vk; vkp1 *= t; vkp1 += (-1) vkm1
     double w = __dmul_rn(t, __dadd_rn(acc, __dmul_rn(ncc, x)));
@@ -195,8 +103,6 @@ __global__ void k_lan_epi(int n, const double *zold, double nbeta, const double 
   }
 }
 
-SellView sell_view(const evslcu_mat *A) { return SellView{A->n, A->cptr, A->cw, A->scol, A->sval}; }
-CsrView csr_view(const evslcu_mat *A) { return CsrView{A->n, A->ia, A->ja, A->a}; }
 
 template <class M>
 int launch_cheb_step(const M &view, int n, bool first, bool epi, const double *vk, const double *vkm1, double *out,
@@ -345,9 +251,90 @@ __global__ void k_randn(int n, uint64_t seed, uint64_t draw, double *v) {
   }
 }
 
+
 }  // namespace
 
+int evslcu::launch_scale_copy(int n, double a, const double *x, double *y) {
+  k_scale_copy<<<grid_for(n), kThreads, 0, stream()>>>(n, a, x, y);
+  EVSLCU_LAUNCH_CHECK("k_scale_copy");
+  return 0;
+}
+
+int evslcu::launch_lan_epi(int n, const evslcu_cheb_epi *epi, double *y) {
+  k_lan_epi<<<grid_for(n), kThreads, 0, stream()>>>(n, epi->zold, epi->nbeta, epi->dotv, y, partials(),
+                                                    counters() + CTR_CHEB, epi->dot_out);
+  EVSLCU_LAUNCH_CHECK("k_lan_epi");
+  return 0;
+}
+
+// User matvec (SetAMatvec): the reference's three-vector rotation
+// (SRC/chebpoly.c:532-589) with the callback computing vkp1 = A vk.  The
+// callback must enqueue on the legacy default stream (which orders with the
+// library stream) or finish its work before returning.
+int evslcu::chebav_user_matvec(const evslcu_op *op, const double *mu, int deg, double cc, double dd,
+                               const double *v, double *y, double *work, const evslcu_cheb_epi *epi) {
+  if (!op->func) return fail(EVSLCU_ERR_STATE, "no matrix or matvec registered");
+  const int n = op->n;
+  const double t1 = 1.0 / dd, t2 = 2.0 / dd;
+  double *vk = work, *vkp1 = work + n, *vkm1 = work + 2 * (size_t)n;
+  if (evslcu_d2d(vk, v, sizeof(double) * n)) return EVSLCU_ERR_CUDA;
+  int rc = launch_scale_copy(n, mu[0], v, y);
+  if (rc) return rc;
+  for (int k = 1; k <= deg; ++k) {
+    const double t = (k == 1) ? t1 : t2;
+    cudaError_t e = cudaStreamSynchronize(stream());
+    if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "sync before matvec: %s", cudaGetErrorString(e));
+    op->func(vk, vkp1, op->data);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "user matvec failed: %s", cudaGetErrorString(e));
+    k_cheb_update<<<grid_for(n), kThreads, 0, stream()>>>(n, k, t, mu[k], -cc, vkp1, vk, vkm1, y);
+    EVSLCU_LAUNCH_CHECK("k_cheb_update");
+    double *tmp = vkm1;
+    vkm1 = vk;
+    vk = vkp1;
+    vkp1 = tmp;
+  }
+  if (epi) return launch_lan_epi(n, epi, y);
+  return 0;
+}
+
+// Per-degree filter: one fused kernel launch per degree (matrix path).
+int evslcu::chebav_per_degree(const evslcu_mat *A, const double *mu, int deg, double cc, double dd, const double *v,
+                      double *y, double *work, const evslcu_cheb_epi *epi) {
+  const int n = A->n;
+  const double t1 = 1.0 / dd, t2 = 2.0 / dd, ncc = -cc;
+  double *W[2] = {work, work + n};
+  for (int k = 1; k <= deg; ++k) {
+    const double t = (k == 1) ? t1 : t2;
+    const double *vk = (k == 1) ? v : W[(k - 2) % 2];
+    const double *vkm1 = (k == 1) ? nullptr : ((k == 2) ? v : W[(k - 1) % 2]);
+    double *out = W[(k - 1) % 2];
+    const bool last = (k == deg);
+    int rc = with_view(A, [&](auto view) {
+      return launch_cheb_step(view, n, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
+    });
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+
+
 extern "C" {
+
+static int g_compress = 1;
+
+int evslcu_set_compression(int on) {
+  g_compress = on ? 1 : 0;
+  return 0;
+}
+
+int evslcu_mat_storage(const evslcu_mat *A, int *vfmt, int *ifmt) {
+  if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
+  if (vfmt) *vfmt = A->vfmt;
+  if (ifmt) *ifmt = A->ifmt;
+  return 0;
+}
 
 evslcu_mat *evslcu_mat_create(int n, int nnz, const int *ia, const int *ja, const double *a, int on_device) {
   if (!evslcu_initialized()) {
@@ -358,7 +345,7 @@ evslcu_mat *evslcu_mat_create(int n, int nnz, const int *ia, const int *ja, cons
     fail(EVSLCU_ERR_ARG, "invalid CSR matrix (n=%d nnz=%d)", n, nnz);
     return nullptr;
   }
-  // Host copies of the CSR arrays for building SELL-32.
+  // Host copies of the CSR arrays for validation and building SELL-32.
   std::vector<int> hia(n + 1), hja;
   std::vector<double> ha;
   const int *pia = ia, *pja = ja;
@@ -385,15 +372,25 @@ evslcu_mat *evslcu_mat_create(int n, int nnz, const int *ia, const int *ja, cons
       return nullptr;
     }
   }
-  for (long long j = 0; j < nnz; ++j) {
-    if (pja[j] < 0 || pja[j] >= n) {
-      fail(EVSLCU_ERR_ARG, "CSR column index %d at position %lld is outside [0, %d)", pja[j], j, n);
-      return nullptr;
+  bool vals_are_float = true, cols_fit_16 = true;
+  for (int r = 0; r < n; ++r) {
+    for (int j = pia[r]; j < pia[r + 1]; ++j) {
+      const int c = pja[j];
+      if (c < 0 || c >= n) {
+        fail(EVSLCU_ERR_ARG, "CSR column index %d at position %d is outside [0, %d)", c, j, n);
+        return nullptr;
+      }
+      if (c - r > 32767 || c - r < -32768) cols_fit_16 = false;
+      const double v = pa[j];
+      if (!(std::isfinite(v) && (double)(float)v == v)) vals_are_float = false;
     }
   }
+  const bool allow = g_compress != 0;
   evslcu_mat *M = new evslcu_mat;
   M->n = n;
   M->nnz = nnz;
+  M->vfmt = (allow && vals_are_float) ? 1 : 0;
+  M->ifmt = (allow && cols_fit_16) ? 1 : 0;
   if (on_device) {
     M->ia = ia;
     M->ja = ja;
@@ -427,34 +424,49 @@ evslcu_mat *evslcu_mat_create(int n, int nnz, const int *ia, const int *ja, cons
     cptr[c + 1] = cptr[c] + 32LL * w;
   }
   const long long padded = cptr[nch];
-  std::vector<int> scol((size_t)std::max(padded, 1LL), 0);
-  std::vector<double> sval((size_t)std::max(padded, 1LL), 0.0);
+  const size_t cap = (size_t)std::max(padded, 1LL);
+  std::vector<int> scol(cap, 0);
+  std::vector<short> scol16(M->ifmt ? cap : 1, 0);
+  std::vector<double> sval(M->vfmt ? 1 : cap, 0.0);
+  std::vector<float> sval32(M->vfmt ? cap : 1, 0.0f);
   for (int c = 0; c < nch; ++c) {
     for (int l = 0; l < 32; ++l) {
       const int r = 32 * c + l;
       const int len = (r < n) ? pia[r + 1] - pia[r] : 0;
       for (int j = 0; j < cw[c]; ++j) {
         const long long p = cptr[c] + 32LL * j + l;
+        int col;
+        double v;
         if (j < len) {
-          scol[p] = pja[pia[r] + j];
-          sval[p] = pa[pia[r] + j];
+          col = pja[pia[r] + j];
+          v = pa[pia[r] + j];
         } else {
-          scol[p] = (r < n) ? r : 0;  // padding: 0 * x[r] adds nothing
-          sval[p] = 0.0;
+          col = (r < n) ? r : 0;  // padding: 0 * x[r] adds nothing
+          v = 0.0;
         }
+        if (M->ifmt)
+          scol16[p] = (short)(col - ((r < n) ? r : 0));
+        else
+          scol[p] = col;
+        if (M->vfmt)
+          sval32[p] = (float)v;
+        else
+          sval[p] = v;
       }
     }
   }
   M->nchunks = nch;
   M->padded = padded;
+  const size_t colb = M->ifmt ? sizeof(short) : sizeof(int);
+  const size_t valb = M->vfmt ? sizeof(float) : sizeof(double);
   M->cptr = (long long *)evslcu_malloc(sizeof(long long) * (nch + 1));
   M->cw = (int *)evslcu_malloc(sizeof(int) * nch);
-  M->scol = (int *)evslcu_malloc(sizeof(int) * (size_t)std::max(padded, 1LL));
-  M->sval = (double *)evslcu_malloc(sizeof(double) * (size_t)std::max(padded, 1LL));
+  M->scol = evslcu_malloc(colb * cap);
+  M->sval = evslcu_malloc(valb * cap);
   if (!M->cptr || !M->cw || !M->scol || !M->sval || evslcu_h2d(M->cptr, cptr.data(), sizeof(long long) * (nch + 1)) ||
       evslcu_h2d(M->cw, cw.data(), sizeof(int) * nch) ||
-      evslcu_h2d(M->scol, scol.data(), sizeof(int) * (size_t)padded) ||
-      evslcu_h2d(M->sval, sval.data(), sizeof(double) * (size_t)padded)) {
+      evslcu_h2d(M->scol, M->ifmt ? (const void *)scol16.data() : (const void *)scol.data(), colb * (size_t)padded) ||
+      evslcu_h2d(M->sval, M->vfmt ? (const void *)sval32.data() : (const void *)sval.data(), valb * (size_t)padded)) {
     evslcu_mat_destroy(M);
     return nullptr;
   }
@@ -491,102 +503,18 @@ int evslcu_mat_get_kernel(const evslcu_mat *A) { return A ? A->kernel : -1; }
 int evslcu_spmv(const evslcu_mat *A, const double *x, double *y) {
   if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
   const int grid = grid_for(A->n);
-  if (A->kernel == 0)
-    k_spmv<SellView><<<grid, kThreads, 0, stream()>>>(sell_view(A), x, y);
-  else
-    k_spmv<CsrView><<<grid, kThreads, 0, stream()>>>(csr_view(A), x, y);
-  EVSLCU_LAUNCH_CHECK("k_spmv");
-  return 0;
+  return with_view(A, [&](auto view) {
+    k_spmv<decltype(view)><<<grid, kThreads, 0, stream()>>>(view, x, y);
+    EVSLCU_LAUNCH_CHECK("k_spmv");
+    return 0;
+  });
 }
+
 
 int evslcu_cheb_update(int n, int k, double t, double s, double cc, double *vkp1, const double *vk,
                        const double *vkm1, double *y) {
   k_cheb_update<<<grid_for(n), kThreads, 0, stream()>>>(n, k, t, s, -cc, vkp1, vk, vkm1, y);
   EVSLCU_LAUNCH_CHECK("k_cheb_update");
-  return 0;
-}
-
-int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, double dd, const double *v, double *y,
-                  double *work, const evslcu_cheb_epi *epi) {
-  if (!op || !mu || deg < 0 || !v || !y || !work) return fail(EVSLCU_ERR_ARG, "evslcu_chebav: bad arguments");
-  const int n = op->n;
-  const double t1 = 1.0 / dd, t2 = 2.0 / dd, ncc = -cc;
-  double *W[2] = {work, work + n};
-  if (deg == 0) {
-    k_scale_copy<<<grid_for(n), kThreads, 0, stream()>>>(n, mu[0], v, y);
-    EVSLCU_LAUNCH_CHECK("k_scale_copy");
-    if (epi) {
-      k_lan_epi<<<grid_for(n), kThreads, 0, stream()>>>(n, epi->zold, epi->nbeta, epi->dotv, y, partials(),
-                                                        counters() + CTR_CHEB, epi->dot_out);
-      EVSLCU_LAUNCH_CHECK("k_lan_epi");
-    }
-    return 0;
-  }
-  if (op->A) {
-    const evslcu_mat *A = op->A;
-    cudaEvent_t ev_a = nullptr;
-    if (g_prof.on) {
-      ev_a = prof_event();
-      cudaEventRecord(ev_a, stream());
-    }
-    for (int k = 1; k <= deg; ++k) {
-      const double t = (k == 1) ? t1 : t2;
-      const double *vk = (k == 1) ? v : W[(k - 2) % 2];
-      const double *vkm1 = (k == 1) ? nullptr : ((k == 2) ? v : W[(k - 1) % 2]);
-      double *out = W[(k - 1) % 2];
-      const bool last = (k == deg);
-      int rc;
-      if (A->kernel == 0)
-        rc = launch_cheb_step(sell_view(A), n, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
-      else
-        rc = launch_cheb_step(csr_view(A), n, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
-      if (rc) return rc;
-    }
-    if (g_prof.on) {
-      // algorithmic bytes: A once per degree (8-byte value + 4-byte column per
-      // nonzero, 4-byte row pointer per row) plus the vectors each kernel
-      // touches: k = 1 reads v, writes w and y; k > 1 reads vk, vkm1, y and
-      // writes w, y; the Lanczos epilogue adds zold and v reads.
-      const double abytes = 12.0 * (double)A->nnz + 4.0 * ((double)n + 1.0);
-      double b = 0.0;
-      for (int k = 1; k <= deg; ++k) {
-        b += abytes + 8.0 * (double)n * ((k == 1) ? 3.0 : 5.0);
-        if (k == deg && epi) b += 8.0 * (double)n * ((epi->zold ? 1.0 : 0.0) + (epi->dotv ? 1.0 : 0.0));
-      }
-      cudaEvent_t ev_b = prof_event();
-      cudaEventRecord(ev_b, stream());
-      g_prof.pending.push_back({ev_a, ev_b, b, deg});
-    }
-    return 0;
-  }
-  // User matvec (SetAMatvec): the reference's three-vector rotation
-  // (SRC/chebpoly.c:532-589) with the callback computing vkp1 = A vk.  The
-  // callback must enqueue on the legacy default stream (which orders with the
-  // library stream) or finish its work before returning.
-  if (!op->func) return fail(EVSLCU_ERR_STATE, "no matrix or matvec registered");
-  double *vk = work, *vkp1 = work + n, *vkm1 = work + 2 * (size_t)n;
-  if (evslcu_d2d(vk, v, sizeof(double) * n)) return EVSLCU_ERR_CUDA;
-  k_scale_copy<<<grid_for(n), kThreads, 0, stream()>>>(n, mu[0], v, y);
-  EVSLCU_LAUNCH_CHECK("k_scale_copy");
-  for (int k = 1; k <= deg; ++k) {
-    const double t = (k == 1) ? t1 : t2;
-    cudaError_t e = cudaStreamSynchronize(stream());
-    if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "sync before matvec: %s", cudaGetErrorString(e));
-    op->func(vk, vkp1, op->data);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "user matvec failed: %s", cudaGetErrorString(e));
-    k_cheb_update<<<grid_for(n), kThreads, 0, stream()>>>(n, k, t, mu[k], ncc, vkp1, vk, vkm1, y);
-    EVSLCU_LAUNCH_CHECK("k_cheb_update");
-    double *tmp = vkm1;
-    vkm1 = vk;
-    vk = vkp1;
-    vkp1 = tmp;
-  }
-  if (epi) {
-    k_lan_epi<<<grid_for(n), kThreads, 0, stream()>>>(n, epi->zold, epi->nbeta, epi->dotv, y, partials(),
-                                                      counters() + CTR_CHEB, epi->dot_out);
-    EVSLCU_LAUNCH_CHECK("k_lan_epi");
-  }
   return 0;
 }
 
@@ -671,24 +599,5 @@ int evslcu_randn(int n, uint64_t seed, uint64_t draw, double *v) {
   EVSLCU_LAUNCH_CHECK("k_randn");
   return 0;
 }
-
-int evslcu_filter_profile(int enable) {
-  prof_resolve();
-  g_prof.on = enable != 0;
-  g_prof.seconds = g_prof.bytes = 0.0;
-  g_prof.launches = g_prof.calls = 0;
-  return 0;
-}
-
-int evslcu_filter_stats(double *seconds, double *bytes, uint64_t *launches, uint64_t *calls) {
-  prof_resolve();
-  if (seconds) *seconds = g_prof.seconds;
-  if (bytes) *bytes = g_prof.bytes;
-  if (launches) *launches = g_prof.launches;
-  if (calls) *calls = g_prof.calls;
-  return 0;
-}
-
-void *evslcu_stream_handle(void) { return (void *)stream(); }
 
 }  // extern "C"

@@ -1,0 +1,113 @@
+// Device representation of the registered sparse matrix and the row kernels
+// shared by the SpMV, filter and KPM kernels.
+#pragma once
+
+#include "common.cuh"
+
+// Prepared matrix.  The filter uses SELL-32: rows in chunks of 32, entries of
+// a chunk stored column-major (entry j of lane l at cptr[c] + 32 j + l),
+// chunks padded to their longest row with zero values pointing at the row
+// itself.  Storage is compressed losslessly when the matrix allows it:
+//   vfmt 1: values stored as float because every value is exactly a float;
+//   ifmt 1: columns stored as int16 offsets from the row (|col-row| < 32768).
+// Every variant multiplies in FP64 in the same order, so results are
+// identical bit for bit across variants.
+struct evslcu_mat {
+  int n = 0;
+  long long nnz = 0;
+  const int *ia = nullptr;  // CSR on the device
+  const int *ja = nullptr;
+  const double *a = nullptr;
+  bool own_csr = false;
+  int nchunks = 0;
+  long long padded = 0;
+  long long *cptr = nullptr;
+  int *cw = nullptr;
+  int vfmt = 0;
+  int ifmt = 0;
+  void *scol = nullptr;
+  void *sval = nullptr;
+  int kernel = 0;      // 0 SELL-32, 1 CSR (thread per row)
+  int persistent = 1;  // allow the single-launch filter
+};
+
+namespace evslcu {
+
+template <class VT, class IT>
+struct SellT {
+  int n;
+  const long long *__restrict__ cptr;
+  const int *__restrict__ cw;
+  const IT *__restrict__ col;
+  const VT *__restrict__ val;
+};
+
+struct CsrView {
+  int n;
+  const int *__restrict__ ia;
+  const int *__restrict__ ja;
+  const double *__restrict__ a;
+};
+
+__device__ __forceinline__ int decode_col(int c, int) { return c; }
+__device__ __forceinline__ int decode_col(short c, int r) { return r + (int)c; }
+
+// Load from a vector that this kernel may have written (bypass L1).
+template <bool COHERENT>
+__device__ __forceinline__ double ldx(const double *p) {
+  if (COHERENT) return __ldcg(p);
+  return __ldg(p);
+}
+
+// Row r of A times x, summed left to right with rounded multiply and add.
+template <bool COHERENT, class VT, class IT>
+__device__ __forceinline__ double row_dot(const SellT<VT, IT> &A, int r, const double *x) {
+  const int c = r >> 5;
+  long long p = A.cptr[c] + (r & 31);
+  const int w = A.cw[c];
+  double acc = 0.0;
+#pragma unroll 4
+  for (int j = 0; j < w; ++j, p += 32) {
+    const double v = (double)__ldg(A.val + p);
+    const int col = decode_col(__ldg(A.col + p), r);
+    acc = __dadd_rn(acc, __dmul_rn(v, ldx<COHERENT>(x + col)));
+  }
+  return acc;
+}
+
+template <bool COHERENT>
+__device__ __forceinline__ double row_dot(const CsrView &A, int r, const double *x) {
+  const int b = A.ia[r], e = A.ia[r + 1];
+  double acc = 0.0;
+#pragma unroll 4
+  for (int j = b; j < e; ++j) acc = __dadd_rn(acc, __dmul_rn(__ldg(A.a + j), ldx<COHERENT>(x + __ldg(A.ja + j))));
+  return acc;
+}
+
+template <class VT, class IT>
+inline SellT<VT, IT> sell_view(const evslcu_mat *A) {
+  return SellT<VT, IT>{A->n, A->cptr, A->cw, (const IT *)A->scol, (const VT *)A->sval};
+}
+
+inline CsrView csr_view(const evslcu_mat *A) { return CsrView{A->n, A->ia, A->ja, A->a}; }
+
+// Calls f(view) with the matrix's storage variant (SELL-32 or CSR).
+template <class F>
+inline int with_view(const evslcu_mat *A, F &&f) {
+  if (A->kernel == 1) return f(csr_view(A));
+  if (A->vfmt == 0 && A->ifmt == 0) return f(sell_view<double, int>(A));
+  if (A->vfmt == 0 && A->ifmt == 1) return f(sell_view<double, short>(A));
+  if (A->vfmt == 1 && A->ifmt == 0) return f(sell_view<float, int>(A));
+  return f(sell_view<float, short>(A));
+}
+
+// Per-degree filter path (sparse.cu): one fused kernel per degree.
+int chebav_per_degree(const evslcu_mat *A, const double *mu, int deg, double cc, double dd, const double *v,
+                      double *y, double *work, const evslcu_cheb_epi *epi);
+// Filter through a user matvec callback (sparse.cu).
+int chebav_user_matvec(const evslcu_op *op, const double *mu, int deg, double cc, double dd, const double *v,
+                       double *y, double *work, const evslcu_cheb_epi *epi);
+int launch_scale_copy(int n, double a, const double *x, double *y);
+int launch_lan_epi(int n, const evslcu_cheb_epi *epi, double *y);
+
+}  // namespace evslcu

@@ -176,6 +176,16 @@ int evslcu_kpm_dots(const evslcu_op *op, int n, int Mdeg, int nvec, const double
 int evslcu_filter_profile(int enable);
 int evslcu_filter_stats(double *seconds, double *bytes, uint64_t *launches, uint64_t *calls);
 void *evslcu_stream_handle(void);
+/* Non-zero (EVSLCU_ERR_TIMEOUT) if a bounded grid barrier of the filter
+ * kernel gave up since the last check; clears the flag.  Synchronous. */
+int evslcu_filter_error(void);
+/* Lossless compression of the SELL copy (values as float when all are exactly
+ * floats, columns as int16 offsets when they fit); applies to matrices
+ * created afterwards.  Default on. */
+int evslcu_set_compression(int on);
+int evslcu_mat_storage(const evslcu_mat *A, int *vfmt, int *ifmt);
+/* Allow (1, default) or forbid (0) the single-launch filter kernel. */
+int evslcu_mat_set_persistent(evslcu_mat *A, int on);
 
 /* ---- random vectors ------------------------------------------------------- */
 /* Counter-based uniform [-1,1) generator: value i of draw d under seed s is

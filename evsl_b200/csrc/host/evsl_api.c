@@ -117,6 +117,7 @@ static int register_csr(csrMat *A, int on_device) {
   evslh.mat = evslcu_mat_create(A->nrows, nnz, A->ia, A->ja, A->a, on_device);
   if (!evslh.mat) return from_cu(EVSLX_ERR_ARG);
   if (evslh.kernel >= 0) evslcu_mat_set_kernel(evslh.mat, evslh.kernel);
+  evslcu_mat_set_persistent(evslh.mat, evslh.no_persistent ? 0 : 1);
   evslh.mat_key = A;
   evslh.op.A = evslh.mat;
   evslh.op.func = NULL;
@@ -519,5 +520,22 @@ int evslx_filter_stats(double *seconds, double *bytes, uint64_t *launches, uint6
 int evslx_last_solve_info(int *lanczos_steps, int *candidates) {
   if (lanczos_steps) *lanczos_steps = evslh.last_kdim;
   if (candidates) *candidates = evslh.last_candidates;
+  return 0;
+}
+
+int evslx_set_filter_persistent(int on) {
+  evslh.no_persistent = on ? 0 : 1;
+  if (evslh.mat) return from_cu(evslcu_mat_set_persistent(evslh.mat, on));
+  return 0;
+}
+
+int evslx_set_matrix_compression(int on) { return from_cu(evslcu_set_compression(on)); }
+
+int evslx_matrix_storage(int *value_bytes, int *index_bytes) {
+  int vf = 0, xf = 0;
+  if (!evslh.mat) return evsl_seterr(EVSLX_ERR_STATE, "no registered CSR matrix");
+  evslcu_mat_storage(evslh.mat, &vf, &xf);
+  if (value_bytes) *value_bytes = vf ? 4 : 8;
+  if (index_bytes) *index_bytes = xf ? 2 : 4;
   return 0;
 }

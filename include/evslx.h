@@ -48,6 +48,19 @@ int evslx_kpmdos_probes(int Mdeg, int damping, int nvec, double *intv, const dou
 int evslx_set_spmv_kernel(int which);
 int evslx_get_spmv_kernel(void);
 
+/* Filter execution: 1 (default) runs all degrees of a filter application in
+ * one cooperative kernel (grid barriers between degrees, per-row state on
+ * chip); 0 launches one fused kernel per degree.  Results are identical. */
+int evslx_set_filter_persistent(int on);
+
+/* Lossless compression of the stored matrix used by the filter: values kept
+ * as float when every value is exactly a float, columns as 16-bit offsets
+ * from the row when they fit.  Applies to matrices registered afterwards;
+ * default on.  Results are identical either way. */
+int evslx_set_matrix_compression(int on);
+/* Bytes per stored value (4 or 8) and per stored column index (2 or 4). */
+int evslx_matrix_storage(int *value_bytes, int *index_bytes);
+
 /* y = A x for the registered matrix on device vectors (rows summed left to
  * right, like the reference CPU matvec SRC/spmat.c:257-298). */
 int evslx_matvec(const double *x, double *y);

@@ -204,3 +204,59 @@ def test_tiny_problem(gpu_lib):
     assert len(lam) == len(ex)
     assert np.max(np.abs(np.sort(lam) - ex)) < 1e-10
     gpu_lib.free_pol(pol)
+
+
+@pytest.mark.parametrize("compress", [True, False])
+@pytest.mark.parametrize("persistent", [True, False])
+def test_filter_variants_bitwise(gpu_lib, compress, persistent):
+    """Every storage variant (float/double values, int16/int32 columns) and
+    both execution modes (one cooperative launch / one launch per degree)
+    give the reference's filtered vector bit for bit."""
+    gpu_lib.set_matrix_compression(compress)
+    gpu_lib.set_filter_persistent(persistent)
+    try:
+        cases = []
+        ia, ja, a = O.lap_csr(24, 24, 24)
+        cases.append((ia, ja, a, [0.6, 0.69331, 0.0, 12.0]))
+        # non-float values and wide bandwidth (forces double values, int32 columns)
+        rng = np.random.default_rng(3)
+        n = 40000
+        rows = np.repeat(np.arange(n), 5)
+        cols = np.concatenate([[r, (r + 1) % n, (r * 7919) % n, (r + 35000) % n, (r * 31) % n] for r in range(n)])
+        vals = rng.uniform(-1, 1, len(rows)) * 0.1
+        key = rows.astype(np.int64) * n + cols
+        _, first = np.unique(key, return_index=True)
+        rows, cols, vals = rows[first], cols[first], vals[first]
+        # symmetric, diagonally dominant
+        R = np.concatenate([rows, cols]); Cc = np.concatenate([cols, rows]); V = np.concatenate([vals, vals])
+        key = R.astype(np.int64) * n + Cc
+        order = np.argsort(key, kind="stable")
+        R, Cc, V = R[order], Cc[order], V[order]
+        uk, start = np.unique(R.astype(np.int64) * n + Cc, return_index=True)
+        V = np.add.reduceat(V, start)
+        R, Cc = (uk // n).astype(np.int64), (uk % n).astype(np.int32)
+        diag = R == Cc
+        V[diag] += 3.0
+        ia2 = np.zeros(n + 1, dtype=np.int64)
+        np.add.at(ia2, R + 1, 1)
+        ia2 = np.cumsum(ia2).astype(np.int32)
+        cases.append((ia2, Cc, V, [0.5, 1.0, -1.0, 8.0]))
+        for ia, ja, a, iv in cases:
+            gpu_lib.set_csr(ia, ja, a)
+            vb, ib = gpu_lib.matrix_storage()
+            if not compress:
+                assert (vb, ib) == (8, 4)
+            pol = gpu_lib.find_pol(iv, max_deg=300)
+            v = O.seeded_normal(len(ia) - 1, 9)
+            y = gpu_lib.chebav(pol, v)
+            y_ref = O.cheb_av(O.find_pol(iv, max_deg=300), ia, ja, a, v)
+            assert np.array_equal(y, y_ref), (vb, ib, np.max(np.abs(y - y_ref)))
+            gpu_lib.free_pol(pol)
+    finally:
+        gpu_lib.set_matrix_compression(True)
+        gpu_lib.set_filter_persistent(True)
+
+
+def test_laplacian_storage_is_compressed(gpu_lib):
+    _lap(gpu_lib, 30, 30, 30)
+    assert gpu_lib.matrix_storage() == (4, 2)
