@@ -27,6 +27,12 @@ constexpr int kNumCounters = 16;
 // Slots 8-10 hold the filter grid barrier (count, generation) and its error flag.
 enum CounterId { CTR_DOT = 0, CTR_NRM = 1, CTR_CHEB = 2, CTR_CGS = 3, CTR_KPM = 4, CTR_COL = 5 };
 
+// Grid-barrier state of the single-launch filter: generation word at [0],
+// top-level arrival count at [32], group arrival counts at [64 + 32 g]
+// (one 128-byte line each).
+constexpr int kBarrierWords = 64 + 32 * 1024;
+unsigned int *barrier_area();
+
 constexpr int kThreads = 256;
 
 inline int grid_for(long long n, int threads = kThreads, int cap = kMaxPartials) {

@@ -18,6 +18,7 @@ struct Context {
   double *partials = nullptr;
   unsigned int *counters = nullptr;
   double *scalars = nullptr;
+  unsigned int *barrier = nullptr;
 };
 Context g_ctx;
 char g_err[512] = "";
@@ -28,6 +29,7 @@ cudaStream_t stream() { return g_ctx.stream; }
 double *partials() { return g_ctx.partials; }
 unsigned int *counters() { return g_ctx.counters; }
 double *dev_scratch_scalars() { return g_ctx.scalars; }
+unsigned int *barrier_area() { return g_ctx.barrier; }
 int sm_count() { return g_ctx.sms; }
 void count_launch(uint64_t k) { g_launches += k; }
 
@@ -85,6 +87,8 @@ int evslcu_init(void) {
   EVSLCU_CUDA(cudaMalloc(&g_ctx.counters, sizeof(unsigned int) * kNumCounters));
   EVSLCU_CUDA(cudaMemset(g_ctx.counters, 0, sizeof(unsigned int) * kNumCounters));
   EVSLCU_CUDA(cudaMalloc(&g_ctx.scalars, sizeof(double) * 64));
+  EVSLCU_CUDA(cudaMalloc(&g_ctx.barrier, sizeof(unsigned int) * kBarrierWords));
+  EVSLCU_CUDA(cudaMemset(g_ctx.barrier, 0, sizeof(unsigned int) * kBarrierWords));
   EVSLCU_CUDA(cudaMemset(g_ctx.scalars, 0, sizeof(double) * 64));
   g_ctx.ready = true;
   return 0;
@@ -96,6 +100,7 @@ int evslcu_finish(void) {
   cudaFree(g_ctx.partials);
   cudaFree(g_ctx.counters);
   cudaFree(g_ctx.scalars);
+  cudaFree(g_ctx.barrier);
   cudaStreamDestroy(g_ctx.stream);
   g_ctx = Context();
   cudaError_t e = cudaGetLastError();

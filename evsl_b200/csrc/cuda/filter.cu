@@ -1,7 +1,9 @@
 // Chebyshev filter application y = p((A - cc)/dd) v (reference ChebAv,
 // SRC/chebpoly.c:519-598) and its dispatch.
 //
-// Main path: one cooperative launch for all degrees.  Every warp owns a fixed
+// Default path: one fused kernel per degree (sparse.cu), launched with
+// programmatic dependent launch.  Optional path (evslx_set_filter_persistent):
+// one cooperative launch for all degrees.  Every warp owns a fixed
 // set of SELL-32 chunks for the whole filter; each lane keeps, for each of
 // its rows, y and v_{k-1} in shared memory, so a degree step only streams A,
 // writes the new vector once and gathers the previous one (mostly from L2).
@@ -87,26 +89,47 @@ double filter_bytes(const evslcu_mat *A, int deg, const evslcu_cheb_epi *epi) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned ld_volatile(const unsigned *p) { return *(const volatile unsigned *)p; }
 
-__device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, int *err) {
+// Two-level barrier: blocks arrive on their group's counter (groups of
+// kBarGroup blocks, each counter on its own 128-byte line); the last block
+// of a group arrives on the top-level counter; the last group bumps the
+// generation word that every block polls.  Polling is tight for the first
+// spins and then backs off; after kBarrierSpinLimit polls the block records
+// an error and the whole grid leaves the kernel.
+constexpr int kBarGroup = 16;
+
+__device__ __forceinline__ bool grid_barrier(unsigned *area, int *err) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
+    unsigned *gen = area;
+    unsigned *top = area + 32;
+    const unsigned ngroups = (gridDim.x + kBarGroup - 1) / kBarGroup;
+    const unsigned g = blockIdx.x / kBarGroup;
+    const unsigned gsize = min((unsigned)kBarGroup, gridDim.x - g * kBarGroup);
+    unsigned *grp = area + 64 + 32 * g;
     int ok = 1;
     const unsigned my = ld_volatile(gen);
     __threadfence();
-    if (atomicAdd(count, 1u) == gridDim.x - 1) {
-      atomicExch(count, 0u);
-      __threadfence();
-      atomicAdd(gen, 1u);
-    } else {
+    bool release = false;
+    if (atomicAdd(grp, 1u) == gsize - 1) {
+      atomicExch(grp, 0u);
+      if (atomicAdd(top, 1u) == ngroups - 1) {
+        atomicExch(top, 0u);
+        __threadfence();
+        atomicAdd(gen, 1u);
+        release = true;
+      }
+    }
+    if (!release) {
       unsigned long long spins = 0;
       while (ld_volatile(gen) == my) {
-        if (++spins > kBarrierSpinLimit) {
+        ++spins;
+        if (spins > kBarrierSpinLimit) {
           atomicExch(err, 1);
           ok = 0;
           break;
         }
-        __nanosleep(32);
+        if (spins > 4096) __nanosleep(64);
       }
     }
     __threadfence();
@@ -131,21 +154,21 @@ struct PersistArgs {
   double *part;
   unsigned *ctr_dot;
   double *dot_out;
-  unsigned *bar_count, *bar_gen;
+  unsigned *bar;
   int *err;
 };
 
 // Per-row state lives in dynamic shared memory: for slot i of thread t,
-// y at st[i*kThreads + t] and v_{k-1} at st[(S + i)*kThreads + t].
-template <class VIEW>
-__global__ void __launch_bounds__(kThreads) k_filter_persistent(VIEW A, PersistArgs P, int S) {
+// y at st[i*NT + t] and v_{k-1} at st[(S + i)*NT + t].
+template <class VIEW, int NT>
+__global__ void __launch_bounds__(NT) k_filter_persistent(VIEW A, PersistArgs P, int S) {
   extern __shared__ double st[];
-  __shared__ double sh[kThreads / 32];
-  double *ys = st, *vs = st + (size_t)S * kThreads;
+  __shared__ double sh[NT / 32];
+  double *ys = st, *vs = st + (size_t)S * NT;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  const int gwarp = blockIdx.x * (kThreads / 32) + (tid >> 5);
-  const int nwarps = gridDim.x * (kThreads / 32);
+  const int gwarp = blockIdx.x * (NT / 32) + (tid >> 5);
+  const int nwarps = gridDim.x * (NT / 32);
   const double mu0 = P.mu[0];
   for (int k = 1; k <= P.deg; ++k) {
     const double t = (k == 1) ? P.t1 : P.t2;
@@ -165,21 +188,21 @@ __global__ void __launch_bounds__(kThreads) k_filter_persistent(VIEW A, PersistA
           xv = __ldcg(x + r);
         }
         double w = __dmul_rn(t, __dadd_rn(acc, __dmul_rn(P.ncc, xv)));
-        if (k > 1) w = __dadd_rn(w, -vs[i * kThreads + tid]);
+        if (k > 1) w = __dadd_rn(w, -vs[i * NT + tid]);
         __stcg(out + r, w);
-        const double yo = (k == 1) ? __dmul_rn(mu0, xv) : ys[i * kThreads + tid];
-        ys[i * kThreads + tid] = __dadd_rn(yo, __dmul_rn(s, w));
-        vs[i * kThreads + tid] = xv;
+        const double yo = (k == 1) ? __dmul_rn(mu0, xv) : ys[i * NT + tid];
+        ys[i * NT + tid] = __dadd_rn(yo, __dmul_rn(s, w));
+        vs[i * NT + tid] = xv;
       }
     }
-    if (k < P.deg && !grid_barrier(P.bar_count, P.bar_gen, P.err)) return;
+    if (k < P.deg && !grid_barrier(P.bar, P.err)) return;
   }
   double dsum = 0.0;
   for (int i = 0; i < S; ++i) {
     const int c = gwarp + i * nwarps;
     const int r = c * 32 + lane;
     if (c < P.nchunks && r < A.n) {
-      double yy = ys[i * kThreads + tid];
+      double yy = ys[i * NT + tid];
       if (P.zold) yy = __dadd_rn(yy, __dmul_rn(P.nbeta, P.zold[r]));
       P.y[r] = yy;
       if (P.dotv) dsum += P.dotv[r] * yy;
@@ -197,10 +220,10 @@ __global__ void __launch_bounds__(kThreads) k_filter_persistent(VIEW A, PersistA
 
 // Launch with the most resident blocks per SM whose shared-memory state
 // still covers every chunk; returns with *launched = false if none does.
-template <class VIEW>
-int launch_persistent(const VIEW &view, int nchunks, PersistArgs &P, bool *launched) {
+template <class VIEW, int NT>
+int launch_persistent_nt(const VIEW &view, int nchunks, PersistArgs &P, bool *launched) {
   static int smem_max = -1;
-  const void *fn = (const void *)k_filter_persistent<VIEW>;
+  const void *fn = (const void *)k_filter_persistent<VIEW, NT>;
   if (smem_max < 0) {
     int dev = 0, coop = 0, optin = 0;
     cudaGetDevice(&dev);
@@ -215,13 +238,13 @@ int launch_persistent(const VIEW &view, int nchunks, PersistArgs &P, bool *launc
   }
   if (smem_max <= 0) return 0;
   const int sms = sm_count();
-  for (int b = 8; b >= 1; --b) {
-    const long long warps = (long long)b * sms * (kThreads / 32);
+  for (int b = 2048 / NT; b >= 1; --b) {
+    const long long warps = (long long)b * sms * (NT / 32);
     const int S = (int)((nchunks + warps - 1) / warps);
-    const size_t smem = (size_t)S * kThreads * 2 * sizeof(double);
+    const size_t smem = (size_t)S * NT * 2 * sizeof(double);
     if ((long long)smem > smem_max) continue;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, smem) != cudaSuccess) {
       cudaGetLastError();
       continue;
     }
@@ -230,13 +253,27 @@ int launch_persistent(const VIEW &view, int nchunks, PersistArgs &P, bool *launc
     if (grid > kMaxPartials) continue;
     int Sarg = S;
     void *args[] = {(void *)&view, (void *)&P, (void *)&Sarg};
-    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, stream());
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(NT), args, smem, stream());
     count_launch();
     if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "cooperative filter launch failed: %s", cudaGetErrorString(e));
     *launched = true;
     return 0;
   }
   return 0;
+}
+
+int g_filter_block = 1024;  // threads per block of the single-launch filter
+
+template <class VIEW>
+int launch_persistent(const VIEW &view, int nchunks, PersistArgs &P, bool *launched) {
+  int rc = 0;
+  if (g_filter_block >= 1024) {
+    if ((rc = launch_persistent_nt<VIEW, 1024>(view, nchunks, P, launched)) || *launched) return rc;
+  }
+  if (g_filter_block >= 512) {
+    if ((rc = launch_persistent_nt<VIEW, 512>(view, nchunks, P, launched)) || *launched) return rc;
+  }
+  return launch_persistent_nt<VIEW, 256>(view, nchunks, P, launched);
 }
 
 // device copy of the coefficients
@@ -286,8 +323,8 @@ int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, dou
       if (!g_mu_dev) return EVSLCU_ERR_NOMEM;
     }
     if ((rc = evslcu_h2d_async(g_mu_dev, mu, sizeof(double) * (deg + 1)))) return rc;
-    unsigned *bar = counters() + 8;
-    if ((rc = evslcu_memset(bar, 0, sizeof(unsigned))) || (rc = evslcu_memset(counters() + 10, 0, sizeof(int))))
+    if ((rc = evslcu_memset(barrier_area(), 0, sizeof(unsigned) * kBarrierWords)) ||
+        (rc = evslcu_memset(counters() + 10, 0, sizeof(int))))
       return rc;
     PersistArgs P;
     P.nchunks = A->nchunks;
@@ -306,8 +343,7 @@ int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, dou
     P.part = partials();
     P.ctr_dot = counters() + CTR_CHEB;
     P.dot_out = epi ? epi->dot_out : nullptr;
-    P.bar_count = counters() + 8;
-    P.bar_gen = counters() + 9;
+    P.bar = barrier_area();
     P.err = (int *)(counters() + 10);
     rc = with_view(A, [&](auto view) { return launch_persistent(view, A->nchunks, P, &launched); });
     if (rc) return rc;
@@ -340,6 +376,13 @@ int evslcu_filter_stats(double *seconds, double *bytes, uint64_t *launches, uint
 }
 
 void *evslcu_stream_handle(void) { return (void *)stream(); }
+
+int evslcu_set_filter_block(int threads) {
+  if (threads != 256 && threads != 512 && threads != 1024)
+    return fail(EVSLCU_ERR_ARG, "filter block size must be 256, 512 or 1024");
+  g_filter_block = threads;
+  return 0;
+}
 
 int evslcu_mat_set_persistent(evslcu_mat *A, int on) {
   if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");

@@ -39,6 +39,11 @@ __global__ void __launch_bounds__(kThreads)
            double ncc, double s, double mu0, const double *__restrict__ zold, double nbeta,
            const double *__restrict__ dotv, double *part, unsigned int *ctr, double *dot_out) {
   __shared__ double sh[kThreads / 32];
+  // Programmatic dependent launch: let the next degree's kernel start its
+  // launch now, and wait here until the previous kernel has completed and its
+  // writes are visible (no-ops when launched without the attribute).
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   double dsum = 0.0;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) {
     const double acc = row_dot<false>(A, r, vk);
@@ -106,26 +111,37 @@ __global__ void k_lan_epi(int n, const double *zold, double nbeta, const double 
 
 template <class M>
 int launch_cheb_step(const M &view, int n, bool first, bool epi, const double *vk, const double *vkm1, double *out,
-                     double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *e) {
+                     double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep) {
   const int grid = grid_for(n);
   cudaStream_t st = stream();
-  const double *zold = (epi && e) ? e->zold : nullptr;
-  const double nbeta = (epi && e) ? e->nbeta : 0.0;
-  const double *dotv = (epi && e) ? e->dotv : nullptr;
-  double *dout = (epi && e) ? e->dot_out : nullptr;
+  const double *zold = (epi && ep) ? ep->zold : nullptr;
+  const double nbeta = (epi && ep) ? ep->nbeta : 0.0;
+  const double *dotv = (epi && ep) ? ep->dotv : nullptr;
+  double *dout = (epi && ep) ? ep->dot_out : nullptr;
   unsigned int *ctr = counters() + CTR_CHEB;
+  void (*fn)(M, const double *, const double *, double *, double *, double, double, double, double,
+             const double *, double, const double *, double *, unsigned int *, double *);
   if (first && epi)
-    k_cheb<M, true, true><<<grid, kThreads, 0, st>>>(view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
-                                                     partials(), ctr, dout);
+    fn = k_cheb<M, true, true>;
   else if (first)
-    k_cheb<M, true, false><<<grid, kThreads, 0, st>>>(view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
-                                                      partials(), ctr, dout);
+    fn = k_cheb<M, true, false>;
   else if (epi)
-    k_cheb<M, false, true><<<grid, kThreads, 0, st>>>(view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
-                                                      partials(), ctr, dout);
+    fn = k_cheb<M, false, true>;
   else
-    k_cheb<M, false, false><<<grid, kThreads, 0, st>>>(view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
-                                                       partials(), ctr, dout);
+    fn = k_cheb<M, false, false>;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, fn, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv, partials(),
+                                     ctr, dout);
+  if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "k_cheb launch failed: %s", cudaGetErrorString(e));
   EVSLCU_LAUNCH_CHECK("k_cheb");
   return 0;
 }

@@ -28,7 +28,7 @@ struct evslcu_mat {
   void *scol = nullptr;
   void *sval = nullptr;
   int kernel = 0;      // 0 SELL-32, 1 CSR (thread per row)
-  int persistent = 1;  // allow the single-launch filter
+  int persistent = 0;  // 1: single cooperative launch per filter application
 };
 
 namespace evslcu {

@@ -184,6 +184,9 @@ int evslcu_filter_error(void);
  * created afterwards.  Default on. */
 int evslcu_set_compression(int on);
 int evslcu_mat_storage(const evslcu_mat *A, int *vfmt, int *ifmt);
+/* Threads per block of the single-launch filter (256, 512, 1024; default
+ * 1024: fewer blocks meet at each grid barrier). */
+int evslcu_set_filter_block(int threads);
 /* Allow (1, default) or forbid (0) the single-launch filter kernel. */
 int evslcu_mat_set_persistent(evslcu_mat *A, int on);
 

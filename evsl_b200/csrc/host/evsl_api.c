@@ -117,7 +117,7 @@ static int register_csr(csrMat *A, int on_device) {
   evslh.mat = evslcu_mat_create(A->nrows, nnz, A->ia, A->ja, A->a, on_device);
   if (!evslh.mat) return from_cu(EVSLX_ERR_ARG);
   if (evslh.kernel >= 0) evslcu_mat_set_kernel(evslh.mat, evslh.kernel);
-  evslcu_mat_set_persistent(evslh.mat, evslh.no_persistent ? 0 : 1);
+  evslcu_mat_set_persistent(evslh.mat, evslh.persistent);
   evslh.mat_key = A;
   evslh.op.A = evslh.mat;
   evslh.op.func = NULL;
@@ -524,7 +524,7 @@ int evslx_last_solve_info(int *lanczos_steps, int *candidates) {
 }
 
 int evslx_set_filter_persistent(int on) {
-  evslh.no_persistent = on ? 0 : 1;
+  evslh.persistent = on ? 1 : 0;
   if (evslh.mat) return from_cu(evslcu_mat_set_persistent(evslh.mat, on));
   return 0;
 }
@@ -539,3 +539,5 @@ int evslx_matrix_storage(int *value_bytes, int *index_bytes) {
   if (index_bytes) *index_bytes = xf ? 2 : 4;
   return 0;
 }
+
+int evslx_set_filter_block(int threads) { return from_cu(evslcu_set_filter_block(threads)); }

@@ -29,7 +29,7 @@ typedef struct {
   uint64_t seed;             /* device RNG seed */
   uint64_t draw;             /* next draw index of the device RNG */
   int kernel;                /* filter kernel choice, -1 = library default */
-  int no_persistent;         /* 1: one launch per filter degree */
+  int persistent;            /* 1: one cooperative launch per filter application */
   double last_kpm_seconds;   /* device time of the last kpmdos moment loop */
   int last_kdim;             /* Lanczos dimension of the last ChebLanNr/ChebLanTr */
   int last_candidates;       /* Ritz values >= bar examined at the end */

@@ -48,10 +48,14 @@ int evslx_kpmdos_probes(int Mdeg, int damping, int nvec, double *intv, const dou
 int evslx_set_spmv_kernel(int which);
 int evslx_get_spmv_kernel(void);
 
-/* Filter execution: 1 (default) runs all degrees of a filter application in
- * one cooperative kernel (grid barriers between degrees, per-row state on
- * chip); 0 launches one fused kernel per degree.  Results are identical. */
+/* Filter execution: 0 (default) launches one fused kernel per degree, each
+ * launched with programmatic dependent launch so consecutive degrees overlap
+ * their launch; 1 runs all degrees of a filter application in one
+ * cooperative kernel (bounded grid barriers between degrees, per-row state in
+ * shared memory).  Results are identical bit for bit. */
 int evslx_set_filter_persistent(int on);
+/* Threads per block of the single-launch filter: 256, 512 or 1024 (default). */
+int evslx_set_filter_block(int threads);
 
 /* Lossless compression of the stored matrix used by the filter: values kept
  * as float when every value is exactly a float, columns as 16-bit offsets
