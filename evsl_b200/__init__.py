@@ -120,6 +120,7 @@ def load():
         "evslx_set_seed": ([C.c_uint64], C.c_int),
         "evslx_get_draw": ([], C.c_uint64),
         "evslx_kpmdos_probes": ([C.c_int, C.c_int, C.c_int, _dp, C.c_void_p, _dp, _dp], C.c_int),
+        "evslx_kpmdos_probes_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, C.c_void_p, _dp, _dp], C.c_int),
         "evslx_set_spmv_kernel": ([C.c_int], C.c_int),
         "evslx_get_spmv_kernel": ([], C.c_int),
         "evslx_matvec": ([C.c_void_p, C.c_void_p], C.c_int),

@@ -268,6 +268,39 @@ __global__ void k_randn(int n, uint64_t seed, uint64_t draw, double *v) {
 }
 
 
+
+// Sequential accumulation of the KPM moments and the eigenvalue count from
+// the raw dot products, in the same order and with the same rounded
+// operations as the host accumulation of kpmdos (probe-major, then degree).
+__global__ void k_kpm_accumulate(int Mdeg, int nvec, const double *jac, const double *sdiff, const double *dots,
+                                 double bdiff, double t, double nd, double *mu, double *ecnt) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int k = 0; k <= Mdeg; ++k) mu[k] = 0.0;
+  double tcnt = 0.0;
+  for (int m = 0; m < nvec; ++m) {
+    mu[0] = __dadd_rn(mu[0], jac[0]);
+    tcnt = __dsub_rn(tcnt, __dmul_rn(jac[0], bdiff));
+    for (int k = 0; k < Mdeg; ++k) {
+      const int k1 = k + 1;
+      const double tk = __dmul_rn(__dmul_rn(2.0, jac[k1]), dots[(size_t)k * nvec + m]);
+      mu[k1] = __dadd_rn(mu[k1], tk);
+      tcnt = __dsub_rn(tcnt, __ddiv_rn(__dmul_rn(tk, sdiff[k]), (double)k1));
+    }
+  }
+  for (int k = 0; k <= Mdeg; ++k) mu[k] = __dmul_rn(t, mu[k]);
+  *ecnt = __dmul_rn(tcnt, __dmul_rn(t, nd));
+}
+
+// Scratch of the allocation-free KPM entry point: a fixed 32 MiB array in the
+// device image of the library.  Every GPU that loads the library holds it
+// until the process exits.  All calls share it.
+constexpr size_t kNoAllocDoubles = (size_t)1 << 22;
+static __device__ __align__(256) double g_kpm_noalloc_scratch[kNoAllocDoubles];
+
+// Device address of the scratch array, looked up once per device.
+constexpr int kMaxDevices = 64;
+double *g_noalloc_ptr[kMaxDevices] = {};
+
 }  // namespace
 
 int evslcu::launch_scale_copy(int n, double a, const double *x, double *y) {
@@ -614,6 +647,97 @@ int evslcu_randn(int n, uint64_t seed, uint64_t draw, double *v) {
   k_randn<<<grid_for(n), kThreads, 0, stream()>>>(n, seed, draw, v);
   EVSLCU_LAUNCH_CHECK("k_randn");
   return 0;
+}
+
+
+size_t evslcu_kpm_noalloc_capacity(void) { return kNoAllocDoubles; }
+
+size_t evslcu_kpm_noalloc_need(int n, int Mdeg, int nvec) {
+  const int G = (int)std::min<long long>(((long long)n + 7) / 8, 4096);
+  const int gx = std::min(grid_for(n), 512);
+  return 64 + (size_t)nvec /* norms */ + (size_t)(Mdeg + 1) /* jac */ + (size_t)Mdeg /* sdiff */ +
+         (size_t)Mdeg * nvec /* dots */ + (size_t)std::max(G, gx) * nvec /* partials */ + (size_t)(Mdeg + 2) /* out */ +
+         3 * (size_t)n * nvec /* block vectors */;
+}
+
+int evslcu_kpm_noalloc(const evslcu_op *op, int n, int Mdeg, int nvec, const double *probes, double ctr, double wid,
+                       const double *jac_h, const double *sdiff_h, double bdiff, double t, double *mu_h,
+                       double *ecnt_h) {
+  if (!op || !op->A) return fail(EVSLCU_ERR_STATE, "KPM needs a registered CSR matrix");
+  if (nvec < 1 || nvec > 128 || Mdeg < 1 || n < 1) return fail(EVSLCU_ERR_ARG, "kpm: bad sizes");
+  const size_t need = evslcu_kpm_noalloc_need(n, Mdeg, nvec);
+  if (need > kNoAllocDoubles)
+    return fail(EVSLCU_ERR_ARG,
+                "allocation-free kpmdos needs %zu doubles of scratch (3*n*nvec + Mdeg*nvec + ...) but the fixed "
+                "scratch holds %zu (32 MiB); use kpmdos/evslx_kpmdos_probes for this size",
+                need, kNoAllocDoubles);
+  // set-up, once per device, with that device current
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return fail(EVSLCU_ERR_ARG, "device ordinal %d out of range", dev);
+  if (!g_noalloc_ptr[dev]) {
+    double *ptr = nullptr;
+    e = cudaGetSymbolAddress((void **)&ptr, g_kpm_noalloc_scratch);
+    if (e != cudaSuccess || !ptr)
+      return fail(EVSLCU_ERR_CUDA, "cudaGetSymbolAddress of the KPM scratch failed: %s", cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = ptr;
+  }
+  double *base = g_noalloc_ptr[dev];
+  unsigned int *ctrs = (unsigned int *)base;  // first 64 doubles: counters
+  const int B = nvec;
+  const int G = (int)std::min<long long>(((long long)n + 7) / 8, 4096);
+  const int gx = std::min(grid_for(n), 512);
+  double *nrm = base + 64;
+  double *jac = nrm + B;
+  double *sdiff = jac + (Mdeg + 1);
+  double *ddots = sdiff + Mdeg;
+  double *part = ddots + (size_t)Mdeg * B;
+  double *out = part + (size_t)std::max(G, gx) * B;
+  double *V0 = out + (Mdeg + 2);
+  const size_t blk = (size_t)n * B;
+  double *W0 = V0 + blk, *W1 = W0 + blk;
+  int rc;
+  // the reduction counters must start at zero; the scratch keeps the last call's contents
+  if ((rc = evslcu_memset(ctrs, 0, 64 * sizeof(double)))) return rc;
+  if ((rc = evslcu_h2d(jac, jac_h, sizeof(double) * (Mdeg + 1))) || (rc = evslcu_h2d(sdiff, sdiff_h, sizeof(double) * Mdeg)))
+    return rc;
+  cudaStream_t st = stream();
+  k_colsq_partial<<<dim3(gx, B), kThreads, 0, st>>>(n, B, probes, part, ctrs + 0, nrm);
+  EVSLCU_LAUNCH_CHECK("k_colsq_partial");
+  k_interleave_scaled<<<grid_for(blk), kThreads, 0, st>>>(n, B, probes, nrm, V0);
+  EVSLCU_LAUNCH_CHECK("k_interleave_scaled");
+  const CsrView A = csr_view(op->A);
+  const double nctr = -ctr;
+  double *W[2] = {W0, W1};
+  for (int k = 0; k < Mdeg; ++k) {
+    const double scal = (k == 0 ? 1.0 : 2.0) / wid;
+    const double *vk = (k == 0) ? V0 : W[(k - 1) % 2];
+    const double *vkm1 = (k == 0) ? nullptr : ((k == 1) ? V0 : W[k % 2]);
+    double *o = W[k % 2];
+    double *drow = ddots + (size_t)k * B;
+    if (B <= 32) {
+      if (k == 0)
+        k_kpm<1, true><<<G, kThreads, 0, st>>>(A, B, vk, vkm1, o, scal, nctr, V0, part, ctrs + 1, drow);
+      else
+        k_kpm<1, false><<<G, kThreads, 0, st>>>(A, B, vk, vkm1, o, scal, nctr, V0, part, ctrs + 1, drow);
+    } else if (B <= 64) {
+      if (k == 0)
+        k_kpm<2, true><<<G, kThreads, 0, st>>>(A, B, vk, vkm1, o, scal, nctr, V0, part, ctrs + 1, drow);
+      else
+        k_kpm<2, false><<<G, kThreads, 0, st>>>(A, B, vk, vkm1, o, scal, nctr, V0, part, ctrs + 1, drow);
+    } else {
+      if (k == 0)
+        k_kpm<4, true><<<G, kThreads, 0, st>>>(A, B, vk, vkm1, o, scal, nctr, V0, part, ctrs + 1, drow);
+      else
+        k_kpm<4, false><<<G, kThreads, 0, st>>>(A, B, vk, vkm1, o, scal, nctr, V0, part, ctrs + 1, drow);
+    }
+    EVSLCU_LAUNCH_CHECK("k_kpm");
+  }
+  k_kpm_accumulate<<<1, 1, 0, st>>>(Mdeg, B, jac, sdiff, ddots, bdiff, t, (double)n, out, out + Mdeg + 1);
+  EVSLCU_LAUNCH_CHECK("k_kpm_accumulate");
+  if ((rc = evslcu_d2h(mu_h, out, sizeof(double) * (Mdeg + 1)))) return rc;
+  return evslcu_d2h(ecnt_h, out + Mdeg + 1, sizeof(double));
 }
 
 }  // extern "C"

@@ -190,6 +190,18 @@ int evslcu_set_filter_block(int threads);
 /* Allow (1, default) or forbid (0) the single-launch filter kernel. */
 int evslcu_mat_set_persistent(evslcu_mat *A, int on);
 
+/* Allocation-free variant of the KPM moments: all scratch (block vectors,
+ * dots, partial sums, counters) lives in a fixed 32 MiB __device__ array
+ * of the library image; jac/sdiff are the host-computed damping factors and
+ * sine differences; mu (Mdeg+1) and ecnt are host outputs.  Synchronous.
+ * Calls no allocation routine; sizes whose scratch exceeds the array are
+ * rejected with EVSLCU_ERR_ARG.  The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress). */
+size_t evslcu_kpm_noalloc_capacity(void);
+size_t evslcu_kpm_noalloc_need(int n, int Mdeg, int nvec);
+int evslcu_kpm_noalloc(const evslcu_op *op, int n, int Mdeg, int nvec, const double *probes, double ctr, double wid,
+                       const double *jac, const double *sdiff, double bdiff, double t, double *mu, double *ecnt);
+
 /* ---- random vectors ------------------------------------------------------- */
 /* Counter-based uniform [-1,1) generator: value i of draw d under seed s is
  * mix64(s*0x9E3779B97F4A7C15 + (d<<32) + i) mapped to [-1,1), where mix64 is

@@ -100,6 +100,41 @@ int evslx_kpmdos_probes(int Mdeg, int damping, int nvec, double *intv, const dou
   return kpm_run(Mdeg, damping, nvec, intv, probes, mu, ecnt);
 }
 
+/* Allocation-free kpmdos with caller probes (no counterpart in the
+ * reference).  Same algorithm and arithmetic as evslx_kpmdos_probes; the
+ * damping factors and sine differences are formed on this thread's stack and
+ * everything else lives in the library's fixed device scratch. */
+int evslx_kpmdos_probes_noalloc(int Mdeg, int damping, int nvec, double *intv, const double *probes, double *mu,
+                                double *ecnt) {
+  int rc = evsl_require_operator();
+  if (rc) return rc;
+  if (evsl_check_intv(intv, stdout) < 0) return -1;
+  if (!probes || !mu || !ecnt) return evsl_seterr(EVSLX_ERR_ARG, "kpmdos: probes, mu and ecnt are required");
+  if (Mdeg < 1 || Mdeg > EVSLX_NOALLOC_KPM_MAX_DEG || nvec < 1 || nvec > 128)
+    return evsl_seterr(EVSLX_ERR_ARG,
+                       "allocation-free kpmdos: need 1 <= Mdeg <= %d and 1 <= nvec <= 128 (got Mdeg=%d nvec=%d)",
+                       EVSLX_NOALLOC_KPM_MAX_DEG, Mdeg, nvec);
+  const int n = evsl_op()->n;
+  const double aa = evsl_max(intv[0], intv[2]), bb = evsl_min(intv[1], intv[3]);
+  const double ctr = (intv[3] + intv[2]) / 2.0, wid = (intv[3] - intv[2]) / 2.0;
+  double t = evsl_max(-1.0 + DBL_EPSILON, (aa - ctr) / wid);
+  const double beta1 = acos(t);
+  t = evsl_min(1.0 - DBL_EPSILON, (bb - ctr) / wid);
+  const double beta2 = acos(t);
+  double jac[EVSLX_NOALLOC_KPM_MAX_DEG + 1];
+  double sdiff[EVSLX_NOALLOC_KPM_MAX_DEG];
+  dampcf(Mdeg, damping, jac);
+  jac[0] = 1.0;
+  for (int k = 0; k < Mdeg; k++) {
+    const int k1 = k + 1;
+    sdiff[k] = sin(k1 * beta2) - sin(k1 * beta1);
+  }
+  const double scale = 1.0 / (((double)nvec) * EVSL_PI);
+  rc = evslcu_kpm_noalloc(evsl_op(), n, Mdeg, nvec, probes, ctr, wid, jac, sdiff, beta2 - beta1, scale, mu, ecnt);
+  if (rc) return evsl_seterr(rc, "%s", evslcu_errstr());
+  return 0;
+}
+
 /* integrals of the KPM DOS from xi[0] to each xi[j] */
 static int int_chx(int Mdeg, const double *mu, int npts, const double *xi, double *yi) {
   double *thetas = (double *)malloc(sizeof(double) * (size_t)npts);

@@ -43,6 +43,32 @@ uint64_t evslx_get_draw(void);
 int evslx_kpmdos_probes(int Mdeg, int damping, int nvec, double *intv, const double *probes,
                         double *mu, double *ecnt);
 
+/* kpmdos with caller probes that allocates nothing -- no counterpart in the
+ * reference.  For callers that must not allocate device memory while they
+ * run: a serving process that reserves the GPU's memory up front (resident
+ * matrices and Lanczos bases under a fixed HBM budget) cannot let a density-
+ * of-states request call cudaMalloc/cudaFree, which would break the budget
+ * and synchronise the device in the middle of other requests.  Results are
+ * the same as evslx_kpmdos_probes.
+ *
+ * All device scratch (block vectors, dot products, partial sums, counters)
+ * lives in one fixed 32 MiB array inside the library's device image, which
+ * every GPU that loads the library holds until the process exits.  Limits:
+ * 1 <= nvec <= 128, 1 <= Mdeg <= EVSLX_NOALLOC_KPM_MAX_DEG, and
+ * 3*n*nvec + Mdeg*nvec + (partial sums) must fit the array (about
+ * n*nvec <= 1.3 million); larger sizes return EVSLX_ERR_ARG with a message.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call uses the same array and keeps the previous call's contents
+ * (the reduction counters are cleared at the start of each call), so calls
+ * that overlap on the GPU -- from several host threads, or enqueued on
+ * different streams -- race and must be serialised by the caller.  Probes
+ * are DEVICE memory (column-major n x nvec); mu and ecnt are host outputs;
+ * the call returns when they are written. */
+#define EVSLX_NOALLOC_KPM_MAX_DEG 4096
+int evslx_kpmdos_probes_noalloc(int Mdeg, int damping, int nvec, double *intv, const double *probes,
+                                double *mu, double *ecnt);
+
 /* Filter SpMV kernel for the registered matrix: 0 = SELL-32 (default),
  * 1 = CSR one thread per row.  Both give identical (bitwise) results. */
 int evslx_set_spmv_kernel(int which);
