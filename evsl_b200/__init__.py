@@ -15,7 +15,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Library", "PolParams", "DeviceBuffer", "EvslError", "library_path", "load"]
+__all__ = ["Library", "PolParams", "DeviceBuffer", "EvslError", "library_path", "load", "kpm_accumulate"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -83,6 +83,20 @@ def _i(a):
 _LIB = None
 
 
+def kpm_accumulate(Mdeg, damping, n, intv, dots):
+    """Host-only accumulation of KPM moments from raw dots (Mdeg x nvec);
+    needs the library but no GPU."""
+    lib = load()
+    dots = np.ascontiguousarray(dots, dtype=np.float64)
+    mu = np.zeros(Mdeg + 1)
+    ec = C.c_double()
+    iv = np.ascontiguousarray(intv, dtype=np.float64)
+    rc = lib.evslx_kpm_accumulate(Mdeg, damping, dots.shape[1], n, _d(iv), _d(dots), _d(mu), C.byref(ec))
+    if rc != 0:
+        raise EvslError(f"evslx_kpm_accumulate returned {rc}")
+    return mu, ec.value
+
+
 def load():
     """Load libevsl_b200.so (raises if it is missing)."""
     global _LIB
@@ -122,6 +136,9 @@ def load():
         "evslx_kpmdos_probes": ([C.c_int, C.c_int, C.c_int, _dp, C.c_void_p, _dp, _dp], C.c_int),
         "evslx_kpmdos_probes_noalloc": ([C.c_int, C.c_int, C.c_int, _dp, C.c_void_p, _dp, _dp], C.c_int),
         "evslx_set_spmv_kernel": ([C.c_int], C.c_int),
+        "evslx_kpm_dots": ([C.c_int, C.c_int, _dp, C.c_void_p, _dp], C.c_int),
+        "evslx_kpm_accumulate": ([C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp], C.c_int),
+        "evslx_rand_device_draws": ([C.c_int, C.c_int, C.c_uint64, C.c_void_p], C.c_int),
         "evslx_get_spmv_kernel": ([], C.c_int),
         "evslx_matvec": ([C.c_void_p, C.c_void_p], C.c_int),
         "evslx_problem_info": ([_ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
@@ -302,6 +319,19 @@ class Library:
         self._check(self.lib.evslx_kpmdos_probes(Mdeg, damping, probes.shape[0], _d(iv), dp.ptr, _d(mu),
                                                  C.byref(ec)), "evslx_kpmdos_probes")
         return mu, ec.value
+
+    def kpm_dots(self, Mdeg, intv, dprobes, nvec):
+        """Raw KPM dot products (Mdeg x nvec) for device probes (DeviceBuffer)."""
+        dots = np.zeros((Mdeg, nvec))
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        self._check(self.lib.evslx_kpm_dots(Mdeg, nvec, _d(iv), dprobes.ptr, _d(dots)), "evslx_kpm_dots")
+        return dots
+
+    def draw_probes(self, n, first, count):
+        """Device probes for draws first .. first+count-1 of the generator."""
+        buf = DeviceBuffer(self.lib, 8 * n * count)
+        self._check(self.lib.evslx_rand_device_draws(n, count, first, buf.ptr), "evslx_rand_device_draws")
+        return buf
 
     def spslicer(self, mu, intv, n_int, npts):
         sli = np.zeros(n_int + 1)

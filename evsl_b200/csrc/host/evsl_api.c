@@ -541,3 +541,12 @@ int evslx_matrix_storage(int *value_bytes, int *index_bytes) {
 }
 
 int evslx_set_filter_block(int threads) { return from_cu(evslcu_set_filter_block(threads)); }
+
+int evslx_rand_device_draws(int n, int count, uint64_t first_draw, double *v) {
+  int rc = evsl_require_started();
+  if (rc) return rc;
+  if (n < 1 || count < 1 || !v) return evsl_seterr(EVSLX_ERR_ARG, "rand draws: bad arguments");
+  rc = evslcu_rand_pm1(n, count, evslh.seed, first_draw, v);
+  if (!rc) rc = evslcu_sync();
+  return from_cu(rc);
+}

@@ -14,33 +14,55 @@
  */
 #include "internal.h"
 
-static int kpm_run(int Mdeg, int damping, int nvec, double *intv, const double *probes, double *mu, double *ecnt) {
-  int rc = evsl_require_operator();
-  if (rc) return rc;
+/* Accumulation of the moments and the eigenvalue count from the raw dot
+ * products dots[k*nvec + m] = (T_{k+1}(A~) v_m) . v_m, in the reference's
+ * order (probe-major, then degree; SRC/spslice.c:76-136).  Host only. */
+int evslx_kpm_accumulate(int Mdeg, int damping, int nvec, int n, double *intv, const double *dots, double *mu,
+                         double *ecnt) {
   if (evsl_check_intv(intv, stdout) < 0) return -1;
-  if (Mdeg < 1 || nvec < 1) return evsl_seterr(EVSLX_ERR_ARG, "kpmdos: Mdeg and nvec must be positive");
-  const int n = evsl_op()->n;
+  if (Mdeg < 1 || nvec < 1 || n < 1 || !dots || !mu || !ecnt)
+    return evsl_seterr(EVSLX_ERR_ARG, "kpm accumulate: bad arguments");
   const double aa = evsl_max(intv[0], intv[2]), bb = evsl_min(intv[1], intv[3]);
-  if (intv[0] < intv[2] || intv[1] > intv[3])
-    fprintf(stdout, " warning [%s (%d)]: interval (%e, %e) is adjusted to (%e, %e)\n", __FILE__, __LINE__, intv[0],
-            intv[1], aa, bb);
   const double ctr = (intv[3] + intv[2]) / 2.0, wid = (intv[3] - intv[2]) / 2.0;
   double t = evsl_max(-1.0 + DBL_EPSILON, (aa - ctr) / wid);
   const double beta1 = acos(t);
   t = evsl_min(1.0 - DBL_EPSILON, (bb - ctr) / wid);
   const double beta2 = acos(t);
   double *jac = (double *)malloc(sizeof(double) * ((size_t)Mdeg + 1));
-  double *dots = (double *)malloc(sizeof(double) * (size_t)Mdeg * (size_t)nvec);
-  if (!jac || !dots) {
-    free(jac);
-    free(dots);
-    return evsl_seterr(EVSLX_ERR_NOMEM, "kpmdos: out of memory");
-  }
+  if (!jac) return evsl_seterr(EVSLX_ERR_NOMEM, "kpmdos: out of memory");
   dampcf(Mdeg, damping, jac);
   jac[0] = 1.0;
-  evslcu_timer *tm = evslcu_timer_start();
-  /* the probes are processed 64 at a time (one block recurrence per group) */
+  memset(mu, 0, sizeof(double) * ((size_t)Mdeg + 1));
+  double tcnt = 0.0;
+  for (int m = 0; m < nvec; m++) {
+    mu[0] += jac[0];
+    tcnt -= jac[0] * (beta2 - beta1);
+    for (int k = 0; k < Mdeg; k++) {
+      const int k1 = k + 1;
+      const double tk = 2 * jac[k1] * dots[(size_t)k * nvec + m];
+      mu[k1] += tk;
+      tcnt -= tk * (sin(k1 * beta2) - sin(k1 * beta1)) / k1;
+    }
+  }
+  t = 1.0 / (((double)nvec) * EVSL_PI);
+  for (int k = 0; k <= Mdeg; k++) mu[k] = t * mu[k];
+  tcnt *= t * ((double)n);
+  *ecnt = tcnt;
+  free(jac);
+  return 0;
+}
+
+/* Raw KPM dot products for device probes (column-major n x nvec), computed
+ * 64 probes at a time as block recurrences. dots: host, Mdeg x nvec. */
+int evslx_kpm_dots(int Mdeg, int nvec, double *intv, const double *probes, double *dots) {
+  int rc = evsl_require_operator();
+  if (rc) return rc;
+  if (evsl_check_intv(intv, stdout) < 0) return -1;
+  if (Mdeg < 1 || nvec < 1 || !probes || !dots) return evsl_seterr(EVSLX_ERR_ARG, "kpm dots: bad arguments");
+  const int n = evsl_op()->n;
+  const double ctr = (intv[3] + intv[2]) / 2.0, wid = (intv[3] - intv[2]) / 2.0;
   const int group = 64;
+  evslcu_timer *tm = evslcu_timer_start();
   for (int g0 = 0; g0 < nvec && !rc; g0 += group) {
     const int cnt = evsl_min(group, nvec - g0);
     double *gd = (double *)malloc(sizeof(double) * (size_t)Mdeg * cnt);
@@ -55,25 +77,22 @@ static int kpm_run(int Mdeg, int damping, int nvec, double *intv, const double *
     free(gd);
   }
   evslh.last_kpm_seconds = evslcu_timer_stop(tm);
-  if (!rc) {
-    memset(mu, 0, sizeof(double) * ((size_t)Mdeg + 1));
-    double tcnt = 0.0;
-    for (int m = 0; m < nvec; m++) {
-      mu[0] += jac[0];
-      tcnt -= jac[0] * (beta2 - beta1);
-      for (int k = 0; k < Mdeg; k++) {
-        const int k1 = k + 1;
-        const double tk = 2 * jac[k1] * dots[(size_t)k * nvec + m];
-        mu[k1] += tk;
-        tcnt -= tk * (sin(k1 * beta2) - sin(k1 * beta1)) / k1;
-      }
-    }
-    t = 1.0 / (((double)nvec) * EVSL_PI);
-    for (int k = 0; k <= Mdeg; k++) mu[k] = t * mu[k];
-    tcnt *= t * ((double)n);
-    *ecnt = tcnt;
-  }
-  free(jac);
+  return rc;
+}
+
+static int kpm_run(int Mdeg, int damping, int nvec, double *intv, const double *probes, double *mu, double *ecnt) {
+  int rc = evsl_require_operator();
+  if (rc) return rc;
+  if (evsl_check_intv(intv, stdout) < 0) return -1;
+  if (Mdeg < 1 || nvec < 1) return evsl_seterr(EVSLX_ERR_ARG, "kpmdos: Mdeg and nvec must be positive");
+  const int n = evsl_op()->n;
+  if (intv[0] < intv[2] || intv[1] > intv[3])
+    fprintf(stdout, " warning [%s (%d)]: interval (%e, %e) is adjusted to (%e, %e)\n", __FILE__, __LINE__, intv[0],
+            intv[1], evsl_max(intv[0], intv[2]), evsl_min(intv[1], intv[3]));
+  double *dots = (double *)malloc(sizeof(double) * (size_t)Mdeg * (size_t)nvec);
+  if (!dots) return evsl_seterr(EVSLX_ERR_NOMEM, "kpmdos: out of memory");
+  rc = evslx_kpm_dots(Mdeg, nvec, intv, probes, dots);
+  if (!rc) rc = evslx_kpm_accumulate(Mdeg, damping, nvec, n, intv, dots, mu, ecnt);
   free(dots);
   return rc;
 }

@@ -69,6 +69,23 @@ int evslx_kpmdos_probes(int Mdeg, int damping, int nvec, double *intv, const dou
 int evslx_kpmdos_probes_noalloc(int Mdeg, int damping, int nvec, double *intv, const double *probes,
                                 double *mu, double *ecnt);
 
+/* The two halves of kpmdos, for callers that distribute the probes (e.g.
+ * one shard of probes per GPU): evslx_kpm_dots returns the raw products
+ * dots[k*nvec + m] = (T_{k+1}(A~) v_m) . v_m of the normalised device probes
+ * (column-major n x nvec); evslx_kpm_accumulate (host only, no GPU needed)
+ * turns the dots of all nvec probes into mu[0..Mdeg] and the eigenvalue
+ * count exactly as kpmdos does (SRC/spslice.c:76-136).  Each probe's dots do
+ * not depend on which other probes share its block, so gathering shards and
+ * accumulating gives bit for bit the single-call result. */
+int evslx_kpm_dots(int Mdeg, int nvec, double *intv, const double *probes, double *dots);
+int evslx_kpm_accumulate(int Mdeg, int damping, int nvec, int n, double *intv, const double *dots, double *mu,
+                         double *ecnt);
+
+/* Device vectors for explicit draws first_draw .. first_draw+count-1 of the
+ * library generator (the draws kpmdos would consume), without advancing the
+ * draw counter; v is column-major n x count. */
+int evslx_rand_device_draws(int n, int count, uint64_t first_draw, double *v);
+
 /* Filter SpMV kernel for the registered matrix: 0 = SELL-32 (default),
  * 1 = CSR one thread per row.  Both give identical (bitwise) results. */
 int evslx_set_spmv_kernel(int which);

@@ -771,3 +771,26 @@ def library_uniform(seed, draw, n):
                + np.arange(n, dtype=np.uint64))
         u = (_mix64(key) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
     return 2.0 * u - 1.0
+
+
+def kpm_raw_dots(Mdeg, probes, intv, ia, ja, a):
+    """Raw KPM products dots[k, m] = (T_{k+1}(A~) v_m) . v_m of the normalised
+    probes (the quantities kpmdos accumulates, SRC/spslice.c:101-125)."""
+    lmin, lmax = intv[2], intv[3]
+    ctr = (lmax + lmin) / 2.0
+    wid = (lmax - lmin) / 2.0
+    probes = np.atleast_2d(probes)
+    out = np.zeros((Mdeg, probes.shape[0]))
+    for m, p in enumerate(probes):
+        v = p * (1.0 / np.linalg.norm(p))
+        vk = v.copy()
+        vkm1 = np.zeros_like(v)
+        for k in range(Mdeg):
+            vkp1 = csr_matvec(ia, ja, a, vk)
+            scal = (1.0 if k == 0 else 2.0) / wid
+            vkp1 = vkp1 + (-ctr) * vk
+            vkp1 = scal * vkp1
+            vkp1 = vkp1 + (-1.0) * vkm1
+            vkm1, vk = vk, vkp1
+            out[k, m] = float(np.dot(vk, v))
+    return out

@@ -108,6 +108,26 @@ def test_kpmdos_many_probes_and_device_rng(gpu_lib):
     assert abs(ec - ec_ref) <= 1e-10 * abs(ec_ref)
 
 
+def test_kpm_shards_are_bitwise_the_full_block(gpu_lib):
+    """Per-probe dot products do not depend on the other probes of the block,
+    so sharding probes over GPUs and accumulating reproduces kpmdos exactly."""
+    import evsl_b200
+
+    ia, ja, a = _lap(gpu_lib, 14, 12, 5)
+    n = len(ia) - 1
+    iv = [0.7, 2.9, 0.0, 12.0]
+    gpu_lib.set_seed(99)
+    mu_ref, ec_ref = gpu_lib.kpmdos(40, 1, 20, iv)
+    full = gpu_lib.draw_probes(n, 0, 20)
+    assert np.array_equal(full.to_host(shape=(20, n))[3], O.library_uniform(99, 3, n))
+    dots = gpu_lib.kpm_dots(40, iv, full, 20)
+    for a0, b0 in ((0, 7), (7, 13), (13, 20)):
+        part = gpu_lib.draw_probes(n, a0, b0 - a0)
+        assert np.array_equal(gpu_lib.kpm_dots(40, iv, part, b0 - a0), dots[:, a0:b0])
+    mu, ec = evsl_b200.kpm_accumulate(40, 1, n, iv, dots)
+    assert np.array_equal(mu, mu_ref) and ec == ec_ref
+
+
 def test_cheblan_nr_small_matches_reference(gpu_lib, golden):
     _lap(gpu_lib, 20, 20, 1)
     pol = gpu_lib.find_pol([0.6, 1.2, 0.0, 8.0])
