@@ -152,6 +152,7 @@ def load():
         "evslx_last_solve_info": ([_ip, _ip], C.c_int),
         "evslx_set_filter_persistent": ([C.c_int], C.c_int),
         "evslx_set_filter_block": ([C.c_int], C.c_int),
+        "evslx_set_filter_rows_per_thread": ([C.c_int], C.c_int),
         "evslx_set_matrix_compression": ([C.c_int], C.c_int),
         "evslx_matrix_storage": ([_ip, _ip], C.c_int),
     }

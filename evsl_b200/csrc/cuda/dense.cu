@@ -83,15 +83,27 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// h[j] = alpha * sum_chunks part[chunk*k + j] (+ beta * h[j] when beta != 0)
-__global__ void k_gemvT_reduce(int nchunks, int k, const double *part, double alpha, double beta, double *h,
-                               const double *state) {
+// h[j] = alpha * sum_chunks part[chunk*k + j] (+ beta * h[j] when beta != 0).
+// Block of 256 threads = 8 warps per 32 columns: lane = column, warp w sums
+// chunks w, w+8, ...; the 8 warp sums are added in warp order (fixed order).
+__global__ void __launch_bounds__(256)
+    k_gemvT_reduce(int nchunks, int k, const double *part, double alpha, double beta, double *h,
+                   const double *state) {
   if (state && state[2] != 0.0) return;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= k) return;
+  __shared__ double sh[8][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j = blockIdx.x * 32 + lane;
   double s = 0.0;
-  for (int c = 0; c < nchunks; ++c) s += part[(long long)c * k + j];
-  h[j] = (beta == 0.0) ? alpha * s : __dadd_rn(__dmul_rn(beta, h[j]), alpha * s);
+  if (j < k)
+    for (int c = warp; c < nchunks; c += 8) s += part[(long long)c * k + j];
+  sh[warp][lane] = s;
+  __syncthreads();
+  if (warp == 0 && j < k) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) t += sh[w][lane];
+    h[j] = (beta == 0.0) ? alpha * t : __dadd_rn(__dmul_rn(beta, h[j]), alpha * t);
+  }
 }
 
 // v[r] <- v[r] + sum_j (alpha*h[j]) * Q[r, j], summed over j in order as the
@@ -335,7 +347,7 @@ int evslcu_cgs_dgks(int n, int k, int imax, const double *Q, long long ldq, doub
   for (int pass = 0; pass < imax; ++pass) {
     k_gemvT_partial<<<gT, kThreads, 0, st>>>(n, k, Q, ldq, v, part, state);
     EVSLCU_LAUNCH_CHECK("k_gemvT_partial");
-    k_gemvT_reduce<<<(k + 255) / 256, 256, 0, st>>>(nchunks, k, part, 1.0, 0.0, h, state);
+    k_gemvT_reduce<<<(k + 31) / 32, 256, 0, st>>>(nchunks, k, part, 1.0, 0.0, h, state);
     EVSLCU_LAUNCH_CHECK("k_gemvT_reduce");
     k_gemvN<<<gN, kThreads, 0, st>>>(n, k, Q, ldq, h, -1.0, v, partials(), counters() + CTR_CGS, state);
     EVSLCU_LAUNCH_CHECK("k_gemvN");
@@ -362,7 +374,7 @@ int evslcu_dgemv(char trans, int m, int n, double alpha, const double *A, long l
     count_launch();
     int rc = check_launch("k_gemvT_partial");
     if (!rc) {
-      k_gemvT_reduce<<<(n + 255) / 256, 256, 0, st>>>(nchunks, n, part, alpha, beta, y, nullptr);
+      k_gemvT_reduce<<<(n + 31) / 32, 256, 0, st>>>(nchunks, n, part, alpha, beta, y, nullptr);
       count_launch();
       rc = check_launch("k_gemvT_reduce");
     }

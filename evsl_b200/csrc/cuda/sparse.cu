@@ -71,6 +71,53 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Two rows per thread (SELL-32 only): thread (warp w, lane l) handles rows
+// 64*w' + l and 64*w' + 32 + l of chunk pair w'.  Same arithmetic per row.
+template <class VT, class IT, bool FIRST, bool EPI>
+__global__ void __launch_bounds__(kThreads)
+    k_cheb2(SellT<VT, IT> A, const double *__restrict__ vk, const double *vkm1, double *out, double *__restrict__ y,
+            double t, double ncc, double s, double mu0, const double *__restrict__ zold, double nbeta,
+            const double *__restrict__ dotv, double *part, unsigned int *ctr, double *dot_out) {
+  __shared__ double sh[kThreads / 32];
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  double dsum = 0.0;
+  const int lane = threadIdx.x & 31;
+  const int nwt = gridDim.x * (kThreads / 32);
+  const int npairs = (A.n + 63) / 64;
+  for (int pr = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); pr < npairs; pr += nwt) {
+    const int r0 = pr * 64 + lane;
+    const bool has1 = (pr * 64 + 32) < A.n;
+    double acc[2];
+    row_dot2<false>(A, r0, has1, vk, acc[0], acc[1]);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = r0 + 32 * h;
+      if (r < A.n) {
+        const double x = vk[r];
+        double w = __dmul_rn(t, __dadd_rn(acc[h], __dmul_rn(ncc, x)));
+        if (!FIRST) w = __dadd_rn(w, -vkm1[r]);
+        out[r] = w;
+        double yv = FIRST ? __dmul_rn(mu0, x) : y[r];
+        yv = __dadd_rn(yv, __dmul_rn(s, w));
+        if (EPI) {
+          if (zold) yv = __dadd_rn(yv, __dmul_rn(nbeta, zold[r]));
+          if (dotv) dsum += dotv[r] * yv;
+        }
+        y[r] = yv;
+      }
+    }
+  }
+  if (EPI && dot_out) {
+    double b = block_sum(dsum, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = b;
+    if (last_block(ctr)) {
+      double tot = reduce_partials(part, gridDim.x, ctr, sh);
+      if (threadIdx.x == 0) *dot_out = tot;
+    }
+  }
+}
+
 // Stand-alone update for a user matvec (SRC/evsl_cuda.cu:175-184 semantics,
 // CPU-build operation order).
 __global__ void k_cheb_update(int n, int k, double t, double s, double ncc, double *vkp1, const double *vk,
@@ -109,6 +156,32 @@ __global__ void k_lan_epi(int n, const double *zold, double nbeta, const double 
 }
 
 
+int g_rows_per_thread = 1;
+
+template <class F, class M>
+int launch_pdl(F fn, int grid, M view, const double *vk, const double *vkm1, double *out, double *y, double t,
+               double ncc, double s, double mu0, const double *zold, double nbeta, const double *dotv, double *dout) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, fn, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv, partials(),
+                                     counters() + CTR_CHEB, dout);
+  if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "filter kernel launch failed: %s", cudaGetErrorString(e));
+  EVSLCU_LAUNCH_CHECK("k_cheb");
+  return 0;
+}
+
+template <class VT, class IT>
+int launch_cheb_step(const SellT<VT, IT> &view, int n, bool first, bool epi, const double *vk, const double *vkm1,
+                     double *out, double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep);
+
 template <class M>
 int launch_cheb_step(const M &view, int n, bool first, bool epi, const double *vk, const double *vkm1, double *out,
                      double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep) {
@@ -146,9 +219,52 @@ int launch_cheb_step(const M &view, int n, bool first, bool epi, const double *v
   return 0;
 }
 
+template <class VT, class IT>
+int launch_cheb_step(const SellT<VT, IT> &view, int n, bool first, bool epi, const double *vk, const double *vkm1,
+                     double *out, double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep) {
+  const double *zold = (epi && ep) ? ep->zold : nullptr;
+  const double nbeta = (epi && ep) ? ep->nbeta : 0.0;
+  const double *dotv = (epi && ep) ? ep->dotv : nullptr;
+  double *dout = (epi && ep) ? ep->dot_out : nullptr;
+  if (g_rows_per_thread == 2) {
+    const int grid = grid_for(((long long)n + 1) / 2);
+    using V = SellT<VT, IT>;
+    if (first && epi)
+      return launch_pdl(k_cheb2<VT, IT, true, true>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
+                        dout);
+    if (first)
+      return launch_pdl(k_cheb2<VT, IT, true, false>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
+                        dotv, dout);
+    if (epi)
+      return launch_pdl(k_cheb2<VT, IT, false, true>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
+                        dotv, dout);
+    (void)sizeof(V);
+    return launch_pdl(k_cheb2<VT, IT, false, false>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
+                      dout);
+  }
+  const int grid = grid_for(n);
+  if (first && epi)
+    return launch_pdl(k_cheb<SellT<VT, IT>, true, true>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
+                      dotv, dout);
+  if (first)
+    return launch_pdl(k_cheb<SellT<VT, IT>, true, false>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
+                      dotv, dout);
+  if (epi)
+    return launch_pdl(k_cheb<SellT<VT, IT>, false, true>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
+                      dotv, dout);
+  return launch_pdl(k_cheb<SellT<VT, IT>, false, false>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
+                    dotv, dout);
+}
+
 // ---------------------------------------------------------------------------
 // KPM block moments: warp per row, lane = probe; vectors interleaved [n][B].
 // ---------------------------------------------------------------------------
+constexpr int kKpmRows = 4;  // rows a warp works on at once (independent chains)
+
+inline int kpm_grid(int n) {
+  return (int)std::min<long long>(((long long)n + 8 * kKpmRows - 1) / (8 * kKpmRows), 4096);
+}
+
 template <int G, bool FIRST>
 __global__ void __launch_bounds__(kThreads)
     k_kpm(CsrView A, int B, const double *__restrict__ vk, const double *vkm1, double *out, double scal, double nctr,
@@ -159,29 +275,48 @@ __global__ void __launch_bounds__(kThreads)
   double dsum[G];
 #pragma unroll
   for (int g = 0; g < G; ++g) dsum[g] = 0.0;
-  for (int r = blockIdx.x * (kThreads / 32) + warp; r < A.n; r += nwarps_total) {
-    const int b = A.ia[r], e = A.ia[r + 1];
-    double acc[G];
+  for (int r0 = (blockIdx.x * (kThreads / 32) + warp) * kKpmRows; r0 < A.n; r0 += nwarps_total * kKpmRows) {
+    int b[kKpmRows], len[kKpmRows], maxlen = 0;
 #pragma unroll
-    for (int g = 0; g < G; ++g) acc[g] = 0.0;
-    for (int j = b; j < e; ++j) {
-      const double aj = __ldg(A.a + j);
-      const long long cj = (long long)__ldg(A.ja + j) * B;
+    for (int i = 0; i < kKpmRows; ++i) {
+      const int r = r0 + i;
+      b[i] = (r < A.n) ? A.ia[r] : 0;
+      len[i] = (r < A.n) ? A.ia[r + 1] - b[i] : 0;
+      maxlen = max(maxlen, len[i]);
+    }
+    double acc[kKpmRows][G];
 #pragma unroll
-      for (int g = 0; g < G; ++g) {
-        const int p = lane + 32 * g;
-        if (p < B) acc[g] = __dadd_rn(acc[g], __dmul_rn(aj, __ldg(vk + cj + p)));
+    for (int i = 0; i < kKpmRows; ++i)
+#pragma unroll
+      for (int g = 0; g < G; ++g) acc[i][g] = 0.0;
+    for (int j = 0; j < maxlen; ++j) {
+#pragma unroll
+      for (int i = 0; i < kKpmRows; ++i) {
+        if (j < len[i]) {
+          const double aj = __ldg(A.a + b[i] + j);
+          const long long cj = (long long)__ldg(A.ja + b[i] + j) * B;
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            const int p = lane + 32 * g;
+            if (p < B) acc[i][g] = __dadd_rn(acc[i][g], __dmul_rn(aj, __ldg(vk + cj + p)));
+          }
+        }
       }
     }
 #pragma unroll
-    for (int g = 0; g < G; ++g) {
-      const int p = lane + 32 * g;
-      if (p < B) {
-        const long long idx = (long long)r * B + p;
-        double w = __dmul_rn(scal, __dadd_rn(acc[g], __dmul_rn(nctr, vk[idx])));
-        if (!FIRST) w = __dadd_rn(w, -vkm1[idx]);
-        out[idx] = w;
-        dsum[g] += w * v0[idx];
+    for (int i = 0; i < kKpmRows; ++i) {
+      const int r = r0 + i;
+      if (r >= A.n) continue;
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const int p = lane + 32 * g;
+        if (p < B) {
+          const long long idx = (long long)r * B + p;
+          double w = __dmul_rn(scal, __dadd_rn(acc[i][g], __dmul_rn(nctr, vk[idx])));
+          if (!FIRST) w = __dadd_rn(w, -vkm1[idx]);
+          out[idx] = w;
+          dsum[g] += w * v0[idx];
+        }
       }
     }
   }
@@ -196,7 +331,7 @@ __global__ void __launch_bounds__(kThreads)
   if (last_block(ctr)) {
     for (int p = threadIdx.x; p < B; p += blockDim.x) {
       double s = 0.0;
-      for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(part + (long long)b * B + p);
+      for (int b2 = 0; b2 < (int)gridDim.x; ++b2) s += __ldcg(part + (long long)b2 * B + p);
       dots_row[p] = s;
     }
     __syncthreads();
@@ -576,8 +711,7 @@ int evslcu_kpm_dots(const evslcu_op *op, int n, int Mdeg, int nvec, const double
   double *buf = (double *)evslcu_malloc(sizeof(double) * blk * 3);
   double *ddots = (double *)evslcu_malloc(sizeof(double) * (size_t)Mdeg * B);
   double *nrm = (double *)evslcu_malloc(sizeof(double) * B);
-  const int rows_per_block = kThreads / 32;
-  int grid = (int)std::min<long long>(((long long)n + rows_per_block - 1) / rows_per_block, 4096);
+  int grid = kpm_grid(n);
   double *part = (double *)evslcu_malloc(sizeof(double) * (size_t)std::max(grid * B, 512 * B));
   if (!buf || !ddots || !nrm || !part) {
     evslcu_free(buf);
@@ -653,7 +787,7 @@ int evslcu_randn(int n, uint64_t seed, uint64_t draw, double *v) {
 size_t evslcu_kpm_noalloc_capacity(void) { return kNoAllocDoubles; }
 
 size_t evslcu_kpm_noalloc_need(int n, int Mdeg, int nvec) {
-  const int G = (int)std::min<long long>(((long long)n + 7) / 8, 4096);
+  const int G = kpm_grid(n);
   const int gx = std::min(grid_for(n), 512);
   return 64 + (size_t)nvec /* norms */ + (size_t)(Mdeg + 1) /* jac */ + (size_t)Mdeg /* sdiff */ +
          (size_t)Mdeg * nvec /* dots */ + (size_t)std::max(G, gx) * nvec /* partials */ + (size_t)(Mdeg + 2) /* out */ +
@@ -686,7 +820,7 @@ int evslcu_kpm_noalloc(const evslcu_op *op, int n, int Mdeg, int nvec, const dou
   double *base = g_noalloc_ptr[dev];
   unsigned int *ctrs = (unsigned int *)base;  // first 64 doubles: counters
   const int B = nvec;
-  const int G = (int)std::min<long long>(((long long)n + 7) / 8, 4096);
+  const int G = kpm_grid(n);
   const int gx = std::min(grid_for(n), 512);
   double *nrm = base + 64;
   double *jac = nrm + B;
@@ -738,6 +872,12 @@ int evslcu_kpm_noalloc(const evslcu_op *op, int n, int Mdeg, int nvec, const dou
   EVSLCU_LAUNCH_CHECK("k_kpm_accumulate");
   if ((rc = evslcu_d2h(mu_h, out, sizeof(double) * (Mdeg + 1)))) return rc;
   return evslcu_d2h(ecnt_h, out + Mdeg + 1, sizeof(double));
+}
+
+int evslcu_set_rows_per_thread(int r) {
+  if (r != 1 && r != 2) return fail(EVSLCU_ERR_ARG, "rows per thread must be 1 or 2");
+  g_rows_per_thread = r;
+  return 0;
 }
 
 }  // extern "C"

@@ -75,6 +75,37 @@ __device__ __forceinline__ double row_dot(const SellT<VT, IT> &A, int r, const d
   return acc;
 }
 
+// Rows r0 and r1 = r0 + 32 (same lane of chunks c and c+1) with their loads
+// interleaved: two independent dependency chains per thread.  Each row is
+// still summed left to right, so results equal row_dot's.
+template <bool COHERENT, class VT, class IT>
+__device__ __forceinline__ void row_dot2(const SellT<VT, IT> &A, int r0, bool has1, const double *x, double &acc0,
+                                         double &acc1) {
+  const int c0 = r0 >> 5;
+  const int lane = r0 & 31;
+  long long p0 = A.cptr[c0] + lane;
+  const int w0 = A.cw[c0];
+  long long p1 = has1 ? A.cptr[c0 + 1] + lane : 0;
+  const int w1 = has1 ? A.cw[c0 + 1] : 0;
+  const int r1 = r0 + 32;
+  acc0 = 0.0;
+  acc1 = 0.0;
+  const int wm = w0 > w1 ? w0 : w1;
+#pragma unroll 4
+  for (int j = 0; j < wm; ++j, p0 += 32, p1 += 32) {
+    if (j < w0) {
+      const double v = (double)__ldg(A.val + p0);
+      const int col = decode_col(__ldg(A.col + p0), r0);
+      acc0 = __dadd_rn(acc0, __dmul_rn(v, ldx<COHERENT>(x + col)));
+    }
+    if (j < w1) {
+      const double v = (double)__ldg(A.val + p1);
+      const int col = decode_col(__ldg(A.col + p1), r1);
+      acc1 = __dadd_rn(acc1, __dmul_rn(v, ldx<COHERENT>(x + col)));
+    }
+  }
+}
+
 template <bool COHERENT>
 __device__ __forceinline__ double row_dot(const CsrView &A, int r, const double *x) {
   const int b = A.ia[r], e = A.ia[r + 1];

@@ -187,6 +187,8 @@ int evslcu_mat_storage(const evslcu_mat *A, int *vfmt, int *ifmt);
 /* Threads per block of the single-launch filter (256, 512, 1024; default
  * 1024: fewer blocks meet at each grid barrier). */
 int evslcu_set_filter_block(int threads);
+/* Rows per thread of the per-degree SELL-32 filter kernel (1 or 2, default 1). */
+int evslcu_set_rows_per_thread(int r);
 /* Allow (1, default) or forbid (0) the single-launch filter kernel. */
 int evslcu_mat_set_persistent(evslcu_mat *A, int on);
 

@@ -196,8 +196,10 @@ int ChebLanTr(int lanm, int nev, double *intv, int maxit, double tol, double *vi
       T[(k - 1) * lanm1_l + k] = beta;
       const int k1 = k - trlen - Ntest;
       if (((k1 >= 0) && (k1 % TR_CYCLE == 0)) || (k == lanm) || it == maxit) {
+        /* eigenvalues only at a test; the wanted eigenvectors are formed
+         * below once the inner loop stops */
         const double te = evsl_timer();
-        rc = evsl_sym_eig(k, T, lanm1, EvecT, lanm1, Rval);
+        rc = evsl_tr_eig(k, trlen, T, lanm1, 0.0, Rval, NULL, 0);
         evslstat.t_eig += evsl_timer() - te;
         if (rc) goto done;
         if (k == lanm || it == maxit) break;
@@ -221,6 +223,13 @@ int ChebLanTr(int lanm, int nev, double *intv, int maxit, double tol, double *vi
         last_tr = tr;
         last_jl = jl;
       }
+    }
+    /* eigenvectors of T for the Ritz values that pass 1 keeps */
+    {
+      const double te = evsl_timer();
+      rc = evsl_tr_eig(k, trlen, T, lanm1, bar - 2 * EVSL_DBL_EPS_MULT * DBL_EPSILON, Rval, EvecT, lanm1);
+      evslstat.t_eig += evsl_timer() - te;
+      if (rc) goto done;
     }
     /* pass 1: Ritz values above bar, their vectors moved to the front */
     jl = 0;

@@ -550,3 +550,5 @@ int evslx_rand_device_draws(int n, int count, uint64_t first_draw, double *v) {
   if (!rc) rc = evslcu_sync();
   return from_cu(rc);
 }
+
+int evslx_set_filter_rows_per_thread(int r) { return from_cu(evslcu_set_rows_per_thread(r)); }

@@ -50,6 +50,7 @@ int evsl_check_intv(const double *intv, FILE *fstats);
 int evsl_trid_eigvals(int n, const double *d, const double *e, double *w);
 int evsl_trid_eigvecs(int n, const double *d, const double *e, int m, const double *w, double *Z, int ldz);
 int evsl_sym_eig(int n, const double *A, int lda, double *Q, int ldq, double *w);
+int evsl_tr_eig(int k, int m, const double *T, int ldt, double thresh, double *w, double *Z, int ldz);
 
 /* device random vectors drawn from the library stream */
 int evsl_rand_device(int n, int count, double *v);

@@ -16,6 +16,13 @@
  *                      re-orthogonalisation inside clusters of close
  *                      eigenvalues (Peters & Wilkinson 1971; the approach
  *                      of LAPACK's dstein), O(n) per vector and iteration.
+ *   evsl_tr_eig        the thick-restart matrix (diagonal block + spike row
+ *                      + tridiagonal tail): the leading block is reduced to
+ *                      tridiagonal form by a Lanczos run on the diagonal
+ *                      block started from the spike (full
+ *                      reorthogonalisation), which leaves the whole matrix
+ *                      tridiagonal; then QL for all eigenvalues and inverse
+ *                      iteration for the wanted vectors only.
  *   evsl_sym_eig       dense symmetric eigenproblem: Householder
  *                      tridiagonalisation, then implicit QL with rotations
  *                      accumulated (eigenvalues ascending, vectors in Q).
@@ -337,4 +344,143 @@ int evsl_sym_eig(int n, const double *A, int lda, double *Q, int ldq, double *w)
   free(V);
   if (rc) return evsl_seterr(EVSLX_ERR_NUMERIC, "dense symmetric QL did not converge");
   return 0;
+}
+
+/* Thick-restart projected matrix T (k x k, column-major, ld ldt):
+ *   T[i,i] = theta_i for i < m (m = trlen), T[m,i] = T[i,m] = s_i for i < m,
+ *   tridiagonal from index m on.
+ * All eigenvalues go to w (ascending).  When Z is not NULL, the eigenvector
+ * of every w[i] >= thresh is written to column i of Z (ld ldz).
+ * Method: orthogonal Q (m x m) with Q^T D Q tridiagonal and Q^T s = |s| e_{m-1}
+ * from a Lanczos run on D = diag(theta) started at s/|s| (vectors placed in
+ * reverse order), so diag(Q, I)^T T diag(Q, I) is tridiagonal. */
+int evsl_tr_eig(int k, int m, const double *T, int ldt, double thresh, double *w, double *Z, int ldz) {
+  if (k <= 0) return 0;
+  double *d = (double *)malloc(sizeof(double) * (size_t)k);
+  double *e = (double *)calloc((size_t)k, sizeof(double));
+  double *Q = NULL;
+  if (!d || !e) {
+    free(d);
+    free(e);
+    return evsl_seterr(EVSLX_ERR_NOMEM, "thick-restart eigensolver: out of memory");
+  }
+  for (int i = 0; i < k; i++) d[i] = T[(size_t)i * ldt + i];
+  for (int i = (m > 0 ? m : 0); i < k - 1; i++) e[i] = T[(size_t)i * ldt + i + 1];
+  if (m > 0) {
+    Q = (double *)calloc((size_t)m * m, sizeof(double));
+    double *r = (double *)malloc(sizeof(double) * (size_t)m);
+    if (!Q || !r) {
+      free(d);
+      free(e);
+      free(Q);
+      free(r);
+      return evsl_seterr(EVSLX_ERR_NOMEM, "thick-restart eigensolver: out of memory");
+    }
+    double dmax = 0.0, sig = 0.0;
+    for (int i = 0; i < m; i++) {
+      dmax = evsl_max(dmax, fabs(T[(size_t)i * ldt + i]));
+      const double si = T[(size_t)i * ldt + m];
+      sig += si * si;
+    }
+    sig = sqrt(sig);
+    const double tiny = 1e3 * DBL_EPSILON * evsl_max(dmax, 1.0);
+    /* start vector */
+    if (sig > 0.0) {
+      for (int i = 0; i < m; i++) r[i] = T[(size_t)i * ldt + m] / sig;
+    } else {
+      for (int i = 0; i < m; i++) r[i] = (i == m - 1) ? 1.0 : 0.0;
+    }
+    double bprev = 0.0;
+    for (int j = 0; j < m; j++) {
+      const int t = m - 1 - j; /* placement of Lanczos vector j */
+      double *q = Q + (size_t)t * m;
+      memcpy(q, r, sizeof(double) * (size_t)m);
+      double a = 0.0;
+      for (int i = 0; i < m; i++) a += q[i] * T[(size_t)i * ldt + i] * q[i];
+      d[t] = a;
+      if (j == m - 1) break;
+      /* r = D q - a q - bprev q_prev, then full reorthogonalisation (twice) */
+      for (int i = 0; i < m; i++) r[i] = T[(size_t)i * ldt + i] * q[i] - a * q[i];
+      if (j > 0) {
+        const double *qp = Q + (size_t)(t + 1) * m;
+        for (int i = 0; i < m; i++) r[i] -= bprev * qp[i];
+      }
+      for (int pass = 0; pass < 2; pass++)
+        for (int jj = 0; jj <= j; jj++) {
+          const double *qq = Q + (size_t)(m - 1 - jj) * m;
+          double dot = 0.0;
+          for (int i = 0; i < m; i++) dot += qq[i] * r[i];
+          for (int i = 0; i < m; i++) r[i] -= dot * qq[i];
+        }
+      double b = 0.0;
+      for (int i = 0; i < m; i++) b += r[i] * r[i];
+      b = sqrt(b);
+      if (b <= tiny) {
+        /* invariant subspace found: continue with a unit vector orthogonal to
+         * the previous ones; the coupling is exactly zero */
+        b = 0.0;
+        int found = 0;
+        for (int cand = 0; cand < m && !found; cand++) {
+          for (int i = 0; i < m; i++) r[i] = (i == cand) ? 1.0 : 0.0;
+          for (int pass = 0; pass < 2; pass++)
+            for (int jj = 0; jj <= j; jj++) {
+              const double *qq = Q + (size_t)(m - 1 - jj) * m;
+              double dot = 0.0;
+              for (int i = 0; i < m; i++) dot += qq[i] * r[i];
+              for (int i = 0; i < m; i++) r[i] -= dot * qq[i];
+            }
+          double nr = 0.0;
+          for (int i = 0; i < m; i++) nr += r[i] * r[i];
+          nr = sqrt(nr);
+          if (nr > 0.5) {
+            for (int i = 0; i < m; i++) r[i] /= nr;
+            found = 1;
+          }
+        }
+      } else {
+        for (int i = 0; i < m; i++) r[i] /= b;
+      }
+      e[t - 1] = b; /* coupling between positions t-1 and t */
+      bprev = b;
+    }
+    e[m - 1] = sig; /* Q^T s = sig e_{m-1} couples position m-1 to the head m */
+    free(r);
+  }
+  int rc = evsl_trid_eigvals(k, d, e, w);
+  if (!rc && Z) {
+    int msel = 0;
+    for (int i = 0; i < k; i++)
+      if (w[i] >= thresh) msel++;
+    if (msel > 0) {
+      double *ws = (double *)malloc(sizeof(double) * (size_t)msel);
+      double *Y = (double *)malloc(sizeof(double) * (size_t)k * msel);
+      if (!ws || !Y) {
+        rc = evsl_seterr(EVSLX_ERR_NOMEM, "thick-restart eigensolver: out of memory");
+      } else {
+        int j = 0;
+        for (int i = 0; i < k; i++)
+          if (w[i] >= thresh) ws[j++] = w[i];
+        rc = evsl_trid_eigvecs(k, d, e, msel, ws, Y, k);
+        j = 0;
+        for (int i = 0; !rc && i < k; i++) {
+          if (w[i] < thresh) continue;
+          const double *y = Y + (size_t)j * k;
+          double *z = Z + (size_t)i * ldz;
+          for (int r = 0; r < m; r++) {
+            double acc = 0.0;
+            for (int c = 0; c < m; c++) acc += Q[(size_t)c * m + r] * y[c];
+            z[r] = acc;
+          }
+          for (int r = m; r < k; r++) z[r] = y[r];
+          j++;
+        }
+      }
+      free(ws);
+      free(Y);
+    }
+  }
+  free(d);
+  free(e);
+  free(Q);
+  return rc;
 }

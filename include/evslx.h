@@ -97,6 +97,10 @@ int evslx_get_spmv_kernel(void);
  * cooperative kernel (bounded grid barriers between degrees, per-row state in
  * shared memory).  Results are identical bit for bit. */
 int evslx_set_filter_persistent(int on);
+/* Rows each thread of the per-degree filter kernel handles (1 or 2, default
+ * 1; 2 gives each thread two independent load chains, measured slower on
+ * the 3-D Laplacian).  Results are identical. */
+int evslx_set_filter_rows_per_thread(int r);
 /* Threads per block of the single-launch filter: 256, 512 or 1024 (default). */
 int evslx_set_filter_block(int threads);
 
