@@ -122,6 +122,11 @@ def load():
         "ChebLanTr": ([C.c_int, C.c_int, _dp, C.c_int, C.c_double, C.c_void_p, C.POINTER(PolParams), _ip,
                        C.POINTER(_dp), C.POINTER(C.c_void_p), C.POINTER(_dp), C.c_void_p], C.c_int),
         "kpmdos": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp], C.c_int),
+        "LanBounds": ([C.c_int, C.c_void_p, _dp, _dp], C.c_int),
+        "evslx_chebav_block": ([C.POINTER(PolParams), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+        "ChebSI": ([C.c_int, _dp, C.c_int, C.c_double, C.c_void_p, C.POINTER(PolParams), _ip, C.POINTER(_dp),
+                    C.POINTER(C.c_void_p), C.POINTER(_dp), C.c_void_p], C.c_int),
+        "LanTrbounds": ([C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int, _dp, _dp, C.c_void_p], C.c_int),
         "spslicer": ([_dp, _dp, C.c_int, _dp, C.c_int, C.c_int], C.c_int),
         "dampcf": ([C.c_int, C.c_int, _dp], C.c_int),
         "_evsl_Malloc_device": ([C.c_size_t], C.c_void_p),
@@ -299,6 +304,31 @@ class Library:
         self._check(self.lib.ChebAv(C.byref(pol), dv.ptr, dy.ptr, dw.ptr), "ChebAv")
         return dy.to_host()
 
+    def chebav_block(self, pol, V):
+        """p(A) applied to the rows of V (ncols x n) with the block filter."""
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        dv = DeviceBuffer.from_host(self.lib, V)
+        dy = DeviceBuffer(self.lib, V.nbytes)
+        dw = DeviceBuffer(self.lib, 2 * V.nbytes)
+        self._check(self.lib.evslx_chebav_block(C.byref(pol), V.shape[0], dv.ptr, dy.ptr, dw.ptr),
+                    "evslx_chebav_block")
+        return dy.to_host().reshape(V.shape)
+
+    # -- spectrum bounds -----------------------------------------------------
+    def lan_bounds(self, msteps, v):
+        """LanBounds on a host start vector (copied to the device)."""
+        dv = DeviceBuffer.from_host(self.lib, np.asarray(v, dtype=np.float64))
+        lo, hi = C.c_double(), C.c_double()
+        self._check(self.lib.LanBounds(msteps, dv.ptr, C.byref(lo), C.byref(hi)), "LanBounds")
+        return lo.value, hi.value
+
+    def lan_trbounds(self, lanm, maxit, tol, v, bndtype=1):
+        dv = DeviceBuffer.from_host(self.lib, np.asarray(v, dtype=np.float64))
+        lo, hi = C.c_double(), C.c_double()
+        self._check(self.lib.LanTrbounds(lanm, maxit, tol, dv.ptr, bndtype, C.byref(lo), C.byref(hi), None),
+                    "LanTrbounds")
+        return lo.value, hi.value
+
     # -- DOS / slicing -----------------------------------------------------
     def set_seed(self, seed):
         self.lib.evslx_set_seed(seed)
@@ -381,6 +411,17 @@ class Library:
                                 C.byref(W), C.byref(res), None)
         self._check(rc, "ChebLanTr")
         return self._outputs(nev2.value, lam, W.value, res, want_vectors)
+
+    def cheb_si(self, nev, intv, maxit, tol, vinit_block, pol, want_vectors=True):
+        """ChebSI with a host start block (nev x n rows = columns of the n x nev block)."""
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        dv = DeviceBuffer.from_host(self.lib, np.ascontiguousarray(vinit_block, dtype=np.float64))
+        nevo = C.c_int()
+        lam, res = _dp(), _dp()
+        W = C.c_void_p()
+        self._check(self.lib.ChebSI(nev, _d(iv), maxit, tol, dv.ptr, C.byref(pol), C.byref(nevo), C.byref(lam),
+                                    C.byref(W), C.byref(res), None), "ChebSI")
+        return self._outputs(nevo.value, lam, W.value, res, want_vectors)
 
     def launch_count(self):
         return int(self.lib.evslx_launch_count())

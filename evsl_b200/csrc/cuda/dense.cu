@@ -174,14 +174,21 @@ constexpr int BM = 64, BN = 64, BK = 16;
 
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(256)
-    k_dgemm(int m, int n, int k, double alpha, const double *__restrict__ A, long long lda,
-            const double *__restrict__ B, long long ldb, double beta, double *C, long long ldc) {
+    k_dgemm(int m, int n, int kbeg, int k, double alpha, const double *__restrict__ A, long long lda,
+            const double *__restrict__ B, long long ldb, double beta, double *C, long long ldc, long long cstride,
+            int kchunk) {
+  // split-K: blockIdx.z selects the inner-dimension range and the output slab
+  if (kchunk > 0) {
+    kbeg = blockIdx.z * kchunk;
+    k = min(k, kbeg + kchunk);
+    C += (long long)blockIdx.z * cstride;
+  }
   __shared__ double sA[BK][BM + 1];
   __shared__ double sB[BK][BN + 1];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   double acc[4][4] = {};
-  for (int k0 = 0; k0 < k; k0 += BK) {
+  for (int k0 = kbeg; k0 < k; k0 += BK) {
     for (int i = threadIdx.x; i < BM * BK; i += 256) {
       const int mm = i % BM, kk = i / BM;
       const int gm = m0 + mm, gk = k0 + kk;
@@ -221,6 +228,18 @@ __global__ void __launch_bounds__(256)
         *c = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*c);
       }
     }
+}
+
+// C = sum over slabs of part (slab stride m*n, ld m) scaled: C = S + beta C
+__global__ void k_splitk_reduce(int m, int n, int slabs, const double *part, double beta, double *C, long long ldc) {
+  const long long total = (long long)m * n;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int z = 0; z < slabs; ++z) s += part[(long long)z * total + i];
+    const int r = (int)(i % m), c = (int)(i / m);
+    double *p = C + (long long)c * ldc + r;
+    *p = (beta == 0.0) ? s : s + beta * (*p);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -396,18 +415,47 @@ int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const doub
                  const double *B, long long ldb, double beta, double *C, long long ldc) {
   if (m <= 0 || n <= 0) return 0;
   const bool TA = (ta == 'T' || ta == 't'), TB = (tb == 'T' || tb == 't');
-  dim3 g((m + BM - 1) / BM, (n + BN - 1) / BN);
   cudaStream_t st = stream();
+  const int gm = (m + BM - 1) / BM, gn = (n + BN - 1) / BN;
+  // Long inner dimension with few output tiles (V^T W): split K into slabs
+  // computed in parallel, then summed in slab order (deterministic).
+  int slabs = 1, kchunk = 0;
+  if ((long long)k >= 32768 && (long long)gm * gn < 512) {
+    slabs = (int)std::min<long long>((k + 16383) / 16384, std::max(1, 2048 / (gm * gn)));
+    kchunk = (int)(((k + slabs - 1) / slabs + BK - 1) / BK * BK);
+    slabs = (k + kchunk - 1) / kchunk;
+  }
+  double *part = nullptr;
+  double *Cout = C;
+  long long ldo = ldc, cstride = 0;
+  double a = alpha, b = beta;
+  if (slabs > 1) {
+    part = (double *)evslcu_malloc(sizeof(double) * (size_t)slabs * m * n);
+    if (!part) return EVSLCU_ERR_NOMEM;
+    Cout = part;
+    ldo = m;
+    cstride = (long long)m * n;
+    b = 0.0;
+  }
+  dim3 g(gm, gn, slabs);
+  const int kc = (slabs > 1) ? kchunk : 0;
   if (!TA && !TB)
-    k_dgemm<false, false><<<g, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    k_dgemm<false, false><<<g, 256, 0, st>>>(m, n, 0, k, a, A, lda, B, ldb, b, Cout, ldo, cstride, kc);
   else if (TA && !TB)
-    k_dgemm<true, false><<<g, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    k_dgemm<true, false><<<g, 256, 0, st>>>(m, n, 0, k, a, A, lda, B, ldb, b, Cout, ldo, cstride, kc);
   else if (!TA && TB)
-    k_dgemm<false, true><<<g, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    k_dgemm<false, true><<<g, 256, 0, st>>>(m, n, 0, k, a, A, lda, B, ldb, b, Cout, ldo, cstride, kc);
   else
-    k_dgemm<true, true><<<g, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-  EVSLCU_LAUNCH_CHECK("k_dgemm");
-  return 0;
+    k_dgemm<true, true><<<g, 256, 0, st>>>(m, n, 0, k, a, A, lda, B, ldb, b, Cout, ldo, cstride, kc);
+  count_launch();
+  int rc = check_launch("k_dgemm");
+  if (!rc && slabs > 1) {
+    k_splitk_reduce<<<grid_for((long long)m * n), kThreads, 0, st>>>(m, n, slabs, part, beta, C, ldc);
+    count_launch();
+    rc = check_launch("k_splitk_reduce");
+  }
+  if (part) evslcu_free(part);
+  return rc;
 }
 
 int evslcu_ritz_eval(const evslcu_op *op, int n, int m, double *U, double *W, double *norm, double *lam,
@@ -448,6 +496,16 @@ int evslcu_gather_cols(int n, int cnt, const int *idx, const double *src, double
     if (rc) return rc;
   }
   return 0;
+}
+
+int evslcu_colnorms(int n, int m, const double *U, double *norms) {
+  if (m <= 0) return 0;
+  double *d = (double *)evslcu_malloc(sizeof(double) * (size_t)m);
+  if (!d) return EVSLCU_ERR_NOMEM;
+  int rc = colred(n, m, 0, U, nullptr, nullptr, d);
+  if (!rc) rc = evslcu_d2h(norms, d, sizeof(double) * m);
+  evslcu_free(d);
+  return rc;
 }
 
 }  // extern "C"

@@ -106,6 +106,18 @@ __device__ __forceinline__ void row_dot2(const SellT<VT, IT> &A, int r0, bool ha
   }
 }
 
+// Calls f(value, column) for the entries of row r, left to right.
+template <class VT, class IT, class F>
+__device__ __forceinline__ void row_for_each(const SellT<VT, IT> &A, int r, F &&f) {
+  const int c = r >> 5;
+  long long p = A.cptr[c] + (r & 31);
+  const int w = A.cw[c];
+  for (int j = 0; j < w; ++j, p += 32) f((double)__ldg(A.val + p), decode_col(__ldg(A.col + p), r));
+}
+
+template <class F>
+__device__ __forceinline__ void row_for_each(const struct CsrView &A, int r, F &&f);
+
 template <bool COHERENT>
 __device__ __forceinline__ double row_dot(const CsrView &A, int r, const double *x) {
   const int b = A.ia[r], e = A.ia[r + 1];
@@ -113,6 +125,12 @@ __device__ __forceinline__ double row_dot(const CsrView &A, int r, const double 
 #pragma unroll 4
   for (int j = b; j < e; ++j) acc = __dadd_rn(acc, __dmul_rn(__ldg(A.a + j), ldx<COHERENT>(x + __ldg(A.ja + j))));
   return acc;
+}
+
+template <class F>
+__device__ __forceinline__ void row_for_each(const CsrView &A, int r, F &&f) {
+  const int b = A.ia[r], e = A.ia[r + 1];
+  for (int j = b; j < e; ++j) f(__ldg(A.a + j), __ldg(A.ja + j));
 }
 
 template <class VT, class IT>

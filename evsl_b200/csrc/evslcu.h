@@ -109,6 +109,13 @@ typedef struct {
 int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, double dd,
                   const double *v, double *y, double *work, const evslcu_cheb_epi *epi);
 
+/* Y = p((A - cc I)/dd) V for the ncols columns of V (column-major n x ncols,
+ * ld = n); work holds 2 n ncols doubles.  With a registered matrix every
+ * degree is one kernel reading A once per group of 8 columns; each column of
+ * Y equals evslcu_chebav of that column bit for bit. */
+int evslcu_chebav_block(const evslcu_op *op, const double *mu, int deg, double cc, double dd, int ncols,
+                        const double *V, double *Y, double *work);
+
 /* One fused Chebyshev update on device vectors (SRC/evsl_cuda.cu:175-191):
  *   w = t*(vkp1 - cc*vk) - (k>1 ? vkm1 : 0); vkp1 = w; y += s*w. */
 int evslcu_cheb_update(int n, int k, double t, double s, double cc, double *vkp1,
@@ -157,6 +164,8 @@ int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const doub
  * n*m doubles of scratch. */
 int evslcu_ritz_eval(const evslcu_op *op, int n, int m, double *U, double *W, double *norm,
                      double *lam, double *res);
+/* norms[c] = ||U_c|| for the m columns of U (n x m, ld n); host output. */
+int evslcu_colnorms(int n, int m, const double *U, double *norms);
 /* Gather columns: dst[:, j] = src[:, idx[j]] for j < cnt (idx host array). */
 int evslcu_gather_cols(int n, int cnt, const int *idx, const double *src, double *dst);
 

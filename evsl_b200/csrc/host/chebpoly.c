@@ -282,6 +282,19 @@ int ChebAv(polparams *pol, double *v, double *y, double *w) {
   return 0;
 }
 
+int evslx_chebav_block(polparams *pol, int ncols, const double *V, double *Y, double *work) {
+  int rc = evsl_require_operator();
+  if (rc) return rc;
+  if (!pol || !pol->mu || ncols < 1) return evsl_seterr(EVSLX_ERR_ARG, "evslx_chebav_block: bad arguments");
+  const double tt = evsl_timer();
+  rc = evslcu_chebav_block(evsl_op(), pol->mu, pol->deg, pol->cc, pol->dd, ncols, V, Y, work);
+  if (!rc) rc = evslcu_sync();
+  if (rc) return evsl_seterr(rc, "%s", evslcu_errstr());
+  evslstat.n_polAv += ncols;
+  evslstat.t_polAv += evsl_timer() - tt;
+  return 0;
+}
+
 void evsl_chebAv_device(int n, int k, double t, double s, double cc, double *vkp1, double *vk, double *vkm1,
                         double *y) {
   evslcu_cheb_update(n, k, t, s, cc, vkp1, vk, vkm1, y);

@@ -479,6 +479,15 @@ int evslx_set_spmv_kernel(int which) {
 
 int evslx_get_spmv_kernel(void) { return evslh.mat ? evslcu_mat_get_kernel(evslh.mat) : evslh.kernel; }
 
+int evsl_apply_A(const double *x, double *y) {
+  int rc = evsl_require_operator();
+  if (rc) return rc;
+  if (evslh.op.A) return from_cu(evslcu_spmv(evslh.op.A, x, y));
+  if ((rc = evslcu_sync())) return from_cu(rc);
+  evslh.op.func((double *)x, y, evslh.op.data);
+  return 0;
+}
+
 int evslx_matvec(const double *x, double *y) {
   int rc = evsl_require_operator();
   if (rc) return rc;

@@ -51,6 +51,11 @@ int evsl_trid_eigvals(int n, const double *d, const double *e, double *w);
 int evsl_trid_eigvecs(int n, const double *d, const double *e, int m, const double *w, double *Z, int ldz);
 int evsl_sym_eig(int n, const double *A, int lda, double *Q, int ldq, double *w);
 int evsl_tr_eig(int k, int m, const double *T, int ldt, double thresh, double *w, double *Z, int ldz);
+int evsl_tr_eig_sel(int k, int m, const double *T, int ldt, int select, double thresh, double *w, double *Z,
+                    int ldz);
+/* y = A x on device vectors with the registered operator (asynchronous for a
+ * registered matrix; a user matvec runs after the stream has drained). */
+int evsl_apply_A(const double *x, double *y);
 
 /* device random vectors drawn from the library stream */
 int evsl_rand_device(int n, int count, double *v);

@@ -355,6 +355,13 @@ int evsl_sym_eig(int n, const double *A, int lda, double *Q, int ldq, double *w)
  * from a Lanczos run on D = diag(theta) started at s/|s| (vectors placed in
  * reverse order), so diag(Q, I)^T T diag(Q, I) is tridiagonal. */
 int evsl_tr_eig(int k, int m, const double *T, int ldt, double thresh, double *w, double *Z, int ldz) {
+  return evsl_tr_eig_sel(k, m, T, ldt, 0, thresh, w, Z, ldz);
+}
+
+/* As evsl_tr_eig; select = 0: vectors of w[i] >= thresh; select = 1: vectors
+ * of the smallest and the largest eigenvalue only (columns 0 and k-1). */
+int evsl_tr_eig_sel(int k, int m, const double *T, int ldt, int select, double thresh, double *w, double *Z,
+                    int ldz) {
   if (k <= 0) return 0;
   double *d = (double *)malloc(sizeof(double) * (size_t)k);
   double *e = (double *)calloc((size_t)k, sizeof(double));
@@ -448,9 +455,10 @@ int evsl_tr_eig(int k, int m, const double *T, int ldt, double thresh, double *w
   }
   int rc = evsl_trid_eigvals(k, d, e, w);
   if (!rc && Z) {
+#define TR_WANT(i) (select ? ((i) == 0 || (i) == k - 1) : (w[(i)] >= thresh))
     int msel = 0;
     for (int i = 0; i < k; i++)
-      if (w[i] >= thresh) msel++;
+      if (TR_WANT(i)) msel++;
     if (msel > 0) {
       double *ws = (double *)malloc(sizeof(double) * (size_t)msel);
       double *Y = (double *)malloc(sizeof(double) * (size_t)k * msel);
@@ -459,11 +467,11 @@ int evsl_tr_eig(int k, int m, const double *T, int ldt, double thresh, double *w
       } else {
         int j = 0;
         for (int i = 0; i < k; i++)
-          if (w[i] >= thresh) ws[j++] = w[i];
+          if (TR_WANT(i)) ws[j++] = w[i];
         rc = evsl_trid_eigvecs(k, d, e, msel, ws, Y, k);
         j = 0;
         for (int i = 0; !rc && i < k; i++) {
-          if (w[i] < thresh) continue;
+          if (!TR_WANT(i)) continue;
           const double *y = Y + (size_t)j * k;
           double *z = Z + (size_t)i * ldz;
           for (int r = 0; r < m; r++) {
@@ -478,6 +486,7 @@ int evsl_tr_eig(int k, int m, const double *T, int ldt, double thresh, double *w
       free(ws);
       free(Y);
     }
+#undef TR_WANT
   }
   free(d);
   free(e);

@@ -200,6 +200,21 @@ int ChebLanTr(int lanm, int nev, double *intv, int maxit, double tol, double *vi
               FILE *fstats);
 
 /* ---------------------------------------------------------------------------
+ * Polynomial-filtered subspace iteration (SRC/chebsi.c:39); vinit is a device
+ * block n x nev, *Yo device, *lamo and *reso host.
+ * ------------------------------------------------------------------------- */
+int ChebSI(int nev, double *intv, int maxit, double tol, double *vinit, polparams *pol, int *nevo,
+           double **lamo, double **Yo, double **reso, FILE *fstats);
+
+/* ---------------------------------------------------------------------------
+ * Spectrum bounds by Lanczos (SRC/lanbounds.c:21, SRC/lanTrbounds.c:35);
+ * v / vinit are device vectors.
+ * ------------------------------------------------------------------------- */
+int LanBounds(int msteps, double *v, double *lmin, double *lmax);
+int LanTrbounds(int lanm, int maxit, double tol, double *vinit, int bndtype, double *lammin, double *lammax,
+                FILE *fstats);
+
+/* ---------------------------------------------------------------------------
  * Density of states and slicing (SRC/spslice.c:29, :205).
  * ------------------------------------------------------------------------- */
 int kpmdos(int Mdeg, int damping, int nvec, double *intv, double *mu, double *ecnt);

@@ -116,6 +116,13 @@ int evslx_matrix_storage(int *value_bytes, int *index_bytes);
  * right, like the reference CPU matvec SRC/spmat.c:257-298). */
 int evslx_matvec(const double *x, double *y);
 
+/* Y = p(A) V for ncols device vectors at once (V, Y: column-major n x ncols;
+ * work: 2 n ncols doubles).  One pass over A per degree serves every group
+ * of 8 columns; each column of Y equals ChebAv (SRC/chebpoly.c:519) of the
+ * same column bit for bit.  No reference counterpart: the reference filters
+ * a block column by column (SRC/chebsi.c:127-129). */
+int evslx_chebav_block(polparams *pol, int ncols, const double *V, double *Y, double *work);
+
 /* Size of the registered problem and of the stored matrix. */
 int evslx_problem_info(int *n, long long *nnz, long long *stored_nnz);
 

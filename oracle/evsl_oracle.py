@@ -117,8 +117,15 @@ class RefLib:
                                               _ip, _ip, _dp, _dp, _dp, C.c_int]
             lib.evslref_slices_nr.restype = C.c_double
             lib._evsl_Free.argtypes = [C.c_void_p]
+            lib.LanBounds.argtypes = [C.c_int, _dp, _dp, _dp]
+            lib.LanBounds.restype = C.c_int
+            lib.LanTrbounds.argtypes = [C.c_int, C.c_int, C.c_double, _dp, C.c_int, _dp, _dp, C.c_void_p]
+            lib.LanTrbounds.restype = C.c_int
             lib.evslref_chebav_multi.argtypes = [C.POINTER(PolParams), C.c_int, _dp, C.c_int]
             lib.evslref_chebav_multi.restype = C.c_double
+            lib.evslref_cheb_si.argtypes = [C.c_int, _dp, C.c_int, C.c_double, _dp, C.POINTER(PolParams), _ip,
+                                            C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp)]
+            lib.evslref_cheb_si.restype = C.c_int
             lib.EVSLStart()
             RefLib._lib = lib
         self.lib = RefLib._lib
@@ -241,6 +248,17 @@ class RefLib:
                                 C.byref(nev2), C.byref(lam), C.byref(W), C.byref(res), None)
         return rc, self._take(nev2.value, lam, W, res, len(v0))
 
+    def cheb_si(self, nev, intv, maxit, tol, vinit_block, pol):
+        """Reference ChebSI (SRC/chebsi.c:39) with start block vinit_block
+        (nev x n: row j is column j of the n x nev block)."""
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        v0 = np.ascontiguousarray(vinit_block, dtype=np.float64)
+        nevo = C.c_int()
+        lam, W, res = _dp(), _dp(), _dp()
+        rc = self.lib.evslref_cheb_si(nev, _dptr(iv), maxit, tol, _dptr(v0), C.byref(pol), C.byref(nevo),
+                                      C.byref(lam), C.byref(W), C.byref(res))
+        return rc, self._take(nevo.value, lam, W, res, v0.shape[1])
+
     def _take(self, m, lam, W, res, n):
         if m > 0:
             out = (np.ctypeslib.as_array(lam, (m,)).copy(),
@@ -252,6 +270,20 @@ class RefLib:
             if p:
                 self.lib._evsl_Free(C.cast(p, C.c_void_p))
         return out
+
+    def lan_bounds(self, msteps, v):
+        """LanBounds (SRC/lanbounds.c:21)."""
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        lo, hi = C.c_double(), C.c_double()
+        rc = self.lib.LanBounds(msteps, _dptr(v), C.byref(lo), C.byref(hi))
+        return rc, lo.value, hi.value
+
+    def lan_trbounds(self, lanm, maxit, tol, v, bndtype):
+        """LanTrbounds (SRC/lanTrbounds.c:35)."""
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        lo, hi = C.c_double(), C.c_double()
+        rc = self.lib.LanTrbounds(lanm, maxit, tol, _dptr(v), bndtype, C.byref(lo), C.byref(hi), None)
+        return rc, lo.value, hi.value
 
     def chebav_multi(self, pol, deg, v, nthreads):
         """Wall seconds of `nthreads` concurrent reference ChebAv calls
@@ -737,6 +769,109 @@ def cheblan_nr(intv, maxit, tol, vinit, pol, ia, ja, a, restart_vectors=()):
             Y.append(u)
             res.append(r)
     return np.array(lam), np.array(Y).reshape(len(lam), n), np.array(res), kdim
+
+
+def lan_bounds(msteps, v, ia, ja, a):
+    """Spectrum bounds from a short Lanczos run with one modified Gram-Schmidt
+    reorthogonalisation pass per step (SRC/lanbounds.c:21-129, standard
+    problem).  On a lucky breakdown the reference keeps the squared beta as
+    the bottom coupling; so does this.  Tridiagonal eigenpairs use scipy's
+    eigh_tridiagonal in place of SymmTridEig."""
+    from scipy.linalg import eigh_tridiagonal
+
+    n = len(v)
+    msteps = min(n, msteps)
+    V = np.zeros((msteps + 1, n))
+    alp = np.zeros(msteps)
+    bet = np.zeros(msteps)
+    V[0] = v * (1.0 / np.linalg.norm(v))
+    wn = 0.0
+    for j in range(msteps):
+        z = csr_matvec(ia, ja, a, V[j])
+        if j:
+            z = z + (-bet[j - 1]) * V[j - 1]
+        alp[j] = z @ V[j]
+        wn += alp[j] * alp[j]
+        z = z + (-alp[j]) * V[j]
+        for i in range(j + 1):
+            z = z + (-(z @ V[i])) * V[i]
+        V[j + 1] = z
+        bet[j] = z @ z
+        if bet[j] * (j + 1) < ORTH_TOL * wn:
+            msteps = j + 1
+            break
+        wn += 2.0 * bet[j]
+        bet[j] = math.sqrt(bet[j])
+        V[j + 1] *= 1.0 / bet[j]
+    bottom = bet[msteps - 1]
+    w, S = eigh_tridiagonal(alp[:msteps], bet[:msteps - 1])
+    return w[0] - abs(bottom * S[msteps - 1, 0]), w[-1] + abs(bottom * S[msteps - 1, msteps - 1])
+
+
+def _orth(V):
+    """Column orthonormalisation (SRC/misc_la.c:317-341): rows of V are the
+    columns; each one CGS-DGKS'd against the previous and normalised."""
+    out = np.array(V, dtype=np.float64, copy=True)
+    out[0] *= 1.0 / np.linalg.norm(out[0])
+    for i in range(1, len(out)):
+        w, nrm = cgs_dgks(out[:i].T, out[i])
+        out[i] = w * (1.0 / nrm)
+    return out
+
+
+def cheb_si(nev, intv, maxit, tol, vinit_block, pol, ia, ja, a):
+    """Polynomial-filtered subspace iteration (SRC/chebsi.c:39-335) for small
+    n: V <- orth(p(A) V) with the active block kept orthogonal to the locked
+    one; every 5 iterations a Rayleigh-Ritz step with p(A), candidates with
+    p(A)-residual < tol/100 confirmed by the A-residual < tol and locked; stop
+    when every column is locked or 2 locked values lie outside [a, b].
+    Rows of vinit_block are the start columns.  Returns (lam, Y, res) of the
+    locked pairs inside [a, b], in locking order."""
+    NBUF, CVCHECK = 2, 5
+    tolP = tol * 0.01
+    aa, bb = intv[0], intv[1]
+    lo_ok, hi_ok = aa - EVSL_DBL_EPS_MULT * DBL_EPS, bb + EVSL_DBL_EPS_MULT * DBL_EPS
+    V = _orth(vinit_block)
+    PV = np.array([cheb_av(pol, ia, ja, a, x) for x in V])
+    Lam, res = np.zeros(nev), np.zeros(nev)
+    nlock, nact, nlock_ab, it, find_more = 0, nev, 0, 0, True
+    while it < maxit and find_more:
+        V[nlock:] = PV[nlock:]
+        if nlock:
+            V[nlock:] -= (V[nlock:] @ V[:nlock].T) @ V[:nlock]
+        V[nlock:] = _orth(V[nlock:])
+        PV[nlock:] = np.array([cheb_av(pol, ia, ja, a, x) for x in V[nlock:]])
+        if nlock:
+            PV[nlock:] -= (PV[nlock:] @ V[:nlock].T) @ V[:nlock]
+        if (it + 1) % CVCHECK == 0 or it + 1 == maxit:
+            T = V[nlock:] @ PV[nlock:].T
+            evalT, evecT = np.linalg.eigh(0.5 * (T + T.T))
+            V[nlock:] = evecT.T @ V[nlock:]
+            PV[nlock:] = evecT.T @ PV[nlock:]
+            locked, active = [], []
+            for i in range(nlock, nev):
+                r = PV[i] - evalT[i - nlock] * V[i]
+                if np.linalg.norm(r) < tolP:
+                    Av = csr_matvec(ia, ja, a, V[i])
+                    rq = V[i] @ Av
+                    ra = np.linalg.norm(Av - rq * V[i])
+                    if ra < tol:
+                        Lam[nlock + len(locked)] = rq
+                        res[nlock + len(locked)] = ra
+                        locked.append(i)
+                        continue
+                active.append(i)
+            order = locked + active
+            V[nlock:] = V[order]
+            PV[nlock:] = PV[order]
+            nlock_ab += sum(1 for k in range(len(locked)) if lo_ok <= Lam[nlock + k] <= hi_ok)
+            nlock += len(locked)
+            nact = len(active)
+            if nlock - nlock_ab >= NBUF or nlock == nev:
+                find_more = False
+        it += 1
+    keep = [i for i in range(nlock) if lo_ok <= Lam[i] <= hi_ok]
+    return Lam[keep], V[keep], res[keep]
 
 
 # ---------------------------------------------------------------------------

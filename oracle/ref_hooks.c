@@ -246,3 +246,14 @@ double evslref_chebav_multi(polparams *pol, int deg, const double *v, int nthrea
   clock_gettime(CLOCK_MONOTONIC, &t1);
   return (t1.tv_sec - t0.tv_sec) + 1e-9 * (t1.tv_nsec - t0.tv_nsec);
 }
+
+/* Reference ChebSI (SRC/chebsi.c:39) writes its statistics to fstats without
+ * a NULL check; run it with fstats on /dev/null. */
+int evslref_cheb_si(int nev, double *intv, int maxit, double tol, double *vinit, polparams *pol, int *nevo,
+                    double **lamo, double **Yo, double **reso) {
+  FILE *f = fopen("/dev/null", "w");
+  if (!f) return -1;
+  int rc = ChebSI(nev, intv, maxit, tol, vinit, pol, nevo, lamo, Yo, reso, f);
+  fclose(f);
+  return rc;
+}

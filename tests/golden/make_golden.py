@@ -87,6 +87,31 @@ def main():
     out["cfg1_res_max"] = np.array([res.max()])
     out["cfg1_vinit_seed"] = np.array([1234])
     R.free_pol(pol)
+    # ---- spectrum bounds: LanBounds / LanTrbounds (simple and Kato-Temple) ----
+    from evsl_b200 import workloads as W
+
+    cases = [("lap2d", R.lap_csr(30, 30, 1)), ("lap3d", R.lap_csr(12, 11, 10)),
+             ("rspd", W.random_spd_csr(3000, 16, 5))]
+    for name, (ia, ja, a) in cases:
+        R.set_csr(ia, ja, a)
+        v = O.seeded_normal(len(ia) - 1, 77)
+        rc, lo, hi = R.lan_bounds(40, v)
+        out[f"lb_{name}"] = np.array([lo, hi])
+        for bt in (1, 2):
+            rc, lo, hi = R.lan_trbounds(30, 200, 1e-8, v, bt)
+            out[f"ltb{bt}_{name}"] = np.array([lo, hi])
+    # ---- ChebSI on the 41x53 Laplacian of the reference's subspace-iteration test --
+    ia, ja, a = R.lap_csr(41, 53, 1)
+    R.set_csr(ia, ja, a)
+    n = len(ia) - 1
+    for name, iv, nev in (("si1", [0.4, 0.5, 0.0, 8.0], 25), ("si2", [0.4, 0.8, 0.0, 8.0], 88)):
+        rc, pol = R.find_pol(iv, damping=0, thresh_int=0.5)
+        V0 = O.seeded_normal(n * nev, 55).reshape(nev, n)
+        rc, (lam, Y, res) = R.cheb_si(nev, iv, 1000, 1e-8, V0, pol)
+        out[f"{name}_cfg"] = np.array(iv + [nev, 55])
+        out[f"{name}_lam"] = np.sort(lam)
+        out[f"{name}_res_max"] = np.array([res.max()])
+        R.free_pol(pol)
     np.savez_compressed(os.path.join(OUT, "evsl_ref_golden.npz"), **out)
     print("wrote", os.path.join(OUT, "evsl_ref_golden.npz"), "keys:", len(out))
 

@@ -72,6 +72,50 @@ def test_cheblan_nr_restatement(golden):
     assert np.all(res < 1e-8)
 
 
+BOUND_CASES = {
+    "lap2d": lambda: O.lap_csr(30, 30, 1),
+    "lap3d": lambda: O.lap_csr(12, 11, 10),
+    "rspd": lambda: __import__("evsl_b200.workloads", fromlist=["x"]).random_spd_csr(3000, 16, 5),
+}
+
+
+@pytest.mark.parametrize("name", sorted(BOUND_CASES))
+def test_lan_bounds_restatement(golden, name):
+    ia, ja, a = BOUND_CASES[name]()
+    lo, hi = O.lan_bounds(40, O.seeded_normal(len(ia) - 1, 77), ia, ja, a)
+    ref = golden[f"lb_{name}"]
+    scale = abs(ref[0]) + abs(ref[1])
+    assert abs(lo - ref[0]) <= 1e-12 * scale and abs(hi - ref[1]) <= 1e-12 * scale
+
+
+def test_cheb_si_restatement(golden):
+    cfg = golden["si1_cfg"]
+    iv, nev, seed = list(cfg[:4]), int(cfg[4]), int(cfg[5])
+    ia, ja, a = O.lap_csr(41, 53, 1)
+    n = len(ia) - 1
+    pol = O.find_pol(iv, damping=0, thresh_int=0.5)
+    lam, Y, res = O.cheb_si(nev, iv, 1000, 1e-8, O.seeded_normal(n * nev, seed).reshape(nev, n), pol, ia, ja, a)
+    assert len(lam) == len(golden["si1_lam"]) == len(O.exeiglap3(41, 53, 1, iv[0], iv[1]))
+    assert np.max(np.abs(np.sort(lam) - golden["si1_lam"])) < 1e-12
+    assert np.all(res < 1e-8)
+
+
+def test_random_spd_matrix():
+    from evsl_b200 import workloads as W
+
+    ia, ja, a = W.random_spd_csr(400, 8, 3)
+    n = len(ia) - 1
+    M = np.zeros((n, n))
+    for i in range(n):
+        cols = ja[ia[i]:ia[i + 1]]
+        assert np.all(np.diff(cols) > 0)
+        M[i, cols] = a[ia[i]:ia[i + 1]]
+    assert np.array_equal(M, M.T)
+    ev = np.linalg.eigvalsh(M)
+    lo, hi = W.gershgorin_bounds(ia, ja, a)
+    assert ev[0] > 0 and lo <= ev[0] and hi >= ev[-1]
+
+
 def test_exact_spectrum_counts(golden):
     ex = O.exeiglap3(100, 100, 1, 0.6, 0.9)
     assert len(ex) == 260 == len(golden["cfg1_lam"])
