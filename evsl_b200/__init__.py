@@ -15,7 +15,8 @@ import os
 
 import numpy as np
 
-__all__ = ["Library", "PolParams", "DeviceBuffer", "EvslError", "library_path", "load", "kpm_accumulate"]
+__all__ = ["Library", "PolParams", "DeviceBuffer", "EvslError", "library_path", "load", "kpm_accumulate",
+           "read_coo_mm", "coo_to_csr_host", "simpson", "spslicer2", "exdos"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -68,6 +69,19 @@ class CsrMat(C.Structure):
     ]
 
 
+class CooMat(C.Structure):
+    """cooMat (INC/struct.h:14-21)."""
+
+    _fields_ = [
+        ("nrows", C.c_int),
+        ("ncols", C.c_int),
+        ("nnz", C.c_int),
+        ("ir", C.POINTER(C.c_int)),
+        ("jc", C.POINTER(C.c_int)),
+        ("vv", C.POINTER(C.c_double)),
+    ]
+
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
@@ -95,6 +109,71 @@ def kpm_accumulate(Mdeg, damping, n, intv, dots):
     if rc != 0:
         raise EvslError(f"evslx_kpm_accumulate returned {rc}")
     return mu, ec.value
+
+
+def read_coo_mm(path, idxin=1, idxout=0):
+    """evslx_read_coo_MM (host only): returns (n, ir, jc, vv) numpy arrays."""
+    lib = load()
+    coo = CooMat()
+    rc = lib.evslx_read_coo_MM(os.fsencode(path), idxin, idxout, C.byref(coo))
+    if rc != 0:
+        raise EvslError(f"evslx_read_coo_MM returned {rc}: {(lib.evslx_last_error() or b'').decode()}")
+    m = coo.nnz
+    out = (coo.nrows,
+           np.ctypeslib.as_array(coo.ir, (m,)).copy() if m else np.zeros(0, np.int32),
+           np.ctypeslib.as_array(coo.jc, (m,)).copy() if m else np.zeros(0, np.int32),
+           np.ctypeslib.as_array(coo.vv, (m,)).copy() if m else np.zeros(0))
+    lib.free_coo(C.byref(coo))
+    return out
+
+
+def coo_to_csr_host(n, ir, jc, vv, cooidx=0):
+    """cooMat_to_csrMat (host only): returns (ia, ja, a)."""
+    lib = load()
+    ir = np.ascontiguousarray(ir, dtype=np.int32)
+    jc = np.ascontiguousarray(jc, dtype=np.int32)
+    vv = np.ascontiguousarray(vv, dtype=np.float64)
+    coo = CooMat(nrows=n, ncols=n, nnz=len(ir), ir=_i(ir), jc=_i(jc), vv=_d(vv))
+    csr = CsrMat()
+    rc = lib.cooMat_to_csrMat(cooidx, C.byref(coo), C.byref(csr))
+    if rc != 0:
+        raise EvslError(f"cooMat_to_csrMat returned {rc}")
+    nnz = csr.ia[n]
+    out = (np.ctypeslib.as_array(csr.ia, (n + 1,)).copy(),
+           np.ctypeslib.as_array(csr.ja, (nnz,)).copy() if nnz else np.zeros(0, np.int32),
+           np.ctypeslib.as_array(csr.a, (nnz,)).copy() if nnz else np.zeros(0))
+    lib.free_csr(C.byref(csr))
+    return out
+
+
+def simpson(xi, yi):
+    """simpson (host only): cumulative integral of yi over xi."""
+    lib = load()
+    xi = np.ascontiguousarray(xi, dtype=np.float64)
+    y = np.array(yi, dtype=np.float64)
+    lib.simpson(_d(xi), _d(y), len(y))
+    return y
+
+
+def spslicer2(xi, yi, n_int):
+    """spslicer2 (host only): slice boundaries from a DOS curve (yi is not
+    modified; the library integrates a copy)."""
+    lib = load()
+    xi = np.ascontiguousarray(xi, dtype=np.float64)
+    y = np.array(yi, dtype=np.float64)
+    sli = np.zeros(n_int + 1)
+    lib.spslicer2(_d(xi), _d(y), n_int, len(y), _d(sli))
+    return sli
+
+
+def exdos(vals, npts, intv):
+    """exDOS (host only): (rc, x, y) for known eigenvalues."""
+    lib = load()
+    v = np.ascontiguousarray(vals, dtype=np.float64)
+    iv = np.ascontiguousarray(intv, dtype=np.float64)
+    x, y = np.zeros(npts), np.zeros(npts)
+    rc = lib.exDOS(_d(v), len(v), npts, _d(x), _d(y), _d(iv))
+    return rc, x, y
 
 
 def load():
@@ -160,6 +239,16 @@ def load():
         "evslx_set_filter_rows_per_thread": ([C.c_int], C.c_int),
         "evslx_set_matrix_compression": ([C.c_int], C.c_int),
         "evslx_matrix_storage": ([_ip, _ip], C.c_int),
+        "evslx_read_coo_MM": ([C.c_char_p, C.c_int, C.c_int, C.POINTER(CooMat)], C.c_int),
+        "evslx_coo_to_csr_device": ([C.c_int, C.POINTER(CooMat), C.c_int, C.POINTER(CsrMat)], C.c_int),
+        "cooMat_to_csrMat": ([C.c_int, C.POINTER(CooMat), C.POINTER(CsrMat)], C.c_int),
+        "free_coo": ([C.POINTER(CooMat)], None),
+        "free_csr": ([C.POINTER(CsrMat)], None),
+        "evsl_free_csr_gpu": ([C.POINTER(CsrMat)], None),
+        "LanDos": ([C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp], C.c_int),
+        "spslicer2": ([_dp, _dp, C.c_int, C.c_int, _dp], None),
+        "simpson": ([_dp, _dp, C.c_int], None),
+        "exDOS": ([_dp, C.c_int, C.c_int, _dp, _dp, _dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -250,6 +339,48 @@ class Library:
         self._check(self.lib.SetAMatrix_device_csr(C.byref(m)), "SetAMatrix_device_csr")
         self.n = n
 
+    def coo_to_csr_device(self, n, ir, jc, vv, cooidx=0, coo_on_device=False):
+        """evslx_coo_to_csr_device: returns the device csrMat (owned by the
+        caller; release with free_csr_device)."""
+        ir = np.ascontiguousarray(ir, dtype=np.int32)
+        jc = np.ascontiguousarray(jc, dtype=np.int32)
+        vv = np.ascontiguousarray(vv, dtype=np.float64)
+        keep = None
+        if coo_on_device:
+            keep = [DeviceBuffer.from_host(self.lib, x) for x in (ir, jc, vv)]
+            coo = CooMat(nrows=n, ncols=n, nnz=len(ir), ir=C.cast(keep[0].ptr, _ip), jc=C.cast(keep[1].ptr, _ip),
+                         vv=C.cast(keep[2].ptr, _dp))
+        else:
+            coo = CooMat(nrows=n, ncols=n, nnz=len(ir), ir=_i(ir), jc=_i(jc), vv=_d(vv))
+        csr = CsrMat()
+        self._check(self.lib.evslx_coo_to_csr_device(cooidx, C.byref(coo), 1 if coo_on_device else 0, C.byref(csr)),
+                    "evslx_coo_to_csr_device")
+        del keep
+        return csr
+
+    def csr_device_to_host(self, csr):
+        n, nnz = csr.nrows, csr.nnz
+        ia = np.zeros(n + 1, np.int32)
+        ja = np.zeros(max(nnz, 1), np.int32)
+        a = np.zeros(max(nnz, 1))
+        self.lib.evsl_memcpy_device_to_host(ia.ctypes.data, C.cast(csr.ia, C.c_void_p), ia.nbytes)
+        if nnz:
+            self.lib.evsl_memcpy_device_to_host(ja.ctypes.data, C.cast(csr.ja, C.c_void_p), 4 * nnz)
+            self.lib.evsl_memcpy_device_to_host(a.ctypes.data, C.cast(csr.a, C.c_void_p), 8 * nnz)
+        return ia, ja[:nnz], a[:nnz]
+
+    def free_csr_device(self, csr):
+        self.lib.evsl_free_csr_gpu(C.byref(csr))
+
+    def set_coo(self, n, ir, jc, vv, cooidx=0, coo_on_device=False):
+        """Device COO -> CSR, then SetAMatrix_device_csr on the result (kept
+        alive with the session)."""
+        csr = self.coo_to_csr_device(n, ir, jc, vv, cooidx, coo_on_device)
+        self._keep = (csr,)
+        self._check(self.lib.SetAMatrix_device_csr(C.byref(csr)), "SetAMatrix_device_csr")
+        self.n = n
+        return csr
+
     def set_filter_persistent(self, on):
         self._check(self.lib.evslx_set_filter_persistent(1 if on else 0), "evslx_set_filter_persistent")
 
@@ -328,6 +459,14 @@ class Library:
         self._check(self.lib.LanTrbounds(lanm, maxit, tol, dv.ptr, bndtype, C.byref(lo), C.byref(hi), None),
                     "LanTrbounds")
         return lo.value, hi.value
+
+    def lan_dos(self, nvec, msteps, npts, intv):
+        """LanDos: returns (xdos, ydos, neig)."""
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        x, y = np.zeros(npts), np.zeros(npts)
+        ne = C.c_double()
+        self._check(self.lib.LanDos(nvec, msteps, npts, _d(x), _d(y), C.byref(ne), _d(iv)), "LanDos")
+        return x, y, ne.value
 
     # -- DOS / slicing -----------------------------------------------------
     def set_seed(self, seed):

@@ -1,0 +1,440 @@
+// Building the device matrix formats on the GPU: COO -> CSR and CSR -> SELL-32.
+//
+// COO -> CSR gives the arrays of the reference's cooMat_to_csrMat
+// (SRC/spmat.c:160-190) followed by sortrow (SRC/spmat.c:67-85): rows in
+// order, and inside each row the entries sorted by column with ties kept in
+// input order (the double transposition of sortrow is a stable sort by
+// column).  Here every entry gets the key (column << 32 | input position);
+// the keys are unique, so a merge sort of each row's keys is deterministic
+// and equals that stable order.
+//
+//   1. check every index (nothing is written before the check passes);
+//   2. count entries per row (integer atomics), exclusive scan -> ia;
+//   3. scatter keys to their rows (slot order inside a row is arbitrary);
+//   4. merge passes of widths 1, 2, 4, ... below the longest row: an element
+//      of run A lands at (its index in A) + (#keys of run B below it), and
+//      the same with A and B swapped -- a pure gather/scatter with no ties;
+//   5. gather ja and a through the sorted keys.
+//
+// CSR -> SELL-32 (the filter's layout): chunk widths, a scan of the chunk
+// sizes, and one fill pass writing every padded slot, with the lossless
+// compression checks (values exactly floats, column offsets within int16)
+// computed on the device as well.
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+#include "sparse_types.cuh"
+
+namespace evslcu {
+
+namespace {
+
+inline int launched(const char *what) {
+  count_launch();
+  return check_launch(what);
+}
+
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kThreads * kScanItems;
+
+// Exclusive scan of one tile of kScanTile inputs; writes the tile's
+// prefixes to out and its total to tsum[blockIdx.x].
+template <class IT, class OT>
+__global__ void __launch_bounds__(kThreads) k_scan_tile(const IT *in, long long m, OT *out, long long *tsum) {
+  __shared__ long long wsum[kThreads / 32];
+  const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+  long long v[kScanItems];
+  long long s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const long long i = base + k;
+    v[k] = (i < m) ? (long long)in[i] : 0;
+    s += v[k];
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  long long x = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    long long t = (lane < kThreads / 32) ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    if (lane < kThreads / 32) wsum[lane] = t;
+  }
+  __syncthreads();
+  long long run = x - s + (w > 0 ? wsum[w - 1] : 0);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const long long i = base + k;
+    if (i < m) out[i] = (OT)run;
+    run += v[k];
+  }
+  if (threadIdx.x == kThreads - 1) tsum[blockIdx.x] = run;
+}
+
+// In-place exclusive scan of the T tile totals by one block; the grand total
+// goes to *total.
+__global__ void __launch_bounds__(kThreads) k_scan_totals(long long *tsum, long long T, long long *total) {
+  __shared__ long long wsum[kThreads / 32];
+  __shared__ long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (long long b = 0; b < T; b += kThreads) {
+    const long long i = b + threadIdx.x;
+    const long long s = (i < T) ? tsum[i] : 0;
+    long long x = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      long long t = (lane < kThreads / 32) ? wsum[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += y;
+      }
+      if (lane < kThreads / 32) wsum[lane] = t;
+    }
+    __syncthreads();
+    const long long ex = x - s + (w > 0 ? wsum[w - 1] : 0);
+    if (i < T) tsum[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == kThreads - 1) carry += ex + s;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+template <class OT>
+__global__ void k_scan_add(OT *out, long long m, const long long *tsum, const long long *total) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (OT)((long long)out[i] + tsum[i / kScanTile]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[m] = (OT)*total;
+}
+
+// out[0..m] = exclusive prefix sums of in[0..m) with out[m] = the total.
+template <class IT, class OT>
+int scan_exclusive(const IT *in, long long m, OT *out) {
+  const long long T = std::max(1LL, (m + kScanTile - 1) / kScanTile);
+  long long *tsum = (long long *)evslcu_malloc(sizeof(long long) * (size_t)(T + 1));
+  if (!tsum) return EVSLCU_ERR_NOMEM;
+  k_scan_tile<IT, OT><<<(unsigned)T, kThreads, 0, stream()>>>(in, m, out, tsum);
+  int rc = launched("k_scan_tile");
+  if (!rc) {
+    k_scan_totals<<<1, kThreads, 0, stream()>>>(tsum, T, tsum + T);
+    rc = launched("k_scan_totals");
+  }
+  if (!rc) {
+    k_scan_add<OT><<<grid_for(std::max(m, 1LL)), kThreads, 0, stream()>>>(out, m, tsum, tsum + T);
+    rc = launched("k_scan_add");
+  }
+  evslcu_free(tsum);
+  return rc;
+}
+
+__device__ __forceinline__ long long lower_bound_u64(const unsigned long long *a, long long len,
+                                                     unsigned long long key) {
+  long long lo = 0, hi = len;
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if (a[mid] < key)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// ---- COO -> CSR ---------------------------------------------------------------
+
+__global__ void k_coo_check(long long nnz, const int *ir, const int *jc, int n, int base,
+                            unsigned long long *first_bad) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
+    const int r = ir[e] - base, c = jc[e] - base;
+    if (r < 0 || r >= n || c < 0 || c >= n) atomicMin(first_bad, (unsigned long long)e);
+  }
+}
+
+__global__ void k_coo_count(long long nnz, const int *ir, int base, int *cnt) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x)
+    atomicAdd(&cnt[ir[e] - base], 1);
+}
+
+__global__ void k_max_len(int n, const int *ia, int *mx) {
+  int m = 0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) m = max(m, ia[r + 1] - ia[r]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(mx, m);
+}
+
+__global__ void k_coo_scatter(long long nnz, const int *ir, const int *jc, int base, const int *ia, int *fill,
+                              unsigned long long *keys, int *rowid) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
+    const int r = ir[e] - base;
+    const int slot = atomicAdd(&fill[r], 1);
+    const long long p = (long long)ia[r] + slot;
+    keys[p] = ((unsigned long long)(unsigned)(jc[e] - base) << 32) | (unsigned long long)(unsigned)e;
+    rowid[p] = r;
+  }
+}
+
+// One merge pass of width w inside every row.
+__global__ void k_row_merge(long long nnz, const int *ia, const int *rowid, const unsigned long long *in,
+                            unsigned long long *out, long long w) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
+    const int r = rowid[e];
+    const long long b0 = ia[r], L = (long long)ia[r + 1] - b0, p = e - b0;
+    const long long k = p / w, pb = (k & ~1LL) * w;
+    const unsigned long long key = in[e];
+    long long dst;
+    if ((k & 1) == 0) {
+      const long long bs = pb + w, be = min(pb + 2 * w, L);
+      const long long below = (bs < be) ? lower_bound_u64(in + b0 + bs, be - bs, key) : 0;
+      dst = b0 + p + below;
+    } else {
+      const long long below = lower_bound_u64(in + b0 + pb, w, key);
+      dst = b0 + pb + (p - pb - w) + below;
+    }
+    out[dst] = key;
+  }
+}
+
+__global__ void k_coo_gather(long long nnz, const unsigned long long *keys, const double *vv, int *ja, double *a) {
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long key = keys[e];
+    ja[e] = (int)(key >> 32);
+    a[e] = vv[key & 0xffffffffull];
+  }
+}
+
+// ---- CSR checks and SELL-32 -----------------------------------------------------
+
+// flags[0]: first row whose pointer decreases (INT_MAX if none).
+__global__ void k_csr_check_ptr(int n, const int *ia, int *flags) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    if (ia[r + 1] < ia[r]) atomicMin(&flags[0], r);
+}
+
+// flags[1]: first entry position with a column outside [0, n) (INT_MAX if
+// none); flags[2]: some value is not exactly a finite float; flags[3]: some
+// |col - row| does not fit int16.
+__global__ void k_csr_check_entries(int n, const int *ia, const int *ja, const double *a, int *flags) {
+  int not_float = 0, not_16 = 0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    for (int j = ia[r]; j < ia[r + 1]; ++j) {
+      const int c = ja[j];
+      if (c < 0 || c >= n) atomicMin(&flags[1], j);
+      if (c - r > 32767 || c - r < -32768) not_16 = 1;
+      const double v = a[j];
+      if (!(isfinite(v) && (double)(float)v == v)) not_float = 1;
+    }
+  }
+  if (__any_sync(0xffffffffu, not_float) && (threadIdx.x & 31) == 0) atomicOr(&flags[2], 1);
+  if (__any_sync(0xffffffffu, not_16) && (threadIdx.x & 31) == 0) atomicOr(&flags[3], 1);
+}
+
+__global__ void k_chunk_width(int n, int nch, const int *ia, int *cw, long long *csize) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nch; c += gridDim.x * blockDim.x) {
+    int w = 0;
+    const int r1 = min(n, 32 * c + 32);
+    for (int r = 32 * c; r < r1; ++r) w = max(w, ia[r + 1] - ia[r]);
+    cw[c] = w;
+    csize[c] = 32LL * w;
+  }
+}
+
+// Thread per (chunk, lane) slot; entry j of lane l at cptr[c] + 32 j + l.
+// Padding: value 0 in the row's own column (adds 0 * x[r]).
+template <class VT, class IT>
+__global__ void k_sell_fill(int n, int nch, const int *ia, const int *ja, const double *a, const long long *cptr,
+                            const int *cw, IT *scol, VT *sval) {
+  const long long slots = 32LL * nch;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(s >> 5), l = (int)(s & 31);
+    const int r = 32 * c + l;
+    const int len = (r < n) ? ia[r + 1] - ia[r] : 0;
+    const int rr = (r < n) ? r : 0;
+    const int beg = (r < n) ? ia[r] : 0;
+    for (int j = 0; j < cw[c]; ++j) {
+      const long long p = cptr[c] + 32LL * j + l;
+      const int col = (j < len) ? ja[beg + j] : rr;
+      const double v = (j < len) ? a[beg + j] : 0.0;
+      if (sizeof(IT) == 2)
+        scol[p] = (IT)(col - rr);
+      else
+        scol[p] = (IT)col;
+      sval[p] = (VT)v;
+    }
+  }
+}
+
+}  // namespace
+
+// Builds the SELL-32 copy of M's device CSR (M->n, M->nnz, M->ia/ja/a set)
+// after validating it.  allow_compress: use the compressed formats when the
+// values and columns allow it.
+int build_sell_device(evslcu_mat *M, int allow_compress) {
+  const int n = M->n;
+  int *flags = (int *)evslcu_malloc(sizeof(int) * 4);
+  if (!flags) return EVSLCU_ERR_NOMEM;
+  const int init[4] = {0x7fffffff, 0x7fffffff, 0, 0};
+  int hf[4];
+  int rc = evslcu_h2d(flags, init, sizeof(init));
+  if (!rc) {
+    k_csr_check_ptr<<<grid_for(n), kThreads, 0, stream()>>>(n, M->ia, flags);
+    rc = launched("k_csr_check_ptr");
+  }
+  if (!rc) rc = evslcu_d2h(hf, flags, sizeof(hf));
+  if (!rc && hf[0] != 0x7fffffff) rc = fail(EVSLCU_ERR_ARG, "CSR row pointer decreases at row %d", hf[0]);
+  if (!rc) {
+    k_csr_check_entries<<<grid_for(n), kThreads, 0, stream()>>>(n, M->ia, M->ja, M->a, flags);
+    rc = launched("k_csr_check_entries");
+  }
+  if (!rc) rc = evslcu_d2h(hf, flags, sizeof(hf));
+  evslcu_free(flags);
+  if (rc) return rc;
+  if (hf[1] != 0x7fffffff) {
+    int bad = 0;
+    evslcu_d2h(&bad, M->ja + hf[1], sizeof(int));
+    return fail(EVSLCU_ERR_ARG, "CSR column index %d at position %d is outside [0, %d)", bad, hf[1], n);
+  }
+  M->vfmt = (allow_compress && !hf[2]) ? 1 : 0;
+  M->ifmt = (allow_compress && !hf[3]) ? 1 : 0;
+  const int nch = (n + 31) / 32;
+  M->nchunks = nch;
+  M->cptr = (long long *)evslcu_malloc(sizeof(long long) * (nch + 1));
+  M->cw = (int *)evslcu_malloc(sizeof(int) * nch);
+  long long *csize = (long long *)evslcu_malloc(sizeof(long long) * nch);
+  if (!M->cptr || !M->cw || !csize) {
+    evslcu_free(csize);
+    return fail(EVSLCU_ERR_NOMEM, "SELL build: out of device memory");
+  }
+  k_chunk_width<<<grid_for(nch), kThreads, 0, stream()>>>(n, nch, M->ia, M->cw, csize);
+  rc = launched("k_chunk_width");
+  if (!rc) rc = scan_exclusive<long long, long long>(csize, nch, M->cptr);
+  evslcu_free(csize);
+  long long padded = 0;
+  if (!rc) rc = evslcu_d2h(&padded, M->cptr + nch, sizeof(long long));
+  if (rc) return rc;
+  M->padded = padded;
+  const size_t cap = (size_t)std::max(padded, 1LL);
+  const size_t colb = M->ifmt ? sizeof(short) : sizeof(int);
+  const size_t valb = M->vfmt ? sizeof(float) : sizeof(double);
+  M->scol = evslcu_malloc(colb * cap);
+  M->sval = evslcu_malloc(valb * cap);
+  if (!M->scol || !M->sval) return fail(EVSLCU_ERR_NOMEM, "SELL build: out of device memory (%lld slots)", padded);
+  const int g = grid_for(32LL * nch);
+  if (M->vfmt && M->ifmt)
+    k_sell_fill<float, short><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->cptr, M->cw,
+                                                            (short *)M->scol, (float *)M->sval);
+  else if (M->vfmt)
+    k_sell_fill<float, int><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->cptr, M->cw,
+                                                          (int *)M->scol, (float *)M->sval);
+  else if (M->ifmt)
+    k_sell_fill<double, short><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->cptr, M->cw,
+                                                             (short *)M->scol, (double *)M->sval);
+  else
+    k_sell_fill<double, int><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->cptr, M->cw,
+                                                           (int *)M->scol, (double *)M->sval);
+  return launched("k_sell_fill");
+}
+
+}  // namespace evslcu
+
+using namespace evslcu;
+
+extern "C" {
+
+int evslcu_coo_to_csr(int n, long long nnz, const int *ir, const int *jc, const double *vv, int base, int **ia_out,
+                      int **ja_out, double **a_out) {
+  if (n <= 0 || nnz < 0 || nnz > 0x7fffffffLL || (nnz > 0 && (!ir || !jc || !vv)) || !ia_out || !ja_out || !a_out)
+    return fail(EVSLCU_ERR_ARG, "coo_to_csr: bad arguments (n=%d nnz=%lld)", n, nnz);
+  *ia_out = nullptr;
+  *ja_out = nullptr;
+  *a_out = nullptr;
+  int *ia = (int *)evslcu_malloc(sizeof(int) * ((size_t)n + 1));
+  int *ja = (int *)evslcu_malloc(sizeof(int) * (size_t)std::max(nnz, 1LL));
+  double *a = (double *)evslcu_malloc(sizeof(double) * (size_t)std::max(nnz, 1LL));
+  int *cnt = (int *)evslcu_malloc(sizeof(int) * (size_t)n + 2 * sizeof(int));
+  unsigned long long *keys = (unsigned long long *)evslcu_malloc(sizeof(unsigned long long) * 2 * (size_t)std::max(nnz, 1LL));
+  int *rowid = (int *)evslcu_malloc(sizeof(int) * (size_t)std::max(nnz, 1LL));
+  unsigned long long *bad = (unsigned long long *)evslcu_malloc(sizeof(unsigned long long));
+  int rc = 0;
+  if (!ia || !ja || !a || !cnt || !keys || !rowid || !bad) rc = fail(EVSLCU_ERR_NOMEM, "coo_to_csr: out of device memory");
+  const unsigned long long none = ~0ull;
+  unsigned long long hb = none;
+  int *maxlen = cnt + n;
+  const int gz = grid_for(std::max(nnz, 1LL));
+  if (!rc) rc = evslcu_h2d(bad, &none, sizeof(none));
+  if (!rc && nnz > 0) {
+    k_coo_check<<<gz, kThreads, 0, stream()>>>(nnz, ir, jc, n, base, bad);
+    rc = launched("k_coo_check");
+    if (!rc) rc = evslcu_d2h(&hb, bad, sizeof(hb));
+    if (!rc && hb != none) {
+      int r = 0, c = 0;
+      evslcu_d2h(&r, ir + hb, sizeof(int));
+      evslcu_d2h(&c, jc + hb, sizeof(int));
+      rc = fail(EVSLCU_ERR_ARG, "COO entry %llu has index (%d, %d) outside the %d x %d matrix (base %d)", hb, r, c, n,
+                n, base);
+    }
+  }
+  if (!rc) rc = evslcu_memset(cnt, 0, sizeof(int) * (size_t)n + 2 * sizeof(int));
+  if (!rc && nnz > 0) {
+    k_coo_count<<<gz, kThreads, 0, stream()>>>(nnz, ir, base, cnt);
+    rc = launched("k_coo_count");
+  }
+  if (!rc) rc = scan_exclusive<int, int>(cnt, n, ia);
+  int hmax = 0;
+  if (!rc && nnz > 0) {
+    k_max_len<<<grid_for(n), kThreads, 0, stream()>>>(n, ia, maxlen);
+    rc = launched("k_max_len");
+    if (!rc) rc = evslcu_d2h(&hmax, maxlen, sizeof(int));
+    if (!rc) rc = evslcu_memset(cnt, 0, sizeof(int) * (size_t)n);
+    if (!rc) {
+      k_coo_scatter<<<gz, kThreads, 0, stream()>>>(nnz, ir, jc, base, ia, cnt, keys, rowid);
+      rc = launched("k_coo_scatter");
+    }
+    unsigned long long *cur = keys, *nxt = keys + nnz;
+    for (long long w = 1; !rc && w < hmax; w *= 2) {
+      k_row_merge<<<gz, kThreads, 0, stream()>>>(nnz, ia, rowid, cur, nxt, w);
+      rc = launched("k_row_merge");
+      std::swap(cur, nxt);
+    }
+    if (!rc) {
+      k_coo_gather<<<gz, kThreads, 0, stream()>>>(nnz, cur, vv, ja, a);
+      rc = launched("k_coo_gather");
+    }
+  }
+  if (!rc) rc = evslcu_sync();
+  evslcu_free(cnt);
+  evslcu_free(keys);
+  evslcu_free(rowid);
+  evslcu_free(bad);
+  if (rc) {
+    evslcu_free(ia);
+    evslcu_free(ja);
+    evslcu_free(a);
+    return rc;
+  }
+  *ia_out = ia;
+  *ja_out = ja;
+  *a_out = a;
+  return 0;
+}
+
+}  // extern "C"

@@ -569,52 +569,27 @@ evslcu_mat *evslcu_mat_create(int n, int nnz, const int *ia, const int *ja, cons
     fail(EVSLCU_ERR_ARG, "invalid CSR matrix (n=%d nnz=%d)", n, nnz);
     return nullptr;
   }
-  // Host copies of the CSR arrays for validation and building SELL-32.
-  std::vector<int> hia(n + 1), hja;
-  std::vector<double> ha;
-  const int *pia = ia, *pja = ja;
-  const double *pa = a;
+  // The row pointer's ends are checked here; monotonicity, column range and
+  // the compression checks run on the device (build_sell_device).
+  int ends[2] = {0, 0};
   if (on_device) {
-    if (evslcu_d2h(hia.data(), ia, sizeof(int) * (n + 1))) return nullptr;
-    nnz = hia[n];
-    hja.resize(nnz);
-    ha.resize(nnz);
-    if (nnz && (evslcu_d2h(hja.data(), ja, sizeof(int) * (size_t)nnz) ||
-                evslcu_d2h(ha.data(), a, sizeof(double) * (size_t)nnz)))
-      return nullptr;
-    pia = hia.data();
-    pja = hja.data();
-    pa = ha.data();
+    if (evslcu_d2h(&ends[0], ia, sizeof(int)) || evslcu_d2h(&ends[1], ia + n, sizeof(int))) return nullptr;
+    nnz = ends[1];
+  } else {
+    ends[0] = ia[0];
+    ends[1] = ia[n];
   }
-  if (pia[0] != 0 || pia[n] != nnz) {
-    fail(EVSLCU_ERR_ARG, "CSR row pointer must start at 0 and end at nnz (%d vs %d)", pia[n], nnz);
+  if (ends[0] != 0 || ends[1] != nnz || nnz < 0) {
+    fail(EVSLCU_ERR_ARG, "CSR row pointer must start at 0 and end at nnz (%d vs %d)", ends[1], nnz);
     return nullptr;
   }
-  for (int r = 0; r < n; ++r) {
-    if (pia[r + 1] < pia[r]) {
-      fail(EVSLCU_ERR_ARG, "CSR row pointer decreases at row %d", r);
-      return nullptr;
-    }
+  if (nnz > 0 && (!ja || !a)) {
+    fail(EVSLCU_ERR_ARG, "invalid CSR matrix (nnz=%d without column/value arrays)", nnz);
+    return nullptr;
   }
-  bool vals_are_float = true, cols_fit_16 = true;
-  for (int r = 0; r < n; ++r) {
-    for (int j = pia[r]; j < pia[r + 1]; ++j) {
-      const int c = pja[j];
-      if (c < 0 || c >= n) {
-        fail(EVSLCU_ERR_ARG, "CSR column index %d at position %d is outside [0, %d)", c, j, n);
-        return nullptr;
-      }
-      if (c - r > 32767 || c - r < -32768) cols_fit_16 = false;
-      const double v = pa[j];
-      if (!(std::isfinite(v) && (double)(float)v == v)) vals_are_float = false;
-    }
-  }
-  const bool allow = g_compress != 0;
   evslcu_mat *M = new evslcu_mat;
   M->n = n;
   M->nnz = nnz;
-  M->vfmt = (allow && vals_are_float) ? 1 : 0;
-  M->ifmt = (allow && cols_fit_16) ? 1 : 0;
   if (on_device) {
     M->ia = ia;
     M->ja = ja;
@@ -624,73 +599,18 @@ evslcu_mat *evslcu_mat_create(int n, int nnz, const int *ia, const int *ja, cons
     int *dia = (int *)evslcu_malloc(sizeof(int) * (n + 1));
     int *dja = (int *)evslcu_malloc(sizeof(int) * (size_t)std::max(nnz, 1));
     double *da = (double *)evslcu_malloc(sizeof(double) * (size_t)std::max(nnz, 1));
-    if (!dia || !dja || !da || evslcu_h2d(dia, ia, sizeof(int) * (n + 1)) ||
-        evslcu_h2d(dja, ja, sizeof(int) * (size_t)nnz) || evslcu_h2d(da, a, sizeof(double) * (size_t)nnz)) {
-      evslcu_free(dia);
-      evslcu_free(dja);
-      evslcu_free(da);
-      delete M;
-      return nullptr;
-    }
     M->ia = dia;
     M->ja = dja;
     M->a = da;
     M->own_csr = true;
-  }
-  // SELL-32: chunk c holds rows 32c..32c+31; entry j of lane l at cptr[c] + 32 j + l.
-  const int nch = (n + 31) / 32;
-  std::vector<long long> cptr(nch + 1, 0);
-  std::vector<int> cw(nch, 0);
-  for (int c = 0; c < nch; ++c) {
-    int w = 0;
-    for (int r = 32 * c; r < std::min(n, 32 * c + 32); ++r) w = std::max(w, pia[r + 1] - pia[r]);
-    cw[c] = w;
-    cptr[c + 1] = cptr[c] + 32LL * w;
-  }
-  const long long padded = cptr[nch];
-  const size_t cap = (size_t)std::max(padded, 1LL);
-  std::vector<int> scol(cap, 0);
-  std::vector<short> scol16(M->ifmt ? cap : 1, 0);
-  std::vector<double> sval(M->vfmt ? 1 : cap, 0.0);
-  std::vector<float> sval32(M->vfmt ? cap : 1, 0.0f);
-  for (int c = 0; c < nch; ++c) {
-    for (int l = 0; l < 32; ++l) {
-      const int r = 32 * c + l;
-      const int len = (r < n) ? pia[r + 1] - pia[r] : 0;
-      for (int j = 0; j < cw[c]; ++j) {
-        const long long p = cptr[c] + 32LL * j + l;
-        int col;
-        double v;
-        if (j < len) {
-          col = pja[pia[r] + j];
-          v = pa[pia[r] + j];
-        } else {
-          col = (r < n) ? r : 0;  // padding: 0 * x[r] adds nothing
-          v = 0.0;
-        }
-        if (M->ifmt)
-          scol16[p] = (short)(col - ((r < n) ? r : 0));
-        else
-          scol[p] = col;
-        if (M->vfmt)
-          sval32[p] = (float)v;
-        else
-          sval[p] = v;
-      }
+    if (!dia || !dja || !da || evslcu_h2d(dia, ia, sizeof(int) * (n + 1)) ||
+        (nnz > 0 && (evslcu_h2d(dja, ja, sizeof(int) * (size_t)nnz) ||
+                     evslcu_h2d(da, a, sizeof(double) * (size_t)nnz)))) {
+      evslcu_mat_destroy(M);
+      return nullptr;
     }
   }
-  M->nchunks = nch;
-  M->padded = padded;
-  const size_t colb = M->ifmt ? sizeof(short) : sizeof(int);
-  const size_t valb = M->vfmt ? sizeof(float) : sizeof(double);
-  M->cptr = (long long *)evslcu_malloc(sizeof(long long) * (nch + 1));
-  M->cw = (int *)evslcu_malloc(sizeof(int) * nch);
-  M->scol = evslcu_malloc(colb * cap);
-  M->sval = evslcu_malloc(valb * cap);
-  if (!M->cptr || !M->cw || !M->scol || !M->sval || evslcu_h2d(M->cptr, cptr.data(), sizeof(long long) * (nch + 1)) ||
-      evslcu_h2d(M->cw, cw.data(), sizeof(int) * nch) ||
-      evslcu_h2d(M->scol, M->ifmt ? (const void *)scol16.data() : (const void *)scol.data(), colb * (size_t)padded) ||
-      evslcu_h2d(M->sval, M->vfmt ? (const void *)sval32.data() : (const void *)sval.data(), valb * (size_t)padded)) {
+  if (build_sell_device(M, g_compress != 0) || evslcu_sync()) {
     evslcu_mat_destroy(M);
     return nullptr;
   }

@@ -33,6 +33,10 @@ struct evslcu_mat {
 
 namespace evslcu {
 
+// Validates M's device CSR and builds its SELL-32 copy on the device
+// (ingest.cu).
+int build_sell_device(evslcu_mat *M, int allow_compress);
+
 template <class VT, class IT>
 struct SellT {
   int n;

@@ -164,6 +164,12 @@ int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const doub
  * n*m doubles of scratch. */
 int evslcu_ritz_eval(const evslcu_op *op, int n, int m, double *U, double *W, double *norm,
                      double *lam, double *res);
+/* COO (device arrays, indices base 0 or 1) -> CSR on the device: rows in
+ * order, entries of a row sorted by column with ties in input order (the
+ * reference's cooMat_to_csrMat + sortrow).  Outputs are new device arrays
+ * (free with evslcu_free). */
+int evslcu_coo_to_csr(int n, long long nnz, const int *ir, const int *jc, const double *vv, int base, int **ia,
+                      int **ja, double **a);
 /* norms[c] = ||U_c|| for the m columns of U (n x m, ld n); host output. */
 int evslcu_colnorms(int n, int m, const double *U, double *norms);
 /* Gather columns: dst[:, j] = src[:, idx[j]] for j < cnt (idx host array). */

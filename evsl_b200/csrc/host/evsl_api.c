@@ -185,9 +185,44 @@ void evsl_last_device_err(void) {
 /* ---------------------------------------------------------------------------
  * CSR helpers (SRC/spmat.c)
  * ------------------------------------------------------------------------- */
-static int cmp_int_double(const void *x, const void *y) {
-  const int a = *(const int *)x, b = *(const int *)y;
-  return (a > b) - (a < b);
+/* Sort the entries of every row by column, ties in their current order --
+ * the result of the reference's sortrow (SRC/spmat.c:67-85), a double
+ * transposition, which is a stable sort by column. */
+struct row_entry {
+  int c, order;
+  double v;
+};
+
+static int cmp_row_entry(const void *x, const void *y) {
+  const struct row_entry *a = (const struct row_entry *)x, *b = (const struct row_entry *)y;
+  if (a->c != b->c) return (a->c > b->c) - (a->c < b->c);
+  return (a->order > b->order) - (a->order < b->order);
+}
+
+static int sort_rows(int n, const int *ia, int *ja, double *a) {
+  int maxlen = 0;
+  for (int r = 0; r < n; r++) maxlen = evsl_max(maxlen, ia[r + 1] - ia[r]);
+  struct row_entry *buf = (struct row_entry *)malloc(sizeof(struct row_entry) * (size_t)(maxlen > 0 ? maxlen : 1));
+  if (!buf) return evsl_seterr(EVSLX_ERR_NOMEM, "sorting CSR rows: out of memory");
+  for (int r = 0; r < n; r++) {
+    const int b = ia[r], len = ia[r + 1] - b;
+    int sorted = 1;
+    for (int j = 1; j < len && sorted; j++)
+      if (ja[b + j] < ja[b + j - 1]) sorted = 0;
+    if (sorted) continue;
+    for (int j = 0; j < len; j++) {
+      buf[j].c = ja[b + j];
+      buf[j].order = j;
+      buf[j].v = a[b + j];
+    }
+    qsort(buf, (size_t)len, sizeof(struct row_entry), cmp_row_entry);
+    for (int j = 0; j < len; j++) {
+      ja[b + j] = buf[j].c;
+      a[b + j] = buf[j].v;
+    }
+  }
+  free(buf);
+  return 0;
 }
 
 int cooMat_to_csrMat(int cooidx, cooMat *coo, csrMat *csr) {
@@ -202,6 +237,18 @@ int cooMat_to_csrMat(int cooidx, cooMat *coo, csrMat *csr) {
   csr->ja = (int *)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
   csr->a = (double *)malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
   if (!csr->ia || !csr->ja || !csr->a) return evsl_seterr(EVSLX_ERR_NOMEM, "cooMat_to_csrMat: out of memory");
+  for (int i = 0; i < nnz; i++) {
+    const int r = coo->ir[i] - cooidx, c = coo->jc[i] - cooidx;
+    if (r < 0 || r >= n || c < 0 || c >= coo->ncols) {
+      free(csr->ia);
+      free(csr->ja);
+      free(csr->a);
+      csr->ia = csr->ja = NULL;
+      csr->a = NULL;
+      return evsl_seterr(EVSLX_ERR_ARG, "cooMat_to_csrMat: entry %d has index (%d, %d) outside the %d x %d matrix", i,
+                         r, c, n, coo->ncols);
+    }
+  }
   for (int i = 0; i < nnz; i++) csr->ia[coo->ir[i] - cooidx + 1]++;
   for (int i = 0; i < n; i++) csr->ia[i + 1] += csr->ia[i];
   int *pos = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
@@ -213,44 +260,7 @@ int cooMat_to_csrMat(int cooidx, cooMat *coo, csrMat *csr) {
     csr->a[k] = coo->vv[i];
   }
   free(pos);
-  /* sort each row by column (the reference sorts by double transposition,
-   * SRC/spmat.c:67-85; duplicates keep their input order either way) */
-  int maxlen = 0;
-  for (int r = 0; r < n; r++) maxlen = evsl_max(maxlen, csr->ia[r + 1] - csr->ia[r]);
-  struct pair {
-    int c;
-    int order;
-    double v;
-  } *buf = (struct pair *)malloc(sizeof(struct pair) * (size_t)(maxlen > 0 ? maxlen : 1));
-  for (int r = 0; r < n; r++) {
-    const int b = csr->ia[r], len = csr->ia[r + 1] - b;
-    int sorted = 1;
-    for (int j = 1; j < len; j++)
-      if (csr->ja[b + j] < csr->ja[b + j - 1]) sorted = 0;
-    if (sorted) continue;
-    for (int j = 0; j < len; j++) {
-      buf[j].c = csr->ja[b + j];
-      buf[j].order = j;
-      buf[j].v = csr->a[b + j];
-    }
-    /* stable insertion sort (rows are short) */
-    for (int j = 1; j < len; j++) {
-      struct pair t = buf[j];
-      int i = j - 1;
-      while (i >= 0 && buf[i].c > t.c) {
-        buf[i + 1] = buf[i];
-        i--;
-      }
-      buf[i + 1] = t;
-    }
-    for (int j = 0; j < len; j++) {
-      csr->ja[b + j] = buf[j].c;
-      csr->a[b + j] = buf[j].v;
-    }
-  }
-  (void)cmp_int_double;
-  free(buf);
-  return 0;
+  return sort_rows(csr->nrows, csr->ia, csr->ja, csr->a);
 }
 
 void free_csr(csrMat *csr) {
@@ -306,7 +316,7 @@ int arrays_copyto_csrMat(int nrow, int ncol, int *ia, int *ja, double *a, csrMat
   memcpy(A->ia, ia, sizeof(int) * ((size_t)nrow + 1));
   memcpy(A->ja, ja, sizeof(int) * (size_t)nnz);
   memcpy(A->a, a, sizeof(double) * (size_t)nnz);
-  return 0;
+  return sort_rows(nrow, A->ia, A->ja, A->a);
 }
 
 /* SRC/spmat.c:626 -- device copy of a host CSR (owndata = 2 marks device data). */

@@ -36,9 +36,11 @@
 #define INVIT_ITERS 3
 #define CLUSTER_TOL 1e-7
 
-/* Implicit QL sweep on (d, e); e[n-1] is scratch.  Z (n x n, column-major,
- * ld ldz) accumulates the rotations when not NULL. */
-static int ql_implicit(int n, double *d, double *e, double *Z, int ldz) {
+/* Implicit QL sweep on (d, e); e[n-1] is scratch.  Z (zrows x n,
+ * column-major, ld ldz) accumulates the rotations when not NULL: zrows = n
+ * gives the eigenvectors, zrows = 1 with Z = e_1^T only their first
+ * components. */
+static int ql_implicit_rows(int n, double *d, double *e, double *Z, int ldz, int zrows) {
   if (n <= 1) return 0;
   e[n - 1] = 0.0;
   for (int l = 0; l < n; l++) {
@@ -74,7 +76,7 @@ static int ql_implicit(int n, double *d, double *e, double *Z, int ldz) {
           g = c * r - b;
           if (Z) {
             double *zi = Z + (size_t)i * ldz, *zi1 = Z + (size_t)(i + 1) * ldz;
-            for (int k = 0; k < n; k++) {
+            for (int k = 0; k < zrows; k++) {
               f = zi1[k];
               zi1[k] = s * zi[k] + c * f;
               zi[k] = c * zi[k] - s * f;
@@ -91,8 +93,12 @@ static int ql_implicit(int n, double *d, double *e, double *Z, int ldz) {
   return 0;
 }
 
+static int ql_implicit(int n, double *d, double *e, double *Z, int ldz) {
+  return ql_implicit_rows(n, d, e, Z, ldz, n);
+}
+
 /* Sort eigenvalues ascending (and the matching columns of Z). */
-static void sort_pairs(int n, double *w, double *Z, int ldz, double *tmp) {
+static void sort_pairs_rows(int n, double *w, double *Z, int ldz, double *tmp, int zrows) {
   for (int i = 0; i < n - 1; i++) {
     int k = i;
     double p = w[i];
@@ -105,13 +111,15 @@ static void sort_pairs(int n, double *w, double *Z, int ldz, double *tmp) {
       w[k] = w[i];
       w[i] = p;
       if (Z) {
-        memcpy(tmp, Z + (size_t)i * ldz, sizeof(double) * n);
-        memcpy(Z + (size_t)i * ldz, Z + (size_t)k * ldz, sizeof(double) * n);
-        memcpy(Z + (size_t)k * ldz, tmp, sizeof(double) * n);
+        memcpy(tmp, Z + (size_t)i * ldz, sizeof(double) * zrows);
+        memcpy(Z + (size_t)i * ldz, Z + (size_t)k * ldz, sizeof(double) * zrows);
+        memcpy(Z + (size_t)k * ldz, tmp, sizeof(double) * zrows);
       }
     }
   }
 }
+
+static void sort_pairs(int n, double *w, double *Z, int ldz, double *tmp) { sort_pairs_rows(n, w, Z, ldz, tmp, n); }
 
 static int cmp_double(const void *a, const void *b) {
   const double x = *(const double *)a, y = *(const double *)b;
@@ -128,6 +136,26 @@ int evsl_trid_eigvals(int n, const double *d, const double *e, double *w) {
   free(ee);
   if (rc) return evsl_seterr(EVSLX_ERR_NUMERIC, "tridiagonal QL did not converge");
   qsort(w, (size_t)n, sizeof(double), cmp_double);
+  return 0;
+}
+
+/* Eigenvalues (ascending) of the symmetric tridiagonal (d, e) and the first
+ * component of each normalised eigenvector (the Lanczos quadrature weights
+ * come from their squares): the QL rotations are applied to e_1^T only. */
+int evsl_trid_eig_first(int n, const double *d, const double *e, double *w, double *z1) {
+  if (n <= 0) return 0;
+  double *ee = (double *)malloc(sizeof(double) * (size_t)n);
+  if (!ee) return evsl_seterr(EVSLX_ERR_NOMEM, "tridiagonal eigensolver: out of memory");
+  memcpy(w, d, sizeof(double) * (size_t)n);
+  if (n > 1) memcpy(ee, e, sizeof(double) * (size_t)(n - 1));
+  for (int i = 0; i < n; i++) z1[i] = (i == 0) ? 1.0 : 0.0;
+  int rc = ql_implicit_rows(n, w, ee, z1, 1, 1);
+  if (!rc) {
+    double tmp;
+    sort_pairs_rows(n, w, z1, 1, &tmp, 1);
+  }
+  free(ee);
+  if (rc) return evsl_seterr(EVSLX_ERR_NUMERIC, "tridiagonal QL did not converge");
   return 0;
 }
 

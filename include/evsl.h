@@ -220,6 +220,17 @@ int LanTrbounds(int lanm, int maxit, double tol, double *vinit, int bndtype, dou
 int kpmdos(int Mdeg, int damping, int nvec, double *intv, double *mu, double *ecnt);
 int spslicer(double *sli, double *mu, int Mdeg, double *intv, int n_int, int npts);
 
+/* Lanczos DOS (SRC/landos.c:37) and its slicer (SRC/spslice2.c:25); xdos,
+ * ydos host arrays of npts.  exDOS (SRC/exDOS.c:17): DOS of known
+ * eigenvalues on the same kind of grid.  simpson (SRC/simpson.c:25, declared
+ * in the reference's INC/internal_header.h:75): cumulative Simpson integral
+ * in place. */
+int LanDos(const int nvec, int msteps, const int npts, double *xdos, double *ydos, double *neig,
+           const double *const intv);
+void spslicer2(double *xi, double *yi, int n_int, int npts, double *sli);
+int exDOS(double *vals, int n, int npts, double *x, double *y, double *intv);
+void simpson(double *xi, double *yi, int npts);
+
 /* ---------------------------------------------------------------------------
  * Vector helpers (SRC/vect.c, SRC/timing.c, SRC/stats.c).
  * ------------------------------------------------------------------------- */

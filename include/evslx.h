@@ -123,6 +123,21 @@ int evslx_matvec(const double *x, double *y);
  * a block column by column (SRC/chebsi.c:127-129). */
 int evslx_chebav_block(polparams *pol, int ncols, const double *V, double *Y, double *work);
 
+/* Matrix-Market coordinate reader with the semantics of the reference
+ * drivers' read_coo_MM (TESTS/COMMON/io.c:115): real or integer, square;
+ * symmetric files are expanded (transposed off-diagonal entries appended in
+ * file order); indices shifted by idxout - idxin.  Returns 0, 1 (unsupported
+ * or malformed header), -1 (fewer entries than announced) or EVSLX_ERR_ARG
+ * (file cannot be opened).  Output arrays are malloc'd (free_coo).  No GPU
+ * needed. */
+int evslx_read_coo_MM(const char *matfile, int idxin, int idxout, cooMat *Acoo);
+
+/* COO -> CSR on the GPU: the CSR of cooMat_to_csrMat (rows sorted by column,
+ * ties in input order) built on the device, as device arrays (owndata = 2,
+ * free with evsl_free_csr_gpu).  coo_on_device: the COO arrays are device
+ * pointers (else host arrays, uploaded).  Ready for SetAMatrix_device_csr. */
+int evslx_coo_to_csr_device(int cooidx, const cooMat *coo, int coo_on_device, csrMat *Agpu);
+
 /* Size of the registered problem and of the stored matrix. */
 int evslx_problem_info(int *n, long long *nnz, long long *stored_nnz);
 

@@ -61,6 +61,18 @@ _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
 
+class CooMat(C.Structure):
+    """cooMat (INC/struct.h:14-21)."""
+    _fields_ = [("nrows", C.c_int), ("ncols", C.c_int), ("nnz", C.c_int), ("ir", _ip), ("jc", _ip), ("vv", _dp)]
+
+
+class CsrMatCPU(C.Structure):
+    """csrMat of the reference CPU build (INC/struct.h:29-42 without the
+    CUDA-only members)."""
+    _fields_ = [("owndata", C.c_int), ("nrows", C.c_int), ("ncols", C.c_int), ("nnz", C.c_int), ("ia", _ip),
+                ("ja", _ip), ("a", _dp)]
+
+
 def _dptr(a):
     return a.ctypes.data_as(_dp)
 
@@ -126,6 +138,18 @@ class RefLib:
             lib.evslref_cheb_si.argtypes = [C.c_int, _dp, C.c_int, C.c_double, _dp, C.POINTER(PolParams), _ip,
                                             C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp)]
             lib.evslref_cheb_si.restype = C.c_int
+            lib.read_coo_MM.argtypes = [C.c_char_p, C.c_int, C.c_int, C.POINTER(CooMat)]
+            lib.read_coo_MM.restype = C.c_int
+            lib.cooMat_to_csrMat.argtypes = [C.c_int, C.POINTER(CooMat), C.POINTER(CsrMatCPU)]
+            lib.cooMat_to_csrMat.restype = C.c_int
+            lib.free_coo.argtypes = [C.POINTER(CooMat)]
+            lib.free_csr.argtypes = [C.POINTER(CsrMatCPU)]
+            lib.LanDos.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp]
+            lib.LanDos.restype = C.c_int
+            lib.spslicer2.argtypes = [_dp, _dp, C.c_int, C.c_int, _dp]
+            lib.simpson.argtypes = [_dp, _dp, C.c_int]
+            lib.exDOS.argtypes = [_dp, C.c_int, C.c_int, _dp, _dp, _dp]
+            lib.exDOS.restype = C.c_int
             lib.EVSLStart()
             RefLib._lib = lib
         self.lib = RefLib._lib
@@ -284,6 +308,61 @@ class RefLib:
         lo, hi = C.c_double(), C.c_double()
         rc = self.lib.LanTrbounds(lanm, maxit, tol, _dptr(v), bndtype, C.byref(lo), C.byref(hi), None)
         return rc, lo.value, hi.value
+
+    # -- matrix input (TESTS/COMMON/io.c:115, SRC/spmat.c:160) ------------------
+    def read_coo_mm(self, path, idxin=1, idxout=0):
+        """Reference read_coo_MM: (rc, n, ir, jc, vv)."""
+        coo = CooMat()
+        rc = self.lib.read_coo_MM(os.fsencode(path), idxin, idxout, C.byref(coo))
+        if rc != 0:
+            return rc, 0, None, None, None
+        m = coo.nnz
+        out = (rc, coo.nrows, np.ctypeslib.as_array(coo.ir, (m,)).copy(),
+               np.ctypeslib.as_array(coo.jc, (m,)).copy(), np.ctypeslib.as_array(coo.vv, (m,)).copy())
+        self.lib.free_coo(C.byref(coo))
+        return out
+
+    def coo_to_csr(self, n, ir, jc, vv, cooidx=0):
+        """Reference cooMat_to_csrMat (with its sortrow): (ia, ja, a)."""
+        ir = np.ascontiguousarray(ir, dtype=np.int32)
+        jc = np.ascontiguousarray(jc, dtype=np.int32)
+        vv = np.ascontiguousarray(vv, dtype=np.float64)
+        coo = CooMat(nrows=n, ncols=n, nnz=len(ir), ir=_iptr(ir), jc=_iptr(jc), vv=_dptr(vv))
+        csr = CsrMatCPU()
+        self.lib.cooMat_to_csrMat(cooidx, C.byref(coo), C.byref(csr))
+        nnz = csr.ia[n]
+        out = (np.ctypeslib.as_array(csr.ia, (n + 1,)).copy(), np.ctypeslib.as_array(csr.ja, (nnz,)).copy(),
+               np.ctypeslib.as_array(csr.a, (nnz,)).copy())
+        self.lib.free_csr(C.byref(csr))
+        return out
+
+    # -- Lanczos DOS (SRC/landos.c:37, SRC/spslice2.c:25, SRC/exDOS.c:17) -------
+    def lan_dos(self, nvec, msteps, npts, intv):
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        x, y = np.zeros(npts), np.zeros(npts)
+        ne = C.c_double()
+        rc = self.lib.LanDos(nvec, msteps, npts, _dptr(x), _dptr(y), C.byref(ne), _dptr(iv))
+        return rc, x, y, ne.value
+
+    def spslicer2(self, x, y, n_int):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.array(y, dtype=np.float64)
+        sli = np.zeros(n_int + 1)
+        self.lib.spslicer2(_dptr(x), _dptr(y), n_int, len(y), _dptr(sli))
+        return sli
+
+    def simpson(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.array(y, dtype=np.float64)
+        self.lib.simpson(_dptr(x), _dptr(y), len(y))
+        return y
+
+    def exdos(self, vals, npts, intv):
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        x, y = np.zeros(npts), np.zeros(npts)
+        rc = self.lib.exDOS(_dptr(v), len(v), npts, _dptr(x), _dptr(y), _dptr(iv))
+        return rc, x, y
 
     def chebav_multi(self, pol, deg, v, nthreads):
         """Wall seconds of `nthreads` concurrent reference ChebAv calls
@@ -872,6 +951,197 @@ def cheb_si(nev, intv, maxit, tol, vinit_block, pol, ia, ja, a):
         it += 1
     keep = [i for i in range(nlock) if lo_ok <= Lam[i] <= hi_ok]
     return Lam[keep], V[keep], res[keep]
+
+
+def read_coo_mm(path, idxin=1, idxout=0):
+    """Matrix-Market coordinate reader (TESTS/COMMON/io.c:115-214 with the
+    banner/size rules of TESTS/COMMON/mmio.c:80-210).  Returns (rc, n, ir,
+    jc, vv); rc 1 for an unsupported or malformed header, -1 for a short
+    file.  Symmetric files: the transposed off-diagonal entries are appended
+    after the stored ones, in file order."""
+    with open(path, "r") as f:
+        lines = f.read().split("\n")
+    tok = lines[0].split()
+    if len(tok) < 5 or not tok[0].startswith("%%MatrixMarket"):
+        return 1, 0, None, None, None
+    obj, fmt, field, sym = (t.lower() for t in tok[1:5])
+    if obj != "matrix" or fmt != "coordinate" or field not in ("real", "integer") or \
+            sym not in ("general", "symmetric", "skew-symmetric"):
+        return 1, 0, None, None, None
+    k = 1
+    while k < len(lines) and lines[k].startswith("%"):
+        k += 1
+    rest = " ".join(lines[k:]).split()
+    if len(rest) < 3:
+        return 1, 0, None, None, None
+    nrow, ncol, nnz = int(rest[0]), int(rest[1]), int(rest[2])
+    if nrow != ncol:
+        return 1, 0, None, None, None
+    vals = rest[3:3 + 3 * nnz]
+    if len(vals) < 3 * nnz:
+        return -1, 0, None, None, None
+    ir = np.array([int(float(t)) for t in vals[0::3]], dtype=np.int32)
+    jc = np.array([int(float(t)) for t in vals[1::3]], dtype=np.int32)
+    vv = np.array([float(t) for t in vals[2::3]])
+    if sym == "symmetric":
+        off = ir != jc
+        ir, jc, vv = (np.concatenate([ir, jc[off]]), np.concatenate([jc, ir[off]]), np.concatenate([vv, vv[off]]))
+    off = idxout - idxin
+    return 0, nrow, ir + off, jc + off, vv
+
+
+def coo_to_csr(n, ir, jc, vv, cooidx=0):
+    """cooMat_to_csrMat + sortrow (SRC/spmat.c:160-190, :67-85): rows in
+    order, each row stably sorted by column (ties in input order)."""
+    r = np.asarray(ir, dtype=np.int64) - cooidx
+    c = np.asarray(jc, dtype=np.int64) - cooidx
+    order = np.lexsort((np.arange(len(r)), c, r))
+    ia = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(ia, r + 1, 1)
+    return np.cumsum(ia).astype(np.int32), c[order].astype(np.int32), np.asarray(vv, dtype=np.float64)[order]
+
+
+def simpson(xi, yi):
+    """Cumulative Simpson integral (SRC/simpson.c:25-50), returned as a new
+    array."""
+    y = np.array(yi, dtype=np.float64)
+    npts = len(y)
+    tc = 0.0
+    i = 1
+    ysav = y[0]
+    y[0] = 0.0
+    while i < npts - 1:
+        ti = (xi[i] - xi[i - 1]) * (ysav + y[i]) / 2.0
+        tm = tc + ti
+        ti = (xi[i + 1] - xi[i - 1]) * (ysav + 4 * y[i] + y[i + 1]) / 6.0
+        tc += ti
+        y[i] = tm
+        ysav = y[i + 1]
+        y[i + 1] = tc
+        i += 2
+    if i == npts - 1:
+        ti = (xi[i] - xi[i - 1]) * (y[i] + ysav) / 2.0
+        y[i] = tc + ti
+    return y
+
+
+def spslicer2(xi, yi, n_int):
+    """Equal-count slices from a DOS curve (SRC/spslice2.c:25-45)."""
+    y = simpson(xi, yi)
+    npts = len(y)
+    t = y[0]
+    want = (y[npts - 1] - y[0]) / float(n_int)
+    sli = np.zeros(n_int + 1)
+    sli[0] = xi[0]
+    ls = 0
+    for k in range(1, npts):
+        if y[k] - t >= want:
+            ls += 1
+            if ls <= n_int:
+                sli[ls] = xi[k]
+            t = y[k]
+    sli[n_int] = xi[npts - 1]
+    return sli
+
+
+def _dos_params(msteps_or_n, intv):
+    lm, lM = intv[2], intv[3]
+    M = min(msteps_or_n, 30)
+    H = (lM - lm) / (M - 1)
+    sigma = H / math.sqrt(8 * math.log(1.25))
+    sigma2 = 2 * sigma * sigma
+    width = sigma * math.sqrt(-2.0 * math.log(1e-08))
+    return sigma2, width
+
+
+def exdos(vals, npts, intv):
+    """DOS of known eigenvalues (SRC/exDOS.c:17-67): (rc, x, y)."""
+    n = len(vals)
+    sigma2, width = _dos_params(n, intv)
+    a, b = intv[0], intv[1]
+    x = linspace(a, b, npts)
+    h = x[1] - x[0]
+    y = np.zeros(npts)
+    j = 0
+    for t in vals:
+        if t < a or t > b:
+            continue
+        j = max(int((t - a - width) / h), 0)
+        xi = a + j * h
+        while xi <= min(t + width, b) and j < npts:
+            y[j] += math.exp(-(xi - t) * (xi - t) / sigma2)
+            j += 1
+            xi += h
+    if j == 0:
+        return 1, x, y
+    scaling = 1.0 / (n * math.sqrt(sigma2 * math.pi))
+    return 0, x, scaling * y
+
+
+def library_normal(seed, draw, n):
+    """randn_double_device of the GPU library and the oracle hook: Box-Muller
+    on the uniform draws 2i and 2i+1 of draw d."""
+    u = library_uniform(seed, draw, 2 * n)
+    u1 = np.maximum(0.5 * (u[0::2] + 1.0), 1e-300)
+    u2 = 0.5 * (u[1::2] + 1.0)
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * math.pi * u2)
+
+
+def lan_dos(nvec, msteps, npts, intv, ia, ja, a, seed):
+    """Lanczos DOS (SRC/landos.c:37-200) for small n with the library's
+    normal draws (one per vector, starting at draw 0 after seeding).  One
+    modified Gram-Schmidt pass per step as in the reference; tridiagonal
+    eigenpairs from scipy.  Returns (x, y, neig)."""
+    from scipy.linalg import eigh_tridiagonal
+
+    n = len(ia) - 1
+    lm, lM = intv[2], intv[3]
+    tol_bd = 1.e-13 * (abs(lM) + abs(lm))
+    aa, bb = max(intv[0], intv[2]), min(intv[1], intv[3])
+    sigma2, width = _dos_params(msteps, intv)
+    x = linspace(aa, bb, npts)
+    y = np.zeros(npts)
+    draw = 0
+    for _ in range(nvec):
+        v = library_normal(seed, draw, n)
+        draw += 1
+        V = np.zeros((msteps + 1, n))
+        V[0] = v * (1.0 / math.sqrt(v @ v))
+        alp, bet = np.zeros(msteps), np.zeros(msteps)
+        wn = 0.0
+        for j in range(msteps):
+            z = csr_matvec(ia, ja, a, V[j])
+            if j:
+                z = z + (-bet[j - 1]) * V[j - 1]
+            alp[j] = z @ V[j]
+            wn += alp[j] * alp[j]
+            z = z + (-alp[j]) * V[j]
+            for i in range(j + 1):
+                z = z + (-(z @ V[i])) * V[i]
+            bet[j] = z @ z
+            if bet[j] * (j + 1) < ORTH_TOL * wn:
+                msteps = j + 1
+                break
+            if bet[j] > tol_bd:
+                wn += 2.0 * bet[j]
+                bet[j] = math.sqrt(bet[j])
+                V[j + 1] = z * (1.0 / bet[j])
+            else:
+                draw += 1
+                for i in range(j + 1):
+                    z = z + (-(z @ V[i])) * V[i]
+                bet[j] = z @ z
+                wn += 2.0 * bet[j]
+                V[j + 1] = z * (1.0 / math.sqrt(bet[j]))
+                bet[j] = 0.0
+        w, S = eigh_tridiagonal(alp[:msteps], bet[:msteps - 1])
+        g2 = S[0, :] ** 2
+        for i in range(msteps):
+            near = np.abs(x - w[i]) < width
+            y[near] += g2[i] * np.exp(-((x[near] - w[i]) * (x[near] - w[i])) / sigma2)
+    y = (1.0 / (nvec * math.sqrt(sigma2 * math.pi))) * y
+    integ = simpson(x, y)
+    return x, y, integ[-1] * n
 
 
 # ---------------------------------------------------------------------------

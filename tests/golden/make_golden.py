@@ -7,7 +7,9 @@ reference sources).  Run from the repository root:
 Every input is seeded; probe and start vectors are injected into the
 reference through its rand_double_device hook (oracle/ref_hooks.c).
 """
+import gzip
 import os
+import shutil
 import sys
 
 import numpy as np
@@ -17,6 +19,64 @@ sys.path.insert(0, ROOT)
 from oracle import evsl_oracle as O  # noqa: E402
 
 OUT = os.path.join(ROOT, "tests", "golden")
+MM_DIR = os.path.join(OUT, "mm")
+REF_MATRICES = "/root/reference/EVSL_1.1.1/MATRICES"
+
+
+def _fmt(v, rng):
+    """Value text in a few of the notations Matrix-Market files use."""
+    k = rng.integers(0, 3)
+    if k == 0:
+        return repr(float(v))
+    if k == 1:
+        return "%.6e" % v
+    return "%.4f" % v
+
+
+def write_mm_fixtures():
+    """Small Matrix-Market files covering the reader's cases (seeded)."""
+    os.makedirs(MM_DIR, exist_ok=True)
+    rng = np.random.default_rng(31)
+    files = {}
+    # general real with comments, unsorted entries and duplicated positions
+    n, m = 40, 200
+    r = rng.integers(1, n + 1, m)
+    c = rng.integers(1, n + 1, m)
+    r[-10:], c[-10:] = r[:10], c[:10]
+    lines = ["%%MatrixMarket matrix coordinate real general", "% seeded test matrix", "%", f"{n} {n} {m}"]
+    lines += [f"{r[k]} {c[k]} {_fmt(rng.standard_normal(), rng)}" for k in range(m)]
+    files["gen_dup"] = lines
+    # symmetric real: lower triangle with the diagonal, random order
+    n = 50
+    pos = [(i, j) for i in range(1, n + 1) for j in range(1, i + 1) if i == j or rng.random() < 0.08]
+    rng.shuffle(pos)
+    lines = ["%%MatrixMarket matrix coordinate real symmetric", f"{n} {n} {len(pos)}"]
+    lines += [f"{i} {j} {_fmt(rng.uniform(-1, 1) + (4.0 if i == j else 0.0), rng)}" for i, j in pos]
+    files["sym"] = lines
+    # integer general with an upper-case banner
+    n, m = 30, 90
+    lines = ["%%MatrixMarket MATRIX Coordinate INTEGER General", f"{n} {n} {m}"]
+    lines += [f"{rng.integers(1, n + 1)} {rng.integers(1, n + 1)} {rng.integers(-9, 10)}" for _ in range(m)]
+    files["int_upper"] = lines
+    # skew-symmetric: read as stored (not expanded)
+    n = 20
+    pos = [(i, j) for i in range(2, n + 1) for j in range(1, i) if rng.random() < 0.2]
+    lines = ["%%MatrixMarket matrix coordinate real skew-symmetric", f"{n} {n} {len(pos)}"]
+    lines += [f"{i} {j} {_fmt(rng.standard_normal(), rng)}" for i, j in pos]
+    files["skew"] = lines
+    # rejected: pattern field, non-square, short file
+    files["pattern"] = ["%%MatrixMarket matrix coordinate pattern general", "3 3 2", "1 1", "2 3"]
+    files["rect"] = ["%%MatrixMarket matrix coordinate real general", "5 6 2", "1 1 1.0", "2 3 2.0"]
+    files["short"] = ["%%MatrixMarket matrix coordinate real general", "4 4 10"] + [f"{k} {k} 1.5" for k in
+                                                                                       range(1, 5)]
+    for name, lines in files.items():
+        with open(os.path.join(MM_DIR, name + ".mtx"), "w") as f:
+            f.write("\n".join(lines) + "\n")
+    # the reference's own test matrix (stiffness matrix, n = 5795), compressed
+    with open(os.path.join(REF_MATRICES, "A.mtx"), "rb") as src, \
+            gzip.GzipFile(os.path.join(MM_DIR, "A.mtx.gz"), "wb", mtime=0) as dst:
+        shutil.copyfileobj(src, dst)
+    return sorted(files)
 
 FIND_POL_CASES = [
     # (intv, damping, thresh_int, thresh_ext, max_deg)
@@ -112,6 +172,55 @@ def main():
         out[f"{name}_lam"] = np.sort(lam)
         out[f"{name}_res_max"] = np.array([res.max()])
         R.free_pol(pol)
+    # ---- Matrix-Market input: reference read_coo_MM + cooMat_to_csrMat ---------
+    for name in write_mm_fixtures():
+        rc, n, ir, jc, vv = R.read_coo_mm(os.path.join(MM_DIR, name + ".mtx"), 1, 0)
+        out[f"mm_{name}_rc"] = np.array([rc])
+        if rc == 0:
+            out[f"mm_{name}_coo"] = np.stack([ir, jc]).astype(np.int32)
+            out[f"mm_{name}_vv"] = vv
+            ia, ja, a = R.coo_to_csr(n, ir, jc, vv, 0)
+            out[f"mm_{name}_ia"], out[f"mm_{name}_ja"], out[f"mm_{name}_a"] = ia, ja, a
+    # ---- Lanczos DOS + spslicer2 on a 30x30 Laplacian; exDOS ------------------------
+    ia, ja, a = R.lap_csr(30, 30, 1)
+    R.set_csr(ia, ja, a)
+    R.set_seed(11)
+    rc, x, y, ec = R.lan_dos(10, 40, 200, [0.5, 2.0, 0.0, 8.0])
+    out["ld30_x"], out["ld30_y"], out["ld30_ecnt"] = x, y, np.array([ec])
+    out["ld30_sli"] = R.spslicer2(x, y, 4)
+    rc, x, y = R.exdos(O.exeiglap3(30, 30, 1, 0.0, 8.0), 300, [0.5, 2.0, 0.0, 8.0])
+    out["exdos30_y"] = y
+    # ---- the reference's Matrix-Market pipeline on A.mtx (TESTS/PLanN/MMPLanN.c):
+    #      LanTrbounds -> LanDos -> spslicer2 -> ChebLanNr per slice, tol 1e-6 --------
+    rc, n, ir, jc, vv = R.read_coo_mm(os.path.join(REF_MATRICES, "A.mtx"), 1, 0)
+    ia, ja, a = R.coo_to_csr(n, ir, jc, vv, 0)
+    R.set_csr(ia, ja, a)
+    vinit = O.library_uniform(2024, 0, n)
+    rc, lo, hi = R.lan_trbounds(50, 200, 1e-8, vinit, 1)
+    R.set_seed(77)
+    rc, x, y, ec = R.lan_dos(30, 80, 500, [0.1, 0.3, lo, hi])
+    sli = R.spslicer2(x, y, 5)
+    out["mmA_bounds"], out["mmA_ecnt"], out["mmA_sli"] = np.array([lo, hi]), np.array([ec]), sli
+    counts = []
+    lams = []
+    for s in range(5):
+        nev = int(1 + ec / 5)
+        nev = int(1.2 * nev)
+        mlan = min(max(5 * nev, 300), n)
+        xi = [sli[s], sli[s + 1], lo, hi]
+        rc, pol = R.find_pol(xi, damping=2, thresh_int=0.8, thresh_ext=0.2)
+        rc, (lam, W, res) = R.cheblan_nr(xi, mlan, 1e-6, vinit, pol)
+        counts.append(len(lam))
+        lams.append(np.sort(lam))
+        R.free_pol(pol)
+    out["mmA_counts"] = np.array(counts)
+    out["mmA_lam"] = np.concatenate(lams)
+    M = np.zeros((n, n))
+    for i in range(n):
+        M[i, ja[ia[i]:ia[i + 1]]] = a[ia[i]:ia[i + 1]]
+    ev = np.linalg.eigvalsh(M)
+    out["mmA_exact"] = ev[(ev >= 0.1) & (ev <= 0.3)]
+    out["mmA_extremes"] = np.array([ev[0], ev[-1]])
     np.savez_compressed(os.path.join(OUT, "evsl_ref_golden.npz"), **out)
     print("wrote", os.path.join(OUT, "evsl_ref_golden.npz"), "keys:", len(out))
 
