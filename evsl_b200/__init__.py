@@ -85,6 +85,32 @@ class CooMat(C.Structure):
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
+PREC_FP64 = 0
+PREC_MIXED = 1
+REQ_SLICE = 1
+REQ_KPM = 2
+
+
+class EvslxResult(C.Structure):
+    """evslx_result (include/evslx.h)."""
+
+    _fields_ = [
+        ("tag", C.c_uint64),
+        ("kind", C.c_int),
+        ("rc", C.c_int),
+        ("nev", C.c_int),
+        ("lam", C.POINTER(C.c_double)),
+        ("res", C.POINTER(C.c_double)),
+        ("Y", C.c_void_p),
+        ("mu", C.POINTER(C.c_double)),
+        ("ecnt", C.c_double),
+        ("lanczos_steps", C.c_int),
+        ("refine_sweeps", C.c_int),
+        ("t_submit", C.c_double),
+        ("t_start", C.c_double),
+        ("t_finish", C.c_double),
+    ]
+
 
 def _d(a):
     return a.ctypes.data_as(_dp)
@@ -249,6 +275,24 @@ def load():
         "spslicer2": ([_dp, _dp, C.c_int, C.c_int, _dp], None),
         "simpson": ([_dp, _dp, C.c_int], None),
         "exDOS": ([_dp, C.c_int, C.c_int, _dp, _dp, _dp], C.c_int),
+        "evslx_matrix_create": ([C.POINTER(CsrMat), C.c_int], C.c_void_p),
+        "evslx_matrix_free": ([C.c_void_p], None),
+        "evslx_matrix_device_bytes": ([C.c_void_p], C.c_longlong),
+        "evslx_engine_create": ([C.c_int, C.c_size_t, C.c_int, C.c_int], C.c_void_p),
+        "evslx_engine_free": ([C.c_void_p], None),
+        "evslx_engine_submit_slice": ([C.c_void_p, C.c_void_p, _dp, C.POINTER(PolParams), C.c_int, C.c_double,
+                                       C.c_void_p, C.c_int, C.c_uint64], C.c_int),
+        "evslx_engine_submit_kpm": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, _dp, C.c_uint64,
+                                     C.c_uint64], C.c_int),
+        "evslx_engine_step": ([C.c_void_p], C.c_int),
+        "evslx_engine_run": ([C.c_void_p], C.c_int),
+        "evslx_engine_pending": ([C.c_void_p], C.c_int),
+        "evslx_engine_bytes_in_use": ([C.c_void_p], C.c_size_t),
+        "evslx_engine_pop_result": ([C.c_void_p, C.POINTER(EvslxResult)], C.c_int),
+        "evslx_result_free": ([C.POINTER(EvslxResult)], None),
+        "evslx_chebav_multi": ([C.c_int, C.POINTER(PolParams), C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+        "evslx_ChebLanNr_batch": ([C.c_int, _dp, C.c_int, C.c_double, C.c_void_p, C.POINTER(PolParams), C.c_int,
+                                   _ip, C.POINTER(_dp), C.POINTER(C.c_void_p), C.POINTER(_dp)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -291,6 +335,98 @@ class DeviceBuffer:
             self.free()
         except Exception:
             pass
+
+
+class Matrix:
+    """A resident device matrix (evslx_matrix) owned by this object."""
+
+    def __init__(self, lib, ia, ja, a):
+        self.lib = lib
+        ia = np.ascontiguousarray(ia, dtype=np.int32)
+        ja = np.ascontiguousarray(ja, dtype=np.int32)
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self.n = len(ia) - 1
+        m = CsrMat(owndata=0, nrows=self.n, ncols=self.n, nnz=int(ia[-1]), ia=_i(ia), ja=_i(ja), a=_d(a))
+        self.ptr = lib.evslx_matrix_create(C.byref(m), 0)
+        if not self.ptr:
+            raise EvslError(f"evslx_matrix_create failed: {(lib.evslx_last_error() or b'').decode()}")
+
+    def device_bytes(self):
+        return self.lib.evslx_matrix_device_bytes(self.ptr)
+
+    def free(self):
+        if self.ptr:
+            self.lib.evslx_matrix_free(self.ptr)
+        self.ptr = None
+
+
+class Engine:
+    """Continuous-batching request engine (evslx_engine)."""
+
+    def __init__(self, lib, max_slots, hbm_budget=0, precision=PREC_FP64, keep_vectors=False):
+        self.lib = lib
+        self.ptr = lib.evslx_engine_create(max_slots, hbm_budget, precision, 1 if keep_vectors else 0)
+        self._info = {}
+        if not self.ptr:
+            raise EvslError(f"evslx_engine_create failed: {(lib.evslx_last_error() or b'').decode()}")
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise EvslError(f"{what} returned {rc}: {(self.lib.evslx_last_error() or b'').decode()}")
+
+    def submit_slice(self, M, intv, pol, maxit, tol, vinit, tag):
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        v = np.ascontiguousarray(vinit, dtype=np.float64)
+        self._check(self.lib.evslx_engine_submit_slice(self.ptr, M.ptr, _d(iv), C.byref(pol), maxit, tol,
+                                                       v.ctypes.data, 0, tag), "evslx_engine_submit_slice")
+        self._info[tag] = {"n": M.n}
+
+    def submit_kpm(self, M, Mdeg, damping, nvec, intv, seed, tag):
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        self._check(self.lib.evslx_engine_submit_kpm(self.ptr, M.ptr, Mdeg, damping, nvec, _d(iv), seed, tag),
+                    "evslx_engine_submit_kpm")
+        self._info[tag] = {"n": M.n, "Mdeg": Mdeg}
+
+    def step(self):
+        rc = self.lib.evslx_engine_step(self.ptr)
+        if rc < 0:
+            self._check(rc, "evslx_engine_step")
+        return rc
+
+    def run(self):
+        self._check(self.lib.evslx_engine_run(self.ptr), "evslx_engine_run")
+
+    def pending(self):
+        return self.lib.evslx_engine_pending(self.ptr)
+
+    def bytes_in_use(self):
+        return self.lib.evslx_engine_bytes_in_use(self.ptr)
+
+    def pop(self):
+        """Next result as a dict (None if the result queue is empty)."""
+        r = EvslxResult()
+        if not self.lib.evslx_engine_pop_result(self.ptr, C.byref(r)):
+            return None
+        info = self._info.pop(r.tag, {})
+        out = {"tag": r.tag, "kind": r.kind, "rc": r.rc, "nev": r.nev, "ecnt": r.ecnt,
+               "lanczos_steps": r.lanczos_steps, "refine_sweeps": r.refine_sweeps,
+               "t_submit": r.t_submit, "t_start": r.t_start, "t_finish": r.t_finish}
+        m = r.nev
+        out["lam"] = np.ctypeslib.as_array(r.lam, (m,)).copy() if m and r.lam else np.zeros(0)
+        out["res"] = np.ctypeslib.as_array(r.res, (m,)).copy() if m and r.res else np.zeros(0)
+        out["mu"] = np.ctypeslib.as_array(r.mu, (info["Mdeg"] + 1,)).copy() if r.mu and "Mdeg" in info else None
+        out["Y"] = None
+        if r.Y and m:
+            Y = np.empty((m, info["n"]))
+            self.lib.evsl_memcpy_device_to_host(Y.ctypes.data, r.Y, Y.nbytes)
+            out["Y"] = Y
+        self.lib.evslx_result_free(C.byref(r))
+        return out
+
+    def free(self):
+        if self.ptr:
+            self.lib.evslx_engine_free(self.ptr)
+        self.ptr = None
 
 
 class Library:
@@ -459,6 +595,35 @@ class Library:
         self._check(self.lib.LanTrbounds(lanm, maxit, tol, dv.ptr, bndtype, C.byref(lo), C.byref(hi), None),
                     "LanTrbounds")
         return lo.value, hi.value
+
+    def chebav_multi(self, pols, X, precision=PREC_FP64):
+        """evslx_chebav_multi: rows of X (ncols x n) filtered by pols[c]."""
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        arr = (PolParams * len(pols))(*pols)
+        dx = DeviceBuffer.from_host(self.lib, X)
+        dy = DeviceBuffer(self.lib, X.nbytes)
+        self._check(self.lib.evslx_chebav_multi(len(pols), arr, dx.ptr, dy.ptr, precision), "evslx_chebav_multi")
+        return dy.to_host().reshape(X.shape)
+
+    def cheblan_nr_batch(self, intvs, maxit, tol, vinit, pols, precision=PREC_FP64, want_vectors=True):
+        """evslx_ChebLanNr_batch: list of (lam, Y, res) per slice."""
+        ns = len(pols)
+        iv = np.ascontiguousarray(np.asarray(intvs, dtype=np.float64).reshape(ns * 4))
+        arr = (PolParams * ns)(*pols)
+        dv = DeviceBuffer.from_host(self.lib, np.asarray(vinit, dtype=np.float64))
+        nev = (C.c_int * ns)()
+        lam = (_dp * ns)()
+        W = (C.c_void_p * ns)()
+        res = (_dp * ns)()
+        rc = self.lib.evslx_ChebLanNr_batch(ns, _d(iv), maxit, tol, dv.ptr, arr, precision, nev, lam, W, res)
+        self._check(rc, "evslx_ChebLanNr_batch")
+        return [self._outputs(nev[s], lam[s], W[s], res[s], want_vectors) for s in range(ns)]
+
+    def matrix(self, ia, ja, a):
+        return Matrix(self.lib, ia, ja, a)
+
+    def engine(self, max_slots, hbm_budget=0, precision=PREC_FP64, keep_vectors=False):
+        return Engine(self.lib, max_slots, hbm_budget, precision, keep_vectors)
 
     def lan_dos(self, nvec, msteps, npts, intv):
         """LanDos: returns (xdos, ydos, neig)."""

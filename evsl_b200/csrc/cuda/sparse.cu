@@ -629,6 +629,7 @@ void evslcu_mat_destroy(evslcu_mat *M) {
   evslcu_free(M->cw);
   evslcu_free(M->scol);
   evslcu_free(M->sval);
+  evslcu_free(M->sval32);
   delete M;
 }
 

@@ -27,6 +27,7 @@ struct evslcu_mat {
   int ifmt = 0;
   void *scol = nullptr;
   void *sval = nullptr;
+  void *sval32 = nullptr;  // FP32 copy of sval for the FP32 filter (when vfmt == 0)
   int kernel = 0;      // 0 SELL-32, 1 CSR (thread per row)
   int persistent = 0;  // 1: single cooperative launch per filter application
 };

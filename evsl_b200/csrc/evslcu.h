@@ -164,6 +164,23 @@ int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const doub
  * n*m doubles of scratch. */
 int evslcu_ritz_eval(const evslcu_op *op, int n, int m, double *U, double *W, double *norm,
                      double *lam, double *res);
+/* Chebyshev filter on many columns at once, each with its own polynomial:
+ * y_c = sum_{k<=deg_c} mu_c[k] T_k((A - cc_c)/dd_c) x_c.  x, y: device FP64
+ * columns; mu: host array of deg+1 coefficients.  fp32 = 0: each column
+ * bitwise equal to evslcu_chebav; fp32 = 1: FP32 values and recurrence
+ * (evslcu_mat_prepare_fp32 first when the values are not floats).  Needs the
+ * SELL-32 storage.  work: evslcu_filter_columns_work bytes of device memory. */
+typedef struct {
+  const double *mu;
+  int deg;
+  double cc, dd;
+  const double *x;
+  double *y;
+} evslcu_filter_col;
+size_t evslcu_filter_columns_work(int n, int fp32, int ncols);
+int evslcu_filter_columns(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_col *cols, void *work,
+                          size_t work_bytes);
+int evslcu_mat_prepare_fp32(evslcu_mat *A);
 /* COO (device arrays, indices base 0 or 1) -> CSR on the device: rows in
  * order, entries of a row sorted by column with ties in input order (the
  * reference's cooMat_to_csrMat + sortrow).  Outputs are new device arrays

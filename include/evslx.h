@@ -138,6 +138,83 @@ int evslx_read_coo_MM(const char *matfile, int idxin, int idxout, cooMat *Acoo);
  * pointers (else host arrays, uploaded).  Ready for SetAMatrix_device_csr. */
 int evslx_coo_to_csr_device(int cooidx, const cooMat *coo, int coo_on_device, csrMat *Agpu);
 
+/* ---------------------------------------------------------------------------
+ * Batched and served slicing (no reference counterpart: the reference solves
+ * one slice per call, SRC/cheblanNr.c:57).
+ *
+ * Resident matrices: evslx_matrix_create uploads a host CSR (on_device = 0)
+ * or borrows a device CSR (on_device = 1) and prepares its SELL-32 copy.
+ *
+ * Engine: a queue of requests -- slice solves (ChebLanNr's algorithm and
+ * outputs) and DOS estimates (kpmdos) -- served with up to max_slots slice
+ * solves in flight.  evslx_engine_step admits queued requests (FIFO) while a
+ * slot is free and the request's device memory fits hbm_budget (0: no
+ * limit), advances every active solve by one Lanczos step (the filters of
+ * all solves on one matrix share one multi-column filter per degree) and
+ * retires finished ones into the result queue; it returns the number of
+ * requests queued or active, or a negative error code.  Results are the
+ * same for a request alone and in any mix.
+ *
+ * precision: EVSLX_PREC_FP64 (filter in FP64) or EVSLX_PREC_MIXED (filter in
+ * FP32; Lanczos, orthogonalisation, Ritz step in FP64; Ritz pairs refined by
+ * FP64 filtered Rayleigh-Ritz sweeps over the candidates plus as many guard
+ * vectors (at least 16) until every pair inside [a, b] meets tol, at most 4
+ * sweeps).
+ * ------------------------------------------------------------------------- */
+#define EVSLX_PREC_FP64 0
+#define EVSLX_PREC_MIXED 1
+#define EVSLX_REQ_SLICE 1
+#define EVSLX_REQ_KPM 2
+
+typedef struct evslx_matrix evslx_matrix;
+typedef struct evslx_engine evslx_engine;
+
+typedef struct {
+  uint64_t tag;        /* the submitter's tag */
+  int kind;            /* EVSLX_REQ_SLICE or EVSLX_REQ_KPM */
+  int rc;              /* 0 or an error code */
+  int nev;             /* slice: eigenpairs found (in [a, b], residual < tol) */
+  double *lam, *res;   /* slice: host arrays of nev (free with evslx_result_free) */
+  double *Y;           /* slice: device n x nev when the engine keeps vectors */
+  double *mu;          /* DOS: host array of Mdeg + 1 moments */
+  double ecnt;         /* DOS: estimated eigenvalue count */
+  int lanczos_steps;   /* slice: Lanczos dimension */
+  int refine_sweeps;   /* slice, mixed precision: FP64 refinement sweeps */
+  double t_submit, t_start, t_finish; /* evsl_timer() seconds */
+} evslx_result;
+
+evslx_matrix *evslx_matrix_create(csrMat *A, int on_device);
+void evslx_matrix_free(evslx_matrix *M);
+long long evslx_matrix_device_bytes(const evslx_matrix *M);
+
+evslx_engine *evslx_engine_create(int max_slots, size_t hbm_budget, int precision, int keep_vectors);
+void evslx_engine_free(evslx_engine *E);
+/* vinit: n doubles, on the device when vinit_on_device (copied at submit). */
+int evslx_engine_submit_slice(evslx_engine *E, evslx_matrix *M, const double *intv, const polparams *pol,
+                              int maxit, double tol, const double *vinit, int vinit_on_device, uint64_t tag);
+/* Probes: the generator's draws 0..nvec-1 of `seed` (kpmdos after
+ * evslx_set_seed(seed) draws the same vectors). */
+int evslx_engine_submit_kpm(evslx_engine *E, evslx_matrix *M, int Mdeg, int damping, int nvec, const double *intv,
+                            uint64_t seed, uint64_t tag);
+int evslx_engine_step(evslx_engine *E);
+int evslx_engine_run(evslx_engine *E); /* step until nothing is queued or active */
+int evslx_engine_pending(const evslx_engine *E);
+size_t evslx_engine_bytes_in_use(const evslx_engine *E);
+int evslx_engine_pop_result(evslx_engine *E, evslx_result *out); /* 1: a result was returned */
+void evslx_result_free(evslx_result *r);
+
+/* Y_c = p_c(A) X_c for ncols columns of the registered CSR matrix, each with
+ * its own polynomial pols[c] (X, Y: device, column-major n x ncols).  FP64:
+ * every column equal to ChebAv bit for bit; MIXED: the FP32 filter. */
+int evslx_chebav_multi(int ncols, const polparams *pols, const double *X, double *Y, int precision);
+
+/* nslices slices of the registered CSR matrix solved together in one engine
+ * (intvs: 4 per slice; pols: one per slice; vinit: device start vector
+ * shared by all).  Outputs per slice as ChebLanNr (lamo/reso host, Wo
+ * device). */
+int evslx_ChebLanNr_batch(int nslices, double *intvs, int maxit, double tol, double *vinit, polparams *pols,
+                          int precision, int *nevOut, double **lamo, double **Wo, double **reso);
+
 /* Size of the registered problem and of the stored matrix. */
 int evslx_problem_info(int *n, long long *nnz, long long *stored_nnz);
 

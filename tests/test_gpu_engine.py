@@ -1,0 +1,241 @@
+"""GPU tests of the multi-column filter, the mixed-precision path and the
+request engine (batched and served slice solves, DOS requests).
+
+Tolerances (written per test):
+  * FP64 multi-column filter: every column bitwise equal to ChebAv;
+  * FP32 multi-column filter: ||y32 - y64|| <= 1e-4 ||y64|| per column;
+  * FP64 engine vs ChebLanNr: counts equal, eigenvalues within 1e-10 x
+    (spectral width), residuals < tol;
+  * mixed precision after FP64 refinement: counts exact against the
+    analytic (or dense) spectrum, eigenvalues within 1e-8 x (spectral
+    width), residuals < tol;
+  * a request alone and in a mix of requests: bitwise equal results;
+  * engine DOS request vs kpmdos with the same generator seed: bitwise.
+"""
+import numpy as np
+import pytest
+
+import evsl_b200 as E
+from evsl_b200 import workloads as W
+from oracle import evsl_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _pols(lib, intvs, **kw):
+    return [lib.find_pol(iv, **kw) for iv in intvs]
+
+
+def test_multi_filter_fp64_bitwise_fp32_close(gpu_lib):
+    cases = [(O.lap_csr(41, 53, 1), 8.0), (O.lap_csr(20, 20, 20), 12.0), (W.random_spd_csr(6000, 16, 2), None)]
+    for (ia, ja, a), hi in cases:
+        gpu_lib.set_csr(ia, ja, a)
+        n = len(ia) - 1
+        if hi is None:
+            lo_b, hi_b = W.gershgorin_bounds(ia, ja, a)
+            lo_b = max(lo_b, 0.0)
+        else:
+            lo_b, hi_b = 0.0, hi
+        w = hi_b - lo_b
+        intvs = [[lo_b + f0 * w, lo_b + f1 * w, lo_b, hi_b] for f0, f1 in
+                 ((0.05, 0.1), (0.2, 0.22), (0.3, 0.5), (0.6, 0.61), (0.0, 0.03), (0.9, 1.0))]
+        pols = _pols(gpu_lib, intvs, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=400)
+        X = O.seeded_normal(n * len(pols), 4).reshape(len(pols), n)
+        Y64 = gpu_lib.chebav_multi(pols, X, E.PREC_FP64)
+        Y32 = gpu_lib.chebav_multi(pols, X, E.PREC_MIXED)
+        for c, pol in enumerate(pols):
+            ref = gpu_lib.chebav(pol, X[c])
+            assert np.array_equal(Y64[c], ref)
+            assert np.linalg.norm(Y32[c] - ref) <= 1e-4 * np.linalg.norm(ref)
+        for p in pols:
+            gpu_lib.free_pol(p)
+
+
+def _lap_slices(ev, starts, count):
+    out = []
+    for s in starts:
+        a, b, cnt = W.gap_interval(ev, s, count)
+        out.append(([a, b], cnt))
+    return out
+
+
+def test_engine_fp64_matches_cheblan_nr(gpu_lib):
+    ia, ja, a = O.lap_csr(100, 100, 1)
+    gpu_lib.set_csr(ia, ja, a)
+    ev = W.laplacian_eigenvalues(100, 100, 1)
+    sl = _lap_slices(ev, (0.6, 0.75, 0.9), 40)
+    intvs = [[x[0][0], x[0][1], 0.0, 8.0] for x in sl]
+    pols = _pols(gpu_lib, intvs)
+    v = O.seeded_normal(10000, 1234)
+    batch = gpu_lib.cheblan_nr_batch(intvs, 2000, 1e-8, v, pols, E.PREC_FP64)
+    for s, (lam_b, Y_b, res_b) in enumerate(batch):
+        lam, Y, res = gpu_lib.cheblan_nr(intvs[s], 2000, 1e-8, v, pols[s], want_vectors=False)
+        exact = ev[(ev >= intvs[s][0]) & (ev <= intvs[s][1])]
+        assert len(lam_b) == len(lam) == len(exact) == sl[s][1]
+        assert np.max(np.abs(np.sort(lam_b) - np.sort(lam))) <= 1e-10 * 8.0
+        assert np.all(res_b < 1e-8)
+        G = Y_b @ Y_b.T
+        assert np.max(np.abs(G - np.eye(len(lam_b)))) < 1e-8
+    for p in pols:
+        gpu_lib.free_pol(p)
+
+
+def test_engine_mixed_precision_accuracy(gpu_lib):
+    """3-D Laplacian 30^3: FP32 filter + FP64 refinement meets tol 1e-8."""
+    ia, ja, a = O.lap_csr(30, 30, 30)
+    gpu_lib.set_csr(ia, ja, a)
+    ev = W.laplacian_eigenvalues(30, 30, 30)
+    sl = _lap_slices(ev, (0.6, 1.0), 50)
+    intvs = [[x[0][0], x[0][1], 0.0, 12.0] for x in sl]
+    pols = _pols(gpu_lib, intvs)
+    v = O.seeded_normal(27000, 9)
+    batch = gpu_lib.cheblan_nr_batch(intvs, 1500, 1e-8, v, pols, E.PREC_MIXED)
+    for s, (lam, Y, res) in enumerate(batch):
+        exact = ev[(ev >= intvs[s][0]) & (ev <= intvs[s][1])]
+        assert len(lam) == len(exact) == sl[s][1]
+        assert np.max(np.abs(np.sort(lam) - exact)) <= 1e-8 * 12.0
+        assert np.all(res < 1e-8)
+    for p in pols:
+        gpu_lib.free_pol(p)
+
+
+@pytest.mark.parametrize("precision", [E.PREC_FP64, E.PREC_MIXED])
+def test_engine_request_same_alone_and_in_mix(gpu_lib, precision):
+    ia, ja, a = O.lap_csr(60, 60, 1)
+    ia2, ja2, a2 = O.lap_csr(18, 17, 16)
+    ev = W.laplacian_eigenvalues(60, 60, 1)
+    ev2 = W.laplacian_eigenvalues(18, 17, 16)
+    gpu_lib.set_csr(ia, ja, a)
+    M1 = gpu_lib.matrix(ia, ja, a)
+    M2 = gpu_lib.matrix(ia2, ja2, a2)
+    (i1, c1), (i2, c2) = _lap_slices(ev, (0.5, 1.1), 30)
+    (i3, c3), = _lap_slices(ev2, (0.8,), 25)
+    iv1, iv2, iv3 = [i1[0], i1[1], 0.0, 8.0], [i2[0], i2[1], 0.0, 8.0], [i3[0], i3[1], 0.0, 12.0]
+    p1, p2, p3 = gpu_lib.find_pol(iv1), gpu_lib.find_pol(iv2), gpu_lib.find_pol(iv3)
+    v1 = O.seeded_normal(3600, 1)
+    v3 = O.seeded_normal(len(ia2) - 1, 3)
+
+    eng = gpu_lib.engine(4, precision=precision)
+    eng.submit_slice(M1, iv1, p1, 1000, 1e-8, v1, 7)
+    eng.run()
+    alone = eng.pop()
+    eng.free()
+
+    eng = gpu_lib.engine(4, precision=precision)
+    eng.submit_slice(M1, iv2, p2, 1000, 1e-8, v1, 1)
+    eng.submit_kpm(M2, 60, 1, 8, iv3, 5, 2)
+    eng.submit_slice(M2, iv3, p3, 1000, 1e-8, v3, 3)
+    eng.step()
+    eng.step()
+    eng.submit_slice(M1, iv1, p1, 1000, 1e-8, v1, 7)  # joins while the others run
+    eng.run()
+    got = {}
+    while True:
+        r = eng.pop()
+        if r is None:
+            break
+        got[r["tag"]] = r
+    eng.free()
+    mixed = got[7]
+    assert alone["rc"] == 0 and mixed["rc"] == 0
+    assert alone["nev"] == mixed["nev"] == c1
+    assert np.array_equal(alone["lam"], mixed["lam"]) and np.array_equal(alone["res"], mixed["res"])
+    assert got[1]["nev"] == c2 and got[3]["nev"] == c3
+    for r in (got[1], got[3], mixed):
+        assert np.all(r["res"] < 1e-8)
+    M1.free()
+    M2.free()
+    for p in (p1, p2, p3):
+        gpu_lib.free_pol(p)
+
+
+def test_engine_kpm_equals_kpmdos(gpu_lib):
+    ia, ja, a = O.lap_csr(30, 30, 12)
+    gpu_lib.set_csr(ia, ja, a)
+    M = gpu_lib.matrix(ia, ja, a)
+    iv = [0.6, 2.0, 0.0, 12.0]
+    eng = gpu_lib.engine(2)
+    eng.submit_kpm(M, 80, 1, 70, iv, 1234, 11)
+    eng.run()
+    r = eng.pop()
+    eng.free()
+    gpu_lib.set_seed(1234)
+    mu, ec = gpu_lib.kpmdos(80, 1, 70, iv)
+    assert r["rc"] == 0 and np.array_equal(r["mu"], mu) and r["ecnt"] == ec
+    M.free()
+
+
+def test_engine_hbm_budget_admission(gpu_lib):
+    ia, ja, a = O.lap_csr(50, 50, 1)
+    gpu_lib.set_csr(ia, ja, a)
+    M = gpu_lib.matrix(ia, ja, a)
+    ev = W.laplacian_eigenvalues(50, 50, 1)
+    sl = _lap_slices(ev, (0.5, 0.9, 1.3), 20)
+    intvs = [[x[0][0], x[0][1], 0.0, 8.0] for x in sl]
+    pols = _pols(gpu_lib, intvs)
+    v = O.seeded_normal(2500, 2)
+    maxit = 600
+    # device bytes the engine reserves for one request (basis, start and
+    # restart vectors, Gram-Schmidt workspace); the budget admits one at a time
+    req = 8 * (2500 * (maxit + 3) + ((2500 + 1023) // 1024) * (maxit + 1) + (maxit + 1) + 8)
+    one = int(1.5 * req)
+    results = []
+    for budget in (0, one):
+        eng = gpu_lib.engine(3, hbm_budget=budget)
+        for s, iv in enumerate(intvs):
+            eng.submit_slice(M, iv, pols[s], maxit, 1e-8, v, s)
+        peak = 0
+        while eng.step() > 0:
+            peak = max(peak, eng.bytes_in_use())
+            if budget:
+                assert eng.bytes_in_use() <= budget
+        out = {}
+        while True:
+            r = eng.pop()
+            if r is None:
+                break
+            out[r["tag"]] = r
+        results.append(out)
+        eng.free()
+        if budget:
+            assert req <= peak <= budget
+    for s in range(3):
+        assert results[0][s]["nev"] == results[1][s]["nev"] == sl[s][1]
+        assert np.array_equal(results[0][s]["lam"], results[1][s]["lam"])
+    # a request larger than the whole budget fails instead of blocking
+    eng = gpu_lib.engine(2, hbm_budget=1 << 20)
+    eng.submit_slice(M, intvs[0], pols[0], maxit, 1e-8, v, 99)
+    eng.run()
+    r = eng.pop()
+    assert r["tag"] == 99 and r["rc"] != 0
+    eng.free()
+    M.free()
+    for p in pols:
+        gpu_lib.free_pol(p)
+
+
+def test_mixed_precision_random_spd(gpu_lib):
+    """The random sparse SPD family of the mixed-precision workload at a size
+    the dense solver checks: a slice of ~30 eigenvalues in the lower
+    interior, FP32 filter + FP64 refinement."""
+    n = 4000
+    ia, ja, a = W.random_spd_csr(n, 16, 21)
+    gpu_lib.set_csr(ia, ja, a)
+    M = np.zeros((n, n))
+    for i in range(n):
+        M[i, ja[ia[i]:ia[i + 1]]] = a[ia[i]:ia[i + 1]]
+    ev = np.linalg.eigvalsh(M)
+    v = O.seeded_normal(n, 5)
+    lo, hi = gpu_lib.lan_trbounds(50, 200, 1e-8, v, 1)
+    a0, b0, cnt = W.gap_interval(ev, ev[n // 4], 30)
+    iv = [a0, b0, lo, hi]
+    pol = gpu_lib.find_pol(iv)
+    (lam64, _, res64), = gpu_lib.cheblan_nr_batch([iv], 2000, 1e-8, v, [pol], E.PREC_FP64, want_vectors=False)
+    (lam32, _, res32), = gpu_lib.cheblan_nr_batch([iv], 2000, 1e-8, v, [pol], E.PREC_MIXED, want_vectors=False)
+    exact = ev[(ev >= a0) & (ev <= b0)]
+    width = hi - lo
+    assert len(lam64) == len(lam32) == len(exact) == cnt
+    assert np.max(np.abs(np.sort(lam64) - exact)) <= 1e-10 * width
+    assert np.max(np.abs(np.sort(lam32) - exact)) <= 1e-8 * width
+    assert np.all(res64 < 1e-8) and np.all(res32 < 1e-8)
+    gpu_lib.free_pol(pol)
