@@ -53,8 +53,18 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--count", type=int, default=COUNT)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter"], default="lap3d-slice",
-                   help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark)")
+    p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve"],
+                   default="lap3d-slice",
+                   help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark); "
+                        "lap3d-batch: several slices through the request engine; serve: a Poisson request stream")
+    p.add_argument("--slices", type=int, default=4, help="lap3d-batch: slices solved together")
+    p.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
+                   help="lap3d-batch / serve: filter precision of the engine")
+    p.add_argument("--rate", type=float, default=2.0, help="serve: mean arrivals per second")
+    p.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
+    p.add_argument("--slots", type=int, default=16, help="serve: slice solves in flight")
+    p.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM budget of the engine")
+    p.add_argument("--max-count", type=int, default=150, help="serve: most eigenvalues in a slice request")
     return p.parse_args()
 
 
@@ -469,12 +479,231 @@ def run_filter(args):
     lib.free_pol(pol)
 
 
+def _slice_plan(ev, start, nslices, count):
+    """Consecutive gap-midpoint intervals of `count` eigenvalues from `start`."""
+    from evsl_b200 import workloads as W
+
+    out, lo = [], start
+    for _ in range(nslices):
+        a0, b0, c = W.gap_interval(ev, lo, count)
+        out.append(([a0, b0, LMIN, LMAX], c))
+        lo = b0 + 1e-12
+    return out
+
+
+def run_batch(args):
+    """lap3d-batch: `--slices` slices of `--count` eigenvalues above 0.6 on the
+    3-D Laplacian 100^3 solved together by the request engine (one Lanczos
+    step per tick for every slice, the filters of all slices sharing one
+    multi-column launch per degree, captured as CUDA graphs), in FP64 or
+    mixed precision (FP32 filter, FP64 Lanczos/orthogonalisation/Ritz, FP64
+    refinement).  One step = the whole batch; checks exact counts and
+    residuals <= tol."""
+    import torch
+
+    import evsl_b200 as E
+    from evsl_b200 import workloads as W
+
+    lib = E.Library()
+    ia, ja, a = W.laplacian_csr(NX, NY, NZ)
+    ev = W.laplacian_eigenvalues(NX, NY, NZ)
+    lib.set_csr(ia, ja, a)
+    M = lib.matrix(ia, ja, a)
+    plan = _slice_plan(ev, 0.6, args.slices, args.count)
+    pols = [lib.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000) for iv, _ in plan]
+    prec = E.PREC_MIXED if args.precision == "mixed" else E.PREC_FP64
+    n = NX * NY * NZ
+    v0 = np.random.default_rng(SEED).standard_normal(n)
+    v0 /= np.linalg.norm(v0)
+    lstream = torch.cuda.ExternalStream(lib.stream_handle())
+
+    def one_batch():
+        eng = lib.engine(args.slices, precision=prec)
+        for s, (iv, _) in enumerate(plan):
+            eng.submit_slice(M, iv, pols[s], MAXIT, TOL, v0, s)
+        eng.run()
+        out = {}
+        while True:
+            r = eng.pop()
+            if r is None:
+                break
+            out[int(r["tag"])] = r
+        eng.free()
+        return out
+
+    for _ in range(args.warmup):
+        one_batch()
+    sampler = ClockSampler(rank_info()[2])
+    sampler.start()
+    launches0 = lib.launch_count()
+    times, found, ok, lat = [], 0, True, []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lstream)
+        res = one_batch()
+        e1.record(lstream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+        for s, (iv, cnt) in enumerate(plan):
+            r = res[s]
+            exact = ev[(ev >= iv[0]) & (ev <= iv[1])]
+            good = r["rc"] == 0 and r["nev"] == cnt == len(exact) and bool(np.all(r["res"] < TOL))
+            if good:
+                good = float(np.max(np.abs(np.sort(r["lam"]) - exact))) <= 1e-8 * (LMAX - LMIN)
+            ok = ok and good
+            found += r["nev"]
+            lat.append(1e3 * (r["t_finish"] - r["t_submit"]))
+    launches = lib.launch_count() - launches0
+    clocks = sampler.stop()
+    t = sum(times)
+    print(json.dumps({
+        "metric": METRIC, "value": found / t, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 filter + f64" if prec == E.PREC_MIXED else "f64",
+        "data": "synthetic (3-D Dirichlet Laplacian, seeded start vector)",
+        "config": {"workload": "lap3d-batch: %d slices of %d eigenvalues above 0.6 on the 3-D Laplacian 100^3, "
+                               "solved together by the request engine, %s" % (args.slices, args.count,
+                                                                              args.precision),
+                   "filter_degrees": [int(p.deg) for p in pols], "tol": TOL, "maxit": MAXIT},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "all_steps_ok": bool(ok), "gpu_launches": int(launches), "clocks": clocks}))
+    for p in pols:
+        lib.free_pol(p)
+    M.free()
+
+
+def run_serve(args):
+    """serve: a seeded Poisson stream of requests at `--rate` per second for
+    `--duration` seconds, served by the request engine under an HBM budget:
+    50% slice solves (2-D 100x100 or 3-D 100^3 Laplacian, a random interval
+    of 10-`--max-count` eigenvalues with end points at gap midpoints), 30%
+    DOS estimates (kpmdos, 100-500 moments, 8-64 probes), 20% slice solves
+    on small 2-D/3-D Laplacians (n log-uniform in [1e3, 2e5], 20-80
+    eigenvalues).  Matrices stay resident.  Latency = submit to result
+    (host clock of the engine); value = eigenpairs delivered per second of
+    the run; every slice result is checked against the analytic spectrum."""
+    import evsl_b200 as E
+    from evsl_b200 import workloads as W
+
+    lib = E.Library()
+    rng = np.random.default_rng(SEED)
+    prec = E.PREC_MIXED if args.precision == "mixed" else E.PREC_FP64
+    mats = {}
+
+    def matrix(dims):
+        if dims not in mats:
+            ia, ja, a = W.laplacian_csr(*dims)
+            mats[dims] = (lib.matrix(ia, ja, a), np.sort(W.laplacian_eigenvalues(*dims)))
+        return mats[dims]
+
+    big = [(100, 100, 1), (NX, NY, NZ)]
+    for d in big:
+        matrix(d)
+    # the arrival schedule and the requests, all drawn before the run
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=int(args.rate * args.duration * 2) + 8))
+    arrivals = arrivals[arrivals < args.duration]
+    reqs = []
+    for t in arrivals:
+        u = rng.random()
+        if u < 0.5 or u >= 0.8:
+            if u < 0.5:
+                dims = big[rng.integers(0, 2)]
+                cnt = int(rng.integers(10, args.max_count + 1))
+            else:
+                nn = int(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
+                if rng.random() < 0.5:
+                    s = max(int(round(np.sqrt(nn))), 8)
+                    dims = (s, s + int(rng.integers(0, 5)), 1)
+                else:
+                    s = max(int(round(nn ** (1 / 3))), 6)
+                    dims = (s, s + int(rng.integers(0, 3)), s)
+                cnt = int(rng.integers(20, 81))
+            Mx, ev = matrix(dims)
+            lo = float(rng.uniform(0.2, 1.5))
+            a0, b0, c = W.gap_interval(ev, lo, cnt)
+            hi_b = 8.0 if dims[2] == 1 else 12.0
+            reqs.append(("slice", t, dims, [a0, b0, 0.0, hi_b], c))
+        else:
+            dims = big[rng.integers(0, 2)]
+            hi_b = 8.0 if dims[2] == 1 else 12.0
+            reqs.append(("kpm", t, dims, [0.5, 1.5, 0.0, hi_b], (int(rng.integers(100, 501)),
+                                                                  int(rng.integers(8, 65)))))
+    eng = lib.engine(args.slots, hbm_budget=int(args.budget_gb * 1e9), precision=prec)
+    pols = {}
+    n_h2d = 0
+    import time as _t
+
+    t0 = _t.perf_counter()
+    i, done, lat, lat_slice, found, ok = 0, 0, [], [], 0, True
+    while i < len(reqs) or eng.pending() > 0:
+        now = _t.perf_counter() - t0
+        while i < len(reqs) and reqs[i][1] <= now:
+            kind, _, dims, iv, extra = reqs[i]
+            Mx, ev = matrix(dims)
+            if kind == "slice":
+                pol = lib.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+                pols[i] = pol
+                v = np.random.default_rng(SEED + i).standard_normal(Mx.n)
+                eng.submit_slice(Mx, iv, pol, MAXIT, TOL, v / np.linalg.norm(v), i)
+                n_h2d += 8 * Mx.n
+            else:
+                eng.submit_kpm(Mx, extra[0], 1, extra[1], iv, SEED + i, i)
+            i += 1
+        if eng.pending() > 0:
+            eng.step()
+        elif i < len(reqs):
+            _t.sleep(max(0.0, min(0.05, reqs[i][1] - (_t.perf_counter() - t0))))
+        while True:
+            r = eng.pop()
+            if r is None:
+                break
+            k = int(r["tag"])
+            kind, t_arr, dims, iv, extra = reqs[k]
+            ms = 1e3 * (r["t_finish"] - r["t_submit"])
+            lat.append(ms)
+            done += 1
+            if kind == "slice":
+                lat_slice.append(ms)
+                Mx, ev = matrix(dims)
+                exact = ev[(ev >= iv[0]) & (ev <= iv[1])]
+                good = r["rc"] == 0 and r["nev"] == len(exact) and bool(np.all(r["res"] < TOL))
+                ok = ok and good
+                found += r["nev"]
+                lib.free_pol(pols.pop(k))
+            else:
+                ok = ok and r["rc"] == 0
+    wall = _t.perf_counter() - t0
+    eng.free()
+    for Mx, _ in mats.values():
+        Mx.free()
+    print(json.dumps({
+        "metric": METRIC, "value": found / wall, "unit": UNIT, "n_gpus": 1, "steps": len(reqs), "warmup": 0,
+        "ms_per_step": 1e3 * wall / max(len(reqs), 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 filter + f64" if prec == E.PREC_MIXED else "f64",
+        "data": "synthetic (seeded Poisson request stream over Dirichlet Laplacians)",
+        "config": {"workload": "serve: Poisson %.2f req/s for %.0f s, %d slots, HBM budget %.0f GB, %s" % (
+            args.rate, args.duration, args.slots, args.budget_gb, args.precision),
+                   "requests": len(reqs), "completed": done},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)) if lat else None,
+                       "p99": float(np.percentile(lat, 99)) if lat else None,
+                       "slice_p50": float(np.percentile(lat_slice, 50)) if lat_slice else None,
+                       "slice_p99": float(np.percentile(lat_slice, 99)) if lat_slice else None},
+        "e2e": {"value": found / wall, "unit": UNIT, "h2d_bytes_per_step": n_h2d / max(len(reqs), 1),
+                "d2h_bytes_per_step": 16 * found / max(len(reqs), 1)},
+        "all_ok": bool(ok)}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "lap3d-filter":
         run_filter(args)
+    elif args.workload == "lap3d-batch":
+        run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

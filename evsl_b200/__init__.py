@@ -290,6 +290,8 @@ def load():
         "evslx_engine_bytes_in_use": ([C.c_void_p], C.c_size_t),
         "evslx_engine_pop_result": ([C.c_void_p, C.POINTER(EvslxResult)], C.c_int),
         "evslx_result_free": ([C.POINTER(EvslxResult)], None),
+        "evslx_engine_use_graphs": ([C.c_void_p, C.c_int], None),
+        "evslx_engine_plan_builds": ([C.c_void_p], C.c_uint64),
         "evslx_chebav_multi": ([C.c_int, C.POINTER(PolParams), C.c_void_p, C.c_void_p, C.c_int], C.c_int),
         "evslx_ChebLanNr_batch": ([C.c_int, _dp, C.c_int, C.c_double, C.c_void_p, C.POINTER(PolParams), C.c_int,
                                    _ip, C.POINTER(_dp), C.POINTER(C.c_void_p), C.POINTER(_dp)], C.c_int),
@@ -401,6 +403,12 @@ class Engine:
 
     def bytes_in_use(self):
         return self.lib.evslx_engine_bytes_in_use(self.ptr)
+
+    def use_graphs(self, on):
+        self.lib.evslx_engine_use_graphs(self.ptr, 1 if on else 0)
+
+    def plan_builds(self):
+        return self.lib.evslx_engine_plan_builds(self.ptr)
 
     def pop(self):
         """Next result as a dict (None if the result queue is empty)."""

@@ -181,6 +181,15 @@ size_t evslcu_filter_columns_work(int n, int fp32, int ncols);
 int evslcu_filter_columns(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_col *cols, void *work,
                           size_t work_bytes);
 int evslcu_mat_prepare_fp32(evslcu_mat *A);
+/* The same filter captured once as a CUDA graph for a fixed set of
+ * polynomials (cols[].x/.y ignored) and replayed on any columns:
+ * plan_run(x[ncols], y[ncols]) (host arrays of device pointers). */
+typedef struct evslcu_filter_plan evslcu_filter_plan;
+evslcu_filter_plan *evslcu_filter_plan_create(const evslcu_mat *A, int fp32, int ncols,
+                                              const evslcu_filter_col *cols);
+int evslcu_filter_plan_run(evslcu_filter_plan *P, const double *const *x, double *const *y);
+int evslcu_filter_plan_columns(const evslcu_filter_plan *P);
+void evslcu_filter_plan_destroy(evslcu_filter_plan *P);
 /* COO (device arrays, indices base 0 or 1) -> CSR on the device: rows in
  * order, entries of a row sorted by column with ties in input order (the
  * reference's cooMat_to_csrMat + sortrow).  Outputs are new device arrays

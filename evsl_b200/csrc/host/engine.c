@@ -66,8 +66,18 @@ typedef struct req_s {
   int Mdeg, damping, nvec;
   double t_submit;
   size_t bytes;
+  uint64_t uid; /* unique for the engine's lifetime */
   struct req_s *next;
 } req_t;
+
+/* A captured filter (CUDA graph) for the slots of one matrix, valid while
+ * the same requests occupy them in the same order. */
+typedef struct {
+  evslx_matrix *M;
+  int ncols, used;
+  uint64_t *uids;
+  evslcu_filter_plan *plan;
+} plan_cache_t;
 
 typedef struct {
   req_t *req;
@@ -92,7 +102,14 @@ struct evslx_engine {
   size_t fwork_bytes;
   evslcu_filter_col *cols;
   int *colslot;
-  uint64_t ticks;
+  const double **xs;
+  double **ys;
+  uint64_t *uidbuf;
+  plan_cache_t *plans;
+  int nplans;
+  uint64_t next_uid;
+  int use_graphs;
+  uint64_t ticks, plan_builds;
 };
 
 /* ---------------------------------------------------------------------------
@@ -159,7 +176,12 @@ evslx_engine *evslx_engine_create(int max_slots, size_t hbm_budget, int precisio
   E->hs = (double *)malloc(sizeof(double) * ENG_NSCAL * (size_t)max_slots);
   E->cols = (evslcu_filter_col *)malloc(sizeof(evslcu_filter_col) * (size_t)max_slots);
   E->colslot = (int *)malloc(sizeof(int) * (size_t)max_slots);
-  if (!E->slots || !E->ds || !E->hs || !E->cols || !E->colslot) {
+  E->xs = (const double **)malloc(sizeof(double *) * (size_t)max_slots);
+  E->ys = (double **)malloc(sizeof(double *) * (size_t)max_slots);
+  E->uidbuf = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)max_slots);
+  E->plans = (plan_cache_t *)calloc((size_t)max_slots, sizeof(plan_cache_t));
+  E->use_graphs = 1;
+  if (!E->slots || !E->ds || !E->hs || !E->cols || !E->colslot || !E->xs || !E->ys || !E->uidbuf || !E->plans) {
     evsl_seterr(EVSLX_ERR_NOMEM, "evslx_engine_create: out of memory");
     evslx_engine_free(E);
     return NULL;
@@ -213,9 +235,71 @@ void evslx_engine_free(evslx_engine *E) {
   evslcu_free(E->ds);
   free(E->hs);
   evslcu_free(E->fwork);
+  for (int i = 0; i < E->nplans; i++) {
+    evslcu_filter_plan_destroy(E->plans[i].plan);
+    free(E->plans[i].uids);
+  }
+  free(E->plans);
   free(E->cols);
   free(E->colslot);
+  free(E->xs);
+  free(E->ys);
+  free(E->uidbuf);
   free(E);
+}
+
+void evslx_engine_use_graphs(evslx_engine *E, int on) {
+  if (E) E->use_graphs = on ? 1 : 0;
+}
+
+uint64_t evslx_engine_plan_builds(const evslx_engine *E) { return E ? E->plan_builds : 0; }
+
+/* Runs the filters of the nc columns cols (all on M, request ids uids)
+ * through a cached graph when the same requests were filtered together
+ * before, else captures one (or, with graphs off, launches directly). */
+static int run_group_filter(evslx_engine *E, evslx_matrix *M, int nc, const evslcu_filter_col *cols,
+                            const uint64_t *uids, int fp32) {
+  if (E->use_graphs) {
+    plan_cache_t *pc = NULL;
+    for (int i = 0; i < E->nplans && !pc; i++)
+      if (E->plans[i].M == M && E->plans[i].ncols == nc && !memcmp(E->plans[i].uids, uids, sizeof(uint64_t) * nc))
+        pc = &E->plans[i];
+    if (!pc && E->nplans < E->max_slots) {
+      pc = &E->plans[E->nplans];
+      pc->uids = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)E->max_slots);
+      if (!pc->uids) return evsl_seterr(EVSLX_ERR_NOMEM, "engine: out of memory");
+      pc->plan = evslcu_filter_plan_create(M->mat, fp32, nc, cols);
+      E->plan_builds++;
+      if (!pc->plan) {
+        free(pc->uids);
+        pc->uids = NULL;
+        pc = NULL;
+      } else {
+        pc->M = M;
+        pc->ncols = nc;
+        memcpy(pc->uids, uids, sizeof(uint64_t) * (size_t)nc);
+        E->nplans++;
+      }
+    }
+    if (pc) {
+      pc->used = 1;
+      for (int c = 0; c < nc; c++) {
+        E->xs[c] = cols[c].x;
+        E->ys[c] = cols[c].y;
+      }
+      int rc = evslcu_filter_plan_run(pc->plan, E->xs, E->ys);
+      return rc ? evsl_seterr(rc, "%s", evslcu_errstr()) : 0;
+    }
+  }
+  const size_t need = evslcu_filter_columns_work(M->op.n, fp32, nc);
+  if (need > E->fwork_bytes) {
+    evslcu_free(E->fwork);
+    E->fwork = evslcu_malloc(need);
+    E->fwork_bytes = E->fwork ? need : 0;
+    if (!E->fwork) return evsl_seterr(EVSLX_ERR_NOMEM, "engine: out of device memory (filter work)");
+  }
+  int rc = evslcu_filter_columns(M->mat, fp32, nc, cols, E->fwork, E->fwork_bytes);
+  return rc ? evsl_seterr(rc, "%s", evslcu_errstr()) : 0;
 }
 
 static int push_result(evslx_engine *E, evslx_result *r) {
@@ -286,6 +370,7 @@ int evslx_engine_submit_slice(evslx_engine *E, evslx_matrix *M, const double *in
   }
   r->bytes = sizeof(double) * ((size_t)n * ((size_t)r->maxit + 3) + evslcu_cgs_work_size(n, r->maxit + 1));
   r->t_submit = evsl_timer();
+  r->uid = ++E->next_uid;
   enqueue(E, r);
   return 0;
 }
@@ -306,6 +391,7 @@ int evslx_engine_submit_kpm(evslx_engine *E, evslx_matrix *M, int Mdeg, int damp
   r->seed = seed;
   r->bytes = sizeof(double) * 4 * (size_t)M->op.n * (size_t)evsl_min(nvec, 64);
   r->t_submit = evsl_timer();
+  r->uid = ++E->next_uid;
   enqueue(E, r);
   return 0;
 }
@@ -629,12 +715,17 @@ int evslx_engine_step(evslx_engine *E) {
   if (rc) return rc;
   if (E->nactive == 0) return evslx_engine_pending(E);
   const int fp32 = (E->precision == EVSLX_PREC_MIXED);
-  /* 1. filters, one multi-column launch sequence per matrix */
+  /* 1. filters: the active slots of each matrix, in order of decreasing
+   * degree, are cut into groups of at most 16 columns whose degrees are at
+   * least half the group's first (a group runs to its largest degree; one
+   * step on B columns costs far less than B single steps);
+   * each group is one captured multi-column filter. */
+  for (int i = 0; i < E->nplans; i++) E->plans[i].used = 0;
   for (int i = 0; i < E->max_slots; i++) E->colslot[i] = -1;
   for (int i = 0; i < E->max_slots; i++) {
-    slot_t *s = &E->slots[i];
-    if (!s->req || E->colslot[i] >= 0) continue;
-    evslx_matrix *M = s->req->M;
+    slot_t *s0 = &E->slots[i];
+    if (!s0->req || E->colslot[i] >= 0) continue;
+    evslx_matrix *M = s0->req->M;
     int nc = 0;
     for (int j = i; j < E->max_slots; j++) {
       slot_t *t = &E->slots[j];
@@ -656,19 +747,41 @@ int evslx_engine_step(evslx_engine *E) {
         c->x = t->V + (size_t)t->k * n_l;
         c->y = t->V + (size_t)(t->k + 1) * n_l;
       }
+      E->uidbuf[nc] = t->req->uid;
       E->colslot[j] = nc++;
     }
-    if (fp32 && (rc = evslcu_mat_prepare_fp32(M->mat))) return evsl_seterr(rc, "%s", evslcu_errstr());
-    const size_t need = evslcu_filter_columns_work(M->op.n, fp32, nc);
-    if (need > E->fwork_bytes) {
-      evslcu_free(E->fwork);
-      E->fwork = evslcu_malloc(need);
-      E->fwork_bytes = E->fwork ? need : 0;
-      if (!E->fwork) return evsl_seterr(EVSLX_ERR_NOMEM, "engine: out of device memory (filter work)");
+    /* order by decreasing degree (stable, insertion sort on the small set) */
+    for (int a2 = 1; a2 < nc; a2++) {
+      evslcu_filter_col cv = E->cols[a2];
+      const uint64_t uv = E->uidbuf[a2];
+      int b2 = a2 - 1;
+      while (b2 >= 0 && E->cols[b2].deg < cv.deg) {
+        E->cols[b2 + 1] = E->cols[b2];
+        E->uidbuf[b2 + 1] = E->uidbuf[b2];
+        b2--;
+      }
+      E->cols[b2 + 1] = cv;
+      E->uidbuf[b2 + 1] = uv;
     }
-    if ((rc = evslcu_filter_columns(M->mat, fp32, nc, E->cols, E->fwork, E->fwork_bytes)))
-      return evsl_seterr(rc, "%s", evslcu_errstr());
+    if (fp32 && (rc = evslcu_mat_prepare_fp32(M->mat))) return evsl_seterr(rc, "%s", evslcu_errstr());
+    for (int g0 = 0; g0 < nc;) {
+      int g1 = g0 + 1;
+      while (g1 < nc && g1 - g0 < 16 && 2 * E->cols[g1].deg >= E->cols[g0].deg) g1++;
+      if ((rc = run_group_filter(E, M, g1 - g0, E->cols + g0, E->uidbuf + g0, fp32))) return rc;
+      g0 = g1;
+    }
     evslstat.n_polAv += nc;
+  }
+  /* drop the captured filters no group used in this tick */
+  for (int i = 0; i < E->nplans;) {
+    if (E->plans[i].used) {
+      i++;
+      continue;
+    }
+    evslcu_filter_plan_destroy(E->plans[i].plan);
+    free(E->plans[i].uids);
+    E->plans[i] = E->plans[--E->nplans];
+    memset(&E->plans[E->nplans], 0, sizeof(plan_cache_t));
   }
   /* 2. device part of the Lanczos step */
   for (int i = 0; i < E->max_slots; i++) {

@@ -197,6 +197,10 @@ int evslx_engine_submit_slice(evslx_engine *E, evslx_matrix *M, const double *in
 int evslx_engine_submit_kpm(evslx_engine *E, evslx_matrix *M, int Mdeg, int damping, int nvec, const double *intv,
                             uint64_t seed, uint64_t tag);
 int evslx_engine_step(evslx_engine *E);
+/* Filters run as captured CUDA graphs, rebuilt when the set of requests on
+ * a matrix changes (default on); plan_builds counts the captures. */
+void evslx_engine_use_graphs(evslx_engine *E, int on);
+uint64_t evslx_engine_plan_builds(const evslx_engine *E);
 int evslx_engine_run(evslx_engine *E); /* step until nothing is queued or active */
 int evslx_engine_pending(const evslx_engine *E);
 size_t evslx_engine_bytes_in_use(const evslx_engine *E);

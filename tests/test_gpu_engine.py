@@ -119,7 +119,16 @@ def test_engine_request_same_alone_and_in_mix(gpu_lib, precision):
     eng.submit_slice(M1, iv1, p1, 1000, 1e-8, v1, 7)
     eng.run()
     alone = eng.pop()
+    assert eng.plan_builds() >= 1
     eng.free()
+    # the same request with the filters launched directly (no captured graphs)
+    eng = gpu_lib.engine(4, precision=precision)
+    eng.use_graphs(False)
+    eng.submit_slice(M1, iv1, p1, 1000, 1e-8, v1, 7)
+    eng.run()
+    direct = eng.pop()
+    eng.free()
+    assert np.array_equal(alone["lam"], direct["lam"]) and np.array_equal(alone["res"], direct["res"])
 
     eng = gpu_lib.engine(4, precision=precision)
     eng.submit_slice(M1, iv2, p2, 1000, 1e-8, v1, 1)
