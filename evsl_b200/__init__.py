@@ -291,6 +291,9 @@ def load():
         "evslx_engine_pop_result": ([C.c_void_p, C.POINTER(EvslxResult)], C.c_int),
         "evslx_result_free": ([C.POINTER(EvslxResult)], None),
         "evslx_engine_use_graphs": ([C.c_void_p, C.c_int], None),
+        "evslx_set_filter_variant": ([C.c_int], C.c_int),
+        "evslx_get_filter_variant": ([], C.c_int),
+        "evslx_tuned_filter_variant": ([C.c_int, C.c_int], C.c_int),
         "evslx_engine_plan_builds": ([C.c_void_p], C.c_uint64),
         "evslx_chebav_multi": ([C.c_int, C.POINTER(PolParams), C.c_void_p, C.c_void_p, C.c_int], C.c_int),
         "evslx_ChebLanNr_batch": ([C.c_int, _dp, C.c_int, C.c_double, C.c_void_p, C.POINTER(PolParams), C.c_int,
@@ -626,6 +629,12 @@ class Library:
         rc = self.lib.evslx_ChebLanNr_batch(ns, _d(iv), maxit, tol, dv.ptr, arr, precision, nev, lam, W, res)
         self._check(rc, "evslx_ChebLanNr_batch")
         return [self._outputs(nev[s], lam[s], W[s], res[s], want_vectors) for s in range(ns)]
+
+    def set_filter_variant(self, v):
+        self._check(self.lib.evslx_set_filter_variant(v), "evslx_set_filter_variant")
+
+    def tuned_filter_variant(self, precision, ncols):
+        return self.lib.evslx_tuned_filter_variant(precision, ncols)
 
     def matrix(self, ia, ja, a):
         return Matrix(self.lib, ia, ja, a)

@@ -121,66 +121,108 @@ __global__ void k_mf_unpack(int n, int ncols, const VT *Y, double *const *ytab) 
   }
 }
 
-// Columns per thread: two doubles or four floats (one 16-byte access); a row
-// is shared by B / CPT threads.
-template <class VT, int B>
+// Columns per thread: CPTB bytes of a row (16: two doubles or four floats;
+// 32: four doubles or eight floats); a row is shared by B / CPT threads.
+template <class VT, int B, int CPTB>
 struct Split {
-  static constexpr int CPT = (B < (int)(16 / sizeof(VT))) ? B : (int)(16 / sizeof(VT));
+  static constexpr int CPT = (B < (int)(CPTB / sizeof(VT))) ? B : (int)(CPTB / sizeof(VT));
   static constexpr int TPR = B / CPT;
 };
 
+// Kernel variants: the column part per thread (16 or 32 bytes) and whether
+// the TPR threads of a row load its stored entries cooperatively (each a
+// share, broadcast by warp shuffles) instead of each loading all of them.
+// -1: each matrix uses the variant the autotuner measured fastest for it
+// (per precision and block width); 0..3: that variant everywhere.
+static int g_mf_variant = -1;
+
 // One degree of the recurrence for all columns: thread (row r, part q)
-// handles columns q*CPT .. q*CPT+CPT-1 of row r.
-template <class VT, int B, class AV, class IT, bool FIRST>
+// handles columns q*CPT .. q*CPT+CPT-1 of row r.  Rows run over the padded
+// SELL-32 range so that every warp is full (rows past n only skip stores).
+template <class VT, int B, int CPTB, bool SHARE, class AV, class IT, bool FIRST>
 __global__ void __launch_bounds__(kThreads)
     k_mf_step(SellT<AV, IT> A, const VT *__restrict__ vk, const VT *vkm1, VT *out, VT *__restrict__ y,
               const VT *__restrict__ coef) {
-  constexpr int CPT = Split<VT, B>::CPT, TPR = Split<VT, B>::TPR;
+  constexpr int CPT = Split<VT, B, CPTB>::CPT, TPR = Split<VT, B, CPTB>::TPR;
+  constexpr bool COOP = SHARE && TPR > 1;
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  const long long total = (long long)A.n * TPR;
+  const int npad = (A.n + 31) & ~31;
+  const long long total = (long long)npad * TPR;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
     const int r = (int)(g / TPR), q = (int)(g % TPR);
+    const bool live = r < A.n;
     const int cb = q * CPT;
     // this row's own values first: independent of the gathers below, so
     // their latency overlaps with them
     const long long base = (long long)r * B + cb;
     VT xr[CPT], wv[CPT], yv[CPT], vm[CPT];
-    load_row<VT, CPT>(vk + base, xr);
-    load_row_cg<VT, CPT>(y + base, yv);
-    if (!FIRST) load_row_cg<VT, CPT>(vkm1 + base, vm);
+    if (live) {
+      load_row<VT, CPT>(vk + base, xr);
+      load_row_cg<VT, CPT>(y + base, yv);
+      if (!FIRST) load_row_cg<VT, CPT>(vkm1 + base, vm);
+    }
     VT acc[CPT];
 #pragma unroll
     for (int c = 0; c < CPT; ++c) acc[c] = (VT)0;
     const int ch = r >> 5;
     long long p = A.cptr[ch] + (r & 31);
     const int w = A.cw[ch];
-    // U stored entries at a time: their gathers are in flight together,
-    // then accumulated in order j = 0, 1, ...  Slots past the row's width
-    // act as 0 * x[r].
-    constexpr int U = 4;
-    for (int j = 0; j < w; j += U, p += 32 * U) {
-      VT v[U];
-      int col[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (j + u < w) {
-          v[u] = (VT)__ldg(A.val + p + 32 * u);
-          col[u] = decode_col(__ldg(A.col + p + 32 * u), r);
-        } else {
-          v[u] = (VT)0;
-          col[u] = r;
+    if constexpr (COOP) {
+      // TPR entries per batch: thread q loads entry j0 + q of its row, the
+      // row's threads exchange them, then gather and accumulate in order
+      const int seg = (threadIdx.x & 31) & ~(TPR - 1);
+      for (int j0 = 0; j0 < w; j0 += TPR) {
+        VT vmine = (VT)0;
+        int cmine = live ? r : 0;
+        if (live && j0 + q < w) {
+          vmine = (VT)__ldg(A.val + p + 32LL * (j0 + q));
+          cmine = decode_col(__ldg(A.col + p + 32LL * (j0 + q)), r);
         }
+        VT v[TPR];
+        int col[TPR];
+#pragma unroll
+        for (int u = 0; u < TPR; ++u) {
+          v[u] = __shfl_sync(0xffffffffu, vmine, seg + u);
+          col[u] = __shfl_sync(0xffffffffu, cmine, seg + u);
+        }
+        VT x[TPR][CPT];
+#pragma unroll
+        for (int u = 0; u < TPR; ++u) load_row<VT, CPT>(vk + (long long)col[u] * B + cb, x[u]);
+#pragma unroll
+        for (int u = 0; u < TPR; ++u)
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) acc[c] = fmadd(v[u], x[u][c], acc[c]);
       }
-      VT x[U][CPT];
+    } else {
+      // U stored entries at a time: their gathers are in flight together,
+      // then accumulated in order j = 0, 1, ...  Slots past the row's width
+      // act as 0 * x[r].
+      constexpr int U = 4;
+      for (int j = 0; j < w; j += U, p += 32 * U) {
+        VT v[U];
+        int col[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) load_row<VT, CPT>(vk + (long long)col[u] * B + cb, x[u]);
+        for (int u = 0; u < U; ++u) {
+          if (live && j + u < w) {
+            v[u] = (VT)__ldg(A.val + p + 32 * u);
+            col[u] = decode_col(__ldg(A.col + p + 32 * u), r);
+          } else {
+            v[u] = (VT)0;
+            col[u] = live ? r : 0; /* rows past n gather row 0, unused */
+          }
+        }
+        VT x[U][CPT];
 #pragma unroll
-      for (int u = 0; u < U; ++u)
+        for (int u = 0; u < U; ++u) load_row<VT, CPT>(vk + (long long)col[u] * B + cb, x[u]);
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) acc[c] = fmadd(v[u], x[u][c], acc[c]);
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) acc[c] = fmadd(v[u], x[u][c], acc[c]);
+      }
     }
+    if (!live) continue;
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
       const VT *cf = coef + kCoef * (cb + c);
@@ -194,11 +236,11 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-template <class VT, int B, class AV, class IT>
-int mf_step(const SellT<AV, IT> &A, int k, const VT *vk, const VT *vkm1, VT *out, VT *y, const VT *coef) {
-  constexpr int TPR = Split<VT, B>::TPR;
+template <class VT, int B, int CPTB, bool SHARE, class AV, class IT>
+int mf_step_v(const SellT<AV, IT> &A, int k, const VT *vk, const VT *vkm1, VT *out, VT *y, const VT *coef) {
+  constexpr int TPR = Split<VT, B, CPTB>::TPR;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid_for((long long)A.n * TPR, kThreads, 1 << 20));
+  cfg.gridDim = dim3(grid_for((long long)((A.n + 31) & ~31) * TPR, kThreads, 1 << 20));
   cfg.blockDim = dim3(kThreads);
   cfg.stream = stream();
   cudaLaunchAttribute attr[1];
@@ -206,10 +248,22 @@ int mf_step(const SellT<AV, IT> &A, int k, const VT *vk, const VT *vkm1, VT *out
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaError_t e = (k == 1) ? cudaLaunchKernelEx(&cfg, k_mf_step<VT, B, AV, IT, true>, A, vk, vkm1, out, y, coef)
-                           : cudaLaunchKernelEx(&cfg, k_mf_step<VT, B, AV, IT, false>, A, vk, vkm1, out, y, coef);
+  cudaError_t e =
+      (k == 1) ? cudaLaunchKernelEx(&cfg, k_mf_step<VT, B, CPTB, SHARE, AV, IT, true>, A, vk, vkm1, out, y, coef)
+               : cudaLaunchKernelEx(&cfg, k_mf_step<VT, B, CPTB, SHARE, AV, IT, false>, A, vk, vkm1, out, y, coef);
   if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "multi-column filter launch failed: %s", cudaGetErrorString(e));
   return check_launch("k_mf_step");
+}
+
+template <class VT, int B, class AV, class IT>
+int mf_step(const SellT<AV, IT> &A, int variant, int k, const VT *vk, const VT *vkm1, VT *out, VT *y,
+            const VT *coef) {
+  switch (variant) {
+    case 1: return mf_step_v<VT, B, 32, false>(A, k, vk, vkm1, out, y, coef);
+    case 2: return mf_step_v<VT, B, 16, true>(A, k, vk, vkm1, out, y, coef);
+    case 3: return mf_step_v<VT, B, 32, true>(A, k, vk, vkm1, out, y, coef);
+    default: return mf_step_v<VT, B, 16, false>(A, k, vk, vkm1, out, y, coef);
+  }
 }
 
 // Number of VT values of the coefficient table of one group.
@@ -242,7 +296,7 @@ void fill_coef(VT *h, int B, int ncols, const evslcu_filter_col *cols, int maxde
 // The launch sequence for one group of <= 16 columns: pack, one step per
 // degree, unpack.  coef: the group's device coefficient table.
 template <class VT, int B, class AV, class IT>
-int mf_group(const SellT<AV, IT> &A, int ncols, int maxdeg, const VT *coef, const double *const *xtab,
+int mf_group(const SellT<AV, IT> &A, int variant, int ncols, int maxdeg, const VT *coef, const double *const *xtab,
              double *const *ytab, VT *P, VT *W0, VT *W1, VT *Y, int *nlaunch) {
   const int n = A.n;
   const int g = grid_for((long long)n * B);
@@ -252,7 +306,7 @@ int mf_group(const SellT<AV, IT> &A, int ncols, int maxdeg, const VT *coef, cons
   for (int k = 1; !rc && k <= maxdeg; ++k) {
     const VT *vk = (k == 1) ? P : W[(k - 2) % 2];
     const VT *vkm1 = (k == 1) ? nullptr : ((k == 2) ? P : W[(k - 1) % 2]);
-    rc = mf_step<VT, B>(A, k, vk, vkm1, W[(k - 1) % 2], Y, coef + (size_t)k * B * kCoef);
+    rc = mf_step<VT, B>(A, variant, k, vk, vkm1, W[(k - 1) % 2], Y, coef + (size_t)k * B * kCoef);
   }
   if (!rc) {
     k_mf_unpack<VT, B><<<g, kThreads, 0, stream()>>>(n, ncols, Y, ytab);
@@ -263,16 +317,18 @@ int mf_group(const SellT<AV, IT> &A, int ncols, int maxdeg, const VT *coef, cons
 }
 
 template <class VT, class AV, class IT>
-int mf_dispatch(const SellT<AV, IT> &A, int B, int ncols, int maxdeg, const VT *coef, const double *const *xtab,
-                double *const *ytab, VT *P, VT *W0, VT *W1, VT *Y, int *nl) {
+int mf_dispatch(const SellT<AV, IT> &A, int variant, int B, int ncols, int maxdeg, const VT *coef,
+                const double *const *xtab, double *const *ytab, VT *P, VT *W0, VT *W1, VT *Y, int *nl) {
   switch (B) {
-    case 1: return mf_group<VT, 1>(A, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
-    case 2: return mf_group<VT, 2>(A, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
-    case 4: return mf_group<VT, 4>(A, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
-    case 8: return mf_group<VT, 8>(A, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
-    default: return mf_group<VT, 16>(A, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
+    case 1: return mf_group<VT, 1>(A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
+    case 2: return mf_group<VT, 2>(A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
+    case 4: return mf_group<VT, 4>(A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
+    case 8: return mf_group<VT, 8>(A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
+    default: return mf_group<VT, 16>(A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
   }
 }
+
+inline int log2_width(int B) { return B <= 1 ? 0 : B <= 2 ? 1 : B <= 4 ? 2 : B <= 8 ? 3 : 4; }
 
 __global__ void k_to_float(long long m, const double *src, float *dst) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
@@ -355,6 +411,90 @@ void *coef_build(int fp32, int ncols, const evslcu_filter_col *cols, int *err) {
   return d;
 }
 
+int variant_of(const evslcu_mat *A, int fp32, int B) {
+  if (g_mf_variant >= 0) return g_mf_variant;
+  const int v = A->mf_variant[fp32 ? 1 : 0][log2_width(B)];
+  return v >= 0 ? v : 0;
+}
+
+// Autotuner: times every kernel variant for this matrix, precision and block
+// width on a few degree steps (CUDA events on the library stream, zero
+// vectors) and records the fastest in the matrix.  Runs once per
+// (matrix, precision, width), outside any stream capture.
+int autotune(evslcu_mat *A, int fp32, int B) {
+  signed char &slot = A->mf_variant[fp32 ? 1 : 0][log2_width(B)];
+  if (slot >= 0 || g_mf_variant >= 0) return 0;
+  const int n = A->n, steps = 6;
+  const size_t vb = fp32 ? sizeof(float) : sizeof(double);
+  const size_t blk = ((size_t)n * B * vb + 255) / 256 * 256;
+  const size_t cf_n = coef_count(B, 1);
+  char *buf = (char *)evslcu_malloc(4 * blk + cf_n * vb);
+  if (!buf) return fail(EVSLCU_ERR_NOMEM, "filter autotune: out of device memory");
+  int rc = evslcu_memset(buf, 0, 4 * blk + cf_n * vb);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int bestv = 0;
+  for (int v = 0; !rc && v < 4; ++v) {
+    float ms = 0.0f;
+    for (int rep = 0; !rc && rep < 2; ++rep) {
+      cudaEventRecord(e0, stream());
+      for (int k = 2; !rc && k < 2 + steps; ++k) {
+        void *P = buf, *W0 = buf + blk, *W1 = buf + 2 * blk, *Y = buf + 3 * blk;
+        const void *cf = buf + 4 * blk;
+        if (fp32) {
+          const void *vals = (A->vfmt == 1) ? A->sval : A->sval32;
+          auto go = [&](auto view) -> int {
+            switch (B) {
+              case 1: return mf_step<float, 1>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
+              case 2: return mf_step<float, 2>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
+              case 4: return mf_step<float, 4>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
+              case 8: return mf_step<float, 8>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
+              default: return mf_step<float, 16>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
+            }
+          };
+          rc = A->ifmt ? go(SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals})
+                       : go(SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals});
+        } else {
+          rc = with_view(A, [&](auto view) -> int {
+            if constexpr (std::is_same<decltype(view), CsrView>::value) {
+              return fail(EVSLCU_ERR_ARG, "filter_columns needs the SELL-32 storage");
+            } else {
+              switch (B) {
+                case 1: return mf_step<double, 1>(view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
+                case 2: return mf_step<double, 2>(view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
+                case 4: return mf_step<double, 4>(view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
+                case 8: return mf_step<double, 8>(view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
+                default: return mf_step<double, 16>(view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
+              }
+            }
+          });
+        }
+        count_launch();
+      }
+      cudaEventRecord(e1, stream());
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(EVSLCU_ERR_CUDA, "filter autotune: timing failed");
+      if (!rc && rep == 1) cudaEventElapsedTime(&ms, e0, e1);
+    }
+    if (!rc && ms < best) {
+      best = ms;
+      bestv = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  evslcu_free(buf);
+  if (!rc) slot = (signed char)bestv;
+  return rc;
+}
+
+int autotune_groups(const evslcu_mat *A, int fp32, int ncols) {
+  int rc = 0;
+  for (int c0 = 0; !rc && c0 < ncols; c0 += kMaxB) rc = autotune((evslcu_mat *)A, fp32, group_width(std::min(kMaxB, ncols - c0)));
+  return rc;
+}
+
 // The whole launch sequence for ncols columns; x and y pointers are read
 // from the device table tab (x[0..ncols), then y[0..ncols)); coef from
 // coef_build.
@@ -379,10 +519,10 @@ int mf_sequence(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_co
       const void *vals = (A->vfmt == 1) ? A->sval : A->sval32;
       if (A->ifmt)
         rc = mf_dispatch<float>(SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals},
-                                B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
+                                variant_of(A, 1, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
       else
-        rc = mf_dispatch<float>(SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals}, B,
-                                gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
+        rc = mf_dispatch<float>(SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals},
+                                variant_of(A, 1, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
     } else {
       double *P = (double *)w, *W0 = (double *)(w + blk), *W1 = (double *)(w + 2 * blk), *Y = (double *)(w + 3 * blk);
       const double *cf = (const double *)coef + off;
@@ -390,7 +530,7 @@ int mf_sequence(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_co
         if constexpr (std::is_same<decltype(view), CsrView>::value) {
           return fail(EVSLCU_ERR_ARG, "filter_columns needs the SELL-32 storage");
         } else {
-          return mf_dispatch<double>(view, B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
+          return mf_dispatch<double>(view, variant_of(A, 0, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
         }
       });
     }
@@ -443,6 +583,7 @@ int evslcu_filter_columns(const evslcu_mat *A, int fp32, int ncols, const evslcu
   }
   rc = evslcu_h2d(tab, htab, tabb);
   free(htab);
+  if (!rc) rc = autotune_groups(A, fp32, ncols);
   void *coef = rc ? nullptr : coef_build(fp32, ncols, cols, &rc);
   int nl = 0;
   if (!rc) rc = mf_sequence(A, fp32, ncols, cols, coef, work, tab_off, tab, &nl);
@@ -469,8 +610,8 @@ evslcu_filter_plan *evslcu_filter_plan_create(const evslcu_mat *A, int fp32, int
     evslcu_filter_plan_destroy(P);
     return nullptr;
   }
-  int err = 0;
-  P->coef = coef_build(fp32, ncols, cols, &err);
+  int err = autotune_groups(A, fp32, ncols);
+  P->coef = err ? nullptr : coef_build(fp32, ncols, cols, &err);
   if (!P->coef) {
     evslcu_filter_plan_destroy(P);
     return nullptr;
@@ -515,6 +656,18 @@ int evslcu_filter_plan_run(evslcu_filter_plan *P, const double *const *x, double
 }
 
 int evslcu_filter_plan_columns(const evslcu_filter_plan *P) { return P ? P->ncols : 0; }
+
+int evslcu_set_filter_variant(int v) {
+  if (v < -1 || v > 3) return fail(EVSLCU_ERR_ARG, "filter variant must be -1 (tuned) or 0..3");
+  g_mf_variant = v;
+  return 0;
+}
+
+int evslcu_get_filter_variant(void) { return g_mf_variant; }
+
+int evslcu_mat_filter_variant(const evslcu_mat *A, int fp32, int B) {
+  return A ? A->mf_variant[fp32 ? 1 : 0][log2_width(B)] : -1;
+}
 
 void evslcu_filter_plan_destroy(evslcu_filter_plan *P) {
   if (!P) return;

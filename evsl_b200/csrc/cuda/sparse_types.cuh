@@ -28,6 +28,7 @@ struct evslcu_mat {
   void *scol = nullptr;
   void *sval = nullptr;
   void *sval32 = nullptr;  // FP32 copy of sval for the FP32 filter (when vfmt == 0)
+  signed char mf_variant[2][5] = {{-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1}};  // tuned kernel per (fp32, log2 B)
   int kernel = 0;      // 0 SELL-32, 1 CSR (thread per row)
   int persistent = 0;  // 1: single cooperative launch per filter application
 };

@@ -189,6 +189,14 @@ evslcu_filter_plan *evslcu_filter_plan_create(const evslcu_mat *A, int fp32, int
                                               const evslcu_filter_col *cols);
 int evslcu_filter_plan_run(evslcu_filter_plan *P, const double *const *x, double *const *y);
 int evslcu_filter_plan_columns(const evslcu_filter_plan *P);
+/* Multi-column kernel variant (0..3): bit 0 = 32-byte column parts per
+ * thread (else 16), bit 1 = rows' stored entries loaded cooperatively;
+ * -1 (default): per matrix, precision and block width, the variant an
+ * autotuner measured fastest (timed once, on first use). */
+int evslcu_set_filter_variant(int v);
+int evslcu_get_filter_variant(void);
+/* Variant the autotuner chose for A (fp32, block width B), -1 if untuned. */
+int evslcu_mat_filter_variant(const evslcu_mat *A, int fp32, int B);
 void evslcu_filter_plan_destroy(evslcu_filter_plan *P);
 /* COO (device arrays, indices base 0 or 1) -> CSR on the device: rows in
  * order, entries of a row sorted by column with ties in input order (the

@@ -26,12 +26,14 @@
  * values, vectors and accumulation; the Lanczos basis, reorthogonalisation,
  * tridiagonal solve and Ritz step stay FP64, and the Ritz pairs are then
  * refined in FP64: the candidate block -- the Ritz vectors of the m Ritz
- * values above bar plus max(16, m) guard vectors from the next Ritz values
- * below it -- is filtered again with the FP64 filter, orthonormalised, and a
- * Rayleigh-Ritz step with A gives the new pairs, repeated (at most 4
- * sweeps) while a pair inside [a, b] misses tol.  (With fewer guards the
- * eigenvectors just outside [a, b], which the filter damps weakly, limit
- * the residuals near 1e-8 and more sweeps are needed.)
+ * values above bar plus max(16, m/2) guard vectors from the next Ritz values
+ * below it -- is filtered with an FP64 filter designed (find_pol, same
+ * settings) for the interval spanned by the candidates' Rayleigh quotients,
+ * orthonormalised, and a Rayleigh-Ritz step with A gives the new pairs,
+ * repeated (at most 4 sweeps) while a pair inside [a, b] misses tol.  The
+ * guards put the eigenvectors next to [a, b], which a filter damps weakly,
+ * inside the Rayleigh-Ritz subspace; the wider interval then needs a filter
+ * of lower degree (about 0.6 of the slice's) and usually one sweep.
  *
  * Every per-slot computation depends only on that slot's data (the filter
  * treats columns independently and the reductions are per slot), so a
@@ -533,6 +535,22 @@ static int refine_fp64(evslx_engine *E, slot_t *s, int m, double *U, double *W, 
   void *fw = evslcu_malloc(need);
   int rc = 0;
   if (!H || !Q || !th || !dH || !cgsw || !cols || !fw) rc = evsl_seterr(EVSLX_ERR_NOMEM, "engine: out of memory");
+  /* The refinement filter: the request's filter design over the interval
+   * spanned by the candidates' Rayleigh quotients (wanted pairs and
+   * guards).  The Rayleigh-Ritz step resolves every eigenvector in that
+   * interval, so the filter only has to damp the rest of the spectrum, which
+   * a wider interval does with a lower degree. */
+  polparams pw = r->pol;
+  pw.mu = NULL;
+  pw.deg = 0;
+  double wiv[4] = {aa, bb, r->intv[2], r->intv[3]};
+  for (int j = 0; j < m; j++) {
+    wiv[0] = evsl_min(wiv[0], rlam[j]);
+    wiv[1] = evsl_max(wiv[1], rlam[j]);
+  }
+  wiv[0] = evsl_max(wiv[0], r->intv[2]);
+  wiv[1] = evsl_min(wiv[1], r->intv[3]);
+  if (!rc && find_pol(wiv, &pw)) rc = evsl_seterr(EVSLX_ERR_NUMERIC, "engine: refinement filter design failed");
 #define CU(x)                                   \
   if ((rc = (x))) {                             \
     rc = evsl_seterr(rc, "%s", evslcu_errstr()); \
@@ -545,10 +563,10 @@ static int refine_fp64(evslx_engine *E, slot_t *s, int m, double *U, double *W, 
     if (!missing) break;
     /* W = p(A) U in FP64 */
     for (int j = 0; j < m; j++) {
-      cols[j].mu = r->pol.mu;
-      cols[j].deg = r->pol.deg;
-      cols[j].cc = r->pol.cc;
-      cols[j].dd = r->pol.dd;
+      cols[j].mu = pw.mu;
+      cols[j].deg = pw.deg;
+      cols[j].cc = pw.cc;
+      cols[j].dd = pw.dd;
       cols[j].x = U + (size_t)j * n_l;
       cols[j].y = W + (size_t)j * n_l;
     }
@@ -579,6 +597,7 @@ static int refine_fp64(evslx_engine *E, slot_t *s, int m, double *U, double *W, 
     CU(evslcu_ritz_eval(&r->M->op, n, m, U, W, rnorm, rlam, rres));
   }
 #undef CU
+  free_pol(&pw);
   free(H);
   free(Q);
   free(th);
@@ -616,7 +635,7 @@ static int finalize(evslx_engine *E, slot_t *s, int kdim, evslx_result *out) {
      * Ritz values below bar, so that the eigenvectors just outside [a, b]
      * are resolved by the Rayleigh-Ritz step instead of damped by the
      * filter (whose damping is weak next to the interval) */
-    const int g = evsl_min(kdim - msel, evsl_max(ENG_MIN_GUARDS, msel));
+    const int g = evsl_min(kdim - msel, evsl_max(ENG_MIN_GUARDS, (msel + 1) / 2));
     const int first = sel[0];
     for (int i = msel - 1; i >= 0; i--) {
       sel[g + i] = sel[i];
@@ -942,4 +961,18 @@ int evslx_chebav_multi(int ncols, const polparams *pols, const double *X, double
   if (rc) return evsl_seterr(rc, "%s", evslcu_errstr());
   evslstat.n_polAv += ncols;
   return 0;
+}
+
+int evslx_set_filter_variant(int v) {
+  int rc = evslcu_set_filter_variant(v);
+  return rc ? evsl_seterr(rc, "%s", evslcu_errstr()) : 0;
+}
+
+int evslx_get_filter_variant(void) { return evslcu_get_filter_variant(); }
+
+int evslx_tuned_filter_variant(int precision, int ncols) {
+  if (evsl_require_operator() || !evsl_op()->A) return -1;
+  int B = 1;
+  while (B < ncols && B < 16) B *= 2;
+  return evslcu_mat_filter_variant(evsl_op()->A, precision == EVSLX_PREC_MIXED, B);
 }

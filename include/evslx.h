@@ -157,8 +157,9 @@ int evslx_coo_to_csr_device(int cooidx, const cooMat *coo, int coo_on_device, cs
  *
  * precision: EVSLX_PREC_FP64 (filter in FP64) or EVSLX_PREC_MIXED (filter in
  * FP32; Lanczos, orthogonalisation, Ritz step in FP64; Ritz pairs refined by
- * FP64 filtered Rayleigh-Ritz sweeps over the candidates plus as many guard
- * vectors (at least 16) until every pair inside [a, b] meets tol, at most 4
+ * FP64 filtered Rayleigh-Ritz sweeps over the candidates plus half as many
+ * guard vectors (at least 16), with a filter designed for the interval the
+ * candidates span, until every pair inside [a, b] meets tol, at most 4
  * sweeps).
  * ------------------------------------------------------------------------- */
 #define EVSLX_PREC_FP64 0
@@ -211,6 +212,17 @@ void evslx_result_free(evslx_result *r);
  * its own polynomial pols[c] (X, Y: device, column-major n x ncols).  FP64:
  * every column equal to ChebAv bit for bit; MIXED: the FP32 filter. */
 int evslx_chebav_multi(int ncols, const polparams *pols, const double *X, double *Y, int precision);
+
+/* Variant of the multi-column filter kernel (results are identical):
+ * bit 0 -- each thread handles 32 bytes of a row's columns (else 16),
+ * bit 1 -- a row's threads load its stored entries cooperatively;
+ * -1 (default) -- autotuned: the first filter on a matrix with a given
+ * precision and block width times the four variants on a few degree steps
+ * and keeps the fastest for that matrix. */
+int evslx_set_filter_variant(int v);
+int evslx_get_filter_variant(void);
+/* The variant tuned for the registered matrix (-1: not tuned yet). */
+int evslx_tuned_filter_variant(int precision, int ncols);
 
 /* nslices slices of the registered CSR matrix solved together in one engine
  * (intvs: 4 per slice; pols: one per slice; vinit: device start vector

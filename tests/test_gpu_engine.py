@@ -51,6 +51,27 @@ def test_multi_filter_fp64_bitwise_fp32_close(gpu_lib):
             gpu_lib.free_pol(p)
 
 
+def test_filter_variants_and_autotuner(gpu_lib):
+    """All kernel variants give the same bits; the autotuner picks one."""
+    ia, ja, a = O.lap_csr(40, 40, 40)
+    gpu_lib.set_csr(ia, ja, a)
+    n = len(ia) - 1
+    pol = gpu_lib.find_pol([0.6, 0.9, 0.0, 12.0])
+    try:
+        for prec in (E.PREC_FP64, E.PREC_MIXED):
+            for B in (1, 3, 8, 16):
+                X = O.seeded_normal(n * B, 30 + B).reshape(B, n)
+                gpu_lib.set_filter_variant(-1)
+                ref = gpu_lib.chebav_multi([pol] * B, X, prec)
+                assert 0 <= gpu_lib.tuned_filter_variant(prec, B) <= 3
+                for v in range(4):
+                    gpu_lib.set_filter_variant(v)
+                    assert np.array_equal(gpu_lib.chebav_multi([pol] * B, X, prec), ref)
+    finally:
+        gpu_lib.set_filter_variant(-1)
+        gpu_lib.free_pol(pol)
+
+
 def _lap_slices(ev, starts, count):
     out = []
     for s in starts:
