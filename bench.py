@@ -42,7 +42,7 @@ METRIC = "eigenpairs/sec + p50/p99 slice latency at resid<=1e-8; filter SpMV GB/
 UNIT = "eigenpairs/s"
 # Lanczos dimension of this request, as the GPU arm measures it (used only to
 # scale the CPU sample to a whole request; the recurrence is the same).
-REQUEST_LANCZOS_STEPS = None
+REQUEST_LANCZOS_STEPS = 451
 
 
 def parse():
@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--count", type=int, default=COUNT)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve"],
+    p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve", "lap3d-multifilter"],
                    default="lap3d-slice",
                    help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark); "
                         "lap3d-batch: several slices through the request engine; serve: a Poisson request stream")
@@ -65,6 +65,10 @@ def parse():
     p.add_argument("--slots", type=int, default=16, help="serve: slice solves in flight")
     p.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM budget of the engine")
     p.add_argument("--max-count", type=int, default=150, help="serve: most eigenvalues in a slice request")
+    p.add_argument("--ncols", type=int, default=16, help="lap3d-multifilter: columns")
+    p.add_argument("--variant", type=int, default=-1, help="lap3d-multifilter: kernel variant (-1 autotuned)")
+    p.add_argument("--sweep", action="store_true", help="lap3d-multifilter: every variant/width/precision once")
+    p.add_argument("--low-degree", action="store_true", help="lap3d-multifilter: only the degree-7 filter")
     return p.parse_args()
 
 
@@ -479,6 +483,85 @@ def run_filter(args):
     lib.free_pol(pol)
 
 
+def run_multifilter(args):
+    """lap3d-multifilter: the multi-column filter kernel alone on the 3-D
+    Laplacian 100^3, `--ncols` columns with the slice request's polynomial
+    (degree 1440).  Per-degree device time = (time of the degree-1440 filter
+    - time of a degree-7 filter) / 1433, CUDA events on the library stream
+    around evslx_chebav_multi, median of K steps.  Algorithmic bytes per
+    degree = stored matrix (values + column indices + chunk tables) + 5 n B
+    vector accesses.  `--sweep`: every kernel variant, width and precision
+    once with the degree-7 filter (a launch list for ncu); `--low-degree`:
+    only the degree-7 filter (a small capture)."""
+    import torch
+
+    import evsl_b200 as E
+    from evsl_b200 import workloads as W
+
+    lib = E.Library()
+    ia, ja, a = W.laplacian_csr(NX, NY, NZ)
+    ev = W.laplacian_eigenvalues(NX, NY, NZ)
+    lib.set_csr(ia, ja, a)
+    n = NX * NY * NZ
+    intv, _ = slice_interval(ev, 0, args.count)
+    p_hi = lib.find_pol(intv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+    p_lo = lib.find_pol([1.0, 3.0, LMIN, LMAX], damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+    prec = E.PREC_MIXED if args.precision == "mixed" else E.PREC_FP64
+    lstream = torch.cuda.ExternalStream(lib.stream_handle())
+    if args.sweep or args.low_degree:
+        combos = [(v, pr, b) for v in range(4) for pr in (E.PREC_FP64, E.PREC_MIXED) for b in (1, 2, 4, 8, 16)] \
+            if args.sweep else [(args.variant, prec, args.ncols)]
+        for v, pr, b in combos:
+            lib.set_filter_variant(v)
+            X = np.random.default_rng(b).standard_normal((b, n))
+            lib.chebav_multi([p_lo] * b, X, pr)
+        print(json.dumps({"workload": "lap3d-multifilter " + ("sweep" if args.sweep else "low-degree"),
+                          "launch_sets": len(combos), "degree": int(p_lo.deg)}))
+        return
+    lib.set_filter_variant(args.variant)
+    B = args.ncols
+    X = np.random.default_rng(B).standard_normal((B, n))
+
+    def timed(pol):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lstream)
+        lib.chebav_multi([pol] * B, X, prec)
+        e1.record(lstream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    for _ in range(args.warmup):
+        timed(p_hi)
+        timed(p_lo)
+    sampler = ClockSampler(rank_info()[2])
+    sampler.start()
+    per = []
+    for _ in range(args.steps):
+        per.append((timed(p_hi) - timed(p_lo)) / (p_hi.deg - p_lo.deg))
+    clocks = sampler.stop()
+    t = statistics.median(per)
+    vb, ib = lib.matrix_storage()
+    _, nnz, stored = lib.problem_info()
+    sx = 4 if prec == E.PREC_MIXED else 8
+    abytes = stored * ((4 if prec == E.PREC_MIXED else vb) + ib) + 12 * ((n + 31) // 32) + 5 * n * B * sx
+    peak, kind = measured_peak_hbm()
+    gbs = abytes / t / 1e9
+    print(json.dumps({
+        "metric": "filter SpMV GB/s", "value": gbs, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t * p_hi.deg, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if prec == E.PREC_MIXED else "f64", "data": "synthetic",
+        "config": {"workload": "lap3d-multifilter: %d columns, degree %d, 3-D Laplacian 100^3" % (B, p_hi.deg),
+                   "variant": args.variant, "tuned_variant": lib.tuned_filter_variant(prec, B),
+                   "us_per_degree": 1e6 * t, "us_per_column_degree": 1e6 * t / B,
+                   "algorithmic_bytes_per_degree": abytes},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "peak_kind": kind, "unit": "GB/s",
+                     "frac": gbs / peak, "traffic": None},
+        "clocks": clocks}))
+    lib.free_pol(p_hi)
+    lib.free_pol(p_lo)
+
+
 def _slice_plan(ev, start, nslices, count):
     """Consecutive gap-midpoint intervals of `count` eigenvalues from `start`."""
     from evsl_b200 import workloads as W
@@ -704,6 +787,8 @@ def main():
         run_batch(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "lap3d-multifilter":
+        run_multifilter(args)
     else:
         run_ours(args)
 
