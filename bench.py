@@ -69,6 +69,10 @@ def parse():
     p.add_argument("--variant", type=int, default=-1, help="lap3d-multifilter: kernel variant (-1 autotuned)")
     p.add_argument("--sweep", action="store_true", help="lap3d-multifilter: every variant/width/precision once")
     p.add_argument("--low-degree", action="store_true", help="lap3d-multifilter: only the degree-7 filter")
+    p.add_argument("--l2-resident", action="store_true",
+                   help="keep the stored matrix persisting in L2 (comparison runs)")
+    p.add_argument("--filter-mode", choices=["per-degree", "wave"], default="per-degree",
+                   help="filter execution: one launch per degree or one pipelined launch")
     return p.parse_args()
 
 
@@ -180,6 +184,9 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     lib = evsl_b200.Library()
+    if args.l2_resident:
+        lib.set_l2_resident(True)
+    lib.set_filter_wave(args.filter_mode == "wave")
     ia, ja, a = W.laplacian_csr(NX, NY, NZ)
     ev = W.laplacian_eigenvalues(NX, NY, NZ)
     lib.set_csr(ia, ja, a)
@@ -451,6 +458,9 @@ def run_filter(args):
     from evsl_b200 import workloads as W
 
     lib = evsl_b200.Library()
+    if args.l2_resident:
+        lib.set_l2_resident(True)
+    lib.set_filter_wave(args.filter_mode == "wave")
     ia, ja, a = W.laplacian_csr(NX, NY, NZ)
     ev = W.laplacian_eigenvalues(NX, NY, NZ)
     lib.set_csr(ia, ja, a)

@@ -292,6 +292,8 @@ def load():
         "evslx_result_free": ([C.POINTER(EvslxResult)], None),
         "evslx_engine_use_graphs": ([C.c_void_p, C.c_int], None),
         "evslx_set_filter_variant": ([C.c_int], C.c_int),
+        "evslx_set_l2_resident": ([C.c_int], C.c_int),
+        "evslx_set_filter_wave": ([C.c_int], C.c_int),
         "evslx_get_filter_variant": ([], C.c_int),
         "evslx_tuned_filter_variant": ([C.c_int, C.c_int], C.c_int),
         "evslx_engine_plan_builds": ([C.c_void_p], C.c_uint64),
@@ -527,6 +529,12 @@ class Library:
         self._check(self.lib.SetAMatrix_device_csr(C.byref(csr)), "SetAMatrix_device_csr")
         self.n = n
         return csr
+
+    def set_filter_wave(self, on):
+        self._check(self.lib.evslx_set_filter_wave(1 if on else 0), "evslx_set_filter_wave")
+
+    def set_l2_resident(self, on):
+        self._check(self.lib.evslx_set_l2_resident(1 if on else 0), "evslx_set_l2_resident")
 
     def set_filter_persistent(self, on):
         self._check(self.lib.evslx_set_filter_persistent(1 if on else 0), "evslx_set_filter_persistent")

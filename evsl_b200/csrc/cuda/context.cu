@@ -5,7 +5,10 @@
 
 #include <atomic>
 
+#include <algorithm>
+
 #include "common.cuh"
+#include "sparse_types.cuh"
 
 namespace evslcu {
 
@@ -94,9 +97,58 @@ int evslcu_init(void) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// L2 residency of the stored matrix: an access-policy window on the library
+// stream marks the SELL arrays persisting, with the context's persisting L2
+// set-aside sized to them (bounded by the device maximum).  The set-aside is
+// a limit of this context and is released when the window is cleared.
+// ---------------------------------------------------------------------------
+static const void *g_l2_owner = nullptr;
+
+extern "C" int evslcu_mat_l2_persist(const evslcu_mat *A, int on) {
+  if (!g_ctx.ready || !A) return 0;
+  if (!on) {
+    if (g_l2_owner != (const void *)A) return 0;
+    cudaStreamAttrValue v = {};
+    v.accessPolicyWindow.base_ptr = nullptr;
+    v.accessPolicyWindow.num_bytes = 0;
+    cudaStreamSetAttribute(g_ctx.stream, cudaStreamAttributeAccessPolicyWindow, &v);
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+    g_l2_owner = nullptr;
+    cudaGetLastError();
+    return 0;
+  }
+  if (!A->sell_block || !A->sell_bytes) return 0;
+  int max_persist = 0, max_window = 0;
+  cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, g_ctx.device);
+  cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, g_ctx.device);
+  if (max_persist <= 0 || max_window <= 0) return 0;
+  const size_t window = std::min(A->sell_bytes, (size_t)max_window);
+  const size_t setaside = std::min(window, (size_t)max_persist);
+  EVSLCU_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, setaside));
+  cudaStreamAttrValue v = {};
+  v.accessPolicyWindow.base_ptr = A->sell_block;
+  v.accessPolicyWindow.num_bytes = window;
+  v.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)setaside / (double)window);
+  v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+  v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  EVSLCU_CUDA(cudaStreamSetAttribute(g_ctx.stream, cudaStreamAttributeAccessPolicyWindow, &v));
+  g_l2_owner = A;
+  return 0;
+}
+
 int evslcu_finish(void) {
   if (!g_ctx.ready) return 0;
   cudaStreamSynchronize(g_ctx.stream);
+  if (g_l2_owner) {
+    cudaStreamAttrValue v = {};
+    cudaStreamSetAttribute(g_ctx.stream, cudaStreamAttributeAccessPolicyWindow, &v);
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+    g_l2_owner = nullptr;
+    cudaGetLastError();
+  }
   cudaFree(g_ctx.partials);
   cudaFree(g_ctx.counters);
   cudaFree(g_ctx.scalars);

@@ -314,7 +314,14 @@ int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, dou
   }
   bool launched = false;
   int rc = 0;
-  const bool allow = A->persistent && A->kernel == 0 && deg >= 2;
+  if (A->wave && A->kernel == 0 && deg >= 2) {
+    rc = chebav_wave((evslcu_mat *)A, mu, deg, cc, dd, v, y, work);
+    if (!rc) rc = evslcu_filter_error();
+    if (!rc && epi) rc = launch_lan_epi(n, epi, y);
+    if (rc) return rc;
+    launched = true;
+  }
+  const bool allow = !launched && A->persistent && A->kernel == 0 && deg >= 2;
   if (allow) {
     if (deg + 1 > g_mu_cap) {
       if (g_mu_dev) evslcu_free(g_mu_dev);
@@ -349,6 +356,7 @@ int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, dou
     if (rc) return rc;
   }
   if (!launched) rc = chebav_per_degree(A, mu, deg, cc, dd, v, y, work, epi);
+  else if (allow && !rc) rc = evslcu_filter_error();
   if (rc) return rc;
   if (g_prof.on) {
     cudaEvent_t ev_b = prof_event();
@@ -387,6 +395,12 @@ int evslcu_set_filter_block(int threads) {
 int evslcu_mat_set_persistent(evslcu_mat *A, int on) {
   if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
   A->persistent = on ? 1 : 0;
+  return 0;
+}
+
+int evslcu_mat_set_wave(evslcu_mat *A, int on) {
+  if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
+  A->wave = on ? 1 : 0;
   return 0;
 }
 

@@ -232,20 +232,24 @@ __global__ void k_csr_check_ptr(int n, const int *ia, int *flags) {
 
 // flags[1]: first entry position with a column outside [0, n) (INT_MAX if
 // none); flags[2]: some value is not exactly a finite float; flags[3]: some
-// |col - row| does not fit int16.
+// |col - row| does not fit int16; flags[4]: the largest |col - row|.
 __global__ void k_csr_check_entries(int n, const int *ia, const int *ja, const double *a, int *flags) {
-  int not_float = 0, not_16 = 0;
+  int not_float = 0, not_16 = 0, bw = 0;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     for (int j = ia[r]; j < ia[r + 1]; ++j) {
       const int c = ja[j];
       if (c < 0 || c >= n) atomicMin(&flags[1], j);
       if (c - r > 32767 || c - r < -32768) not_16 = 1;
+      bw = max(bw, abs(c - r));
       const double v = a[j];
       if (!(isfinite(v) && (double)(float)v == v)) not_float = 1;
     }
   }
   if (__any_sync(0xffffffffu, not_float) && (threadIdx.x & 31) == 0) atomicOr(&flags[2], 1);
   if (__any_sync(0xffffffffu, not_16) && (threadIdx.x & 31) == 0) atomicOr(&flags[3], 1);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bw = max(bw, __shfl_down_sync(0xffffffffu, bw, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(&flags[4], bw);
 }
 
 __global__ void k_chunk_width(int n, int nch, const int *ia, int *cw, long long *csize) {
@@ -290,10 +294,10 @@ __global__ void k_sell_fill(int n, int nch, const int *ia, const int *ja, const 
 // values and columns allow it.
 int build_sell_device(evslcu_mat *M, int allow_compress) {
   const int n = M->n;
-  int *flags = (int *)evslcu_malloc(sizeof(int) * 4);
+  int *flags = (int *)evslcu_malloc(sizeof(int) * 5);
   if (!flags) return EVSLCU_ERR_NOMEM;
-  const int init[4] = {0x7fffffff, 0x7fffffff, 0, 0};
-  int hf[4];
+  const int init[5] = {0x7fffffff, 0x7fffffff, 0, 0, 0};
+  int hf[5];
   int rc = evslcu_h2d(flags, init, sizeof(init));
   if (!rc) {
     k_csr_check_ptr<<<grid_for(n), kThreads, 0, stream()>>>(n, M->ia, flags);
@@ -313,6 +317,7 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
     evslcu_d2h(&bad, M->ja + hf[1], sizeof(int));
     return fail(EVSLCU_ERR_ARG, "CSR column index %d at position %d is outside [0, %d)", bad, hf[1], n);
   }
+  M->bandwidth = hf[4];
   M->vfmt = (allow_compress && !hf[2]) ? 1 : 0;
   M->ifmt = (allow_compress && !hf[3]) ? 1 : 0;
   const int nch = (n + 31) / 32;
@@ -335,9 +340,14 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
   const size_t cap = (size_t)std::max(padded, 1LL);
   const size_t colb = M->ifmt ? sizeof(short) : sizeof(int);
   const size_t valb = M->vfmt ? sizeof(float) : sizeof(double);
-  M->scol = evslcu_malloc(colb * cap);
-  M->sval = evslcu_malloc(valb * cap);
-  if (!M->scol || !M->sval) return fail(EVSLCU_ERR_NOMEM, "SELL build: out of device memory (%lld slots)", padded);
+  // scol and sval in one allocation so that one L2 access-policy window
+  // covers the stored matrix
+  const size_t colbytes = (colb * cap + 255) / 256 * 256;
+  M->sell_bytes = colbytes + valb * cap;
+  M->sell_block = evslcu_malloc(M->sell_bytes);
+  if (!M->sell_block) return fail(EVSLCU_ERR_NOMEM, "SELL build: out of device memory (%lld slots)", padded);
+  M->scol = M->sell_block;
+  M->sval = (char *)M->sell_block + colbytes;
   const int g = grid_for(32LL * nch);
   if (M->vfmt && M->ifmt)
     k_sell_fill<float, short><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->cptr, M->cw,

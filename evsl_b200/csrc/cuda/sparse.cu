@@ -627,8 +627,10 @@ void evslcu_mat_destroy(evslcu_mat *M) {
   }
   evslcu_free(M->cptr);
   evslcu_free(M->cw);
-  evslcu_free(M->scol);
-  evslcu_free(M->sval);
+  evslcu_mat_l2_persist(M, 0);
+  evslcu_free(M->sell_block);
+  evslcu_free(M->wave_ctl);
+  evslcu_free(M->wave_mu);
   evslcu_free(M->sval32);
   delete M;
 }

@@ -27,8 +27,16 @@ struct evslcu_mat {
   int ifmt = 0;
   void *scol = nullptr;
   void *sval = nullptr;
+  void *sell_block = nullptr;  // one allocation holding scol and sval (L2 window)
+  size_t sell_bytes = 0;
   void *sval32 = nullptr;  // FP32 copy of sval for the FP32 filter (when vfmt == 0)
   signed char mf_variant[2][5] = {{-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1}};  // tuned kernel per (fp32, log2 B)
+  long long bandwidth = 0;  // max |col - row| over the stored entries
+  int wave = 0;             // 1: pipelined single-launch filter (wavefilter.cu)
+  unsigned *wave_ctl = nullptr;
+  size_t wave_ctl_words = 0;
+  double *wave_mu = nullptr;
+  int wave_mu_cap = 0;
   int kernel = 0;      // 0 SELL-32, 1 CSR (thread per row)
   int persistent = 0;  // 1: single cooperative launch per filter application
 };
@@ -156,6 +164,9 @@ inline int with_view(const evslcu_mat *A, F &&f) {
   return f(sell_view<float, short>(A));
 }
 
+// Pipelined single-launch filter (wavefilter.cu); work: 2n doubles.
+int chebav_wave(evslcu_mat *A, const double *mu, int deg, double cc, double dd, const double *v, double *y,
+                double *work);
 // Per-degree filter path (sparse.cu): one fused kernel per degree.
 int chebav_per_degree(const evslcu_mat *A, const double *mu, int deg, double cc, double dd, const double *v,
                       double *y, double *work, const evslcu_cheb_epi *epi);

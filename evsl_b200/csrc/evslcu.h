@@ -233,6 +233,9 @@ int evslcu_filter_error(void);
  * created afterwards.  Default on. */
 int evslcu_set_compression(int on);
 int evslcu_mat_storage(const evslcu_mat *A, int *vfmt, int *ifmt);
+/* Keep A's stored matrix resident in L2 (persisting access-policy window on
+ * the library stream, set-aside sized to it) or release that (on = 0). */
+int evslcu_mat_l2_persist(const evslcu_mat *A, int on);
 /* Threads per block of the single-launch filter (256, 512, 1024; default
  * 1024: fewer blocks meet at each grid barrier). */
 int evslcu_set_filter_block(int threads);
@@ -240,6 +243,9 @@ int evslcu_set_filter_block(int threads);
 int evslcu_set_rows_per_thread(int r);
 /* Allow (1, default) or forbid (0) the single-launch filter kernel. */
 int evslcu_mat_set_persistent(evslcu_mat *A, int on);
+/* 1: the filter runs as one pipelined launch (tiles of rows, step s of a tile
+ * waits only for step s-1 of the tiles its rows reach); bitwise the same. */
+int evslcu_mat_set_wave(evslcu_mat *A, int on);
 
 /* Allocation-free variant of the KPM moments: all scratch (block vectors,
  * dots, partial sums, counters) lives in a fixed 32 MiB __device__ array

@@ -81,6 +81,7 @@ int EVSLStart(void) {
     memset(&evslh, 0, sizeof(evslh));
     evslh.seed = 0x5EEDULL;
     evslh.kernel = -1;
+    evslh.l2_resident = 0;
   }
   evslh.started = 1;
   return 0;
@@ -118,6 +119,8 @@ static int register_csr(csrMat *A, int on_device) {
   if (!evslh.mat) return from_cu(EVSLX_ERR_ARG);
   if (evslh.kernel >= 0) evslcu_mat_set_kernel(evslh.mat, evslh.kernel);
   evslcu_mat_set_persistent(evslh.mat, evslh.persistent);
+  if (evslh.l2_resident) evslcu_mat_l2_persist(evslh.mat, 1);
+  evslcu_mat_set_wave(evslh.mat, evslh.wave);
   evslh.mat_key = A;
   evslh.op.A = evslh.mat;
   evslh.op.func = NULL;
@@ -472,6 +475,18 @@ void evsl_dgemm_device(const char *transa, const char *transb, int *m, int *n, i
 /* ---------------------------------------------------------------------------
  * Extensions (include/evslx.h)
  * ------------------------------------------------------------------------- */
+int evslx_set_filter_wave(int on) {
+  evslh.wave = on ? 1 : 0;
+  if (evslh.mat) return from_cu(evslcu_mat_set_wave(evslh.mat, evslh.wave));
+  return 0;
+}
+
+int evslx_set_l2_resident(int on) {
+  evslh.l2_resident = on ? 1 : 0;
+  if (evslh.mat) return from_cu(evslcu_mat_l2_persist(evslh.mat, evslh.l2_resident));
+  return 0;
+}
+
 int evslx_set_seed(uint64_t seed) {
   evslh.seed = seed;
   evslh.draw = 0;

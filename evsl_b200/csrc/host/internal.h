@@ -30,6 +30,8 @@ typedef struct {
   uint64_t draw;             /* next draw index of the device RNG */
   int kernel;                /* filter kernel choice, -1 = library default */
   int persistent;            /* 1: one cooperative launch per filter application */
+  int l2_resident;           /* 1: keep the stored matrix persisting in L2 */
+  int wave;                  /* 1: pipelined single-launch filter */
   double last_kpm_seconds;   /* device time of the last kpmdos moment loop */
   int last_kdim;             /* Lanczos dimension of the last ChebLanNr/ChebLanTr */
   int last_candidates;       /* Ritz values >= bar examined at the end */

@@ -109,6 +109,19 @@ int evslx_set_filter_block(int threads);
  * from the row when they fit.  Applies to matrices registered afterwards;
  * default on.  Results are identical either way. */
 int evslx_set_matrix_compression(int on);
+/* Run each filter application as one pipelined launch: rows in tiles, work
+ * items (degree, tile) handed out in order, a tile's degree k waiting only
+ * for degree k-1 of the tiles its rows reach (bounded waits).  Results are
+ * bitwise those of the per-degree launches. */
+int evslx_set_filter_wave(int on);
+
+/* Keep the registered matrix's stored arrays resident in L2 (a persisting
+ * access-policy window on the library stream with this process's persisting
+ * L2 set-aside sized to them, up to the device maximum; released when the
+ * matrix is dropped or at EVSLFinish).  Default off (measured no gain for the
+ * 3-D Laplacian 100^3, whose working set already stays in L2); results are
+ * identical either way. */
+int evslx_set_l2_resident(int on);
 /* Bytes per stored value (4 or 8) and per stored column index (2 or 4). */
 int evslx_matrix_storage(int *value_bytes, int *index_bytes);
 

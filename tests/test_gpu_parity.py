@@ -227,13 +227,14 @@ def test_tiny_problem(gpu_lib):
 
 
 @pytest.mark.parametrize("compress", [True, False])
-@pytest.mark.parametrize("persistent", [True, False])
-def test_filter_variants_bitwise(gpu_lib, compress, persistent):
+@pytest.mark.parametrize("mode", ["per-degree", "persistent", "wave"])
+def test_filter_variants_bitwise(gpu_lib, compress, mode):
     """Every storage variant (float/double values, int16/int32 columns) and
-    both execution modes (one cooperative launch / one launch per degree)
-    give the reference's filtered vector bit for bit."""
+    every execution mode (one launch per degree / one cooperative launch /
+    one pipelined launch) give the reference's filtered vector bit for bit."""
     gpu_lib.set_matrix_compression(compress)
-    gpu_lib.set_filter_persistent(persistent)
+    gpu_lib.set_filter_persistent(mode == "persistent")
+    gpu_lib.set_filter_wave(mode == "wave")
     try:
         cases = []
         ia, ja, a = O.lap_csr(24, 24, 24)
@@ -274,7 +275,8 @@ def test_filter_variants_bitwise(gpu_lib, compress, persistent):
             gpu_lib.free_pol(pol)
     finally:
         gpu_lib.set_matrix_compression(True)
-        gpu_lib.set_filter_persistent(True)
+        gpu_lib.set_filter_persistent(False)
+        gpu_lib.set_filter_wave(False)
 
 
 def test_laplacian_storage_is_compressed(gpu_lib):
