@@ -423,7 +423,7 @@ int variant_of(const evslcu_mat *A, int fp32, int B) {
 // (matrix, precision, width), outside any stream capture.
 int autotune(evslcu_mat *A, int fp32, int B) {
   signed char &slot = A->mf_variant[fp32 ? 1 : 0][log2_width(B)];
-  if (slot >= 0 || g_mf_variant >= 0) return 0;
+  if (slot >= 0) return 0;
   const int n = A->n, steps = 6;
   const size_t vb = fp32 ? sizeof(float) : sizeof(double);
   const size_t blk = ((size_t)n * B * vb + 255) / 256 * 256;
@@ -437,6 +437,7 @@ int autotune(evslcu_mat *A, int fp32, int B) {
   float best = 1e30f;
   int bestv = 0;
   for (int v = 0; !rc && v < 4; ++v) {
+    if (g_mf_variant >= 0 && v != g_mf_variant) continue;  // a forced variant is only timed
     float ms = 0.0f;
     for (int rep = 0; !rc && rep < 2; ++rep) {
       cudaEventRecord(e0, stream());
@@ -485,7 +486,10 @@ int autotune(evslcu_mat *A, int fp32, int B) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   evslcu_free(buf);
-  if (!rc) slot = (signed char)bestv;
+  if (!rc) {
+    slot = (signed char)bestv;
+    A->mf_cost_us[fp32 ? 1 : 0][log2_width(B)] = 1000.0f * best / steps;
+  }
   return rc;
 }
 
@@ -667,6 +671,14 @@ int evslcu_get_filter_variant(void) { return g_mf_variant; }
 
 int evslcu_mat_filter_variant(const evslcu_mat *A, int fp32, int B) {
   return A ? A->mf_variant[fp32 ? 1 : 0][log2_width(B)] : -1;
+}
+
+double evslcu_filter_step_cost(evslcu_mat *A, int fp32, int B) {
+  if (!A || A->kernel != 0 || B < 1) return -1.0;
+  if (fp32 && A->vfmt == 0 && !A->sval32) return -1.0;
+  const int Bp = group_width(std::min(B, kMaxB));
+  if (autotune(A, fp32, Bp)) return -1.0;
+  return (double)A->mf_cost_us[fp32 ? 1 : 0][log2_width(Bp)];
 }
 
 void evslcu_filter_plan_destroy(evslcu_filter_plan *P) {

@@ -31,6 +31,7 @@ struct evslcu_mat {
   size_t sell_bytes = 0;
   void *sval32 = nullptr;  // FP32 copy of sval for the FP32 filter (when vfmt == 0)
   signed char mf_variant[2][5] = {{-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1}};  // tuned kernel per (fp32, log2 B)
+  float mf_cost_us[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};  // its measured time per degree step
   long long bandwidth = 0;  // max |col - row| over the stored entries
   int wave = 0;             // 1: pipelined single-launch filter (wavefilter.cu)
   unsigned *wave_ctl = nullptr;

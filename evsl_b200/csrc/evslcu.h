@@ -197,6 +197,10 @@ int evslcu_set_filter_variant(int v);
 int evslcu_get_filter_variant(void);
 /* Variant the autotuner chose for A (fp32, block width B), -1 if untuned. */
 int evslcu_mat_filter_variant(const evslcu_mat *A, int fp32, int B);
+/* Measured device time (µs) of one degree step of the multi-column filter on
+ * A with B columns (rounded up to the block width), from the autotuner
+ * (timed on first use); < 0 if unavailable. */
+double evslcu_filter_step_cost(evslcu_mat *A, int fp32, int B);
 void evslcu_filter_plan_destroy(evslcu_filter_plan *P);
 /* COO (device arrays, indices base 0 or 1) -> CSR on the device: rows in
  * order, entries of a row sorted by column with ties in input order (the

@@ -30,7 +30,9 @@
  * below it -- is filtered with an FP64 filter designed (find_pol, same
  * settings) for the interval spanned by the candidates' Rayleigh quotients,
  * orthonormalised, and a Rayleigh-Ritz step with A gives the new pairs,
- * repeated (at most 4 sweeps) while a pair inside [a, b] misses tol.  The
+ * repeated while a pair inside [a, b] misses tol (at most 4 sweeps for
+ * filters of degree >= 128, up to 24 for low degrees, whose sweeps are cheap
+ * but damp little).  The
  * guards put the eigenvectors next to [a, b], which a filter damps weakly,
  * inside the Rayleigh-Ritz subspace; the wider interval then needs a filter
  * of lower degree (about 0.6 of the slice's) and usually one sweep.
@@ -107,6 +109,8 @@ struct evslx_engine {
   const double **xs;
   double **ys;
   uint64_t *uidbuf;
+  double *gbest;
+  int *gcut, *gstart;
   plan_cache_t *plans;
   int nplans;
   uint64_t next_uid;
@@ -181,9 +185,13 @@ evslx_engine *evslx_engine_create(int max_slots, size_t hbm_budget, int precisio
   E->xs = (const double **)malloc(sizeof(double *) * (size_t)max_slots);
   E->ys = (double **)malloc(sizeof(double *) * (size_t)max_slots);
   E->uidbuf = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)max_slots);
+  E->gbest = (double *)malloc(sizeof(double) * ((size_t)max_slots + 1));
+  E->gcut = (int *)malloc(sizeof(int) * ((size_t)max_slots + 1));
+  E->gstart = (int *)malloc(sizeof(int) * ((size_t)max_slots + 1));
   E->plans = (plan_cache_t *)calloc((size_t)max_slots, sizeof(plan_cache_t));
   E->use_graphs = 1;
-  if (!E->slots || !E->ds || !E->hs || !E->cols || !E->colslot || !E->xs || !E->ys || !E->uidbuf || !E->plans) {
+  if (!E->slots || !E->ds || !E->hs || !E->cols || !E->colslot || !E->xs || !E->ys || !E->uidbuf || !E->plans ||
+      !E->gbest || !E->gcut || !E->gstart) {
     evsl_seterr(EVSLX_ERR_NOMEM, "evslx_engine_create: out of memory");
     evslx_engine_free(E);
     return NULL;
@@ -247,6 +255,9 @@ void evslx_engine_free(evslx_engine *E) {
   free(E->xs);
   free(E->ys);
   free(E->uidbuf);
+  free(E->gbest);
+  free(E->gcut);
+  free(E->gstart);
   free(E);
 }
 
@@ -556,7 +567,10 @@ static int refine_fp64(evslx_engine *E, slot_t *s, int m, double *U, double *W, 
     rc = evsl_seterr(rc, "%s", evslcu_errstr()); \
     break;                                      \
   }
-  for (*sweeps = 0; !rc && *sweeps < ENG_MAX_SWEEPS; (*sweeps)++) {
+  /* a sweep costs (m + guards) x degree column-degree steps; low-degree
+   * filters damp little per sweep but are cheap, so they get more sweeps */
+  const int max_sweeps = evsl_max(ENG_MAX_SWEEPS, evsl_min(24, (ENG_MAX_SWEEPS * 128 + pw.deg - 1) / evsl_max(pw.deg, 1)));
+  for (*sweeps = 0; !rc && *sweeps < max_sweeps; (*sweeps)++) {
     int missing = 0;
     for (int j = 0; j < m; j++)
       if (rlam[j] >= aa - slack && rlam[j] <= bb + slack && !(rres[j] < tol)) missing++;
@@ -735,10 +749,9 @@ int evslx_engine_step(evslx_engine *E) {
   if (E->nactive == 0) return evslx_engine_pending(E);
   const int fp32 = (E->precision == EVSLX_PREC_MIXED);
   /* 1. filters: the active slots of each matrix, in order of decreasing
-   * degree, are cut into groups of at most 16 columns whose degrees are at
-   * least half the group's first (a group runs to its largest degree; one
-   * step on B columns costs far less than B single steps);
-   * each group is one captured multi-column filter. */
+   * degree, are cut into groups of at most 16 columns (a group runs to its
+   * largest degree) by the measured cost of each width; each group is one
+   * captured multi-column filter. */
   for (int i = 0; i < E->nplans; i++) E->plans[i].used = 0;
   for (int i = 0; i < E->max_slots; i++) E->colslot[i] = -1;
   for (int i = 0; i < E->max_slots; i++) {
@@ -783,11 +796,51 @@ int evslx_engine_step(evslx_engine *E) {
       E->uidbuf[b2 + 1] = uv;
     }
     if (fp32 && (rc = evslcu_mat_prepare_fp32(M->mat))) return evsl_seterr(rc, "%s", evslcu_errstr());
-    for (int g0 = 0; g0 < nc;) {
-      int g1 = g0 + 1;
-      while (g1 < nc && g1 - g0 < 16 && 2 * E->cols[g1].deg >= E->cols[g0].deg) g1++;
+    /* groups: contiguous runs of the degree-sorted columns chosen to minimise
+     * sum over groups of (largest degree) x (measured time of one degree step
+     * at that width) -- the autotuner's timings for this matrix */
+    double cost[17];
+    int have_cost = 1;
+    for (int b = 1; b <= 16 && have_cost; b++) {
+      cost[b] = evslcu_filter_step_cost(M->mat, fp32, b);
+      if (cost[b] <= 0.0) have_cost = 0;
+    }
+    int ng = 0;
+    if (have_cost) {
+      double *best = E->gbest;
+      int *cut = E->gcut;
+      best[0] = 0.0;
+      for (int i2 = 1; i2 <= nc; i2++) {
+        best[i2] = 1e300;
+        for (int g = 1; g <= 16 && g <= i2; g++) {
+          const int j2 = i2 - g;
+          const double v = best[j2] + (double)E->cols[j2].deg * cost[g];
+          if (v < best[i2]) {
+            best[i2] = v;
+            cut[i2] = j2;
+          }
+        }
+      }
+      for (int i2 = nc; i2 > 0; i2 = cut[i2]) E->gstart[ng++] = cut[i2];
+    } else {
+      for (int g0 = 0; g0 < nc;) {
+        int g1 = g0 + 1;
+        while (g1 < nc && g1 - g0 < 16 && 2 * E->cols[g1].deg >= E->cols[g0].deg) g1++;
+        E->gstart[ng++] = g0;
+        g0 = g1;
+      }
+      for (int a3 = 0, b3 = ng - 1; a3 < b3; a3++, b3--) {
+        const int t3 = E->gstart[a3];
+        E->gstart[a3] = E->gstart[b3];
+        E->gstart[b3] = t3;
+      }
+    }
+    /* gstart holds the group starts in decreasing order (DP) or increasing
+     * order (fallback, reversed above to decreasing) */
+    for (int gi = 0; gi < ng; gi++) {
+      const int g0 = E->gstart[gi];
+      const int g1 = (gi == 0) ? nc : E->gstart[gi - 1];
       if ((rc = run_group_filter(E, M, g1 - g0, E->cols + g0, E->uidbuf + g0, fp32))) return rc;
-      g0 = g1;
     }
     evslstat.n_polAv += nc;
   }

@@ -172,8 +172,8 @@ int evslx_coo_to_csr_device(int cooidx, const cooMat *coo, int coo_on_device, cs
  * FP32; Lanczos, orthogonalisation, Ritz step in FP64; Ritz pairs refined by
  * FP64 filtered Rayleigh-Ritz sweeps over the candidates plus half as many
  * guard vectors (at least 16), with a filter designed for the interval the
- * candidates span, until every pair inside [a, b] meets tol, at most 4
- * sweeps).
+ * candidates span, until every pair inside [a, b] meets tol: at most 4
+ * sweeps for filters of degree >= 128, up to 24 for low degrees).
  * ------------------------------------------------------------------------- */
 #define EVSLX_PREC_FP64 0
 #define EVSLX_PREC_MIXED 1

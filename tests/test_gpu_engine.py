@@ -269,3 +269,50 @@ def test_mixed_precision_random_spd(gpu_lib):
     assert np.max(np.abs(np.sort(lam32) - exact)) <= 1e-8 * width
     assert np.all(res64 < 1e-8) and np.all(res32 < 1e-8)
     gpu_lib.free_pol(pol)
+
+
+@pytest.mark.parametrize("precision", [E.PREC_FP64, E.PREC_MIXED])
+def test_engine_many_uneven_instances(gpu_lib, precision):
+    """Batched uneven instances: 12 independent 2-D/3-D Laplacians with n
+    log-uniform in [1e3, 3e4] (sizes from a seed), each with its own interval
+    of 20-60 eigenvalues and its own filter degree, all in one engine."""
+    rng = np.random.default_rng(4)
+    eng = gpu_lib.engine(12, precision=precision)
+    mats, expect, pols = [], {}, []
+    for i in range(12):
+        nn = int(np.exp(rng.uniform(np.log(1e3), np.log(3e4))))
+        if i % 2 == 0:
+            s = max(int(round(np.sqrt(nn))), 10)
+            dims, hi = (s, s + i % 3, 1), 8.0
+        else:
+            s = max(int(round(nn ** (1 / 3))), 8)
+            dims, hi = (s, s + 1, s), 12.0
+        ia, ja, a = O.lap_csr(*dims)
+        ev = np.sort(W.laplacian_eigenvalues(*dims))
+        a0, b0, cnt = W.gap_interval(ev, float(rng.uniform(0.3, 1.5)), int(rng.integers(20, 61)))
+        iv = [a0, b0, 0.0, hi]
+        M = gpu_lib.matrix(ia, ja, a)
+        pol = gpu_lib.find_pol(iv)
+        mats.append(M)
+        pols.append(pol)
+        expect[i] = ev[(ev >= a0) & (ev <= b0)]
+        eng.submit_slice(M, iv, pol, 2000, 1e-8, O.seeded_normal(len(ia) - 1, i), i)
+    eng.run()
+    n_done = 0
+    while True:
+        r = eng.pop()
+        if r is None:
+            break
+        ex = expect[r["tag"]]
+        assert r["rc"] == 0 and r["nev"] == len(ex)
+        width = 8.0 if r["tag"] % 2 == 0 else 12.0
+        tol_eig = (1e-10 if precision == E.PREC_FP64 else 1e-8) * width
+        assert np.max(np.abs(np.sort(r["lam"]) - ex)) <= tol_eig
+        assert np.all(r["res"] < 1e-8)
+        n_done += 1
+    assert n_done == 12
+    eng.free()
+    for M in mats:
+        M.free()
+    for p in pols:
+        gpu_lib.free_pol(p)
