@@ -53,7 +53,8 @@ def parse():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--count", type=int, default=COUNT)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve", "lap3d-multifilter"],
+    p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve", "lap3d-multifilter",
+                                          "lap3d-reorth"],
                    default="lap3d-slice",
                    help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark); "
                         "lap3d-batch: several slices through the request engine; serve: a Poisson request stream")
@@ -71,6 +72,7 @@ def parse():
     p.add_argument("--low-degree", action="store_true", help="lap3d-multifilter: only the degree-7 filter")
     p.add_argument("--l2-resident", action="store_true",
                    help="keep the stored matrix persisting in L2 (comparison runs)")
+    p.add_argument("--maxit-reorth", type=int, default=600, help="lap3d-reorth: Lanczos steps")
     p.add_argument("--filter-mode", choices=["per-degree", "wave"], default="per-degree",
                    help="filter execution: one launch per degree or one pipelined launch")
     return p.parse_args()
@@ -572,6 +574,49 @@ def run_multifilter(args):
     lib.free_pol(p_lo)
 
 
+def run_reorth(args):
+    """lap3d-reorth: ChebLanNr FP64 on the 3-D Laplacian 100^3 over [0.6, 0.9]
+    (thousands of eigenvalues, so the restricted-trace test does not stop it)
+    with maxit = `--maxit-reorth` (default 600): a run where the full
+    reorthogonalisation (classical Gram-Schmidt + DGKS against the whole
+    basis, 16 n k bytes per pass at step k) is a large share of the time.
+    Reports the time per Lanczos step; the CGS kernels' own numbers come from
+    ncu on this command."""
+    import torch
+
+    import evsl_b200
+    from evsl_b200 import workloads as W
+
+    lib = evsl_b200.Library()
+    ia, ja, a = W.laplacian_csr(NX, NY, NZ)
+    lib.set_csr(ia, ja, a)
+    iv = [0.6, 0.9, LMIN, LMAX]
+    pol = lib.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+    n = NX * NY * NZ
+    v0 = np.random.default_rng(SEED).standard_normal(n)
+    v0 /= np.linalg.norm(v0)
+    lstream = torch.cuda.ExternalStream(lib.stream_handle())
+    k = args.maxit_reorth
+    times = []
+    for step in range(args.warmup + args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lstream)
+        lam, Y, res = lib.cheblan_nr(iv, k, TOL, v0, pol, want_vectors=False)
+        e1.record(lstream)
+        e1.synchronize()
+        if step >= args.warmup:
+            times.append(e0.elapsed_time(e1) / 1e3)
+    t = statistics.median(times)
+    kdim, _ = lib.last_solve_info()
+    cgs_bytes = 2 * 16.0 * n * kdim * (kdim + 1) / 2  # two passes over V^T and V per step
+    print(json.dumps({"workload": "lap3d-reorth: ChebLanNr FP64, [0.6, 0.9], maxit %d, filter degree %d" % (k, pol.deg),
+                      "seconds_per_solve": t, "ms_per_lanczos_step": 1e3 * t / max(kdim, 1),
+                      "lanczos_steps": int(kdim), "cgs_bytes_two_passes": cgs_bytes,
+                      "eigenpairs": int(len(lam))}))
+    lib.free_pol(pol)
+
+
 def _slice_plan(ev, start, nslices, count):
     """Consecutive gap-midpoint intervals of `count` eigenvalues from `start`."""
     from evsl_b200 import workloads as W
@@ -734,6 +779,7 @@ def run_serve(args):
 
     t0 = _t.perf_counter()
     i, done, lat, lat_slice, found, ok = 0, 0, [], [], 0, True
+    failures = []
     while i < len(reqs) or eng.pending() > 0:
         now = _t.perf_counter() - t0
         while i < len(reqs) and reqs[i][1] <= now:
@@ -767,10 +813,16 @@ def run_serve(args):
                 exact = ev[(ev >= iv[0]) & (ev <= iv[1])]
                 good = r["rc"] == 0 and r["nev"] == len(exact) and bool(np.all(r["res"] < TOL))
                 ok = ok and good
+                if not good and len(failures) < 10:
+                    failures.append({"kind": kind, "dims": dims, "interval": iv[:2], "rc": r["rc"], "nev": r["nev"],
+                                     "exact": int(len(exact)), "lanczos_steps": r["lanczos_steps"],
+                                     "max_res": float(np.max(r["res"])) if r["nev"] else None})
                 found += r["nev"]
                 lib.free_pol(pols.pop(k))
             else:
                 ok = ok and r["rc"] == 0
+                if r["rc"] != 0 and len(failures) < 10:
+                    failures.append({"kind": kind, "dims": dims, "rc": r["rc"]})
     wall = _t.perf_counter() - t0
     eng.free()
     for Mx, _ in mats.values():
@@ -789,7 +841,7 @@ def run_serve(args):
                        "slice_p99": float(np.percentile(lat_slice, 99)) if lat_slice else None},
         "e2e": {"value": found / wall, "unit": UNIT, "h2d_bytes_per_step": n_h2d / max(len(reqs), 1),
                 "d2h_bytes_per_step": 16 * found / max(len(reqs), 1)},
-        "all_ok": bool(ok)}))
+        "all_ok": bool(ok), "failures": failures}))
 
 
 def main():
@@ -804,6 +856,8 @@ def main():
         run_serve(args)
     elif args.workload == "lap3d-multifilter":
         run_multifilter(args)
+    elif args.workload == "lap3d-reorth":
+        run_reorth(args)
     else:
         run_ours(args)
 

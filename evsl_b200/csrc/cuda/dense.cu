@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(kThreads)
     const double *q = Q + (long long)j * ld + r0;
     double acc = 0.0;
 #pragma unroll 8
-    for (int i = lane; i < rows; i += 32) acc += __ldg(q + i) * sv[i];
+    for (int i = lane; i < rows; i += 32) acc += __ldg(q + i) * sv[i];  // 32 loads per lane, unrolled
     acc = warp_sum(acc);
     if (lane == 0) part[(long long)blockIdx.x * k + j] = acc;
   }
@@ -125,9 +125,18 @@ __global__ void __launch_bounds__(kThreads)
       for (int j = threadIdx.x; j < cnt; j += blockDim.x) sh_h[j] = alpha * h[j0 + j];
       __syncthreads();
       if (r < n) {
+        // 16 column loads in flight per thread, then the updates in column
+        // order (the summation order is unchanged)
         const double *q = Q + (long long)j0 * ld + r;
-#pragma unroll 8
-        for (int j = 0; j < cnt; ++j) z = __dadd_rn(z, __dmul_rn(sh_h[j], __ldg(q + (long long)j * ld)));
+        int j = 0;
+        for (; j + 16 <= cnt; j += 16) {
+          double x[16];
+#pragma unroll
+          for (int u = 0; u < 16; ++u) x[u] = __ldg(q + (long long)(j + u) * ld);
+#pragma unroll
+          for (int u = 0; u < 16; ++u) z = __dadd_rn(z, __dmul_rn(sh_h[j + u], x[u]));
+        }
+        for (; j < cnt; ++j) z = __dadd_rn(z, __dmul_rn(sh_h[j], __ldg(q + (long long)j * ld)));
       }
     }
     if (r < n) {

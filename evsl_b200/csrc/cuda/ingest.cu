@@ -336,6 +336,19 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
   long long padded = 0;
   if (!rc) rc = evslcu_d2h(&padded, M->cptr + nch, sizeof(long long));
   if (rc) return rc;
+  // uniform chunk width: the filter kernels compute row offsets instead of
+  // loading them (one dependent load less per row)
+  {
+    int *hcw = (int *)malloc(sizeof(int) * (size_t)nch);
+    M->ellw = 0;
+    if (hcw && !evslcu_d2h(hcw, M->cw, sizeof(int) * (size_t)nch)) {
+      int u = hcw[0];
+      for (int c = 1; c < nch && u > 0; ++c)
+        if (hcw[c] != u) u = 0;
+      M->ellw = u > 0 ? u : 0;
+    }
+    free(hcw);
+  }
   M->padded = padded;
   const size_t cap = (size_t)std::max(padded, 1LL);
   const size_t colb = M->ifmt ? sizeof(short) : sizeof(int);

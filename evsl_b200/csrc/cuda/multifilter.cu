@@ -166,9 +166,9 @@ __global__ void __launch_bounds__(kThreads)
     VT acc[CPT];
 #pragma unroll
     for (int c = 0; c < CPT; ++c) acc[c] = (VT)0;
-    const int ch = r >> 5;
-    long long p = A.cptr[ch] + (r & 31);
-    const int w = A.cw[ch];
+    long long p;
+    int w;
+    row_start(A, r, p, w);
     if constexpr (COOP) {
       // TPR entries per batch: thread q loads entry j0 + q of its row, the
       // row's threads exchange them, then gather and accumulate in order
@@ -455,8 +455,8 @@ int autotune(evslcu_mat *A, int fp32, int B) {
               default: return mf_step<float, 16>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
             }
           };
-          rc = A->ifmt ? go(SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals})
-                       : go(SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals});
+          rc = A->ifmt ? go(SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals, A->ellw})
+                       : go(SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals, A->ellw});
         } else {
           rc = with_view(A, [&](auto view) -> int {
             if constexpr (std::is_same<decltype(view), CsrView>::value) {
@@ -522,10 +522,10 @@ int mf_sequence(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_co
       const float *cf = (const float *)coef + off;
       const void *vals = (A->vfmt == 1) ? A->sval : A->sval32;
       if (A->ifmt)
-        rc = mf_dispatch<float>(SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals},
+        rc = mf_dispatch<float>(SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals, A->ellw},
                                 variant_of(A, 1, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
       else
-        rc = mf_dispatch<float>(SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals},
+        rc = mf_dispatch<float>(SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals, A->ellw},
                                 variant_of(A, 1, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
     } else {
       double *P = (double *)w, *W0 = (double *)(w + blk), *W1 = (double *)(w + 2 * blk), *Y = (double *)(w + 3 * blk);

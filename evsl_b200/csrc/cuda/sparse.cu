@@ -118,46 +118,6 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Filter step for a block of columns (column-major n x ncols blocks).  The
-// row's entries are read once per group of kBlockCols columns; every column
-// gets exactly the arithmetic of k_cheb, so each column of the result equals
-// the single-vector filter bit for bit.
-constexpr int kBlockCols = 8;
-
-template <class M, bool FIRST>
-__global__ void __launch_bounds__(kThreads)
-    k_cheb_block(M A, int ncols, const double *__restrict__ vk, const double *vkm1, double *out,
-                 double *__restrict__ Y, double t, double ncc, double s, double mu0) {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  const long long n = A.n;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) {
-    for (int c0 = 0; c0 < ncols; c0 += kBlockCols) {
-      const int cn = min(kBlockCols, ncols - c0);
-      double acc[kBlockCols];
-#pragma unroll
-      for (int c = 0; c < kBlockCols; ++c) acc[c] = 0.0;
-      const double *xb = vk + (long long)c0 * n;
-      row_for_each(A, r, [&](double v, int col) {
-#pragma unroll
-        for (int c = 0; c < kBlockCols; ++c)
-          if (c < cn) acc[c] = __dadd_rn(acc[c], __dmul_rn(v, __ldg(xb + (long long)c * n + col)));
-      });
-#pragma unroll
-      for (int c = 0; c < kBlockCols; ++c) {
-        if (c >= cn) break;
-        const long long idx = (long long)(c0 + c) * n + r;
-        const double x = vk[idx];
-        double w = __dmul_rn(t, __dadd_rn(acc[c], __dmul_rn(ncc, x)));
-        if (!FIRST) w = __dadd_rn(w, -vkm1[idx]);
-        out[idx] = w;
-        const double yo = FIRST ? __dmul_rn(mu0, x) : Y[idx];
-        Y[idx] = __dadd_rn(yo, __dmul_rn(s, w));
-      }
-    }
-  }
-}
-
 // Stand-alone update for a user matvec (SRC/evsl_cuda.cu:175-184 semantics,
 // CPU-build operation order).
 __global__ void k_cheb_update(int n, int k, double t, double s, double ncc, double *vkp1, const double *vk,
@@ -847,45 +807,23 @@ int evslcu_chebav_block(const evslcu_op *op, const double *mu, int deg, double c
                         const double *V, double *Y, double *work) {
   if (!op || !mu || deg < 0 || ncols < 1 || !V || !Y || !work) return fail(EVSLCU_ERR_ARG, "chebav_block: bad args");
   const int n = op->n;
-  if (!op->A || deg == 0) {
+  if (!op->A || deg == 0 || op->A->kernel != 0) {
     for (int c = 0; c < ncols; ++c) {
       int rc = evslcu_chebav(op, mu, deg, cc, dd, V + (size_t)c * n, Y + (size_t)c * n, work, nullptr);
       if (rc) return rc;
     }
     return 0;
   }
-  const evslcu_mat *A = op->A;
-  const double t1 = 1.0 / dd, t2 = 2.0 / dd, ncc = -cc;
-  const size_t blk = (size_t)n * ncols;
-  double *W[2] = {work, work + blk};
-  const int grid = grid_for(n);
-  for (int k = 1; k <= deg; ++k) {
-    const double t = (k == 1) ? t1 : t2;
-    const double *vk = (k == 1) ? V : W[(k - 2) % 2];
-    const double *vkm1 = (k == 1) ? nullptr : ((k == 2) ? V : W[(k - 1) % 2]);
-    double *out = W[(k - 1) % 2];
-    int rc = with_view(A, [&](auto view) {
-      using VIEW = decltype(view);
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(grid);
-      cfg.blockDim = dim3(kThreads);
-      cfg.stream = stream();
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-      attr[0].val.programmaticStreamSerializationAllowed = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      cudaError_t e = (k == 1) ? cudaLaunchKernelEx(&cfg, k_cheb_block<VIEW, true>, view, ncols, vk, vkm1, out, Y, t,
-                                                    ncc, mu[k], mu[0])
-                               : cudaLaunchKernelEx(&cfg, k_cheb_block<VIEW, false>, view, ncols, vk, vkm1, out, Y,
-                                                    t, ncc, mu[k], mu[0]);
-      if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "block filter launch failed: %s", cudaGetErrorString(e));
-      EVSLCU_LAUNCH_CHECK("k_cheb_block");
-      return 0;
-    });
-    if (rc) return rc;
-  }
-  return 0;
+  // the multi-column filter (interleaved blocks of up to 16 columns); each
+  // column bitwise equal to evslcu_chebav
+  std::vector<evslcu_filter_col> cols((size_t)ncols);
+  for (int c = 0; c < ncols; ++c) cols[c] = evslcu_filter_col{mu, deg, cc, dd, V + (size_t)c * n, Y + (size_t)c * n};
+  const size_t need = evslcu_filter_columns_work(n, 0, ncols);
+  void *w = evslcu_malloc(need);
+  if (!w) return fail(EVSLCU_ERR_NOMEM, "chebav_block: out of device memory");
+  int rc = evslcu_filter_columns(op->A, 0, ncols, cols.data(), w, need);
+  evslcu_free(w);
+  return rc;
 }
 
 }  // extern "C"

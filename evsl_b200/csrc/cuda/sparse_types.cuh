@@ -33,6 +33,7 @@ struct evslcu_mat {
   signed char mf_variant[2][5] = {{-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1}};  // tuned kernel per (fp32, log2 B)
   float mf_cost_us[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};  // its measured time per degree step
   long long bandwidth = 0;  // max |col - row| over the stored entries
+  int ellw = 0;             // > 0: every SELL-32 chunk has this width
   int wave = 0;             // 1: pipelined single-launch filter (wavefilter.cu)
   unsigned *wave_ctl = nullptr;
   size_t wave_ctl_words = 0;
@@ -55,7 +56,21 @@ struct SellT {
   const int *__restrict__ cw;
   const IT *__restrict__ col;
   const VT *__restrict__ val;
+  int ellw;  // > 0: every chunk has this width (offsets computed, not loaded)
 };
+
+// Start of row r's entries and the width of its chunk.
+template <class VT, class IT>
+__device__ __forceinline__ void row_start(const SellT<VT, IT> &A, int r, long long &p, int &w) {
+  const int c = r >> 5;
+  if (A.ellw > 0) {
+    w = A.ellw;
+    p = (long long)c * 32 * A.ellw + (r & 31);
+  } else {
+    p = A.cptr[c] + (r & 31);
+    w = A.cw[c];
+  }
+}
 
 struct CsrView {
   int n;
@@ -77,9 +92,9 @@ __device__ __forceinline__ double ldx(const double *p) {
 // Row r of A times x, summed left to right with rounded multiply and add.
 template <bool COHERENT, class VT, class IT>
 __device__ __forceinline__ double row_dot(const SellT<VT, IT> &A, int r, const double *x) {
-  const int c = r >> 5;
-  long long p = A.cptr[c] + (r & 31);
-  const int w = A.cw[c];
+  long long p;
+  int w;
+  row_start(A, r, p, w);
   double acc = 0.0;
 #pragma unroll 4
   for (int j = 0; j < w; ++j, p += 32) {
@@ -96,12 +111,10 @@ __device__ __forceinline__ double row_dot(const SellT<VT, IT> &A, int r, const d
 template <bool COHERENT, class VT, class IT>
 __device__ __forceinline__ void row_dot2(const SellT<VT, IT> &A, int r0, bool has1, const double *x, double &acc0,
                                          double &acc1) {
-  const int c0 = r0 >> 5;
-  const int lane = r0 & 31;
-  long long p0 = A.cptr[c0] + lane;
-  const int w0 = A.cw[c0];
-  long long p1 = has1 ? A.cptr[c0 + 1] + lane : 0;
-  const int w1 = has1 ? A.cw[c0 + 1] : 0;
+  long long p0, p1 = 0;
+  int w0, w1 = 0;
+  row_start(A, r0, p0, w0);
+  if (has1) row_start(A, r0 + 32, p1, w1);
   const int r1 = r0 + 32;
   acc0 = 0.0;
   acc1 = 0.0;
@@ -124,9 +137,9 @@ __device__ __forceinline__ void row_dot2(const SellT<VT, IT> &A, int r0, bool ha
 // Calls f(value, column) for the entries of row r, left to right.
 template <class VT, class IT, class F>
 __device__ __forceinline__ void row_for_each(const SellT<VT, IT> &A, int r, F &&f) {
-  const int c = r >> 5;
-  long long p = A.cptr[c] + (r & 31);
-  const int w = A.cw[c];
+  long long p;
+  int w;
+  row_start(A, r, p, w);
   for (int j = 0; j < w; ++j, p += 32) f((double)__ldg(A.val + p), decode_col(__ldg(A.col + p), r));
 }
 
@@ -150,7 +163,7 @@ __device__ __forceinline__ void row_for_each(const CsrView &A, int r, F &&f) {
 
 template <class VT, class IT>
 inline SellT<VT, IT> sell_view(const evslcu_mat *A) {
-  return SellT<VT, IT>{A->n, A->cptr, A->cw, (const IT *)A->scol, (const VT *)A->sval};
+  return SellT<VT, IT>{A->n, A->cptr, A->cw, (const IT *)A->scol, (const VT *)A->sval, A->ellw};
 }
 
 inline CsrView csr_view(const evslcu_mat *A) { return CsrView{A->n, A->ia, A->ja, A->a}; }

@@ -104,9 +104,9 @@ __global__ void __launch_bounds__(kWaveThreads) k_filter_wave(SellT<VT, IT> A, W
     const double mu0 = P.mu[0];
     const int r0 = t * kWaveRows, r1 = min(P.n, r0 + kWaveRows);
     for (int r = r0 + (int)threadIdx.x; r < r1; r += kWaveThreads) {
-      const int c = r >> 5;
-      long long p = A.cptr[c] + (r & 31);
-      const int w = A.cw[c];
+      long long p;
+      int w;
+      row_start(A, r, p, w);
       double acc = 0.0;
 #pragma unroll 4
       for (int j = 0; j < w; ++j, p += 32) {
