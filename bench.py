@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--slots", type=int, default=16, help="serve: slice solves in flight")
     p.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM budget of the engine")
     p.add_argument("--max-count", type=int, default=150, help="serve: most eigenvalues in a slice request")
+    p.add_argument("--serve-mix", choices=["default", "small"], default="default",
+                   help="serve: 'small' draws the large-matrix requests on the 2-D 100x100 Laplacian only")
     p.add_argument("--ncols", type=int, default=16, help="lap3d-multifilter: columns")
     p.add_argument("--variant", type=int, default=-1, help="lap3d-multifilter: kernel variant (-1 autotuned)")
     p.add_argument("--sweep", action="store_true", help="lap3d-multifilter: every variant/width/precision once")
@@ -740,7 +742,7 @@ def run_serve(args):
             mats[dims] = (lib.matrix(ia, ja, a), np.sort(W.laplacian_eigenvalues(*dims)))
         return mats[dims]
 
-    big = [(100, 100, 1), (NX, NY, NZ)]
+    big = [(100, 100, 1), (NX, NY, NZ)] if args.serve_mix == "default" else [(100, 100, 1), (100, 100, 1)]
     for d in big:
         matrix(d)
     # the arrival schedule and the requests, all drawn before the run
@@ -832,8 +834,8 @@ def run_serve(args):
         "ms_per_step": 1e3 * wall / max(len(reqs), 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 filter + f64" if prec == E.PREC_MIXED else "f64",
         "data": "synthetic (seeded Poisson request stream over Dirichlet Laplacians)",
-        "config": {"workload": "serve: Poisson %.2f req/s for %.0f s, %d slots, HBM budget %.0f GB, %s" % (
-            args.rate, args.duration, args.slots, args.budget_gb, args.precision),
+        "config": {"workload": "serve (%s mix): Poisson %.2f req/s for %.0f s, %d slots, HBM budget %.0f GB, %s" % (
+            args.serve_mix, args.rate, args.duration, args.slots, args.budget_gb, args.precision),
                    "requests": len(reqs), "completed": done},
         "latency_ms": {"p50": float(np.percentile(lat, 50)) if lat else None,
                        "p99": float(np.percentile(lat, 99)) if lat else None,

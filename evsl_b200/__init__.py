@@ -291,6 +291,7 @@ def load():
         "evslx_engine_pop_result": ([C.c_void_p, C.POINTER(EvslxResult)], C.c_int),
         "evslx_result_free": ([C.POINTER(EvslxResult)], None),
         "evslx_engine_use_graphs": ([C.c_void_p, C.c_int], None),
+        "evslx_set_mixed_min_rows": ([C.c_int], None),
         "evslx_set_filter_variant": ([C.c_int], C.c_int),
         "evslx_set_l2_resident": ([C.c_int], C.c_int),
         "evslx_set_filter_wave": ([C.c_int], C.c_int),
@@ -637,6 +638,11 @@ class Library:
         rc = self.lib.evslx_ChebLanNr_batch(ns, _d(iv), maxit, tol, dv.ptr, arr, precision, nev, lam, W, res)
         self._check(rc, "evslx_ChebLanNr_batch")
         return [self._outputs(nev[s], lam[s], W[s], res[s], want_vectors) for s in range(ns)]
+
+    def set_mixed_min_rows(self, rows):
+        """Engines created afterwards use the FP32 filter only on matrices
+        with at least this many rows."""
+        self.lib.evslx_set_mixed_min_rows(int(rows))
 
     def set_filter_variant(self, v):
         self._check(self.lib.evslx_set_filter_variant(v), "evslx_set_filter_variant")

@@ -94,6 +94,7 @@ typedef struct {
 
 struct evslx_engine {
   int max_slots, precision, keep_vectors;
+  int mixed_min_rows; /* mixed precision only for matrices with at least this many rows */
   size_t budget, in_use;
   slot_t *slots;
   int nactive;
@@ -165,6 +166,17 @@ long long evslx_matrix_device_bytes(const evslx_matrix *M) {
 /* ---------------------------------------------------------------------------
  * engine
  * ------------------------------------------------------------------------- */
+/* Below this many rows the FP32 filter saves little (the launches are latency
+ * bound) and the FP64 refinement costs more than it saves, so mixed-precision
+ * engines filter small matrices in FP64. */
+static int g_mixed_min_rows = 131072;
+
+void evslx_set_mixed_min_rows(int rows) { g_mixed_min_rows = rows < 0 ? 0 : rows; }
+
+static int slot_fp32(const evslx_engine *E, const evslx_matrix *M) {
+  return E->precision == EVSLX_PREC_MIXED && M->op.n >= E->mixed_min_rows;
+}
+
 evslx_engine *evslx_engine_create(int max_slots, size_t hbm_budget, int precision, int keep_vectors) {
   if (evsl_require_started()) return NULL;
   if (max_slots < 1 || (precision != EVSLX_PREC_FP64 && precision != EVSLX_PREC_MIXED)) {
@@ -177,6 +189,7 @@ evslx_engine *evslx_engine_create(int max_slots, size_t hbm_budget, int precisio
   E->precision = precision;
   E->keep_vectors = keep_vectors;
   E->budget = hbm_budget ? hbm_budget : (size_t)-1;
+  E->mixed_min_rows = g_mixed_min_rows;
   E->slots = (slot_t *)calloc((size_t)max_slots, sizeof(slot_t));
   E->ds = (double *)evslcu_malloc(sizeof(double) * ENG_NSCAL * (size_t)max_slots);
   E->hs = (double *)malloc(sizeof(double) * ENG_NSCAL * (size_t)max_slots);
@@ -644,7 +657,7 @@ static int finalize(evslx_engine *E, slot_t *s, int kdim, evslx_result *out) {
       sel[msel++] = i;
     }
   if (msel == 0) goto done;
-  if (E->precision == EVSLX_PREC_MIXED) {
+  if (slot_fp32(E, r->M)) {
     /* guard vectors for the refinement: the Ritz vectors of the next largest
      * Ritz values below bar, so that the eigenvectors just outside [a, b]
      * are resolved by the Rayleigh-Ritz step instead of damped by the
@@ -686,7 +699,7 @@ static int finalize(evslx_engine *E, slot_t *s, int kdim, evslx_result *out) {
       rc = 2; /* zero Ritz vector */
       goto done;
     }
-  if (E->precision == EVSLX_PREC_MIXED) {
+  if (slot_fp32(E, r->M)) {
     evslcu_free(EvecT_dev);
     EvecT_dev = NULL;
     if ((rc = refine_fp64(E, s, msel, Rvec, W, rnorm, rlam, rres, &out->refine_sweeps))) goto done;
@@ -747,7 +760,6 @@ int evslx_engine_step(evslx_engine *E) {
   int rc = admit(E);
   if (rc) return rc;
   if (E->nactive == 0) return evslx_engine_pending(E);
-  const int fp32 = (E->precision == EVSLX_PREC_MIXED);
   /* 1. filters: the active slots of each matrix, in order of decreasing
    * degree, are cut into groups of at most 16 columns (a group runs to its
    * largest degree) by the measured cost of each width; each group is one
@@ -758,6 +770,7 @@ int evslx_engine_step(evslx_engine *E) {
     slot_t *s0 = &E->slots[i];
     if (!s0->req || E->colslot[i] >= 0) continue;
     evslx_matrix *M = s0->req->M;
+    const int fp32 = slot_fp32(E, M);
     int nc = 0;
     for (int j = i; j < E->max_slots; j++) {
       slot_t *t = &E->slots[j];

@@ -211,6 +211,10 @@ int evslx_engine_submit_slice(evslx_engine *E, evslx_matrix *M, const double *in
 int evslx_engine_submit_kpm(evslx_engine *E, evslx_matrix *M, int Mdeg, int damping, int nvec, const double *intv,
                             uint64_t seed, uint64_t tag);
 int evslx_engine_step(evslx_engine *E);
+/* Mixed-precision engines created afterwards run the FP32 filter only on
+ * matrices with at least `rows` rows (default 131072) and filter smaller ones
+ * in FP64, where FP32 saves little and the refinement costs more. */
+void evslx_set_mixed_min_rows(int rows);
 /* Filters run as captured CUDA graphs, rebuilt when the set of requests on
  * a matrix changes (default on); plan_builds counts the captures. */
 void evslx_engine_use_graphs(evslx_engine *E, int on);

@@ -22,6 +22,15 @@ from oracle import evsl_oracle as O
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def mixed_on_small(gpu_lib):
+    """These tests check the mixed-precision path on small matrices, which
+    the engine would otherwise filter in FP64."""
+    gpu_lib.set_mixed_min_rows(0)
+    yield
+    gpu_lib.set_mixed_min_rows(131072)
+
+
 def _pols(lib, intvs, **kw):
     return [lib.find_pol(iv, **kw) for iv in intvs]
 
@@ -316,3 +325,26 @@ def test_engine_many_uneven_instances(gpu_lib, precision):
         M.free()
     for p in pols:
         gpu_lib.free_pol(p)
+
+
+def test_mixed_engine_filters_small_matrices_in_fp64(gpu_lib):
+    """With the default threshold a mixed engine runs small matrices in
+    FP64: the result equals the FP64 engine's bit for bit."""
+    gpu_lib.set_mixed_min_rows(131072)
+    ia, ja, a = O.lap_csr(40, 40, 1)
+    gpu_lib.set_csr(ia, ja, a)
+    M = gpu_lib.matrix(ia, ja, a)
+    iv = [0.7, 0.9, 0.0, 8.0]
+    pol = gpu_lib.find_pol(iv)
+    v = O.seeded_normal(1600, 3)
+    out = []
+    for prec in (E.PREC_FP64, E.PREC_MIXED):
+        eng = gpu_lib.engine(2, precision=prec)
+        eng.submit_slice(M, iv, pol, 1000, 1e-8, v, 1)
+        eng.run()
+        out.append(eng.pop())
+        eng.free()
+    assert out[0]["nev"] == out[1]["nev"] > 0 and out[1]["refine_sweeps"] == 0
+    assert np.array_equal(out[0]["lam"], out[1]["lam"])
+    M.free()
+    gpu_lib.free_pol(pol)
