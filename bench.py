@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--slots", type=int, default=16, help="serve: slice solves in flight")
     p.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM budget of the engine")
     p.add_argument("--max-count", type=int, default=150, help="serve: most eigenvalues in a slice request")
+    p.add_argument("--compare-sequential", action="store_true",
+                   help="lap3d-batch: also time ChebLanNr on the same slices one after another")
     p.add_argument("--serve-mix", choices=["default", "small"], default="default",
                    help="serve: 'small' draws the large-matrix requests on the 2-D 100x100 Laplacian only")
     p.add_argument("--ncols", type=int, default=16, help="lap3d-multifilter: columns")
@@ -656,6 +658,7 @@ def run_batch(args):
     v0 = np.random.default_rng(SEED).standard_normal(n)
     v0 /= np.linalg.norm(v0)
     lstream = torch.cuda.ExternalStream(lib.stream_handle())
+    widths = []
 
     def one_batch():
         eng = lib.engine(args.slices, precision=prec)
@@ -668,6 +671,7 @@ def run_batch(args):
             if r is None:
                 break
             out[int(r["tag"])] = r
+        widths.append(eng.group_widths())
         eng.free()
         return out
 
@@ -700,6 +704,20 @@ def run_batch(args):
     launches = lib.launch_count() - launches0
     clocks = sampler.stop()
     t = sum(times)
+    seq = None
+    if args.compare_sequential:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lstream)
+        nseq = 0
+        for s_, (iv, _) in enumerate(plan):
+            lam, _, _ = lib.cheblan_nr(iv, MAXIT, TOL, v0, pols[s_], want_vectors=False)
+            nseq += len(lam)
+        e1.record(lstream)
+        e1.synchronize()
+        tseq = e0.elapsed_time(e1) / 1e3
+        seq = {"eigenpairs": nseq, "seconds": tseq, "eigenpairs_per_s": nseq / tseq,
+               "engine_speedup": (found / t) / (nseq / tseq)}
     print(json.dumps({
         "metric": METRIC, "value": found / t, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -710,6 +728,8 @@ def run_batch(args):
                                                                               args.precision),
                    "filter_degrees": [int(p.deg) for p in pols], "tol": TOL, "maxit": MAXIT},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "filter_groups_by_width": widths[-1] if widths else None,
+        "sequential_chebLanNr_same_slices": seq,
         "accuracy": {"max_abs_eig_err_vs_analytic": max_err, "max_residual": max_res,
                      "bar": "counts exact, |err| <= 1e-8 x width, residual < 1e-8"},
         "all_steps_ok": bool(ok), "gpu_launches": int(launches), "clocks": clocks}))

@@ -298,6 +298,7 @@ def load():
         "evslx_get_filter_variant": ([], C.c_int),
         "evslx_tuned_filter_variant": ([C.c_int, C.c_int], C.c_int),
         "evslx_engine_plan_builds": ([C.c_void_p], C.c_uint64),
+        "evslx_engine_group_widths": ([C.c_void_p, C.POINTER(C.c_uint64)], None),
         "evslx_chebav_multi": ([C.c_int, C.POINTER(PolParams), C.c_void_p, C.c_void_p, C.c_int], C.c_int),
         "evslx_ChebLanNr_batch": ([C.c_int, _dp, C.c_int, C.c_double, C.c_void_p, C.POINTER(PolParams), C.c_int,
                                    _ip, C.POINTER(_dp), C.POINTER(C.c_void_p), C.POINTER(_dp)], C.c_int),
@@ -415,6 +416,12 @@ class Engine:
 
     def plan_builds(self):
         return self.lib.evslx_engine_plan_builds(self.ptr)
+
+    def group_widths(self):
+        """Filter groups launched so far by block width {1, 2, 4, 8, 16}."""
+        out = (C.c_uint64 * 5)()
+        self.lib.evslx_engine_group_widths(self.ptr, out)
+        return dict(zip((1, 2, 4, 8, 16), (int(x) for x in out)))
 
     def pop(self):
         """Next result as a dict (None if the result queue is empty)."""

@@ -117,6 +117,7 @@ struct evslx_engine {
   uint64_t next_uid;
   int use_graphs;
   uint64_t ticks, plan_builds;
+  uint64_t width_hist[5]; /* filter groups launched, by block width 1, 2, 4, 8, 16 */
 };
 
 /* ---------------------------------------------------------------------------
@@ -280,11 +281,32 @@ void evslx_engine_use_graphs(evslx_engine *E, int on) {
 
 uint64_t evslx_engine_plan_builds(const evslx_engine *E) { return E ? E->plan_builds : 0; }
 
+void evslx_engine_group_widths(const evslx_engine *E, uint64_t counts[5]) {
+  for (int i = 0; i < 5; i++) counts[i] = E ? E->width_hist[i] : 0;
+}
+
 /* Runs the filters of the nc columns cols (all on M, request ids uids)
  * through a cached graph when the same requests were filtered together
  * before, else captures one (or, with graphs off, launches directly). */
 static int run_group_filter(evslx_engine *E, evslx_matrix *M, int nc, const evslcu_filter_col *cols,
                             const uint64_t *uids, int fp32) {
+  int wb = 0;
+  while ((1 << wb) < nc && wb < 4) wb++;
+  E->width_hist[wb]++;
+  if (nc == 1 && !fp32) {
+    /* one FP64 column: the single-vector filter (per-degree launches with
+     * programmatic dependent launch), bitwise the same as the block kernel */
+    const size_t need = 2 * sizeof(double) * (size_t)M->op.n;
+    if (need > E->fwork_bytes) {
+      evslcu_free(E->fwork);
+      E->fwork = evslcu_malloc(need);
+      E->fwork_bytes = E->fwork ? need : 0;
+      if (!E->fwork) return evsl_seterr(EVSLX_ERR_NOMEM, "engine: out of device memory (filter work)");
+    }
+    int rc = evslcu_chebav(&M->op, cols[0].mu, cols[0].deg, cols[0].cc, cols[0].dd, cols[0].x, cols[0].y,
+                           (double *)E->fwork, NULL);
+    return rc ? evsl_seterr(rc, "%s", evslcu_errstr()) : 0;
+  }
   if (E->use_graphs) {
     plan_cache_t *pc = NULL;
     for (int i = 0; i < E->nplans && !pc; i++)

@@ -219,6 +219,9 @@ void evslx_set_mixed_min_rows(int rows);
  * a matrix changes (default on); plan_builds counts the captures. */
 void evslx_engine_use_graphs(evslx_engine *E, int on);
 uint64_t evslx_engine_plan_builds(const evslx_engine *E);
+/* Filter groups launched so far, by block width 1, 2, 4, 8, 16 (a group of
+ * one FP64 column runs the single-vector filter). */
+void evslx_engine_group_widths(const evslx_engine *E, uint64_t counts[5]);
 int evslx_engine_run(evslx_engine *E); /* step until nothing is queued or active */
 int evslx_engine_pending(const evslx_engine *E);
 size_t evslx_engine_bytes_in_use(const evslx_engine *E);
