@@ -79,6 +79,8 @@ def parse():
     p.add_argument("--maxit-reorth", type=int, default=600, help="lap3d-reorth: Lanczos steps")
     p.add_argument("--filter-mode", choices=["per-degree", "wave"], default="per-degree",
                    help="filter execution: one launch per degree or one pipelined launch")
+    p.add_argument("--row-patterns", choices=["on", "off"], default="on",
+                   help="row-pattern dictionary of the stored matrix (on: used when the rows allow it)")
     return p.parse_args()
 
 
@@ -193,6 +195,7 @@ def run_ours(args):
     if args.l2_resident:
         lib.set_l2_resident(True)
     lib.set_filter_wave(args.filter_mode == "wave")
+    lib.set_row_patterns(args.row_patterns == "on")
     ia, ja, a = W.laplacian_csr(NX, NY, NZ)
     ev = W.laplacian_eigenvalues(NX, NY, NZ)
     lib.set_csr(ia, ja, a)
@@ -332,6 +335,7 @@ def run_ours(args):
                 "lanczos_steps": int(kdim),
                 "parallelism": f"replicas x{world} (independent slices)",
                 "l2": "256 MB buffer written between steps; per-step working set (A + basis) > L2",
+                "storage": storage_desc(lib),
             },
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "per_step": lat},
@@ -453,6 +457,19 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def storage_desc(lib):
+    """How the registered matrix is stored for the FP64 filter, and which
+    single-vector filter kernel the timing-based selection chose."""
+    npat = lib.row_pattern_count()
+    vb, ib = lib.matrix_storage()
+    desc = "SELL-32: %d-byte values, %d-byte column indices" % (vb, ib)
+    if npat:
+        desc += "; row-pattern dictionary: %d patterns, 2-byte pattern id per row" % npat
+    v, us = lib.filter_kernel()
+    return {"matrix": desc, "filter_kernel": lib.FILTER_KERNELS[v] if v >= 0 else None,
+            "us_per_degree_step_by_kernel": {k: round(t, 3) for k, t in us.items()}}
+
+
 def run_filter(args):
     """The dominant kernel alone: W + K applications of the request's filter
     p(A)v (ChebAv, degree ~1440) on the 3-D Laplacian 100^3."""
@@ -467,6 +484,7 @@ def run_filter(args):
     if args.l2_resident:
         lib.set_l2_resident(True)
     lib.set_filter_wave(args.filter_mode == "wave")
+    lib.set_row_patterns(args.row_patterns == "on")
     ia, ja, a = W.laplacian_csr(NX, NY, NZ)
     ev = W.laplacian_eigenvalues(NX, NY, NZ)
     lib.set_csr(ia, ja, a)
@@ -491,7 +509,8 @@ def run_filter(args):
     print(json.dumps({"metric": "filter SpMV GB/s", "value": gbs, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
                       "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
                       "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                      "config": {"workload": "lap3d-filter: ChebAv degree %d on the 3-D Laplacian 100^3" % pol.deg},
+                      "config": {"workload": "lap3d-filter: ChebAv degree %d on the 3-D Laplacian 100^3" % pol.deg,
+                                 "storage": storage_desc(lib)},
                       "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "peak_kind": kind, "unit": "GB/s",
                                    "frac": gbs / peak, "traffic": profiled_traffic("k_cheb", "lap3d-filter"),
                                    "avg_launch_us": 1e6 * sec / launches},

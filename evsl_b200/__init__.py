@@ -294,6 +294,10 @@ def load():
         "evslx_set_mixed_min_rows": ([C.c_int], None),
         "evslx_set_filter_variant": ([C.c_int], C.c_int),
         "evslx_set_l2_resident": ([C.c_int], C.c_int),
+        "evslx_set_row_patterns": ([C.c_int], C.c_int),
+        "evslx_row_pattern_count": ([], C.c_int),
+        "evslx_set_filter_kernel": ([C.c_int], C.c_int),
+        "evslx_filter_kernel": ([C.POINTER(C.c_double)], C.c_int),
         "evslx_set_filter_wave": ([C.c_int], C.c_int),
         "evslx_get_filter_variant": ([], C.c_int),
         "evslx_tuned_filter_variant": ([C.c_int, C.c_int], C.c_int),
@@ -540,6 +544,31 @@ class Library:
 
     def set_filter_wave(self, on):
         self._check(self.lib.evslx_set_filter_wave(1 if on else 0), "evslx_set_filter_wave")
+
+    def set_row_patterns(self, on):
+        """Use (default) or stop using the row-pattern dictionary of the stored matrix."""
+        self._check(self.lib.evslx_set_row_patterns(1 if on else 0), "evslx_set_row_patterns")
+
+    def row_pattern_count(self):
+        """Distinct row patterns of the registered matrix (0: no dictionary)."""
+        return int(self.lib.evslx_row_pattern_count())
+
+    FILTER_KERNELS = ("sell-loop", "sell-unrolled", "pattern-global-unrolled", "pattern-global-loop",
+                      "pattern-constant-loop", "pattern-constant-unrolled")
+
+    def set_filter_kernel(self, variant):
+        """Force a single-vector filter kernel (index or name), or -1/None for timed selection."""
+        if variant is None:
+            variant = -1
+        if isinstance(variant, str):
+            variant = self.FILTER_KERNELS.index(variant)
+        self._check(self.lib.evslx_set_filter_kernel(int(variant)), "evslx_set_filter_kernel")
+
+    def filter_kernel(self):
+        """(chosen variant or -1, {variant name: measured us per degree step}) of the registered matrix."""
+        us = (C.c_double * 6)()
+        v = int(self.lib.evslx_filter_kernel(us))
+        return v, {self.FILTER_KERNELS[i]: us[i] for i in range(6) if us[i] > 0}
 
     def set_l2_resident(self, on):
         self._check(self.lib.evslx_set_l2_resident(1 if on else 0), "evslx_set_l2_resident")

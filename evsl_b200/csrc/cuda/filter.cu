@@ -352,7 +352,10 @@ int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, dou
     P.dot_out = epi ? epi->dot_out : nullptr;
     P.bar = barrier_area();
     P.err = (int *)(counters() + 10);
-    rc = with_view(A, [&](auto view) { return launch_persistent(view, A->nchunks, P, &launched); });
+    if (evslcu_mat_uses_patterns(A))
+      rc = launch_persistent(pat_view(A), A->nchunks, P, &launched);
+    else
+      rc = with_view(A, [&](auto view) { return launch_persistent(view, A->nchunks, P, &launched); });
     if (rc) return rc;
   }
   if (!launched) rc = chebav_per_degree(A, mu, deg, cc, dd, v, y, work, epi);

@@ -22,6 +22,8 @@
 // computed on the device as well.
 #include <algorithm>
 #include <cmath>
+#include <utility>
+#include <vector>
 
 #include "common.cuh"
 #include "sparse_types.cuh"
@@ -287,7 +289,206 @@ __global__ void k_sell_fill(int n, int nch, const int *ia, const int *ja, const 
   }
 }
 
+// ---- row-pattern dictionary --------------------------------------------------
+//
+// A row's pattern is its sequence of (value bits, column - row) pairs in CSR
+// order.  Pass 1 hashes every row into an open-addressing table of 64-bit
+// keys (insert-or-find by compare-and-swap; the smallest row with a key is its
+// representative); pass 2 compares every row with its representative entry
+// by entry, so a hash collision can only cancel the dictionary, never change
+// a result.  The build gives up as soon as more than kPatMax distinct keys
+// appear.
+
+constexpr int kPatSlots = 4096;  // hash slots (power of two)
+constexpr int kPatMax = 1024;    // most distinct patterns kept
+constexpr int kPatMaxEntries = 1 << 16;
+
+// 64-bit finaliser of MurmurHash3 (fmix64).
+__device__ __forceinline__ unsigned long long pat_mix(unsigned long long z) {
+  z ^= z >> 33;
+  z *= 0xff51afd7ed558ccdULL;
+  z ^= z >> 33;
+  z *= 0xc4ceb9fe1a85ec53ULL;
+  z ^= z >> 33;
+  return z;
+}
+
+// ctl[0]: distinct keys inserted; ctl[1]: gave up (too many patterns);
+// ctl[2]: a row differs from its representative (hash collision).
+__global__ void k_pat_insert(int n, const int *ia, const int *ja, const double *a, unsigned long long *keys,
+                             int *rep, int *slot_of, int *ctl) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    if (*(volatile int *)(ctl + 1)) return;
+    const int b = ia[r], e = ia[r + 1];
+    unsigned long long h = pat_mix(0x9e3779b97f4a7c15ULL + (unsigned long long)(e - b));
+    for (int j = b; j < e; ++j) {
+      h = pat_mix(h ^ (unsigned long long)(unsigned)(ja[j] - r));
+      h = pat_mix(h ^ (unsigned long long)__double_as_longlong(a[j]));
+    }
+    h |= 1ULL;  // 0 marks an empty slot
+    int s = (int)(h & (kPatSlots - 1)), found = -1;
+    for (int i = 0; i < kPatSlots; ++i) {
+      if (*(volatile int *)(ctl + 1)) return;
+      const unsigned long long prev = atomicCAS(keys + s, 0ULL, h);
+      if (prev == 0ULL) {
+        if (atomicAdd(ctl, 1) >= kPatMax) atomicExch(ctl + 1, 1);
+        found = s;
+        break;
+      }
+      if (prev == h) {
+        found = s;
+        break;
+      }
+      s = (s + 1) & (kPatSlots - 1);
+    }
+    if (found < 0) {
+      atomicExch(ctl + 1, 1);
+      return;
+    }
+    atomicMin(rep + found, r);
+    slot_of[r] = found;
+  }
+}
+
+__global__ void k_pat_verify(int n, const int *ia, const int *ja, const double *a, const int *rep,
+                             const int *slot_of, int *ctl) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int q = rep[slot_of[r]];
+    if (q == r) continue;
+    const int b = ia[r], len = ia[r + 1] - b;
+    const int bq = ia[q];
+    bool same = (ia[q + 1] - bq) == len;
+    for (int j = 0; same && j < len; ++j)
+      same = (ja[b + j] - r == ja[bq + j] - q) &&
+             (__double_as_longlong(a[b + j]) == __double_as_longlong(a[bq + j]));
+    if (!same) atomicExch(ctl + 2, 1);
+  }
+}
+
+__global__ void k_pat_len(int npat, const int *reps, const int *ia, int *lens) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npat; p += gridDim.x * blockDim.x)
+    lens[p] = ia[reps[p] + 1] - ia[reps[p]];
+}
+
+__global__ void k_pat_fill(int npat, const int *reps, const int *ia, const int *ja, const double *a,
+                           const int2 *hdr, double2 *ent) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npat; p += gridDim.x * blockDim.x) {
+    const int q = reps[p], b = ia[q];
+    for (int j = 0; j < hdr[p].y; ++j)
+      ent[hdr[p].x + j] = make_double2(a[b + j], __longlong_as_double((long long)(ja[b + j] - q)));
+  }
+}
+
+__global__ void k_pat_assign(int n, const int *slot_of, const int *slot2id, unsigned short *pid) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    pid[r] = (unsigned short)slot2id[slot_of[r]];
+}
+
 }  // namespace
+
+int build_patterns_device(evslcu_mat *M) {
+  const int n = M->n;
+  if (n <= 0) return 0;
+  // scratch: keys, rep, ctl, slot_of
+  const size_t kb = sizeof(unsigned long long) * kPatSlots, rb = sizeof(int) * kPatSlots, cb = 256;
+  char *scr = (char *)evslcu_malloc(kb + rb + cb + sizeof(int) * (size_t)n);
+  if (!scr) return 0;  // the dictionary is optional
+  unsigned long long *keys = (unsigned long long *)scr;
+  int *rep = (int *)(scr + kb);
+  int *ctl = (int *)(scr + kb + rb);
+  int *slot_of = (int *)(scr + kb + rb + cb);
+  std::vector<int> hrep(kPatSlots, 0x7fffffff);
+  int rc = evslcu_memset(keys, 0, kb);
+  if (!rc) rc = evslcu_memset(ctl, 0, cb);
+  if (!rc) rc = evslcu_h2d_async(rep, hrep.data(), rb);
+  if (!rc) {
+    k_pat_insert<<<grid_for(n), kThreads, 0, stream()>>>(n, M->ia, M->ja, M->a, keys, rep, slot_of, ctl);
+    rc = launched("k_pat_insert");
+  }
+  int hctl[3] = {0, 0, 0};
+  if (!rc) rc = evslcu_d2h(hctl, ctl, sizeof(hctl));
+  if (!rc && !hctl[1]) {
+    k_pat_verify<<<grid_for(n), kThreads, 0, stream()>>>(n, M->ia, M->ja, M->a, rep, slot_of, ctl);
+    rc = launched("k_pat_verify");
+    if (!rc) rc = evslcu_d2h(hctl, ctl, sizeof(hctl));
+  }
+  if (rc || hctl[1] || hctl[2] || hctl[0] <= 0) {
+    evslcu_free(scr);
+    return rc;
+  }
+  std::vector<unsigned long long> hkeys(kPatSlots);
+  rc = evslcu_d2h(hkeys.data(), keys, kb);
+  if (!rc) rc = evslcu_d2h(hrep.data(), rep, rb);
+  if (rc) {
+    evslcu_free(scr);
+    return rc;
+  }
+  // patterns numbered in the order of their first row
+  std::vector<std::pair<int, int>> used;  // (representative row, slot)
+  for (int s = 0; s < kPatSlots; ++s)
+    if (hkeys[s]) used.push_back({hrep[s], s});
+  std::sort(used.begin(), used.end());
+  const int npat = (int)used.size();
+  std::vector<int> slot2id(kPatSlots, 0), reps(npat), lens(npat);
+  for (int p = 0; p < npat; ++p) {
+    slot2id[used[p].second] = p;
+    reps[p] = used[p].first;
+  }
+  // device: slot2id [kPatSlots], reps [npat], lens [npat] (reuses the key area)
+  int *d_slot2id = (int *)keys, *d_reps = d_slot2id + kPatSlots, *d_lens = d_reps + kPatMax;
+  rc = evslcu_h2d_async(d_slot2id, slot2id.data(), sizeof(int) * kPatSlots);
+  if (!rc) rc = evslcu_h2d_async(d_reps, reps.data(), sizeof(int) * npat);
+  if (!rc) {
+    k_pat_len<<<grid_for(npat), kThreads, 0, stream()>>>(npat, d_reps, M->ia, d_lens);
+    rc = launched("k_pat_len");
+  }
+  if (!rc) rc = evslcu_d2h(lens.data(), d_lens, sizeof(int) * npat);
+  std::vector<int2> hdr(npat);
+  long long total = 0;
+  int maxlen = 0;
+  for (int p = 0; p < npat; ++p) {
+    hdr[p] = make_int2((int)total, lens[p]);
+    total += lens[p];
+    maxlen = std::max(maxlen, lens[p]);
+  }
+  if (rc || total > kPatMaxEntries) {
+    evslcu_free(scr);
+    return rc;
+  }
+  const size_t hbytes = ((size_t)npat * sizeof(int2) + 15) / 16 * 16;
+  void *table = evslcu_malloc(hbytes + sizeof(double2) * (size_t)std::max(total, 1LL));
+  unsigned short *pid = (unsigned short *)evslcu_malloc(sizeof(unsigned short) * (size_t)n);
+  if (!table || !pid) {
+    evslcu_free(table);
+    evslcu_free(pid);
+    evslcu_free(scr);
+    return 0;
+  }
+  int2 *d_hdr = (int2 *)table;
+  double2 *d_ent = (double2 *)((char *)table + hbytes);
+  rc = evslcu_h2d_async(d_hdr, hdr.data(), sizeof(int2) * npat);
+  if (!rc) {
+    k_pat_fill<<<grid_for(npat), kThreads, 0, stream()>>>(npat, d_reps, M->ia, M->ja, M->a, d_hdr, d_ent);
+    rc = launched("k_pat_fill");
+  }
+  if (!rc) {
+    k_pat_assign<<<grid_for(n), kThreads, 0, stream()>>>(n, slot_of, d_slot2id, pid);
+    rc = launched("k_pat_assign");
+  }
+  if (!rc) rc = evslcu_sync();  // the host vectors above are read by queued copies
+  evslcu_free(scr);
+  if (rc) {
+    evslcu_free(table);
+    evslcu_free(pid);
+    return rc;
+  }
+  M->pat_id = pid;
+  M->pat_table = table;
+  M->npat = npat;
+  M->pat_entries = (int)total;
+  M->pat_maxlen = maxlen;
+  return 0;
+}
 
 // Builds the SELL-32 copy of M's device CSR (M->n, M->nnz, M->ia/ja/a set)
 // after validating it.  allow_compress: use the compressed formats when the
@@ -342,10 +543,13 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
     int *hcw = (int *)malloc(sizeof(int) * (size_t)nch);
     M->ellw = 0;
     if (hcw && !evslcu_d2h(hcw, M->cw, sizeof(int) * (size_t)nch)) {
-      int u = hcw[0];
-      for (int c = 1; c < nch && u > 0; ++c)
+      int u = hcw[0], mx = 0;
+      for (int c = 0; c < nch; ++c) {
         if (hcw[c] != u) u = 0;
+        mx = std::max(mx, hcw[c]);
+      }
       M->ellw = u > 0 ? u : 0;
+      M->maxw = mx;
     }
     free(hcw);
   }

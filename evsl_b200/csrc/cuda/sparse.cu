@@ -18,11 +18,147 @@
 
 #include <algorithm>
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "sparse_types.cuh"
 
 using namespace evslcu;
+
+// ---------------------------------------------------------------------------
+// Constant-memory copy of the row-pattern tables.  The rows of a warp mostly
+// share one pattern, so the table reads are warp-uniform and the constant
+// cache serves them without using the L1 data path that the vector gathers
+// need.  Matrices claim regions of this fixed pool when they are created; a
+// table that does not fit is read from global memory instead (PatView).
+// ---------------------------------------------------------------------------
+constexpr int kCPoolEntries = 3072;
+constexpr int kCPoolHeaders = 1024;
+__constant__ double c_pat_val[kCPoolEntries];
+__constant__ int c_pat_off[kCPoolEntries];
+__constant__ int2 c_pat_hdr[kCPoolHeaders];
+
+namespace evslcu {
+
+struct PatCView {
+  int n;
+  const unsigned short *__restrict__ pid;
+  int hbase;  // this matrix's first header in the pool
+};
+
+template <bool COHERENT>
+__device__ __forceinline__ double row_dot(const PatCView &A, int r, const double *x) {
+  const int2 h = c_pat_hdr[A.hbase + __ldg(A.pid + r)];
+  const double *xr = x + r;
+  double acc = 0.0;
+  for (int j = 0; j < h.y; ++j)
+    acc = __dadd_rn(acc, __dmul_rn(c_pat_val[h.x + j], ldx<COHERENT>(xr + c_pat_off[h.x + j])));
+  return acc;
+}
+
+template <int WMAX, bool COHERENT>
+__device__ __forceinline__ double row_dot_w(const PatCView &A, int r, const double *x) {
+  const int2 h = c_pat_hdr[A.hbase + __ldg(A.pid + r)];
+  const double *xr = x + r;
+  double g[WMAX];
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < h.y) g[j] = ldx<COHERENT>(xr + c_pat_off[h.x + j]);
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < h.y) acc = __dadd_rn(acc, __dmul_rn(c_pat_val[h.x + j], g[j]));
+  return acc;
+}
+
+}  // namespace evslcu
+
+namespace {
+
+// First-fit allocator of pool slots (host side; the library runs on one
+// stream and one host thread per process).
+struct SlotPool {
+  int cap;
+  std::vector<std::pair<int, int>> used;  // (base, length), sorted by base
+  int claim(int len) {
+    int at = 0;
+    size_t i = 0;
+    for (; i < used.size(); ++i) {
+      if (used[i].first - at >= len) break;
+      at = used[i].first + used[i].second;
+    }
+    if (len <= 0 || at + len > cap) return -1;
+    used.insert(used.begin() + (long)i, {at, len});
+    return at;
+  }
+  void release(int base) {
+    for (size_t i = 0; i < used.size(); ++i)
+      if (used[i].first == base) {
+        used.erase(used.begin() + (long)i);
+        return;
+      }
+  }
+};
+
+SlotPool g_cpool_ent{kCPoolEntries, {}};
+SlotPool g_cpool_hdr{kCPoolHeaders, {}};
+int g_pattern_const = 1;
+
+// Copies M's pattern table into the constant pool when there is room.
+int pat_const_claim(evslcu_mat *M) {
+  if (!M->pat_id || M->npat <= 0) return 0;
+  const int eb = g_cpool_ent.claim(M->pat_entries), hb = g_cpool_hdr.claim(M->npat);
+  if (eb < 0 || hb < 0) {
+    if (eb >= 0) g_cpool_ent.release(eb);
+    if (hb >= 0) g_cpool_hdr.release(hb);
+    return 0;
+  }
+  const size_t hbytes = ((size_t)M->npat * sizeof(int2) + 15) / 16 * 16;
+  std::vector<int2> hdr(M->npat);
+  std::vector<double2> ent(M->pat_entries);
+  int rc = evslcu_d2h(hdr.data(), M->pat_table, sizeof(int2) * M->npat);
+  if (!rc) rc = evslcu_d2h(ent.data(), (const char *)M->pat_table + hbytes, sizeof(double2) * M->pat_entries);
+  std::vector<double> val(M->pat_entries);
+  std::vector<int> off(M->pat_entries);
+  for (int j = 0; j < M->pat_entries; ++j) {
+    long long bits;
+    memcpy(&bits, &ent[j].y, sizeof(bits));
+    val[j] = ent[j].x;
+    off[j] = (int)bits;
+  }
+  for (auto &h : hdr) h.x += eb;
+  cudaError_t e = cudaSuccess;
+  if (!rc) {
+    e = cudaMemcpyToSymbolAsync(c_pat_val, val.data(), sizeof(double) * val.size(), sizeof(double) * eb,
+                                cudaMemcpyHostToDevice, stream());
+    if (e == cudaSuccess)
+      e = cudaMemcpyToSymbolAsync(c_pat_off, off.data(), sizeof(int) * off.size(), sizeof(int) * eb,
+                                  cudaMemcpyHostToDevice, stream());
+    if (e == cudaSuccess)
+      e = cudaMemcpyToSymbolAsync(c_pat_hdr, hdr.data(), sizeof(int2) * hdr.size(), sizeof(int2) * hb,
+                                  cudaMemcpyHostToDevice, stream());
+    if (e == cudaSuccess) rc = evslcu_sync();
+  }
+  if (rc || e != cudaSuccess) {
+    g_cpool_ent.release(eb);
+    g_cpool_hdr.release(hb);
+    if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "pattern table copy failed: %s", cudaGetErrorString(e));
+    return rc;
+  }
+  M->pat_cent = eb;
+  M->pat_chdr = hb;
+  return 0;
+}
+
+void pat_const_release(evslcu_mat *M) {
+  if (M->pat_chdr < 0) return;
+  g_cpool_ent.release(M->pat_cent);
+  g_cpool_hdr.release(M->pat_chdr);
+  M->pat_cent = M->pat_chdr = -1;
+}
+
+}  // namespace
+
 
 namespace {
 
@@ -33,7 +169,10 @@ __global__ void __launch_bounds__(kThreads) k_spmv(M A, const double *__restrict
 
 // One Chebyshev degree step k (FIRST: k == 1; EPI: k == deg, Lanczos epilogue).
 //   out may alias vkm1 (each thread reads vkm1[r] before writing out[r]).
-template <class M, bool FIRST, bool EPI>
+//   WMAX > 0: rows have at most WMAX stored entries (unrolled row products);
+//   the epilogue's loads of vkm1[r] and y[r] are issued before the row's
+//   gathers so that their latency overlaps.
+template <class M, bool FIRST, bool EPI, int WMAX>
 __global__ void __launch_bounds__(kThreads)
     k_cheb(M A, const double *__restrict__ vk, const double *vkm1, double *out, double *__restrict__ y, double t,
            double ncc, double s, double mu0, const double *__restrict__ zold, double nbeta,
@@ -46,14 +185,16 @@ __global__ void __launch_bounds__(kThreads)
   asm volatile("griddepcontrol.wait;" ::: "memory");
   double dsum = 0.0;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) {
-    const double acc = row_dot<false>(A, r, vk);
+    const double xm1 = FIRST ? 0.0 : vkm1[r];
+    const double yo = FIRST ? 0.0 : y[r];
+    const double acc = row_dot_any<WMAX, false>(A, r, vk);
     const double x = vk[r];
     // vkp1 = A vk; vkp1 += (-cc) vk; vkp1 *= t; vkp1 += (-1) vkm1
     double w = __dmul_rn(t, __dadd_rn(acc, __dmul_rn(ncc, x)));
-    if (!FIRST) w = __dadd_rn(w, -vkm1[r]);
+    if (!FIRST) w = __dadd_rn(w, -xm1);
     out[r] = w;
     // k == 1: y = mu0 * v (v == vk); then y += mu_k * w
-    double yv = FIRST ? __dmul_rn(mu0, x) : y[r];
+    double yv = FIRST ? __dmul_rn(mu0, x) : yo;
     yv = __dadd_rn(yv, __dmul_rn(s, w));
     if (EPI) {
       if (zold) yv = __dadd_rn(yv, __dmul_rn(nbeta, zold[r]));
@@ -178,82 +319,74 @@ int launch_pdl(F fn, int grid, M view, const double *vk, const double *vkm1, dou
   return 0;
 }
 
-template <class VT, class IT>
-int launch_cheb_step(const SellT<VT, IT> &view, int n, bool first, bool epi, const double *vk, const double *vkm1,
-                     double *out, double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep);
+int g_row_unroll = 1;
 
-template <class M>
-int launch_cheb_step(const M &view, int n, bool first, bool epi, const double *vk, const double *vkm1, double *out,
-                     double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep) {
-  const int grid = grid_for(n);
-  cudaStream_t st = stream();
-  const double *zold = (epi && ep) ? ep->zold : nullptr;
-  const double nbeta = (epi && ep) ? ep->nbeta : 0.0;
-  const double *dotv = (epi && ep) ? ep->dotv : nullptr;
-  double *dout = (epi && ep) ? ep->dot_out : nullptr;
-  unsigned int *ctr = counters() + CTR_CHEB;
-  void (*fn)(M, const double *, const double *, double *, double *, double, double, double, double,
-             const double *, double, const double *, double *, unsigned int *, double *);
-  if (first && epi)
-    fn = k_cheb<M, true, true>;
-  else if (first)
-    fn = k_cheb<M, true, false>;
-  else if (epi)
-    fn = k_cheb<M, false, true>;
-  else
-    fn = k_cheb<M, false, false>;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, fn, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv, partials(),
-                                     ctr, dout);
-  if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "k_cheb launch failed: %s", cudaGetErrorString(e));
-  EVSLCU_LAUNCH_CHECK("k_cheb");
+// Unroll width for rows of at most wmax stored entries (0: loop form).
+inline int unroll_width(int wmax) {
+  if (!g_row_unroll || wmax <= 0) return 0;
+  if (wmax <= 8) return 8;
+  if (wmax <= 16) return 16;
   return 0;
 }
 
-template <class VT, class IT>
-int launch_cheb_step(const SellT<VT, IT> &view, int n, bool first, bool epi, const double *vk, const double *vkm1,
+template <class M>
+using ChebFn = void (*)(M, const double *, const double *, double *, double *, double, double, double, double,
+                        const double *, double, const double *, double *, unsigned int *, double *);
+
+template <class M, int W>
+ChebFn<M> cheb_fn(bool first, bool epi) {
+  if (first && epi) return k_cheb<M, true, true, W>;
+  if (first) return k_cheb<M, true, false, W>;
+  if (epi) return k_cheb<M, false, true, W>;
+  return k_cheb<M, false, false, W>;
+}
+
+// One degree step, one thread per row.
+template <class M>
+int launch_cheb_rows(const M &view, int n, int wmax, bool first, bool epi, const double *vk, const double *vkm1,
                      double *out, double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep) {
   const double *zold = (epi && ep) ? ep->zold : nullptr;
   const double nbeta = (epi && ep) ? ep->nbeta : 0.0;
   const double *dotv = (epi && ep) ? ep->dotv : nullptr;
   double *dout = (epi && ep) ? ep->dot_out : nullptr;
-  if (g_rows_per_thread == 2) {
-    const int grid = grid_for(((long long)n + 1) / 2);
-    using V = SellT<VT, IT>;
-    if (first && epi)
-      return launch_pdl(k_cheb2<VT, IT, true, true>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
-                        dout);
-    if (first)
-      return launch_pdl(k_cheb2<VT, IT, true, false>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
-                        dotv, dout);
-    if (epi)
-      return launch_pdl(k_cheb2<VT, IT, false, true>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
-                        dotv, dout);
-    (void)sizeof(V);
-    return launch_pdl(k_cheb2<VT, IT, false, false>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
-                      dout);
-  }
   const int grid = grid_for(n);
+  ChebFn<M> fn;
+  switch (unroll_width(wmax)) {
+    case 8: fn = cheb_fn<M, 8>(first, epi); break;
+    case 16: fn = cheb_fn<M, 16>(first, epi); break;
+    default: fn = cheb_fn<M, 0>(first, epi); break;
+  }
+  return launch_pdl(fn, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv, dout);
+}
+
+template <class M>
+int launch_cheb_step(const M &view, int n, int wmax, bool first, bool epi, const double *vk, const double *vkm1,
+                     double *out, double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep) {
+  return launch_cheb_rows(view, n, wmax, first, epi, vk, vkm1, out, y, t, ncc, s, mu0, ep);
+}
+
+template <class VT, class IT>
+int launch_cheb_step(const SellT<VT, IT> &view, int n, int wmax, bool first, bool epi, const double *vk,
+                     const double *vkm1, double *out, double *y, double t, double ncc, double s, double mu0,
+                     const evslcu_cheb_epi *ep) {
+  if (g_rows_per_thread != 2)
+    return launch_cheb_rows(view, n, wmax, first, epi, vk, vkm1, out, y, t, ncc, s, mu0, ep);
+  const double *zold = (epi && ep) ? ep->zold : nullptr;
+  const double nbeta = (epi && ep) ? ep->nbeta : 0.0;
+  const double *dotv = (epi && ep) ? ep->dotv : nullptr;
+  double *dout = (epi && ep) ? ep->dot_out : nullptr;
+  const int grid = grid_for(((long long)n + 1) / 2);
   if (first && epi)
-    return launch_pdl(k_cheb<SellT<VT, IT>, true, true>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
-                      dotv, dout);
+    return launch_pdl(k_cheb2<VT, IT, true, true>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
+                      dout);
   if (first)
-    return launch_pdl(k_cheb<SellT<VT, IT>, true, false>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
-                      dotv, dout);
+    return launch_pdl(k_cheb2<VT, IT, true, false>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
+                      dout);
   if (epi)
-    return launch_pdl(k_cheb<SellT<VT, IT>, false, true>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
-                      dotv, dout);
-  return launch_pdl(k_cheb<SellT<VT, IT>, false, false>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta,
-                    dotv, dout);
+    return launch_pdl(k_cheb2<VT, IT, false, true>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
+                      dout);
+  return launch_pdl(k_cheb2<VT, IT, false, false>, grid, view, vk, vkm1, out, y, t, ncc, s, mu0, zold, nbeta, dotv,
+                    dout);
 }
 
 // ---------------------------------------------------------------------------
@@ -482,20 +615,143 @@ int evslcu::chebav_user_matvec(const evslcu_op *op, const double *mu, int deg, d
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Per-matrix choice of the single-vector filter kernel.  The variants give
+// identical results (same rounded operations in the same order) and differ
+// only in where the row entries come from and how the row loop is issued:
+//   0  SELL-32, loop form            1  SELL-32, unrolled
+//   2  pattern table (global), unrolled   3  pattern table (global), loop form
+//   4  pattern table (constant), loop form  5  pattern table (constant), unrolled
+// Which is fastest depends on the size of the matrix (latency-bound small
+// operators favour the unrolled forms, L2-bound large ones the constant
+// table), so the first filter call on a matrix times every allowed variant on
+// scratch vectors and keeps the fastest.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kChebVariants = 6;
+int g_cheb_force = -1;
+
+bool cheb_variant_ok(const evslcu_mat *A, int v) {
+  if (A->kernel != 0) return false;
+  const bool pat = evslcu_mat_uses_patterns(A) != 0;
+  const bool pconst = pat && A->pat_chdr >= 0 && g_pattern_const;
+  switch (v) {
+    case 0: return true;
+    case 1: return unroll_width(A->maxw) > 0;
+    case 2: return pat && unroll_width(A->pat_maxlen) > 0;
+    case 3: return pat;
+    case 4: return pconst;
+    case 5: return pconst && unroll_width(A->pat_maxlen) > 0;
+    default: return false;
+  }
+}
+
+int launch_variant(const evslcu_mat *A, int v, bool first, bool epi, const double *vk, const double *vkm1,
+                   double *out, double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep) {
+  const int n = A->n;
+  switch (v) {
+    case 0:
+    case 1: {
+      const int wmax = (v == 1) ? A->maxw : 0;
+      return with_view(A, [&](auto view) {
+        return launch_cheb_step(view, n, wmax, first, epi, vk, vkm1, out, y, t, ncc, s, mu0, ep);
+      });
+    }
+    case 2:
+    case 3:
+      return launch_cheb_step(pat_view(A), n, (v == 2) ? A->pat_maxlen : 0, first, epi, vk, vkm1, out, y, t, ncc, s,
+                              mu0, ep);
+    default:
+      return launch_cheb_step(PatCView{n, A->pat_id, A->pat_chdr}, n, (v == 5) ? A->pat_maxlen : 0, first, epi, vk,
+                              vkm1, out, y, t, ncc, s, mu0, ep);
+  }
+}
+
+// Times every allowed variant (12 degree steps each after 3 untimed ones) on
+// zero-filled scratch vectors; keeps the fastest in A->cheb_variant.
+int tune_cheb(evslcu_mat *A) {
+  static const int pref[kChebVariants] = {4, 2, 3, 1, 0, 5};
+  int fallback = 0;
+  for (int v : pref)
+    if (cheb_variant_ok(A, v)) {
+      fallback = v;
+      break;
+    }
+  for (int v = 0; v < kChebVariants; ++v) A->cheb_us[v] = 0.0f;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream(), &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return fallback;
+  const int n = A->n;
+  double *scr = (double *)evslcu_malloc(sizeof(double) * 3 * (size_t)n);
+  if (!scr) return fallback;
+  int best = fallback;
+  float best_us = 0.0f;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = evslcu_memset(scr, 0, sizeof(double) * 3 * (size_t)n);
+  if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) rc = EVSLCU_ERR_CUDA;
+  for (int v = 0; v < kChebVariants && !rc; ++v) {
+    if (!cheb_variant_ok(A, v)) continue;
+    constexpr int kWarm = 3, kTimed = 12;
+    for (int i = 0; i < kWarm + kTimed && !rc; ++i) {
+      if (i == kWarm) cudaEventRecord(e0, stream());
+      rc = launch_variant(A, v, false, false, scr, scr + n, scr + n, scr + 2 * (size_t)n, 2.0, 0.0, 1.0, 1.0,
+                          nullptr);
+    }
+    cudaEventRecord(e1, stream());
+    float ms = 0.0f;
+    if (!rc && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
+      A->cheb_us[v] = 1e3f * ms / kTimed;
+      if (best_us == 0.0f || A->cheb_us[v] < best_us) {
+        best_us = A->cheb_us[v];
+        best = v;
+      }
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  evslcu_free(scr);
+  if (rc) return rc;  // an error code (<= EVSLCU_ERR_CUDA)
+  return best;
+}
+
+// The variant for this call: forced, tuned earlier, or tuned now.  -1: the
+// CSR kernel is selected; -2: the forced variant is not available; an error
+// code (<= EVSLCU_ERR_CUDA) if timing failed.
+int cheb_variant(const evslcu_mat *A_) {
+  evslcu_mat *A = const_cast<evslcu_mat *>(A_);
+  if (A->kernel != 0) return -1;
+  if (g_cheb_force >= 0) return cheb_variant_ok(A, g_cheb_force) ? g_cheb_force : -2;
+  if (A->cheb_variant >= 0 && cheb_variant_ok(A, A->cheb_variant)) return A->cheb_variant;
+  const int v = tune_cheb(A);
+  if (v < 0) return v;
+  A->cheb_variant = v;
+  return v;
+}
+
+}  // namespace
+
 // Per-degree filter: one fused kernel launch per degree (matrix path).
 int evslcu::chebav_per_degree(const evslcu_mat *A, const double *mu, int deg, double cc, double dd, const double *v,
                       double *y, double *work, const evslcu_cheb_epi *epi) {
   const int n = A->n;
   const double t1 = 1.0 / dd, t2 = 2.0 / dd, ncc = -cc;
   double *W[2] = {work, work + n};
+  const int var = cheb_variant(A);
+  if (var == -2) return fail(EVSLCU_ERR_ARG, "filter kernel variant %d is not available for this matrix", g_cheb_force);
+  if (var <= EVSLCU_ERR_CUDA) return var;
   for (int k = 1; k <= deg; ++k) {
     const double t = (k == 1) ? t1 : t2;
     const double *vk = (k == 1) ? v : W[(k - 2) % 2];
     const double *vkm1 = (k == 1) ? nullptr : ((k == 2) ? v : W[(k - 1) % 2]);
     double *out = W[(k - 1) % 2];
     const bool last = (k == deg);
+    if (var >= 0) {
+      const int rc = launch_variant(A, var, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
+      if (rc) return rc;
+      continue;
+    }
     int rc = with_view(A, [&](auto view) {
-      return launch_cheb_step(view, n, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
+      return launch_cheb_step(view, n, A->maxw, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
     });
     if (rc) return rc;
   }
@@ -507,11 +763,49 @@ int evslcu::chebav_per_degree(const evslcu_mat *A, const double *mu, int deg, do
 extern "C" {
 
 static int g_compress = 1;
+static int g_patterns = 1;
 
 int evslcu_set_compression(int on) {
   g_compress = on ? 1 : 0;
   return 0;
 }
+
+int evslcu_set_row_patterns(int on) {
+  g_patterns = on ? 1 : 0;
+  return 0;
+}
+
+int evslcu_set_pattern_const(int on) {
+  g_pattern_const = on ? 1 : 0;
+  return 0;
+}
+
+int evslcu_set_cheb_variant(int v) {
+  if (v < -1 || v >= kChebVariants) return fail(EVSLCU_ERR_ARG, "filter kernel variant must be -1..%d", kChebVariants - 1);
+  g_cheb_force = v;
+  return 0;
+}
+
+int evslcu_mat_cheb_variant(const evslcu_mat *A, float *us) {
+  if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
+  if (us)
+    for (int v = 0; v < kChebVariants; ++v) us[v] = A->cheb_us[v];
+  return A->cheb_variant;
+}
+
+int evslcu_set_row_unroll(int on) {
+  g_row_unroll = on ? 1 : 0;
+  return 0;
+}
+
+int evslcu_mat_set_patterns(evslcu_mat *A, int on) {
+  if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
+  A->use_pat = (on && A->pat_id) ? 1 : 0;
+  return 0;
+}
+
+int evslcu_mat_pattern_count(const evslcu_mat *A) { return (A && A->pat_id) ? A->npat : 0; }
+int evslcu_mat_uses_patterns(const evslcu_mat *A) { return (A && A->pat_id && A->use_pat && A->kernel == 0) ? 1 : 0; }
 
 int evslcu_mat_storage(const evslcu_mat *A, int *vfmt, int *ifmt) {
   if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
@@ -570,11 +864,13 @@ evslcu_mat *evslcu_mat_create(int n, int nnz, const int *ia, const int *ja, cons
       return nullptr;
     }
   }
-  if (build_sell_device(M, g_compress != 0) || evslcu_sync()) {
+  if (build_sell_device(M, g_compress != 0) || evslcu_sync() || (g_patterns && build_patterns_device(M)) ||
+      pat_const_claim(M)) {
     evslcu_mat_destroy(M);
     return nullptr;
   }
   M->kernel = 0;
+  M->use_pat = M->pat_id ? 1 : 0;
   return M;
 }
 
@@ -592,6 +888,9 @@ void evslcu_mat_destroy(evslcu_mat *M) {
   evslcu_free(M->wave_ctl);
   evslcu_free(M->wave_mu);
   evslcu_free(M->sval32);
+  pat_const_release(M);
+  evslcu_free(M->pat_id);
+  evslcu_free(M->pat_table);
   delete M;
 }
 
@@ -610,6 +909,14 @@ int evslcu_mat_get_kernel(const evslcu_mat *A) { return A ? A->kernel : -1; }
 int evslcu_spmv(const evslcu_mat *A, const double *x, double *y) {
   if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
   const int grid = grid_for(A->n);
+  if (evslcu_mat_uses_patterns(A)) {
+    if (A->pat_chdr >= 0 && g_pattern_const)
+      k_spmv<PatCView><<<grid, kThreads, 0, stream()>>>(PatCView{A->n, A->pat_id, A->pat_chdr}, x, y);
+    else
+      k_spmv<PatView><<<grid, kThreads, 0, stream()>>>(pat_view(A), x, y);
+    EVSLCU_LAUNCH_CHECK("k_spmv");
+    return 0;
+  }
   return with_view(A, [&](auto view) {
     k_spmv<decltype(view)><<<grid, kThreads, 0, stream()>>>(view, x, y);
     EVSLCU_LAUNCH_CHECK("k_spmv");

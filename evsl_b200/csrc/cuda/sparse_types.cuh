@@ -34,6 +34,7 @@ struct evslcu_mat {
   float mf_cost_us[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};  // its measured time per degree step
   long long bandwidth = 0;  // max |col - row| over the stored entries
   int ellw = 0;             // > 0: every SELL-32 chunk has this width
+  int maxw = 0;             // widest SELL-32 chunk
   int wave = 0;             // 1: pipelined single-launch filter (wavefilter.cu)
   unsigned *wave_ctl = nullptr;
   size_t wave_ctl_words = 0;
@@ -41,6 +42,19 @@ struct evslcu_mat {
   int wave_mu_cap = 0;
   int kernel = 0;      // 0 SELL-32, 1 CSR (thread per row)
   int persistent = 0;  // 1: single cooperative launch per filter application
+  // Row-pattern dictionary, built when the rows take few distinct forms
+  // (structured-grid operators): row r holds the entries of pattern
+  // pat_id[r], each a (value, column - r) pair, in the CSR order of the row.
+  unsigned short *pat_id = nullptr;
+  void *pat_table = nullptr;  // int2 {first entry, count} per pattern, then double2 entries
+  int npat = 0;
+  int pat_entries = 0;
+  int pat_maxlen = 0;  // longest pattern
+  int pat_cent = -1;   // first entry of the table's copy in the constant pool (-1: not there)
+  int pat_chdr = -1;   // first header there
+  int use_pat = 0;     // 1: the FP64 single-vector filter and SpMV read the dictionary
+  int cheb_variant = -1;      // single-vector filter kernel chosen by timing (-1: not yet)
+  float cheb_us[6] = {0, 0, 0, 0, 0, 0};  // measured time per degree step of each variant
 };
 
 namespace evslcu {
@@ -48,6 +62,9 @@ namespace evslcu {
 // Validates M's device CSR and builds its SELL-32 copy on the device
 // (ingest.cu).
 int build_sell_device(evslcu_mat *M, int allow_compress);
+// Builds M's row-pattern dictionary when its rows take at most 1024
+// distinct forms; leaves M->pat_id null otherwise (ingest.cu).
+int build_patterns_device(evslcu_mat *M);
 
 template <class VT, class IT>
 struct SellT {
@@ -159,6 +176,89 @@ template <class F>
 __device__ __forceinline__ void row_for_each(const CsrView &A, int r, F &&f) {
   const int b = A.ia[r], e = A.ia[r + 1];
   for (int j = b; j < e; ++j) f(__ldg(A.a + j), __ldg(A.ja + j));
+}
+
+// Row-pattern dictionary view.  The table is a few KB and is read through the
+// L1 cache; per row only the 2-byte pattern id comes from memory.
+struct PatView {
+  int n;
+  const unsigned short *__restrict__ pid;
+  const int2 *__restrict__ hdr;     // {first entry, count} per pattern
+  const double2 *__restrict__ ent;  // {value, column offset as 64-bit integer bits}
+};
+
+// Same products in the same order as the CSR row (no padding entries).
+template <bool COHERENT>
+__device__ __forceinline__ double row_dot(const PatView &A, int r, const double *x) {
+  const int2 h = __ldg(A.hdr + __ldg(A.pid + r));
+  const double *xr = x + r;
+  double acc = 0.0;
+#pragma unroll 4
+  for (int j = 0; j < h.y; ++j) {
+    const double2 e = __ldg(A.ent + h.x + j);
+    const int off = (int)__double_as_longlong(e.y);
+    acc = __dadd_rn(acc, __dmul_rn(e.x, ldx<COHERENT>(xr + off)));
+  }
+  return acc;
+}
+
+// Row products with every load of the row issued before the first add:
+// widths up to WMAX are unrolled and predicated, so the row's gathers are in
+// flight together instead of one per loop trip.  Same order of rounded
+// operations as row_dot.
+template <int WMAX, bool COHERENT>
+__device__ __forceinline__ double row_dot_w(const PatView &A, int r, const double *x) {
+  const int2 h = __ldg(A.hdr + __ldg(A.pid + r));
+  const double *xr = x + r;
+  double g[WMAX];
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < h.y) g[j] = ldx<COHERENT>(xr + (int)__double_as_longlong(__ldg(&A.ent[h.x + j].y)));
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < h.y) acc = __dadd_rn(acc, __dmul_rn(__ldg(&A.ent[h.x + j].x), g[j]));
+  return acc;
+}
+
+template <int WMAX, bool COHERENT, class VT, class IT>
+__device__ __forceinline__ double row_dot_w(const SellT<VT, IT> &A, int r, const double *x) {
+  long long p;
+  int w;
+  row_start(A, r, p, w);
+  VT v[WMAX];
+  double g[WMAX];
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < w) {
+      v[j] = __ldg(A.val + p + 32 * j);
+      g[j] = ldx<COHERENT>(x + decode_col(__ldg(A.col + p + 32 * j), r));
+    }
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < w) acc = __dadd_rn(acc, __dmul_rn((double)v[j], g[j]));
+  return acc;
+}
+
+template <int WMAX, bool COHERENT>
+__device__ __forceinline__ double row_dot_w(const CsrView &A, int r, const double *x) {
+  return row_dot<COHERENT>(A, r, x);
+}
+
+// WMAX 0: the loop form (any width).
+template <int WMAX, bool COHERENT, class M>
+__device__ __forceinline__ double row_dot_any(const M &A, int r, const double *x) {
+  if constexpr (WMAX == 0)
+    return row_dot<COHERENT>(A, r, x);
+  else
+    return row_dot_w<WMAX, COHERENT>(A, r, x);
+}
+
+inline PatView pat_view(const evslcu_mat *A) {
+  const size_t hbytes = ((size_t)A->npat * sizeof(int2) + 15) / 16 * 16;
+  return PatView{A->n, A->pat_id, (const int2 *)A->pat_table,
+                 (const double2 *)((const char *)A->pat_table + hbytes)};
 }
 
 template <class VT, class IT>

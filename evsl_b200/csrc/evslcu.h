@@ -237,6 +237,31 @@ int evslcu_filter_error(void);
  * created afterwards.  Default on. */
 int evslcu_set_compression(int on);
 int evslcu_mat_storage(const evslcu_mat *A, int *vfmt, int *ifmt);
+/* Row-pattern dictionary: built at registration when the rows take at most
+ * 1024 distinct (value, column - row) sequences (default on; applies to
+ * matrices created afterwards).  When built and in use, the FP64
+ * single-vector filter and the SpMV read a 2-byte pattern id per row and the
+ * pattern table instead of the stored entries; results are identical. */
+int evslcu_set_row_patterns(int on);
+int evslcu_mat_set_patterns(evslcu_mat *A, int on);
+int evslcu_mat_pattern_count(const evslcu_mat *A); /* 0: no dictionary */
+int evslcu_mat_uses_patterns(const evslcu_mat *A);
+/* Row products of the per-degree filter kernel: unrolled and predicated for
+ * rows of at most 8 or 16 stored entries (1, default) or the loop form (0).
+ * Same arithmetic either way. */
+int evslcu_set_row_unroll(int on);
+/* Pattern tables read from the constant-memory pool when they fit there (1,
+ * default) or always from global memory (0).  Same arithmetic either way. */
+int evslcu_set_pattern_const(int on);
+/* Single-vector filter kernel variant: -1 (default) times the allowed
+ * variants on a matrix's first filter call and keeps the fastest; 0..5 forces
+ * one (0/1 SELL-32 loop/unrolled, 2/3 pattern table in global memory
+ * unrolled/loop, 4/5 pattern table in constant memory loop/unrolled).  All
+ * give identical results. */
+int evslcu_set_cheb_variant(int v);
+/* A's chosen variant (-1: not chosen yet) and, in us[0..5], the measured
+ * microseconds per degree step of each variant timed (0: not timed). */
+int evslcu_mat_cheb_variant(const evslcu_mat *A, float *us);
 /* Keep A's stored matrix resident in L2 (persisting access-policy window on
  * the library stream, set-aside sized to it) or release that (on = 0). */
 int evslcu_mat_l2_persist(const evslcu_mat *A, int on);

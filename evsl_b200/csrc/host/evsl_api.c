@@ -481,6 +481,24 @@ int evslx_set_filter_wave(int on) {
   return 0;
 }
 
+int evslx_set_row_patterns(int on) {
+  evslcu_set_row_patterns(on);
+  if (evslh.mat) return from_cu(evslcu_mat_set_patterns(evslh.mat, on));
+  return 0;
+}
+
+int evslx_row_pattern_count(void) { return evslh.mat ? evslcu_mat_pattern_count(evslh.mat) : 0; }
+
+int evslx_set_filter_kernel(int variant) { return from_cu(evslcu_set_cheb_variant(variant)); }
+
+int evslx_filter_kernel(double *us) {
+  float f[6] = {0, 0, 0, 0, 0, 0};
+  const int v = evslh.mat ? evslcu_mat_cheb_variant(evslh.mat, f) : -1;
+  if (us)
+    for (int i = 0; i < 6; ++i) us[i] = f[i];
+  return v;
+}
+
 int evslx_set_l2_resident(int on) {
   evslh.l2_resident = on ? 1 : 0;
   if (evslh.mat) return from_cu(evslcu_mat_l2_persist(evslh.mat, evslh.l2_resident));

@@ -122,6 +122,29 @@ int evslx_set_filter_wave(int on);
  * 3-D Laplacian 100^3, whose working set already stays in L2); results are
  * identical either way. */
 int evslx_set_l2_resident(int on);
+/* Row-pattern dictionary of the stored matrix: when the rows take at most
+ * 1024 distinct sequences of (value, column - row) pairs, as on structured
+ * grids, registration also builds one table entry per distinct sequence and
+ * a 2-byte pattern id per row, and the FP64 single-vector filter and the
+ * matvec read those (same products in the same order as the CSR row, so
+ * results are identical).  on = 0 stops using the dictionary for the
+ * registered matrix and skips building it for matrices registered
+ * afterwards.  Default on. */
+int evslx_set_row_patterns(int on);
+/* Distinct row patterns of the registered matrix (0: no dictionary). */
+int evslx_row_pattern_count(void);
+/* Kernel of the FP64 single-vector filter.  variant -1 (default): the first
+ * filter call on a matrix times each variant allowed for it and keeps the
+ * fastest; 0..5 forces one: 0/1 SELL-32 with looped/unrolled row products,
+ * 2/3 pattern table in global memory unrolled/looped, 4/5 pattern table in
+ * constant memory looped/unrolled (2-5 need the row-pattern dictionary;
+ * filtering fails with EVSLX_ERR_ARG when the forced variant is not
+ * available).  Every variant gives the same result bit for bit. */
+int evslx_set_filter_kernel(int variant);
+/* The registered matrix's chosen variant (-1: not chosen yet) and, when us is
+ * not NULL, us[0..5] = measured microseconds per degree step of each variant
+ * timed (0: not timed). */
+int evslx_filter_kernel(double *us);
 /* Bytes per stored value (4 or 8) and per stored column index (2 or 4). */
 int evslx_matrix_storage(int *value_bytes, int *index_bytes);
 

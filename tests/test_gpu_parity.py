@@ -23,14 +23,85 @@ def _lap(lib, nx, ny, nz):
     return ia, ja, a
 
 
+@pytest.mark.parametrize("patterns", [True, False])
 @pytest.mark.parametrize("kernel", [0, 1])
-def test_spmv_bitwise(gpu_lib, kernel):
-    for dims in ((37, 23, 1), (17, 13, 11)):
-        ia, ja, a = _lap(gpu_lib, *dims)
-        gpu_lib.set_spmv_kernel(kernel)
-        x = np.random.default_rng(5).standard_normal(len(ia) - 1)
-        assert np.array_equal(gpu_lib.matvec(x), O.csr_matvec(ia, ja, a, x))
-    gpu_lib.set_spmv_kernel(0)
+def test_spmv_bitwise(gpu_lib, kernel, patterns):
+    try:
+        for dims in ((37, 23, 1), (17, 13, 11)):
+            ia, ja, a = _lap(gpu_lib, *dims)
+            gpu_lib.set_spmv_kernel(kernel)
+            gpu_lib.set_row_patterns(patterns)
+            x = np.random.default_rng(5).standard_normal(len(ia) - 1)
+            assert np.array_equal(gpu_lib.matvec(x), O.csr_matvec(ia, ja, a, x))
+    finally:
+        gpu_lib.set_spmv_kernel(0)
+        gpu_lib.set_row_patterns(True)
+
+
+def _csr_from_rows(rows):
+    """CSR arrays from a list of (columns, values) per row."""
+    ia = np.zeros(len(rows) + 1, dtype=np.int32)
+    ia[1:] = np.cumsum([len(c) for c, _ in rows])
+    ja = np.concatenate([np.asarray(c, dtype=np.int32) for c, _ in rows] + [np.zeros(0, np.int32)])
+    a = np.concatenate([np.asarray(v, dtype=np.float64) for _, v in rows] + [np.zeros(0)])
+    return ia, ja, a
+
+
+@pytest.mark.parametrize("table", ["constant", "global"])
+def test_row_pattern_dictionary(gpu_lib, table):
+    """The row-pattern dictionary: exact pattern counts on grids, its limit of
+    1024 distinct rows, and bitwise SpMV / ChebAv with and without it on rows
+    that are empty, hold signed zeros or differ only in one value's last bit,
+    with the pattern table read from constant or from global memory."""
+    gpu_lib.lib.evslcu_set_pattern_const(1 if table == "constant" else 0)
+    try:
+        _lap(gpu_lib, 37, 23, 1)
+        assert gpu_lib.row_pattern_count() == 9  # corners, edges, interior of a 2-D grid
+        _lap(gpu_lib, 17, 13, 11)
+        assert gpu_lib.row_pattern_count() == 27
+        # a diagonal with 1024 distinct values is kept, with 1025 it is not
+        for m, expect in ((1024, 1024), (1025, 0)):
+            n = 5000
+            d = 1.0 + (np.arange(n) % m)
+            gpu_lib.set_csr(np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), d)
+            assert gpu_lib.row_pattern_count() == expect, m
+            if expect:
+                x = np.random.default_rng(2).standard_normal(n)
+                assert np.array_equal(gpu_lib.matvec(x), d * x)
+        # a 3-D Laplacian with empty rows, explicit +0/-0 entries and one value
+        # changed in its last bit: still few patterns, each kept exact
+        ia, ja, a = O.lap_csr(12, 11, 10)
+        n = len(ia) - 1
+        rows = [(list(ja[ia[r]:ia[r + 1]]), list(a[ia[r]:ia[r + 1]])) for r in range(n)]
+        for r in range(0, n, 97):
+            rows[r] = ([], [])
+        for r in range(5, n, 89):
+            c, v = rows[r]
+            if c:
+                rows[r] = (c, [(-0.0 if k == 0 else x) for k, x in enumerate(v)])
+        for r in range(7, n, 83):
+            c, v = rows[r]
+            if c:
+                rows[r] = (c, [np.nextafter(v[0], 10.0)] + v[1:])
+        ia, ja, a = _csr_from_rows(rows)
+        rng = np.random.default_rng(17)
+        x = rng.standard_normal(n)
+        x[::13] = -0.0
+        iv = [0.6, 0.9, 0.0, 12.0]
+        y_ref = O.cheb_av(O.find_pol(iv, max_deg=200), ia, ja, a, x)
+        for on in (True, False):
+            gpu_lib.set_csr(ia, ja, a)
+            gpu_lib.set_row_patterns(on)
+            if on:
+                assert 0 < gpu_lib.row_pattern_count() <= 1024
+            assert np.array_equal(gpu_lib.matvec(x), O.csr_matvec(ia, ja, a, x))
+            pol = gpu_lib.find_pol(iv, max_deg=200)
+            y = gpu_lib.chebav(pol, x)
+            gpu_lib.free_pol(pol)
+            assert np.array_equal(y, y_ref), (on, np.max(np.abs(y - y_ref)))
+    finally:
+        gpu_lib.set_row_patterns(True)
+        gpu_lib.lib.evslcu_set_pattern_const(1)
 
 
 def test_spmv_irregular_rows(gpu_lib):
@@ -227,14 +298,19 @@ def test_tiny_problem(gpu_lib):
 
 
 @pytest.mark.parametrize("compress", [True, False])
-@pytest.mark.parametrize("mode", ["per-degree", "persistent", "wave"])
+@pytest.mark.parametrize("mode", ["per-degree", "persistent", "wave", "pattern", "pattern-persistent",
+                                  "loop-rows"])
 def test_filter_variants_bitwise(gpu_lib, compress, mode):
-    """Every storage variant (float/double values, int16/int32 columns) and
-    every execution mode (one launch per degree / one cooperative launch /
-    one pipelined launch) give the reference's filtered vector bit for bit."""
+    """Every storage variant (float/double values, int16/int32 columns, the
+    row-pattern dictionary) and every execution mode (one launch per degree
+    with unrolled or looped row products / one cooperative launch / one
+    pipelined launch) give the reference's filtered vector bit for bit."""
+    patterns = mode.startswith("pattern")
     gpu_lib.set_matrix_compression(compress)
-    gpu_lib.set_filter_persistent(mode == "persistent")
+    gpu_lib.set_filter_persistent(mode.endswith("persistent"))
     gpu_lib.set_filter_wave(mode == "wave")
+    gpu_lib.set_row_patterns(patterns)
+    gpu_lib.lib.evslcu_set_row_unroll(0 if mode == "loop-rows" else 1)
     try:
         cases = []
         ia, ja, a = O.lap_csr(24, 24, 24)
@@ -267,6 +343,8 @@ def test_filter_variants_bitwise(gpu_lib, compress, mode):
             vb, ib = gpu_lib.matrix_storage()
             if not compress:
                 assert (vb, ib) == (8, 4)
+            # the grid has 27 row patterns; the random matrix has no dictionary
+            assert gpu_lib.row_pattern_count() == ((27 if ia is cases[0][0] else 0) if patterns else 0)
             pol = gpu_lib.find_pol(iv, max_deg=300)
             v = O.seeded_normal(len(ia) - 1, 9)
             y = gpu_lib.chebav(pol, v)
@@ -277,6 +355,55 @@ def test_filter_variants_bitwise(gpu_lib, compress, mode):
         gpu_lib.set_matrix_compression(True)
         gpu_lib.set_filter_persistent(False)
         gpu_lib.set_filter_wave(False)
+        gpu_lib.set_row_patterns(True)
+        gpu_lib.lib.evslcu_set_row_unroll(1)
+
+
+@pytest.mark.parametrize("variant", range(6))
+def test_filter_kernel_variants_bitwise(gpu_lib, variant):
+    """Each single-vector filter kernel, forced, gives the reference's filtered
+    vector bit for bit on a grid operator (which has a row-pattern
+    dictionary); forcing a pattern kernel on a matrix without one fails with a
+    clear error instead of running something else."""
+    gpu_lib.set_filter_kernel(variant)
+    try:
+        ia, ja, a = _lap(gpu_lib, 23, 21, 19)
+        iv = [0.6, 0.8, 0.0, 12.0]
+        v = O.seeded_normal(len(ia) - 1, 4)
+        pol = gpu_lib.find_pol(iv, max_deg=150)
+        y = gpu_lib.chebav(pol, v)
+        gpu_lib.free_pol(pol)
+        assert np.array_equal(y, O.cheb_av(O.find_pol(iv, max_deg=150), ia, ja, a, v))
+        # a diagonal with distinct values: no dictionary
+        n = 3000
+        d = 1.0 + np.arange(n) / n
+        gpu_lib.set_csr(np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), d)
+        assert gpu_lib.row_pattern_count() == 0
+        pol = gpu_lib.find_pol([1.2, 1.5, 1.0, 2.0], max_deg=60)
+        x = O.seeded_normal(n, 5)
+        if variant >= 2:
+            with pytest.raises(Exception, match="not available"):
+                gpu_lib.chebav(pol, x)
+        else:
+            di = np.arange(n + 1, dtype=np.int32)
+            y_ref = O.cheb_av(O.find_pol([1.2, 1.5, 1.0, 2.0], max_deg=60), di, di[:-1], d, x)
+            assert np.array_equal(gpu_lib.chebav(pol, x), y_ref)
+        gpu_lib.free_pol(pol)
+    finally:
+        gpu_lib.set_filter_kernel(-1)
+
+
+def test_filter_kernel_is_chosen_by_timing(gpu_lib):
+    """With no variant forced, the first filter call times every variant the
+    matrix allows and records its choice."""
+    _lap(gpu_lib, 30, 30, 30)
+    assert gpu_lib.filter_kernel()[0] == -1
+    pol = gpu_lib.find_pol([0.6, 0.8, 0.0, 12.0], max_deg=50)
+    gpu_lib.chebav(pol, O.seeded_normal(27000, 1))
+    gpu_lib.free_pol(pol)
+    v, us = gpu_lib.filter_kernel()
+    assert len(us) == 6 and v in range(6)
+    assert us[gpu_lib.FILTER_KERNELS[v]] == min(us.values())
 
 
 def test_laplacian_storage_is_compressed(gpu_lib):
