@@ -81,6 +81,10 @@ def parse():
                    help="filter execution: one launch per degree or one pipelined launch")
     p.add_argument("--row-patterns", choices=["on", "off"], default="on",
                    help="row-pattern dictionary of the stored matrix (on: used when the rows allow it)")
+    p.add_argument("--filter-kernel", default="auto",
+                   help="single-vector FP64 filter kernel: auto (timed choice per matrix) or one of "
+                        "sell-loop, sell-unrolled, pattern-global-unrolled, pattern-global-loop, "
+                        "pattern-constant-loop, pattern-constant-unrolled (profiling runs)")
     return p.parse_args()
 
 
@@ -196,6 +200,7 @@ def run_ours(args):
         lib.set_l2_resident(True)
     lib.set_filter_wave(args.filter_mode == "wave")
     lib.set_row_patterns(args.row_patterns == "on")
+    lib.set_filter_kernel(None if args.filter_kernel == "auto" else args.filter_kernel)
     ia, ja, a = W.laplacian_csr(NX, NY, NZ)
     ev = W.laplacian_eigenvalues(NX, NY, NZ)
     lib.set_csr(ia, ja, a)
@@ -485,6 +490,7 @@ def run_filter(args):
         lib.set_l2_resident(True)
     lib.set_filter_wave(args.filter_mode == "wave")
     lib.set_row_patterns(args.row_patterns == "on")
+    lib.set_filter_kernel(None if args.filter_kernel == "auto" else args.filter_kernel)
     ia, ja, a = W.laplacian_csr(NX, NY, NZ)
     ev = W.laplacian_eigenvalues(NX, NY, NZ)
     lib.set_csr(ia, ja, a)
