@@ -347,7 +347,7 @@ def run_ours(args):
             "check": checks[-1],
             "all_steps_ok": all(c["ok"] for c in checks),
             "roofline": {
-                "kernel": "k_cheb (fused FP64 SELL-32 SpMV + Chebyshev step)",
+                "kernel": "k_cheb (fused FP64 SpMV + Chebyshev step; storage and variant in config.storage)",
                 "bound": "hbm",
                 "achieved": achieved,
                 "peak": peak,
