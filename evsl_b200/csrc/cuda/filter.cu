@@ -353,7 +353,8 @@ int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, dou
     P.bar = barrier_area();
     P.err = (int *)(counters() + 10);
     if (evslcu_mat_uses_patterns(A))
-      rc = launch_persistent(pat_view(A), A->nchunks, P, &launched);
+      rc = A->pat_f32 ? launch_persistent(pat_pview(A), A->nchunks, P, &launched)
+                      : launch_persistent(pat_view(A), A->nchunks, P, &launched);
     else
       rc = with_view(A, [&](auto view) { return launch_persistent(view, A->nchunks, P, &launched); });
     if (rc) return rc;

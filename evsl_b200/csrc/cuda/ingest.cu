@@ -20,6 +20,8 @@
 // sizes, and one fill pass writing every padded slot, with the lossless
 // compression checks (values exactly floats, column offsets within int16)
 // computed on the device as well.
+#include <string.h>
+
 #include <algorithm>
 #include <cmath>
 #include <utility>
@@ -455,8 +457,8 @@ int build_patterns_device(evslcu_mat *M) {
     evslcu_free(scr);
     return rc;
   }
-  const size_t hbytes = ((size_t)npat * sizeof(int2) + 15) / 16 * 16;
-  void *table = evslcu_malloc(hbytes + sizeof(double2) * (size_t)std::max(total, 1LL));
+  const size_t hbytes = pat_hdr_bytes(npat);
+  void *table = evslcu_malloc(hbytes + (sizeof(double2) + sizeof(unsigned long long)) * (size_t)std::max(total, 1LL));
   unsigned short *pid = (unsigned short *)evslcu_malloc(sizeof(unsigned short) * (size_t)n);
   if (!table || !pid) {
     evslcu_free(table);
@@ -477,11 +479,34 @@ int build_patterns_device(evslcu_mat *M) {
   }
   if (!rc) rc = evslcu_sync();  // the host vectors above are read by queued copies
   evslcu_free(scr);
+  // packed entries when every value is exactly a float
+  int f32 = 0;
+  if (!rc) {
+    std::vector<double2> ent((size_t)total);
+    std::vector<unsigned long long> pk((size_t)total);
+    rc = evslcu_d2h(ent.data(), d_ent, sizeof(double2) * (size_t)total);
+    f32 = 1;
+    for (long long j = 0; j < total && !rc && f32; ++j) {
+      const double v = ent[j].x;
+      if (!(std::isfinite(v) && (double)(float)v == v)) {
+        f32 = 0;
+        break;
+      }
+      const float fv = (float)v;
+      unsigned fb;
+      long long ob;
+      memcpy(&fb, &fv, sizeof(fb));
+      memcpy(&ob, &ent[j].y, sizeof(ob));
+      pk[j] = ((unsigned long long)fb << 32) | (unsigned long long)(unsigned)(int)ob;
+    }
+    if (!rc && f32) rc = evslcu_h2d(d_ent + total, pk.data(), sizeof(unsigned long long) * (size_t)total);
+  }
   if (rc) {
     evslcu_free(table);
     evslcu_free(pid);
     return rc;
   }
+  M->pat_f32 = f32;
   M->pat_id = pid;
   M->pat_table = table;
   M->npat = npat;

@@ -34,7 +34,10 @@ using namespace evslcu;
 // ---------------------------------------------------------------------------
 constexpr int kCPoolEntries = 3072;
 constexpr int kCPoolHeaders = 1024;
-__constant__ double c_pat_val[kCPoolEntries];
+// c_pat_w: packed entries (float value, offset) for tables whose values are
+// all exactly floats, otherwise the double value bits with the offset in
+// c_pat_off.
+__constant__ unsigned long long c_pat_w[kCPoolEntries];
 __constant__ int c_pat_off[kCPoolEntries];
 __constant__ int2 c_pat_hdr[kCPoolHeaders];
 
@@ -52,7 +55,8 @@ __device__ __forceinline__ double row_dot(const PatCView &A, int r, const double
   const double *xr = x + r;
   double acc = 0.0;
   for (int j = 0; j < h.y; ++j)
-    acc = __dadd_rn(acc, __dmul_rn(c_pat_val[h.x + j], ldx<COHERENT>(xr + c_pat_off[h.x + j])));
+    acc = __dadd_rn(acc, __dmul_rn(__longlong_as_double((long long)c_pat_w[h.x + j]),
+                                   ldx<COHERENT>(xr + c_pat_off[h.x + j])));
   return acc;
 }
 
@@ -67,7 +71,45 @@ __device__ __forceinline__ double row_dot_w(const PatCView &A, int r, const doub
   double acc = 0.0;
 #pragma unroll
   for (int j = 0; j < WMAX; ++j)
-    if (j < h.y) acc = __dadd_rn(acc, __dmul_rn(c_pat_val[h.x + j], g[j]));
+    if (j < h.y) acc = __dadd_rn(acc, __dmul_rn(__longlong_as_double((long long)c_pat_w[h.x + j]), g[j]));
+  return acc;
+}
+
+// Packed constant table: one constant load per entry.
+struct PatCPView {
+  int n;
+  const unsigned short *__restrict__ pid;
+  int hbase;
+};
+
+template <bool COHERENT>
+__device__ __forceinline__ double row_dot(const PatCPView &A, int r, const double *x) {
+  const int2 h = c_pat_hdr[A.hbase + __ldg(A.pid + r)];
+  const double *xr = x + r;
+  double acc = 0.0;
+  for (int j = 0; j < h.y; ++j) {
+    const unsigned long long e = c_pat_w[h.x + j];
+    acc = __dadd_rn(acc, __dmul_rn(pat_val(e), ldx<COHERENT>(xr + pat_off(e))));
+  }
+  return acc;
+}
+
+template <int WMAX, bool COHERENT>
+__device__ __forceinline__ double row_dot_w(const PatCPView &A, int r, const double *x) {
+  const int2 h = c_pat_hdr[A.hbase + __ldg(A.pid + r)];
+  const double *xr = x + r;
+  unsigned long long e[WMAX];
+  double g[WMAX];
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < h.y) {
+      e[j] = c_pat_w[h.x + j];
+      g[j] = ldx<COHERENT>(xr + pat_off(e[j]));
+    }
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < h.y) acc = __dadd_rn(acc, __dmul_rn(pat_val(e[j]), g[j]));
   return acc;
 }
 
@@ -113,24 +155,27 @@ int pat_const_claim(evslcu_mat *M) {
     if (hb >= 0) g_cpool_hdr.release(hb);
     return 0;
   }
-  const size_t hbytes = ((size_t)M->npat * sizeof(int2) + 15) / 16 * 16;
+  const size_t hbytes = pat_hdr_bytes(M->npat);
   std::vector<int2> hdr(M->npat);
   std::vector<double2> ent(M->pat_entries);
+  std::vector<unsigned long long> w(M->pat_entries);
   int rc = evslcu_d2h(hdr.data(), M->pat_table, sizeof(int2) * M->npat);
   if (!rc) rc = evslcu_d2h(ent.data(), (const char *)M->pat_table + hbytes, sizeof(double2) * M->pat_entries);
-  std::vector<double> val(M->pat_entries);
+  if (!rc && M->pat_f32)
+    rc = evslcu_d2h(w.data(), (const char *)M->pat_table + hbytes + sizeof(double2) * M->pat_entries,
+                    sizeof(unsigned long long) * M->pat_entries);
   std::vector<int> off(M->pat_entries);
   for (int j = 0; j < M->pat_entries; ++j) {
     long long bits;
     memcpy(&bits, &ent[j].y, sizeof(bits));
-    val[j] = ent[j].x;
     off[j] = (int)bits;
+    if (!M->pat_f32) memcpy(&w[j], &ent[j].x, sizeof(double));
   }
   for (auto &h : hdr) h.x += eb;
   cudaError_t e = cudaSuccess;
   if (!rc) {
-    e = cudaMemcpyToSymbolAsync(c_pat_val, val.data(), sizeof(double) * val.size(), sizeof(double) * eb,
-                                cudaMemcpyHostToDevice, stream());
+    e = cudaMemcpyToSymbolAsync(c_pat_w, w.data(), sizeof(unsigned long long) * w.size(),
+                                sizeof(unsigned long long) * eb, cudaMemcpyHostToDevice, stream());
     if (e == cudaSuccess)
       e = cudaMemcpyToSymbolAsync(c_pat_off, off.data(), sizeof(int) * off.size(), sizeof(int) * eb,
                                   cudaMemcpyHostToDevice, stream());
@@ -659,12 +704,20 @@ int launch_variant(const evslcu_mat *A, int v, bool first, bool epi, const doubl
       });
     }
     case 2:
-    case 3:
-      return launch_cheb_step(pat_view(A), n, (v == 2) ? A->pat_maxlen : 0, first, epi, vk, vkm1, out, y, t, ncc, s,
+    case 3: {
+      const int wmax = (v == 2) ? A->pat_maxlen : 0;
+      if (A->pat_f32)
+        return launch_cheb_step(pat_pview(A), n, wmax, first, epi, vk, vkm1, out, y, t, ncc, s, mu0, ep);
+      return launch_cheb_step(pat_view(A), n, wmax, first, epi, vk, vkm1, out, y, t, ncc, s, mu0, ep);
+    }
+    default: {
+      const int wmax = (v == 5) ? A->pat_maxlen : 0;
+      if (A->pat_f32)
+        return launch_cheb_step(PatCPView{n, A->pat_id, A->pat_chdr}, n, wmax, first, epi, vk, vkm1, out, y, t, ncc,
+                                s, mu0, ep);
+      return launch_cheb_step(PatCView{n, A->pat_id, A->pat_chdr}, n, wmax, first, epi, vk, vkm1, out, y, t, ncc, s,
                               mu0, ep);
-    default:
-      return launch_cheb_step(PatCView{n, A->pat_id, A->pat_chdr}, n, (v == 5) ? A->pat_maxlen : 0, first, epi, vk,
-                              vkm1, out, y, t, ncc, s, mu0, ep);
+    }
   }
 }
 
@@ -910,8 +963,12 @@ int evslcu_spmv(const evslcu_mat *A, const double *x, double *y) {
   if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
   const int grid = grid_for(A->n);
   if (evslcu_mat_uses_patterns(A)) {
-    if (A->pat_chdr >= 0 && g_pattern_const)
+    if (A->pat_chdr >= 0 && g_pattern_const && A->pat_f32)
+      k_spmv<PatCPView><<<grid, kThreads, 0, stream()>>>(PatCPView{A->n, A->pat_id, A->pat_chdr}, x, y);
+    else if (A->pat_chdr >= 0 && g_pattern_const)
       k_spmv<PatCView><<<grid, kThreads, 0, stream()>>>(PatCView{A->n, A->pat_id, A->pat_chdr}, x, y);
+    else if (A->pat_f32)
+      k_spmv<PatPView><<<grid, kThreads, 0, stream()>>>(pat_pview(A), x, y);
     else
       k_spmv<PatView><<<grid, kThreads, 0, stream()>>>(pat_view(A), x, y);
     EVSLCU_LAUNCH_CHECK("k_spmv");

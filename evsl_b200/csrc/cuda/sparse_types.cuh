@@ -50,6 +50,7 @@ struct evslcu_mat {
   int npat = 0;
   int pat_entries = 0;
   int pat_maxlen = 0;  // longest pattern
+  int pat_f32 = 0;     // 1: every table value is exactly a float (packed entries exist)
   int pat_cent = -1;   // first entry of the table's copy in the constant pool (-1: not there)
   int pat_chdr = -1;   // first header there
   int use_pat = 0;     // 1: the FP64 single-vector filter and SpMV read the dictionary
@@ -253,6 +254,62 @@ __device__ __forceinline__ double row_dot_any(const M &A, int r, const double *x
     return row_dot<COHERENT>(A, r, x);
   else
     return row_dot_w<WMAX, COHERENT>(A, r, x);
+}
+
+// Packed table (every value exactly a float): one 64-bit entry per stored
+// value, float bits in the high word, column offset in the low word; the
+// float widens to the same double, so products are unchanged.  One table
+// load per entry instead of two.
+struct PatPView {
+  int n;
+  const unsigned short *__restrict__ pid;
+  const int2 *__restrict__ hdr;
+  const unsigned long long *__restrict__ pk;
+};
+
+__device__ __forceinline__ double pat_val(unsigned long long e) { return (double)__uint_as_float((unsigned)(e >> 32)); }
+__device__ __forceinline__ int pat_off(unsigned long long e) { return (int)(unsigned)(e & 0xffffffffULL); }
+
+template <bool COHERENT>
+__device__ __forceinline__ double row_dot(const PatPView &A, int r, const double *x) {
+  const int2 h = __ldg(A.hdr + __ldg(A.pid + r));
+  const double *xr = x + r;
+  double acc = 0.0;
+#pragma unroll 4
+  for (int j = 0; j < h.y; ++j) {
+    const unsigned long long e = __ldg(A.pk + h.x + j);
+    acc = __dadd_rn(acc, __dmul_rn(pat_val(e), ldx<COHERENT>(xr + pat_off(e))));
+  }
+  return acc;
+}
+
+template <int WMAX, bool COHERENT>
+__device__ __forceinline__ double row_dot_w(const PatPView &A, int r, const double *x) {
+  const int2 h = __ldg(A.hdr + __ldg(A.pid + r));
+  const double *xr = x + r;
+  unsigned long long e[WMAX];
+  double g[WMAX];
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < h.y) {
+      e[j] = __ldg(A.pk + h.x + j);
+      g[j] = ldx<COHERENT>(xr + pat_off(e[j]));
+    }
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < h.y) acc = __dadd_rn(acc, __dmul_rn(pat_val(e[j]), g[j]));
+  return acc;
+}
+
+// Bytes of the global table: headers (padded to 16), double2 entries, then
+// the packed entries.
+inline size_t pat_hdr_bytes(int npat) { return ((size_t)npat * sizeof(int2) + 15) / 16 * 16; }
+
+inline PatPView pat_pview(const evslcu_mat *A) {
+  const size_t hbytes = pat_hdr_bytes(A->npat);
+  return PatPView{A->n, A->pat_id, (const int2 *)A->pat_table,
+                  (const unsigned long long *)((const char *)A->pat_table + hbytes + 16 * (size_t)A->pat_entries)};
 }
 
 inline PatView pat_view(const evslcu_mat *A) {

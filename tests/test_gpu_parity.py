@@ -68,37 +68,40 @@ def test_row_pattern_dictionary(gpu_lib, table):
             if expect:
                 x = np.random.default_rng(2).standard_normal(n)
                 assert np.array_equal(gpu_lib.matvec(x), d * x)
-        # a 3-D Laplacian with empty rows, explicit +0/-0 entries and one value
-        # changed in its last bit: still few patterns, each kept exact
-        ia, ja, a = O.lap_csr(12, 11, 10)
-        n = len(ia) - 1
-        rows = [(list(ja[ia[r]:ia[r + 1]]), list(a[ia[r]:ia[r + 1]])) for r in range(n)]
-        for r in range(0, n, 97):
-            rows[r] = ([], [])
-        for r in range(5, n, 89):
-            c, v = rows[r]
-            if c:
-                rows[r] = (c, [(-0.0 if k == 0 else x) for k, x in enumerate(v)])
-        for r in range(7, n, 83):
-            c, v = rows[r]
-            if c:
-                rows[r] = (c, [np.nextafter(v[0], 10.0)] + v[1:])
-        ia, ja, a = _csr_from_rows(rows)
-        rng = np.random.default_rng(17)
-        x = rng.standard_normal(n)
-        x[::13] = -0.0
-        iv = [0.6, 0.9, 0.0, 12.0]
-        y_ref = O.cheb_av(O.find_pol(iv, max_deg=200), ia, ja, a, x)
-        for on in (True, False):
-            gpu_lib.set_csr(ia, ja, a)
-            gpu_lib.set_row_patterns(on)
-            if on:
-                assert 0 < gpu_lib.row_pattern_count() <= 1024
-            assert np.array_equal(gpu_lib.matvec(x), O.csr_matvec(ia, ja, a, x))
-            pol = gpu_lib.find_pol(iv, max_deg=200)
-            y = gpu_lib.chebav(pol, x)
-            gpu_lib.free_pol(pol)
-            assert np.array_equal(y, y_ref), (on, np.max(np.abs(y - y_ref)))
+        # a 3-D Laplacian with empty rows and explicit +0/-0 entries (values
+        # all exactly floats: packed table), and the same with one value
+        # changed in its last bit (not a float: unpacked table)
+        for tweak in (False, True):
+            ia, ja, a = O.lap_csr(12, 11, 10)
+            n = len(ia) - 1
+            rows = [(list(ja[ia[r]:ia[r + 1]]), list(a[ia[r]:ia[r + 1]])) for r in range(n)]
+            for r in range(0, n, 97):
+                rows[r] = ([], [])
+            for r in range(5, n, 89):
+                c, v = rows[r]
+                if c:
+                    rows[r] = (c, [(-0.0 if k == 0 else x) for k, x in enumerate(v)])
+            for r in range(7, n, 83):
+                c, v = rows[r]
+                if c and tweak:
+                    rows[r] = (c, [np.nextafter(v[0], 10.0)] + v[1:])
+            ia, ja, a = _csr_from_rows(rows)
+            rng = np.random.default_rng(17)
+            x = rng.standard_normal(n)
+            x[::13] = -0.0
+            iv = [0.6, 0.9, 0.0, 12.0]
+            y_ref = O.cheb_av(O.find_pol(iv, max_deg=200), ia, ja, a, x)
+            for on in (True, False):
+                gpu_lib.set_row_patterns(True)  # build the dictionary at registration
+                gpu_lib.set_csr(ia, ja, a)
+                gpu_lib.set_row_patterns(on)
+                if on:
+                    assert 0 < gpu_lib.row_pattern_count() <= 1024
+                assert np.array_equal(gpu_lib.matvec(x), O.csr_matvec(ia, ja, a, x))
+                pol = gpu_lib.find_pol(iv, max_deg=200)
+                y = gpu_lib.chebav(pol, x)
+                gpu_lib.free_pol(pol)
+                assert np.array_equal(y, y_ref), (tweak, on, np.max(np.abs(y - y_ref)))
     finally:
         gpu_lib.set_row_patterns(True)
         gpu_lib.lib.evslcu_set_pattern_const(1)
@@ -367,13 +370,25 @@ def test_filter_kernel_variants_bitwise(gpu_lib, variant):
     clear error instead of running something else."""
     gpu_lib.set_filter_kernel(variant)
     try:
-        ia, ja, a = _lap(gpu_lib, 23, 21, 19)
         iv = [0.6, 0.8, 0.0, 12.0]
-        v = O.seeded_normal(len(ia) - 1, 4)
-        pol = gpu_lib.find_pol(iv, max_deg=150)
-        y = gpu_lib.chebav(pol, v)
-        gpu_lib.free_pol(pol)
-        assert np.array_equal(y, O.cheb_av(O.find_pol(iv, max_deg=150), ia, ja, a, v))
+        # values all exactly floats (packed pattern table), then a diagonal
+        # shifted by 1e-9 every 7th row (double table, 2 patterns more per form)
+        for shift in (False, True):
+            ia, ja, a = O.lap_csr(23, 21, 19)
+            if shift:
+                a = a.copy()
+                n = len(ia) - 1
+                for r in range(0, n, 7):
+                    for j in range(ia[r], ia[r + 1]):
+                        if ja[j] == r:
+                            a[j] += 1e-9
+            gpu_lib.set_csr(ia, ja, a)
+            assert 0 < gpu_lib.row_pattern_count() <= 1024
+            v = O.seeded_normal(len(ia) - 1, 4)
+            pol = gpu_lib.find_pol(iv, max_deg=150)
+            y = gpu_lib.chebav(pol, v)
+            gpu_lib.free_pol(pol)
+            assert np.array_equal(y, O.cheb_av(O.find_pol(iv, max_deg=150), ia, ja, a, v)), shift
         # a diagonal with distinct values: no dictionary
         n = 3000
         d = 1.0 + np.arange(n) / n
