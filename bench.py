@@ -472,6 +472,7 @@ def storage_desc(lib):
         desc += "; row-pattern dictionary: %d patterns, 2-byte pattern id per row" % npat
     v, us = lib.filter_kernel()
     return {"matrix": desc, "filter_kernel": lib.FILTER_KERNELS[v] if v >= 0 else None,
+            "filter_grid_blocks": lib.filter_kernel_grid() or "one row per thread",
             "us_per_degree_step_by_kernel": {k: round(t, 3) for k, t in us.items()}}
 
 

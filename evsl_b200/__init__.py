@@ -298,6 +298,7 @@ def load():
         "evslx_row_pattern_count": ([], C.c_int),
         "evslx_set_filter_kernel": ([C.c_int], C.c_int),
         "evslx_filter_kernel": ([C.POINTER(C.c_double)], C.c_int),
+        "evslx_filter_kernel_grid": ([], C.c_int),
         "evslx_set_filter_wave": ([C.c_int], C.c_int),
         "evslx_get_filter_variant": ([], C.c_int),
         "evslx_tuned_filter_variant": ([C.c_int, C.c_int], C.c_int),
@@ -569,6 +570,10 @@ class Library:
         us = (C.c_double * 6)()
         v = int(self.lib.evslx_filter_kernel(us))
         return v, {self.FILTER_KERNELS[i]: us[i] for i in range(6) if us[i] > 0}
+
+    def filter_kernel_grid(self):
+        """Blocks per degree step chosen with the filter kernel (0: one row per thread)."""
+        return int(self.lib.evslx_filter_kernel_grid())
 
     def set_l2_resident(self, on):
         self._check(self.lib.evslx_set_l2_resident(1 if on else 0), "evslx_set_l2_resident")

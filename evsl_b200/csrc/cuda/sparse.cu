@@ -365,6 +365,8 @@ int launch_pdl(F fn, int grid, M view, const double *vk, const double *vkm1, dou
 }
 
 int g_row_unroll = 1;
+int g_cheb_max_grid = 0;  // > 0: at most this many blocks per degree step (grid-stride rows)
+int g_call_grid = 0;      // the limit of the launches being issued (forced or the matrix's tuned one)
 
 // Unroll width for rows of at most wmax stored entries (0: loop form).
 inline int unroll_width(int wmax) {
@@ -394,7 +396,7 @@ int launch_cheb_rows(const M &view, int n, int wmax, bool first, bool epi, const
   const double nbeta = (epi && ep) ? ep->nbeta : 0.0;
   const double *dotv = (epi && ep) ? ep->dotv : nullptr;
   double *dout = (epi && ep) ? ep->dot_out : nullptr;
-  const int grid = grid_for(n);
+  const int grid = g_call_grid > 0 ? std::min(grid_for(n), g_call_grid) : grid_for(n);
   ChebFn<M> fn;
   switch (unroll_width(wmax)) {
     case 8: fn = cheb_fn<M, 8>(first, epi); break;
@@ -693,8 +695,10 @@ bool cheb_variant_ok(const evslcu_mat *A, int v) {
 }
 
 int launch_variant(const evslcu_mat *A, int v, bool first, bool epi, const double *vk, const double *vkm1,
-                   double *out, double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep) {
+                   double *out, double *y, double t, double ncc, double s, double mu0, const evslcu_cheb_epi *ep,
+                   int grid_limit) {
   const int n = A->n;
+  g_call_grid = g_cheb_max_grid > 0 ? g_cheb_max_grid : grid_limit;
   switch (v) {
     case 0:
     case 1: {
@@ -721,8 +725,23 @@ int launch_variant(const evslcu_mat *A, int v, bool first, bool epi, const doubl
   }
 }
 
-// Times every allowed variant (12 degree steps each after 3 untimed ones) on
-// zero-filled scratch vectors; keeps the fastest in A->cheb_variant.
+// Microseconds per degree step of variant v with grid limit g (12 timed
+// steps after 3 untimed ones) on the zero-filled scratch vectors; 0 on error.
+float time_variant(const evslcu_mat *A, int v, int g, double *scr, cudaEvent_t e0, cudaEvent_t e1, int *rc) {
+  constexpr int kWarm = 3, kTimed = 12;
+  const size_t n = (size_t)A->n;
+  for (int i = 0; i < kWarm + kTimed && !*rc; ++i) {
+    if (i == kWarm) cudaEventRecord(e0, stream());
+    *rc = launch_variant(A, v, false, false, scr, scr + n, scr + n, scr + 2 * n, 2.0, 0.0, 1.0, 1.0, nullptr, g);
+  }
+  cudaEventRecord(e1, stream());
+  float ms = 0.0f;
+  if (*rc || cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) return 0.0f;
+  return 1e3f * ms / kTimed;
+}
+
+// Times every allowed variant on zero-filled scratch vectors and keeps the
+// fastest in A->cheb_variant, then its best grid limit in A->cheb_grid.
 int tune_cheb(evslcu_mat *A) {
   static const int pref[kChebVariants] = {4, 2, 3, 1, 0, 5};
   int fallback = 0;
@@ -744,20 +763,24 @@ int tune_cheb(evslcu_mat *A) {
   if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) rc = EVSLCU_ERR_CUDA;
   for (int v = 0; v < kChebVariants && !rc; ++v) {
     if (!cheb_variant_ok(A, v)) continue;
-    constexpr int kWarm = 3, kTimed = 12;
-    for (int i = 0; i < kWarm + kTimed && !rc; ++i) {
-      if (i == kWarm) cudaEventRecord(e0, stream());
-      rc = launch_variant(A, v, false, false, scr, scr + n, scr + n, scr + 2 * (size_t)n, 2.0, 0.0, 1.0, 1.0,
-                          nullptr);
-    }
-    cudaEventRecord(e1, stream());
-    float ms = 0.0f;
-    if (!rc && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
-      A->cheb_us[v] = 1e3f * ms / kTimed;
-      if (best_us == 0.0f || A->cheb_us[v] < best_us) {
-        best_us = A->cheb_us[v];
+    const float us = time_variant(A, v, 0, scr, e0, e1, &rc);
+    if (us > 0.0f) {
+      A->cheb_us[v] = us;
+      if (best_us == 0.0f || us < best_us) {
+        best_us = us;
         best = v;
       }
+    }
+  }
+  // then the grid limit for the chosen variant: one row per thread, or
+  // 16 / 8 blocks per SM going round a grid-stride loop
+  A->cheb_grid = 0;
+  for (int g : {16 * sm_count(), 8 * sm_count()}) {
+    if (rc || best_us == 0.0f) break;
+    const float us = time_variant(A, best, g, scr, e0, e1, &rc);
+    if (us > 0.0f && us < best_us) {
+      best_us = us;
+      A->cheb_grid = g;
     }
   }
   if (e0) cudaEventDestroy(e0);
@@ -799,10 +822,12 @@ int evslcu::chebav_per_degree(const evslcu_mat *A, const double *mu, int deg, do
     double *out = W[(k - 1) % 2];
     const bool last = (k == deg);
     if (var >= 0) {
-      const int rc = launch_variant(A, var, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
+      const int rc =
+          launch_variant(A, var, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi, A->cheb_grid);
       if (rc) return rc;
       continue;
     }
+    g_call_grid = g_cheb_max_grid;
     int rc = with_view(A, [&](auto view) {
       return launch_cheb_step(view, n, A->maxw, k == 1, last && epi, vk, vkm1, out, y, t, ncc, mu[k], mu[0], epi);
     });
@@ -839,11 +864,19 @@ int evslcu_set_cheb_variant(int v) {
   return 0;
 }
 
+int evslcu_mat_cheb_grid(const evslcu_mat *A) { return A ? A->cheb_grid : 0; }
+
 int evslcu_mat_cheb_variant(const evslcu_mat *A, float *us) {
   if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
   if (us)
     for (int v = 0; v < kChebVariants; ++v) us[v] = A->cheb_us[v];
   return A->cheb_variant;
+}
+
+int evslcu_set_cheb_max_grid(int blocks) {
+  if (blocks < 0) return fail(EVSLCU_ERR_ARG, "grid limit must be >= 0");
+  g_cheb_max_grid = blocks;
+  return 0;
 }
 
 int evslcu_set_row_unroll(int on) {

@@ -56,6 +56,7 @@ struct evslcu_mat {
   int use_pat = 0;     // 1: the FP64 single-vector filter and SpMV read the dictionary
   int cheb_variant = -1;      // single-vector filter kernel chosen by timing (-1: not yet)
   float cheb_us[6] = {0, 0, 0, 0, 0, 0};  // measured time per degree step of each variant
+  int cheb_grid = 0;                      // tuned block limit per degree step (0: one row per thread)
 };
 
 namespace evslcu {

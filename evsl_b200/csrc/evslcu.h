@@ -259,9 +259,14 @@ int evslcu_set_pattern_const(int on);
  * unrolled/loop, 4/5 pattern table in constant memory loop/unrolled).  All
  * give identical results. */
 int evslcu_set_cheb_variant(int v);
+/* At most this many blocks per degree step of the single-vector filter
+ * (0, default: one row per thread); rows beyond go round a grid-stride loop. */
+int evslcu_set_cheb_max_grid(int blocks);
 /* A's chosen variant (-1: not chosen yet) and, in us[0..5], the measured
  * microseconds per degree step of each variant timed (0: not timed). */
 int evslcu_mat_cheb_variant(const evslcu_mat *A, float *us);
+/* The block limit per degree step chosen with the variant (0: none). */
+int evslcu_mat_cheb_grid(const evslcu_mat *A);
 /* Keep A's stored matrix resident in L2 (persisting access-policy window on
  * the library stream, set-aside sized to it) or release that (on = 0). */
 int evslcu_mat_l2_persist(const evslcu_mat *A, int on);

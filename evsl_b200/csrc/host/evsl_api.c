@@ -491,6 +491,8 @@ int evslx_row_pattern_count(void) { return evslh.mat ? evslcu_mat_pattern_count(
 
 int evslx_set_filter_kernel(int variant) { return from_cu(evslcu_set_cheb_variant(variant)); }
 
+int evslx_filter_kernel_grid(void) { return evslh.mat ? evslcu_mat_cheb_grid(evslh.mat) : 0; }
+
 int evslx_filter_kernel(double *us) {
   float f[6] = {0, 0, 0, 0, 0, 0};
   const int v = evslh.mat ? evslcu_mat_cheb_variant(evslh.mat, f) : -1;

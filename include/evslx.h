@@ -145,6 +145,9 @@ int evslx_set_filter_kernel(int variant);
  * not NULL, us[0..5] = measured microseconds per degree step of each variant
  * timed (0: not timed). */
 int evslx_filter_kernel(double *us);
+/* Blocks per degree step chosen with that variant (0: one row per thread;
+ * otherwise rows go round a grid-stride loop of that many blocks). */
+int evslx_filter_kernel_grid(void);
 /* Bytes per stored value (4 or 8) and per stored column index (2 or 4). */
 int evslx_matrix_storage(int *value_bytes, int *index_bytes);
 
