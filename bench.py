@@ -551,7 +551,7 @@ def run_multifilter(args):
     prec = E.PREC_MIXED if args.precision == "mixed" else E.PREC_FP64
     lstream = torch.cuda.ExternalStream(lib.stream_handle())
     if args.sweep or args.low_degree:
-        combos = [(v, pr, b) for v in range(4) for pr in (E.PREC_FP64, E.PREC_MIXED) for b in (1, 2, 4, 8, 16)] \
+        combos = [(v, pr, b) for v in range(6) for pr in (E.PREC_FP64, E.PREC_MIXED) for b in (1, 2, 4, 8, 16)] \
             if args.sweep else [(args.variant, prec, args.ncols)]
         for v, pr, b in combos:
             lib.set_filter_variant(v)

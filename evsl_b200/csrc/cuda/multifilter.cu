@@ -131,10 +131,12 @@ struct Split {
 
 // Kernel variants: the column part per thread (16 or 32 bytes) and whether
 // the TPR threads of a row load its stored entries cooperatively (each a
-// share, broadcast by warp shuffles) instead of each loading all of them.
-// -1: each matrix uses the variant the autotuner measured fastest for it
-// (per precision and block width); 0..3: that variant everywhere.
+// share, broadcast by warp shuffles) instead of each loading all of them
+// (0..3, SELL-32), or the row-pattern dictionary with 16- or 32-byte parts
+// (4, 5).  -1: each matrix uses the variant the autotuner measured fastest
+// for it (per precision and block width); 0..5: that variant everywhere.
 static int g_mf_variant = -1;
+constexpr int kMfVariants = 6;
 
 // One degree of the recurrence for all columns: thread (row r, part q)
 // handles columns q*CPT .. q*CPT+CPT-1 of row r.  Rows run over the padded
@@ -255,13 +257,120 @@ int mf_step_v(const SellT<AV, IT> &A, int k, const VT *vk, const VT *vkm1, VT *o
   return check_launch("k_mf_step");
 }
 
+// One table entry of a row pattern: the value as a double and the column
+// offset from the row.
+__device__ __forceinline__ void pat_entry(const PatPView &A, int idx, double &v, int &off) {
+  const unsigned long long e = __ldg(A.pk + idx);
+  v = pat_val(e);
+  off = pat_off(e);
+}
+__device__ __forceinline__ void pat_entry(const PatView &A, int idx, double &v, int &off) {
+  const double2 e = __ldg(A.ent + idx);
+  v = e.x;
+  off = (int)__double_as_longlong(e.y);
+}
+
+// The same degree step on the row-pattern dictionary: a row's entries come
+// from the pattern table (a few KB, read through L1) instead of the stored
+// matrix, in CSR order and without padding entries.  Each table entry is
+// read once per row part and applied to all CPT columns of the part.
+template <class VT, int B, int CPTB, class PV, bool FIRST>
+__global__ void __launch_bounds__(kThreads)
+    k_mf_step_pat(PV A, const VT *__restrict__ vk, const VT *vkm1, VT *out, VT *__restrict__ y,
+                  const VT *__restrict__ coef) {
+  constexpr int CPT = Split<VT, B, CPTB>::CPT, TPR = Split<VT, B, CPTB>::TPR;
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const long long total = (long long)A.n * TPR;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+    const int r = (int)(g / TPR), q = (int)(g % TPR);
+    const int cb = q * CPT;
+    const long long base = (long long)r * B + cb;
+    VT xr[CPT], wv[CPT], yv[CPT], vm[CPT];
+    load_row<VT, CPT>(vk + base, xr);
+    load_row_cg<VT, CPT>(y + base, yv);
+    if (!FIRST) load_row_cg<VT, CPT>(vkm1 + base, vm);
+    VT acc[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] = (VT)0;
+    const int2 h = __ldg(A.hdr + __ldg(A.pid + r));
+    constexpr int U = 4;
+    for (int j = 0; j < h.y; j += U) {
+      VT v[U];
+      int col[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        col[u] = r;
+        v[u] = (VT)0;
+        if (j + u < h.y) {
+          double dv;
+          int off;
+          pat_entry(A, h.x + j + u, dv, off);
+          v[u] = (VT)dv;
+          col[u] = r + off;
+        }
+      }
+      VT x[U][CPT];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (j + u < h.y) load_row<VT, CPT>(vk + (long long)col[u] * B + cb, x[u]);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (j + u < h.y)
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) acc[c] = fmadd(v[u], x[u][c], acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const VT *cf = coef + kCoef * (cb + c);
+      VT t = mul(__ldg(cf), add(acc[c], mul(__ldg(cf + 1), xr[c])));
+      if (!FIRST) t = add(t, -vm[c]);
+      wv[c] = t;
+      if (__ldg(cf + 3) != (VT)0) yv[c] = add(yv[c], mul(__ldg(cf + 2), t));
+    }
+    store_row<VT, CPT>(out + base, wv);
+    store_row<VT, CPT>(y + base, yv);
+  }
+}
+
+template <class VT, int B, int CPTB, class PV>
+int mf_step_pat_v(const PV &A, int k, const VT *vk, const VT *vkm1, VT *out, VT *y, const VT *coef) {
+  constexpr int TPR = Split<VT, B, CPTB>::TPR;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid_for((long long)A.n * TPR, kThreads, 1 << 20));
+  cfg.blockDim = dim3(kThreads);
+  cfg.stream = stream();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = (k == 1) ? cudaLaunchKernelEx(&cfg, k_mf_step_pat<VT, B, CPTB, PV, true>, A, vk, vkm1, out, y, coef)
+                           : cudaLaunchKernelEx(&cfg, k_mf_step_pat<VT, B, CPTB, PV, false>, A, vk, vkm1, out, y, coef);
+  if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "multi-column filter launch failed: %s", cudaGetErrorString(e));
+  return check_launch("k_mf_step_pat");
+}
+
+// Variants 4 and 5 (16- or 32-byte column parts) read the row-pattern
+// dictionary; they need one (A->pat_id and in use).
+inline bool mf_pattern_ok(const evslcu_mat *M) { return M->pat_id && M->use_pat && M->kernel == 0; }
+
 template <class VT, int B, class AV, class IT>
-int mf_step(const SellT<AV, IT> &A, int variant, int k, const VT *vk, const VT *vkm1, VT *out, VT *y,
-            const VT *coef) {
+int mf_step(const evslcu_mat *M, const SellT<AV, IT> &A, int variant, int k, const VT *vk, const VT *vkm1, VT *out,
+            VT *y, const VT *coef) {
   switch (variant) {
     case 1: return mf_step_v<VT, B, 32, false>(A, k, vk, vkm1, out, y, coef);
     case 2: return mf_step_v<VT, B, 16, true>(A, k, vk, vkm1, out, y, coef);
     case 3: return mf_step_v<VT, B, 32, true>(A, k, vk, vkm1, out, y, coef);
+    case 4:
+    case 5:
+      if (!mf_pattern_ok(M)) return fail(EVSLCU_ERR_ARG, "filter variant %d needs the row-pattern dictionary", variant);
+      if (variant == 4)
+        return M->pat_f32 ? mf_step_pat_v<VT, B, 16>(pat_pview(M), k, vk, vkm1, out, y, coef)
+                          : mf_step_pat_v<VT, B, 16>(pat_view(M), k, vk, vkm1, out, y, coef);
+      return M->pat_f32 ? mf_step_pat_v<VT, B, 32>(pat_pview(M), k, vk, vkm1, out, y, coef)
+                        : mf_step_pat_v<VT, B, 32>(pat_view(M), k, vk, vkm1, out, y, coef);
     default: return mf_step_v<VT, B, 16, false>(A, k, vk, vkm1, out, y, coef);
   }
 }
@@ -296,7 +405,7 @@ void fill_coef(VT *h, int B, int ncols, const evslcu_filter_col *cols, int maxde
 // The launch sequence for one group of <= 16 columns: pack, one step per
 // degree, unpack.  coef: the group's device coefficient table.
 template <class VT, int B, class AV, class IT>
-int mf_group(const SellT<AV, IT> &A, int variant, int ncols, int maxdeg, const VT *coef, const double *const *xtab,
+int mf_group(const evslcu_mat *M, const SellT<AV, IT> &A, int variant, int ncols, int maxdeg, const VT *coef, const double *const *xtab,
              double *const *ytab, VT *P, VT *W0, VT *W1, VT *Y, int *nlaunch) {
   const int n = A.n;
   const int g = grid_for((long long)n * B);
@@ -306,7 +415,7 @@ int mf_group(const SellT<AV, IT> &A, int variant, int ncols, int maxdeg, const V
   for (int k = 1; !rc && k <= maxdeg; ++k) {
     const VT *vk = (k == 1) ? P : W[(k - 2) % 2];
     const VT *vkm1 = (k == 1) ? nullptr : ((k == 2) ? P : W[(k - 1) % 2]);
-    rc = mf_step<VT, B>(A, variant, k, vk, vkm1, W[(k - 1) % 2], Y, coef + (size_t)k * B * kCoef);
+    rc = mf_step<VT, B>(M, A, variant, k, vk, vkm1, W[(k - 1) % 2], Y, coef + (size_t)k * B * kCoef);
   }
   if (!rc) {
     k_mf_unpack<VT, B><<<g, kThreads, 0, stream()>>>(n, ncols, Y, ytab);
@@ -317,14 +426,14 @@ int mf_group(const SellT<AV, IT> &A, int variant, int ncols, int maxdeg, const V
 }
 
 template <class VT, class AV, class IT>
-int mf_dispatch(const SellT<AV, IT> &A, int variant, int B, int ncols, int maxdeg, const VT *coef,
+int mf_dispatch(const evslcu_mat *M, const SellT<AV, IT> &A, int variant, int B, int ncols, int maxdeg, const VT *coef,
                 const double *const *xtab, double *const *ytab, VT *P, VT *W0, VT *W1, VT *Y, int *nl) {
   switch (B) {
-    case 1: return mf_group<VT, 1>(A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
-    case 2: return mf_group<VT, 2>(A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
-    case 4: return mf_group<VT, 4>(A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
-    case 8: return mf_group<VT, 8>(A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
-    default: return mf_group<VT, 16>(A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
+    case 1: return mf_group<VT, 1>(M, A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
+    case 2: return mf_group<VT, 2>(M, A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
+    case 4: return mf_group<VT, 4>(M, A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
+    case 8: return mf_group<VT, 8>(M, A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
+    default: return mf_group<VT, 16>(M, A, variant, ncols, maxdeg, coef, xtab, ytab, P, W0, W1, Y, nl);
   }
 }
 
@@ -436,8 +545,9 @@ int autotune(evslcu_mat *A, int fp32, int B) {
   cudaEventCreate(&e1);
   float best = 1e30f;
   int bestv = 0;
-  for (int v = 0; !rc && v < 4; ++v) {
+  for (int v = 0; !rc && v < kMfVariants; ++v) {
     if (g_mf_variant >= 0 && v != g_mf_variant) continue;  // a forced variant is only timed
+    if (v >= 4 && !mf_pattern_ok(A)) continue;
     float ms = 0.0f;
     for (int rep = 0; !rc && rep < 2; ++rep) {
       cudaEventRecord(e0, stream());
@@ -448,11 +558,11 @@ int autotune(evslcu_mat *A, int fp32, int B) {
           const void *vals = (A->vfmt == 1) ? A->sval : A->sval32;
           auto go = [&](auto view) -> int {
             switch (B) {
-              case 1: return mf_step<float, 1>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
-              case 2: return mf_step<float, 2>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
-              case 4: return mf_step<float, 4>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
-              case 8: return mf_step<float, 8>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
-              default: return mf_step<float, 16>(view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
+              case 1: return mf_step<float, 1>(A, view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
+              case 2: return mf_step<float, 2>(A, view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
+              case 4: return mf_step<float, 4>(A, view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
+              case 8: return mf_step<float, 8>(A, view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
+              default: return mf_step<float, 16>(A, view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
             }
           };
           rc = A->ifmt ? go(SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals, A->ellw})
@@ -463,11 +573,11 @@ int autotune(evslcu_mat *A, int fp32, int B) {
               return fail(EVSLCU_ERR_ARG, "filter_columns needs the SELL-32 storage");
             } else {
               switch (B) {
-                case 1: return mf_step<double, 1>(view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
-                case 2: return mf_step<double, 2>(view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
-                case 4: return mf_step<double, 4>(view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
-                case 8: return mf_step<double, 8>(view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
-                default: return mf_step<double, 16>(view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
+                case 1: return mf_step<double, 1>(A, view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
+                case 2: return mf_step<double, 2>(A, view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
+                case 4: return mf_step<double, 4>(A, view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
+                case 8: return mf_step<double, 8>(A, view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
+                default: return mf_step<double, 16>(A, view, v, k, (const double *)P, (const double *)W0, (double *)W1, (double *)Y, (const double *)cf);
               }
             }
           });
@@ -522,10 +632,10 @@ int mf_sequence(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_co
       const float *cf = (const float *)coef + off;
       const void *vals = (A->vfmt == 1) ? A->sval : A->sval32;
       if (A->ifmt)
-        rc = mf_dispatch<float>(SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals, A->ellw},
+        rc = mf_dispatch<float>(A, SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals, A->ellw},
                                 variant_of(A, 1, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
       else
-        rc = mf_dispatch<float>(SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals, A->ellw},
+        rc = mf_dispatch<float>(A, SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals, A->ellw},
                                 variant_of(A, 1, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
     } else {
       double *P = (double *)w, *W0 = (double *)(w + blk), *W1 = (double *)(w + 2 * blk), *Y = (double *)(w + 3 * blk);
@@ -534,7 +644,7 @@ int mf_sequence(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_co
         if constexpr (std::is_same<decltype(view), CsrView>::value) {
           return fail(EVSLCU_ERR_ARG, "filter_columns needs the SELL-32 storage");
         } else {
-          return mf_dispatch<double>(view, variant_of(A, 0, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
+          return mf_dispatch<double>(A, view, variant_of(A, 0, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
         }
       });
     }
@@ -662,7 +772,7 @@ int evslcu_filter_plan_run(evslcu_filter_plan *P, const double *const *x, double
 int evslcu_filter_plan_columns(const evslcu_filter_plan *P) { return P ? P->ncols : 0; }
 
 int evslcu_set_filter_variant(int v) {
-  if (v < -1 || v > 3) return fail(EVSLCU_ERR_ARG, "filter variant must be -1 (tuned) or 0..3");
+  if (v < -1 || v >= kMfVariants) return fail(EVSLCU_ERR_ARG, "filter variant must be -1 (tuned) or 0..5");
   g_mf_variant = v;
   return 0;
 }

@@ -259,12 +259,17 @@ void evslx_result_free(evslx_result *r);
  * every column equal to ChebAv bit for bit; MIXED: the FP32 filter. */
 int evslx_chebav_multi(int ncols, const polparams *pols, const double *X, double *Y, int precision);
 
-/* Variant of the multi-column filter kernel (results are identical):
- * bit 0 -- each thread handles 32 bytes of a row's columns (else 16),
- * bit 1 -- a row's threads load its stored entries cooperatively;
+/* Variant of the multi-column filter kernel (results are identical; the
+ * SELL-32 forms add the zero padding of a chunk, which can only turn an
+ * exactly zero row sum of -0 into +0):
+ * 0..3 -- SELL-32; bit 0: each thread handles 32 bytes of a row's columns
+ * (else 16), bit 1: a row's threads load its stored entries cooperatively;
+ * 4, 5 -- the row-pattern dictionary (see evslx_set_row_patterns), 16- or
+ * 32-byte column parts; filtering fails with EVSLX_ERR_ARG when the matrix
+ * has none;
  * -1 (default) -- autotuned: the first filter on a matrix with a given
- * precision and block width times the four variants on a few degree steps
- * and keeps the fastest for that matrix. */
+ * precision and block width times the variants available for it on a few
+ * degree steps and keeps the fastest for that matrix. */
 int evslx_set_filter_variant(int v);
 int evslx_get_filter_variant(void);
 /* The variant tuned for the registered matrix (-1: not tuned yet). */

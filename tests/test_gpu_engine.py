@@ -61,9 +61,12 @@ def test_multi_filter_fp64_bitwise_fp32_close(gpu_lib):
 
 
 def test_filter_variants_and_autotuner(gpu_lib):
-    """All kernel variants give the same bits; the autotuner picks one."""
+    """All kernel variants (SELL-32 and row-pattern dictionary) give the same
+    bits; the autotuner picks one; a dictionary variant forced on a matrix
+    without a dictionary fails with an error."""
     ia, ja, a = O.lap_csr(40, 40, 40)
     gpu_lib.set_csr(ia, ja, a)
+    assert gpu_lib.row_pattern_count() == 27
     n = len(ia) - 1
     pol = gpu_lib.find_pol([0.6, 0.9, 0.0, 12.0])
     try:
@@ -72,10 +75,19 @@ def test_filter_variants_and_autotuner(gpu_lib):
                 X = O.seeded_normal(n * B, 30 + B).reshape(B, n)
                 gpu_lib.set_filter_variant(-1)
                 ref = gpu_lib.chebav_multi([pol] * B, X, prec)
-                assert 0 <= gpu_lib.tuned_filter_variant(prec, B) <= 3
-                for v in range(4):
+                assert 0 <= gpu_lib.tuned_filter_variant(prec, B) <= 5
+                for v in range(6):
                     gpu_lib.set_filter_variant(v)
-                    assert np.array_equal(gpu_lib.chebav_multi([pol] * B, X, prec), ref)
+                    assert np.array_equal(gpu_lib.chebav_multi([pol] * B, X, prec), ref), (prec, B, v)
+        ia, ja, a = W.random_spd_csr(3000, 8, 5)
+        gpu_lib.set_csr(ia, ja, a)
+        assert gpu_lib.row_pattern_count() == 0
+        lo, hi = W.gershgorin_bounds(ia, ja, a)
+        pol2 = gpu_lib.find_pol([lo + 0.3 * (hi - lo), lo + 0.4 * (hi - lo), lo, hi], max_deg=50)
+        gpu_lib.set_filter_variant(4)
+        with pytest.raises(Exception, match="dictionary"):
+            gpu_lib.chebav_multi([pol2] * 2, O.seeded_normal(6000, 3).reshape(2, 3000), E.PREC_FP64)
+        gpu_lib.free_pol(pol2)
     finally:
         gpu_lib.set_filter_variant(-1)
         gpu_lib.free_pol(pol)
