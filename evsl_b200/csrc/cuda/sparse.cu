@@ -783,6 +783,7 @@ int tune_cheb(evslcu_mat *A) {
       A->cheb_grid = g;
     }
   }
+  A->cheb_best_us = best_us;
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   evslcu_free(scr);
@@ -865,6 +866,13 @@ int evslcu_set_cheb_variant(int v) {
 }
 
 int evslcu_mat_cheb_grid(const evslcu_mat *A) { return A ? A->cheb_grid : 0; }
+
+double evslcu_chebav_step_cost(evslcu_mat *A) {
+  if (!A || A->kernel != 0) return -1.0;
+  const int v = cheb_variant(A);  // tunes on first use
+  if (v < 0) return -1.0;
+  return A->cheb_best_us > 0.0f ? (double)A->cheb_best_us : (double)A->cheb_us[v];
+}
 
 int evslcu_mat_cheb_variant(const evslcu_mat *A, float *us) {
   if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");

@@ -57,6 +57,7 @@ struct evslcu_mat {
   int cheb_variant = -1;      // single-vector filter kernel chosen by timing (-1: not yet)
   float cheb_us[6] = {0, 0, 0, 0, 0, 0};  // measured time per degree step of each variant
   int cheb_grid = 0;                      // tuned block limit per degree step (0: one row per thread)
+  float cheb_best_us = 0.0f;              // time per degree step of the chosen variant and grid
 };
 
 namespace evslcu {

@@ -267,6 +267,9 @@ int evslcu_set_cheb_max_grid(int blocks);
 int evslcu_mat_cheb_variant(const evslcu_mat *A, float *us);
 /* The block limit per degree step chosen with the variant (0: none). */
 int evslcu_mat_cheb_grid(const evslcu_mat *A);
+/* Measured microseconds per degree step of the single-vector FP64 filter
+ * kernel chosen for A (times the variants on first use; -1 on failure). */
+double evslcu_chebav_step_cost(evslcu_mat *A);
 /* Keep A's stored matrix resident in L2 (persisting access-policy window on
  * the library stream, set-aside sized to it) or release that (on = 0). */
 int evslcu_mat_l2_persist(const evslcu_mat *A, int on);

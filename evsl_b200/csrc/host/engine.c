@@ -840,6 +840,11 @@ int evslx_engine_step(evslx_engine *E) {
       cost[b] = evslcu_filter_step_cost(M->mat, fp32, b);
       if (cost[b] <= 0.0) have_cost = 0;
     }
+    /* one-column FP64 groups run the single-vector filter (run_group_filter) */
+    if (have_cost && !fp32) {
+      const double c1 = evslcu_chebav_step_cost(M->mat);
+      if (c1 > 0.0) cost[1] = c1;
+    }
     int ng = 0;
     if (have_cost) {
       double *best = E->gbest;
