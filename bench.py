@@ -84,7 +84,7 @@ def parse():
     p.add_argument("--filter-kernel", default="auto",
                    help="single-vector FP64 filter kernel: auto (timed choice per matrix) or one of "
                         "sell-loop, sell-unrolled, pattern-global-unrolled, pattern-global-loop, "
-                        "pattern-constant-loop, pattern-constant-unrolled (profiling runs)")
+                        "pattern-constant-loop, pattern-constant-unrolled, pattern-constant-rowdesc (profiling runs)")
     return p.parse_args()
 
 

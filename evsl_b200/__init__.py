@@ -555,7 +555,7 @@ class Library:
         return int(self.lib.evslx_row_pattern_count())
 
     FILTER_KERNELS = ("sell-loop", "sell-unrolled", "pattern-global-unrolled", "pattern-global-loop",
-                      "pattern-constant-loop", "pattern-constant-unrolled")
+                      "pattern-constant-loop", "pattern-constant-unrolled", "pattern-constant-rowdesc")
 
     def set_filter_kernel(self, variant):
         """Force a single-vector filter kernel (index or name), or -1/None for timed selection."""
@@ -567,9 +567,9 @@ class Library:
 
     def filter_kernel(self):
         """(chosen variant or -1, {variant name: measured us per degree step}) of the registered matrix."""
-        us = (C.c_double * 6)()
+        us = (C.c_double * 7)()
         v = int(self.lib.evslx_filter_kernel(us))
-        return v, {self.FILTER_KERNELS[i]: us[i] for i in range(6) if us[i] > 0}
+        return v, {self.FILTER_KERNELS[i]: us[i] for i in range(7) if us[i] > 0}
 
     def filter_kernel_grid(self):
         """Blocks per degree step chosen with the filter kernel (0: one row per thread)."""

@@ -113,9 +113,74 @@ __device__ __forceinline__ double row_dot_w(const PatCPView &A, int r, const dou
   return acc;
 }
 
+// Constant table addressed by a per-row descriptor (first pool entry << 8 |
+// count) instead of a pattern id: no header lookup on the row's dependent
+// chain, for 2 more bytes per row.  PACKED: entries as in PatCPView, else
+// double values with the offsets in c_pat_off.
+template <bool PACKED>
+struct PatCDView {
+  int n;
+  const unsigned *__restrict__ desc;
+};
+
+template <bool PACKED>
+__device__ __forceinline__ void pat_centry(int idx, double &v, int &off) {
+  const unsigned long long e = c_pat_w[idx];
+  if (PACKED) {
+    v = pat_val(e);
+    off = pat_off(e);
+  } else {
+    v = __longlong_as_double((long long)e);
+    off = c_pat_off[idx];
+  }
+}
+
+template <bool COHERENT, bool PACKED>
+__device__ __forceinline__ double row_dot(const PatCDView<PACKED> &A, int r, const double *x) {
+  const unsigned d = __ldg(A.desc + r);
+  const int b = (int)(d >> 8), len = (int)(d & 255u);
+  const double *xr = x + r;
+  double acc = 0.0;
+  for (int j = 0; j < len; ++j) {
+    double v;
+    int off;
+    pat_centry<PACKED>(b + j, v, off);
+    acc = __dadd_rn(acc, __dmul_rn(v, ldx<COHERENT>(xr + off)));
+  }
+  return acc;
+}
+
+template <int WMAX, bool COHERENT, bool PACKED>
+__device__ __forceinline__ double row_dot_w(const PatCDView<PACKED> &A, int r, const double *x) {
+  const unsigned d = __ldg(A.desc + r);
+  const int b = (int)(d >> 8), len = (int)(d & 255u);
+  const double *xr = x + r;
+  double v[WMAX], g[WMAX];
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < len) {
+      int off;
+      pat_centry<PACKED>(b + j, v[j], off);
+      g[j] = ldx<COHERENT>(xr + off);
+    }
+  double acc = 0.0;
+#pragma unroll
+  for (int j = 0; j < WMAX; ++j)
+    if (j < len) acc = __dadd_rn(acc, __dmul_rn(v[j], g[j]));
+  return acc;
+}
+
 }  // namespace evslcu
 
 namespace {
+
+// desc[r] = (first pool entry of r's pattern) << 8 | its count.
+__global__ void k_pat_desc(int n, const unsigned short *pid, const int2 *hdr, int ebase, unsigned *desc) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int2 h = hdr[pid[r]];
+    desc[r] = ((unsigned)(h.x + ebase) << 8) | (unsigned)h.y;
+  }
+}
 
 // First-fit allocator of pool slots (host side; the library runs on one
 // stream and one host thread per process).
@@ -192,10 +257,25 @@ int pat_const_claim(evslcu_mat *M) {
   }
   M->pat_cent = eb;
   M->pat_chdr = hb;
+  // per-row descriptors (optional: counts must fit 8 bits)
+  if (M->pat_maxlen <= 255) {
+    M->pat_desc = (unsigned *)evslcu_malloc(sizeof(unsigned) * (size_t)M->n);
+    if (M->pat_desc) {
+      k_pat_desc<<<grid_for(M->n), kThreads, 0, stream()>>>(M->n, M->pat_id, (const int2 *)M->pat_table, eb,
+                                                            M->pat_desc);
+      count_launch();
+      if (check_launch("k_pat_desc")) {
+        evslcu_free(M->pat_desc);
+        M->pat_desc = nullptr;
+      }
+    }
+  }
   return 0;
 }
 
 void pat_const_release(evslcu_mat *M) {
+  evslcu_free(M->pat_desc);
+  M->pat_desc = nullptr;
   if (M->pat_chdr < 0) return;
   g_cpool_ent.release(M->pat_cent);
   g_cpool_hdr.release(M->pat_chdr);
@@ -676,7 +756,7 @@ int evslcu::chebav_user_matvec(const evslcu_op *op, const double *mu, int deg, d
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr int kChebVariants = 6;
+constexpr int kChebVariants = 7;
 int g_cheb_force = -1;
 
 bool cheb_variant_ok(const evslcu_mat *A, int v) {
@@ -690,6 +770,7 @@ bool cheb_variant_ok(const evslcu_mat *A, int v) {
     case 3: return pat;
     case 4: return pconst;
     case 5: return pconst && unroll_width(A->pat_maxlen) > 0;
+    case 6: return pconst && A->pat_desc;
     default: return false;
   }
 }
@@ -714,6 +795,12 @@ int launch_variant(const evslcu_mat *A, int v, bool first, bool epi, const doubl
         return launch_cheb_step(pat_pview(A), n, wmax, first, epi, vk, vkm1, out, y, t, ncc, s, mu0, ep);
       return launch_cheb_step(pat_view(A), n, wmax, first, epi, vk, vkm1, out, y, t, ncc, s, mu0, ep);
     }
+    case 6:
+      if (A->pat_f32)
+        return launch_cheb_step(PatCDView<true>{n, A->pat_desc}, n, 0, first, epi, vk, vkm1, out, y, t, ncc, s, mu0,
+                                ep);
+      return launch_cheb_step(PatCDView<false>{n, A->pat_desc}, n, 0, first, epi, vk, vkm1, out, y, t, ncc, s, mu0,
+                              ep);
     default: {
       const int wmax = (v == 5) ? A->pat_maxlen : 0;
       if (A->pat_f32)
@@ -743,7 +830,7 @@ float time_variant(const evslcu_mat *A, int v, int g, double *scr, cudaEvent_t e
 // Times every allowed variant on zero-filled scratch vectors and keeps the
 // fastest in A->cheb_variant, then its best grid limit in A->cheb_grid.
 int tune_cheb(evslcu_mat *A) {
-  static const int pref[kChebVariants] = {4, 2, 3, 1, 0, 5};
+  static const int pref[kChebVariants] = {4, 6, 2, 3, 1, 0, 5};
   int fallback = 0;
   for (int v : pref)
     if (cheb_variant_ok(A, v)) {

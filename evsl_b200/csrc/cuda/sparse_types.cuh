@@ -53,9 +53,10 @@ struct evslcu_mat {
   int pat_f32 = 0;     // 1: every table value is exactly a float (packed entries exist)
   int pat_cent = -1;   // first entry of the table's copy in the constant pool (-1: not there)
   int pat_chdr = -1;   // first header there
+  unsigned *pat_desc = nullptr;  // per row: (first pool entry << 8) | count, when in the pool
   int use_pat = 0;     // 1: the FP64 single-vector filter and SpMV read the dictionary
   int cheb_variant = -1;      // single-vector filter kernel chosen by timing (-1: not yet)
-  float cheb_us[6] = {0, 0, 0, 0, 0, 0};  // measured time per degree step of each variant
+  float cheb_us[7] = {0, 0, 0, 0, 0, 0, 0};  // measured time per degree step of each variant
   int cheb_grid = 0;                      // tuned block limit per degree step (0: one row per thread)
   float cheb_best_us = 0.0f;              // time per degree step of the chosen variant and grid
 };

@@ -254,15 +254,16 @@ int evslcu_set_row_unroll(int on);
  * default) or always from global memory (0).  Same arithmetic either way. */
 int evslcu_set_pattern_const(int on);
 /* Single-vector filter kernel variant: -1 (default) times the allowed
- * variants on a matrix's first filter call and keeps the fastest; 0..5 forces
+ * variants on a matrix's first filter call and keeps the fastest; 0..6 forces
  * one (0/1 SELL-32 loop/unrolled, 2/3 pattern table in global memory
- * unrolled/loop, 4/5 pattern table in constant memory loop/unrolled).  All
- * give identical results. */
+ * unrolled/loop, 4/5 pattern table in constant memory loop/unrolled, 6 the
+ * constant table addressed by a per-row descriptor).  All give identical
+ * results. */
 int evslcu_set_cheb_variant(int v);
 /* At most this many blocks per degree step of the single-vector filter
  * (0, default: one row per thread); rows beyond go round a grid-stride loop. */
 int evslcu_set_cheb_max_grid(int blocks);
-/* A's chosen variant (-1: not chosen yet) and, in us[0..5], the measured
+/* A's chosen variant (-1: not chosen yet) and, in us[0..6], the measured
  * microseconds per degree step of each variant timed (0: not timed). */
 int evslcu_mat_cheb_variant(const evslcu_mat *A, float *us);
 /* The block limit per degree step chosen with the variant (0: none). */

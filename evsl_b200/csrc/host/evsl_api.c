@@ -494,10 +494,10 @@ int evslx_set_filter_kernel(int variant) { return from_cu(evslcu_set_cheb_varian
 int evslx_filter_kernel_grid(void) { return evslh.mat ? evslcu_mat_cheb_grid(evslh.mat) : 0; }
 
 int evslx_filter_kernel(double *us) {
-  float f[6] = {0, 0, 0, 0, 0, 0};
+  float f[7] = {0, 0, 0, 0, 0, 0, 0};
   const int v = evslh.mat ? evslcu_mat_cheb_variant(evslh.mat, f) : -1;
   if (us)
-    for (int i = 0; i < 6; ++i) us[i] = f[i];
+    for (int i = 0; i < 7; ++i) us[i] = f[i];
   return v;
 }
 

@@ -135,14 +135,16 @@ int evslx_set_row_patterns(int on);
 int evslx_row_pattern_count(void);
 /* Kernel of the FP64 single-vector filter.  variant -1 (default): the first
  * filter call on a matrix times each variant allowed for it and keeps the
- * fastest; 0..5 forces one: 0/1 SELL-32 with looped/unrolled row products,
+ * fastest; 0..6 forces one: 0/1 SELL-32 with looped/unrolled row products,
  * 2/3 pattern table in global memory unrolled/looped, 4/5 pattern table in
- * constant memory looped/unrolled (2-5 need the row-pattern dictionary;
- * filtering fails with EVSLX_ERR_ARG when the forced variant is not
- * available).  Every variant gives the same result bit for bit. */
+ * constant memory looped/unrolled, 6 constant-memory table addressed by a
+ * 4-byte descriptor per row (2-6 need the row-pattern dictionary, 4-6 its
+ * table in the constant pool; filtering fails with EVSLX_ERR_ARG when the
+ * forced variant is not available).  Every variant gives the same result
+ * bit for bit. */
 int evslx_set_filter_kernel(int variant);
 /* The registered matrix's chosen variant (-1: not chosen yet) and, when us is
- * not NULL, us[0..5] = measured microseconds per degree step of each variant
+ * not NULL, us[0..6] = measured microseconds per degree step of each variant
  * timed (0: not timed). */
 int evslx_filter_kernel(double *us);
 /* Blocks per degree step chosen with that variant (0: one row per thread;

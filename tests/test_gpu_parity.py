@@ -362,7 +362,7 @@ def test_filter_variants_bitwise(gpu_lib, compress, mode):
         gpu_lib.lib.evslcu_set_row_unroll(1)
 
 
-@pytest.mark.parametrize("variant", range(6))
+@pytest.mark.parametrize("variant", range(7))
 def test_filter_kernel_variants_bitwise(gpu_lib, variant):
     """Each single-vector filter kernel, forced, gives the reference's filtered
     vector bit for bit on a grid operator (which has a row-pattern
@@ -417,7 +417,7 @@ def test_filter_kernel_is_chosen_by_timing(gpu_lib):
     gpu_lib.chebav(pol, O.seeded_normal(27000, 1))
     gpu_lib.free_pol(pol)
     v, us = gpu_lib.filter_kernel()
-    assert len(us) == 6 and v in range(6)
+    assert len(us) == 7 and v in range(7)
     assert us[gpu_lib.FILTER_KERNELS[v]] == min(us.values())
 
 
