@@ -250,6 +250,11 @@ int evslcu_mat_uses_patterns(const evslcu_mat *A);
  * rows of at most 8 or 16 stored entries (1, default) or the loop form (0).
  * Same arithmetic either way. */
 int evslcu_set_row_unroll(int on);
+/* All k eigenvalues (ascending) of the symmetric tridiagonal matrix with
+ * diagonal d[0..k) and off-diagonal e[0..k-1), all host arrays, computed on
+ * the GPU by multisection on Sturm counts (one warp per eigenvalue);
+ * synchronous. */
+int evslcu_trid_eigvals(int k, const double *d, const double *e, double *w);
 /* Pattern tables read from the constant-memory pool when they fit there (1,
  * default) or always from global memory (0).  Same arithmetic either way. */
 int evslcu_set_pattern_const(int on);

@@ -117,7 +117,7 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
     if ((k < NR_NTEST || (k - NR_NTEST) % NR_CYCLE != 0) && k != maxit - 1) continue;
     kdim = k + 1;
     const double te = evsl_timer();
-    if ((rc = evsl_trid_eigvals(kdim, dT, eT, EvalT))) goto done;
+    if ((rc = evsl_trid_eigvals_test(kdim, dT, eT, EvalT))) goto done;
     evslstat.t_eig += evsl_timer() - te;
     count = kdim;
     tr1 = 0.0;

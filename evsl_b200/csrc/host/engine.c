@@ -961,7 +961,7 @@ int evslx_engine_step(evslx_engine *E) {
     const int k = s->k;
     int finished = 0, kdim = k + 1;
     if (!((k < ENG_NTEST || (k - ENG_NTEST) % ENG_NCYCLE != 0) && k != r->maxit - 1)) {
-      if ((rc = evsl_trid_eigvals(kdim, s->dT, s->eT, s->EvalT))) return rc;
+      if ((rc = evsl_trid_eigvals_test(kdim, s->dT, s->eT, s->EvalT))) return rc;
       double tr1 = 0.0;
       for (int j = 0; j < kdim; j++)
         if (s->EvalT[j] + EVSL_DBL_EPS_MULT * DBL_EPSILON >= r->pol.bar) tr1 += s->EvalT[j];

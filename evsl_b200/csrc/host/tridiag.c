@@ -139,6 +139,18 @@ int evsl_trid_eigvals(int n, const double *d, const double *e, double *w) {
   return 0;
 }
 
+/* Eigenvalues for the Lanczos convergence tests: on the GPU (multisection,
+ * evslcu_trid_eigvals) from TRID_GPU_MIN rows on, where the host QL's
+ * O(k^2) work per test would dominate small-matrix solves; the host QL below
+ * that.  Both are backward stable; they agree to a few ulps. */
+#define TRID_GPU_MIN 64
+int evsl_trid_eigvals_test(int n, const double *d, const double *e, double *w) {
+  if (n < TRID_GPU_MIN) return evsl_trid_eigvals(n, d, e, w);
+  const int rc = evslcu_trid_eigvals(n, d, e, w);
+  if (rc) return evsl_seterr(EVSLX_ERR_CUDA, "%s", evslcu_errstr());
+  return 0;
+}
+
 /* Eigenvalues (ascending) of the symmetric tridiagonal (d, e) and the first
  * component of each normalised eigenvector (the Lanczos quadrature weights
  * come from their squares): the QL rotations are applied to e_1^T only. */

@@ -424,3 +424,37 @@ def test_filter_kernel_is_chosen_by_timing(gpu_lib):
 def test_laplacian_storage_is_compressed(gpu_lib):
     _lap(gpu_lib, 30, 30, 30)
     assert gpu_lib.matrix_storage() == (4, 2)
+
+
+def test_tridiagonal_eigenvalues_on_gpu(gpu_lib):
+    """The convergence tests' tridiagonal eigenvalues (GPU multisection on
+    Sturm counts) agree with LAPACK's to 1e-13 of the matrix norm, on sizes
+    1..2000, split blocks (exactly repeated eigenvalues), the Wilkinson W21+
+    matrix (pairs closer than 1e-13) and tiny off-diagonals."""
+    import ctypes as C
+
+    f = gpu_lib.lib.evslcu_trid_eigvals
+    f.restype = C.c_int
+    f.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(8)
+    cases = []
+    for k in (1, 2, 3, 64, 65, 500, 2000):
+        cases.append((rng.standard_normal(k), rng.standard_normal(max(k - 1, 0))))
+    d = np.tile([2.0, -1.0, 0.5], 40)
+    e = np.ones(119)
+    e[2::3] = 0.0  # 40 identical 3x3 blocks
+    cases.append((d, e))
+    m = 10
+    cases.append((np.abs(np.arange(-m, m + 1)).astype(float), np.ones(2 * m)))  # W21+
+    cases.append((np.linspace(0, 1, 300), np.full(299, 1e-170)))
+    for d, e in cases:
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        k = len(d)
+        w = np.zeros(k)
+        assert f(k, d.ctypes.data, e.ctypes.data if k > 1 else None, w.ctypes.data) == 0
+        T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+        ref = np.linalg.eigvalsh(T)
+        scale = max(np.abs(ref).max(), 1e-300)
+        assert np.all(np.diff(w) >= 0)
+        assert np.max(np.abs(w - ref)) <= 1e-13 * scale, (k, np.max(np.abs(w - ref)) / scale)
