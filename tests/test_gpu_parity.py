@@ -458,3 +458,36 @@ def test_tridiagonal_eigenvalues_on_gpu(gpu_lib):
         scale = max(np.abs(ref).max(), 1e-300)
         assert np.all(np.diff(w) >= 0)
         assert np.max(np.abs(w - ref)) <= 1e-13 * scale, (k, np.max(np.abs(w - ref)) / scale)
+
+
+def test_long_rows_on_the_dictionary(gpu_lib):
+    """A banded matrix with 261 entries per interior row keeps a row-pattern
+    dictionary (261 row forms, 51,091 table entries) but has rows too long
+    for the per-row descriptors and the unrolled forms (16 entries at most),
+    and a table too large for the constant-memory pool: the looped SELL-32
+    and global-table kernels give the reference's vector bit for bit, and
+    every other variant reports that it is not available."""
+    n, hb = 2000, 130
+    rows = []
+    for r in range(n):
+        cols = list(range(max(0, r - hb), min(n, r + hb + 1)))
+        rows.append((cols, [4.0 * hb if c == r else -1.0 + 0.5 * ((c - r) % 3) for c in cols]))
+    ia, ja, a = _csr_from_rows(rows)
+    lo, hi = 4.0 * hb - 2.0 * hb, 4.0 * hb + 2.0 * hb
+    iv = [lo + 0.4 * (hi - lo), lo + 0.45 * (hi - lo), lo, hi]
+    v = O.seeded_normal(n, 12)
+    y_ref = O.cheb_av(O.find_pol(iv, max_deg=80), ia, ja, a, v)
+    try:
+        for variant in range(7):
+            gpu_lib.set_filter_kernel(variant)
+            gpu_lib.set_csr(ia, ja, a)
+            assert 0 < gpu_lib.row_pattern_count() <= 1024
+            pol = gpu_lib.find_pol(iv, max_deg=80)
+            if variant not in (0, 3):
+                with pytest.raises(Exception, match="not available"):
+                    gpu_lib.chebav(pol, v)
+            else:
+                assert np.array_equal(gpu_lib.chebav(pol, v), y_ref), variant
+            gpu_lib.free_pol(pol)
+    finally:
+        gpu_lib.set_filter_kernel(-1)
