@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--count", type=int, default=COUNT)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve", "lap3d-multifilter",
-                                          "lap3d-reorth"],
+                                          "lap3d-reorth", "lap3d-kpm"],
                    default="lap3d-slice",
                    help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark); "
                         "lap3d-batch: several slices through the request engine; serve: a Poisson request stream")
@@ -77,6 +77,10 @@ def parse():
     p.add_argument("--l2-resident", action="store_true",
                    help="keep the stored matrix persisting in L2 (comparison runs)")
     p.add_argument("--maxit-reorth", type=int, default=600, help="lap3d-reorth: Lanczos steps")
+    p.add_argument("--kpm-probes", type=int, default=30, help="lap3d-kpm: probe vectors")
+    p.add_argument("--kpm-moments", type=int, default=300, help="lap3d-kpm: Chebyshev moments")
+    p.add_argument("--kpm-direct", action="store_true",
+                   help="lap3d-kpm: one dot with the probe per degree instead of the product identities")
     p.add_argument("--filter-mode", choices=["per-degree", "wave"], default="per-degree",
                    help="filter execution: one launch per degree or one pipelined launch")
     p.add_argument("--row-patterns", choices=["on", "off"], default="on",
@@ -647,6 +651,56 @@ def run_reorth(args):
     lib.free_pol(pol)
 
 
+def run_kpm(args):
+    """lap3d-kpm: kpmdos on the 3-D Laplacian 100^3 with the config-2
+    settings (30 Rademacher probes, 300 moments, Jackson damping; `--kpm-probes`,
+    `--kpm-moments`), device time of the block recurrence (CUDA events around
+    the KPM kernels).  Algorithmic bytes per block step: the CSR matrix
+    (12 B per nonzero + 4 B per row) and 8 bytes per probe entry of each
+    vector the step touches (read v_k, v_k-1; write v_k+1: 3 vectors with the
+    product identities, 4 with a dot against the probe per degree); the
+    identities need ceil(M/2) steps for M moments, the direct form M."""
+    import ctypes as C
+
+    import evsl_b200
+    from evsl_b200 import workloads as W
+
+    lib = evsl_b200.Library()
+    lib.lib.evslx_last_kpm_seconds.restype = C.c_double
+    lib.lib.evslcu_set_kpm_doubling(0 if args.kpm_direct else 1)
+    ia, ja, a = W.laplacian_csr(NX, NY, NZ)
+    lib.set_csr(ia, ja, a)
+    n, nnz = NX * NY * NZ, int(ia[-1])
+    B, M = args.kpm_probes, args.kpm_moments
+    iv = [0.6, 1.2, LMIN, LMAX]
+    for _ in range(args.warmup):
+        lib.kpmdos(M, 1, B, iv)
+    sampler = ClockSampler(rank_info()[2])
+    sampler.start()
+    secs = []
+    for _ in range(args.steps):
+        lib.kpmdos(M, 1, B, iv)
+        secs.append(lib.lib.evslx_last_kpm_seconds())
+    clocks = sampler.stop()
+    t = statistics.median(secs)
+    steps = M if args.kpm_direct else (M + 1) // 2
+    nvec_bytes = (4 if args.kpm_direct else 3) * 8.0 * n * B
+    abytes = steps * (12.0 * nnz + 4.0 * (n + 1) + nvec_bytes)
+    peak, kind = measured_peak_hbm()
+    gbs = abytes / t / 1e9
+    print(json.dumps({
+        "metric": "KPM moments/s", "value": M / t, "unit": "moments/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (3-D Laplacian, device Rademacher probes)",
+        "config": {"workload": "lap3d-kpm: kpmdos, %d probes, %d moments, 3-D Laplacian 100^3" % (B, M),
+                   "method": "direct dots" if args.kpm_direct else "product identities",
+                   "block_steps": steps, "us_per_block_step": 1e6 * t / steps},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "peak_kind": kind, "unit": "GB/s",
+                     "frac": gbs / peak, "algorithmic_bytes": abytes},
+        "clocks": clocks}))
+    lib.lib.evslcu_set_kpm_doubling(1)
+
+
 def _slice_plan(ev, start, nslices, count):
     """Consecutive gap-midpoint intervals of `count` eigenvalues from `start`."""
     from evsl_b200 import workloads as W
@@ -906,6 +960,8 @@ def main():
         run_multifilter(args)
     elif args.workload == "lap3d-reorth":
         run_reorth(args)
+    elif args.workload == "lap3d-kpm":
+        run_kpm(args)
     else:
         run_ours(args)
 

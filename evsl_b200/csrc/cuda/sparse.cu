@@ -583,20 +583,131 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
   for (int g = 0; g < G; ++g) sh[warp][lane + 32 * g] = dsum[g];
   __syncthreads();
+  // block partials stored probe-major (part[p * gridDim.x + block]) so that
+  // the last block's reduction reads them coalesced
   for (int p = threadIdx.x; p < B; p += blockDim.x) {
     double s = 0.0;
     for (int w = 0; w < kThreads / 32; ++w) s += sh[w][p];
-    part[(long long)blockIdx.x * B + p] = s;
+    part[(long long)p * gridDim.x + blockIdx.x] = s;
   }
   if (last_block(ctr)) {
-    for (int p = threadIdx.x; p < B; p += blockDim.x) {
+    // one warp per probe: lanes sum strided blocks, then a shuffle tree;
+    // the order depends only on the grid (a function of n), not on B
+    for (int p = warp; p < B; p += kThreads / 32) {
       double s = 0.0;
-      for (int b2 = 0; b2 < (int)gridDim.x; ++b2) s += __ldcg(part + (long long)b2 * B + p);
-      dots_row[p] = s;
+      for (int b2 = lane; b2 < (int)gridDim.x; b2 += 32) s += __ldcg(part + (long long)p * gridDim.x + b2);
+      s = warp_sum(s);
+      if (lane == 0) dots_row[p] = s;
     }
     __syncthreads();
     if (threadIdx.x == 0) *ctr = 0u;
   }
+}
+
+// KPM degree step that yields two moments per matrix product (Chebyshev
+// product identities T_2k = 2 T_k^2 - T_0 and T_2k+1 = 2 T_k+1 T_k - T_1):
+// per probe, <w_k+1, w_k+1> and <w_k+1, w_k> (and <w_0, w_0> at the first
+// step).  No pass over the probes per degree, and ceil(M/2) products give M
+// moments.  One launch handles probes p0 .. p0+nb-1 (nb <= 32, lane = probe)
+// of the interleaved [n][B] block; rows as in k_kpm (warps over groups of
+// kKpmRows rows, grid a function of n only).  Block sums go to
+// part[(s * B + p0 + lane) * gridDim.x + block] and k_kpm_reduce adds them
+// up, so the summation order does not depend on B or on the slicing.
+template <bool FIRST>
+__global__ void __launch_bounds__(kThreads)
+    k_kpm_dbl(CsrView A, int B, int p0, int nb, const double *__restrict__ vk, const double *vkm1, double *out,
+              double scal, double nctr, double *part) {
+  constexpr int NS = FIRST ? 3 : 2;
+  __shared__ double sh[NS][kThreads / 32][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps_total = gridDim.x * (kThreads / 32);
+  const bool on = lane < nb;
+  const int p = p0 + lane;
+  double sum[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) sum[s] = 0.0;
+  for (int r0 = (blockIdx.x * (kThreads / 32) + warp) * kKpmRows; r0 < A.n; r0 += nwarps_total * kKpmRows) {
+    int b[kKpmRows], len[kKpmRows], maxlen = 0;
+#pragma unroll
+    for (int i = 0; i < kKpmRows; ++i) {
+      const int r = r0 + i;
+      b[i] = (r < A.n) ? A.ia[r] : 0;
+      len[i] = (r < A.n) ? A.ia[r + 1] - b[i] : 0;
+      maxlen = max(maxlen, len[i]);
+    }
+    double acc[kKpmRows];
+#pragma unroll
+    for (int i = 0; i < kKpmRows; ++i) acc[i] = 0.0;
+    if (maxlen <= 8) {
+      // the 4 rows' entries in one warp load (lane = row * 8 + entry), then
+      // broadcast by shuffles: a row's gathers are in flight together
+      static_assert(kKpmRows * 8 == 32, "one entry per lane");
+      const int li = lane >> 3, lj = lane & 7;
+      double ae = 0.0;
+      int ce = 0;
+      if (lj < len[li]) {
+        ae = __ldg(A.a + b[li] + lj);
+        ce = __ldg(A.ja + b[li] + lj);
+      }
+#pragma unroll
+      for (int i = 0; i < kKpmRows; ++i) {
+        double av[8], xv[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          av[j] = __shfl_sync(0xffffffffu, ae, i * 8 + j);
+          const int cj = __shfl_sync(0xffffffffu, ce, i * 8 + j);
+          xv[j] = (on && j < len[i]) ? __ldg(vk + (long long)cj * B + p) : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (j < len[i]) acc[i] = __dadd_rn(acc[i], __dmul_rn(av[j], xv[j]));
+      }
+    } else {
+      for (int j = 0; j < maxlen; ++j) {
+#pragma unroll
+        for (int i = 0; i < kKpmRows; ++i) {
+          if (j < len[i]) {
+            const double aj = __ldg(A.a + b[i] + j);
+            const long long cj = (long long)__ldg(A.ja + b[i] + j) * B;
+            if (on) acc[i] = __dadd_rn(acc[i], __dmul_rn(aj, __ldg(vk + cj + p)));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kKpmRows; ++i) {
+      const int r = r0 + i;
+      if (r >= A.n || !on) continue;
+      const long long idx = (long long)r * B + p;
+      const double x = vk[idx];
+      double w = __dmul_rn(scal, __dadd_rn(acc[i], __dmul_rn(nctr, x)));
+      if (!FIRST) w = __dadd_rn(w, -vkm1[idx]);
+      out[idx] = w;
+      sum[0] += w * w;
+      sum[1] += w * x;
+      if (FIRST) sum[NS - 1] += x * x;
+    }
+  }
+#pragma unroll
+  for (int s = 0; s < NS; ++s) sh[s][warp][lane] = sum[s];
+  __syncthreads();
+  for (int q = threadIdx.x; q < NS * 32; q += blockDim.x) {
+    const int s = q / 32, l = q % 32;
+    if (l >= nb) continue;
+    double t = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) t += sh[s][w][l];
+    part[((long long)s * B + p0 + l) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// raw[q] = sum over the nb block partials of sum q (block q; fixed order).
+__global__ void __launch_bounds__(kThreads) k_kpm_reduce(int nb, const double *__restrict__ part, double *raw) {
+  __shared__ double sh[kThreads / 32];
+  const double *pq = part + (long long)blockIdx.x * nb;
+  double t = 0.0;
+  for (int i = threadIdx.x; i < nb; i += kThreads) t += pq[i];
+  t = block_sum(t, sh);
+  if (threadIdx.x == 0) raw[blockIdx.x] = t;
 }
 
 // Column sums of squares of a column-major n x B block: part[blk*B + p].
@@ -1117,10 +1228,91 @@ int evslcu_cheb_update(int n, int k, double t, double s, double cc, double *vkp1
   return 0;
 }
 
+static int g_kpm_doubling = 1;
+
+int evslcu_set_kpm_doubling(int on) {
+  g_kpm_doubling = on ? 1 : 0;
+  return 0;
+}
+
+// KPM dots through the product identities: K = ceil(Mdeg/2) block steps,
+// raw sums a_k = <w_k+1, w_k+1>, b_k = <w_k+1, w_k>, c = <w_0, w_0>; then
+// mu_2k+1 = 2 b_k - mu_1 (mu_1 = b_0) and mu_2k+2 = 2 a_k - c, per probe.
+static int kpm_dots_doubling(const evslcu_op *op, int n, int Mdeg, int nvec, const double *probes, double ctr,
+                             double wid, double *dots) {
+  const int B = nvec;
+  const int K = (Mdeg + 1) / 2;
+  const size_t blk = (size_t)n * B;
+  const int grid = kpm_grid(n);  // a function of n only: the summation order does not depend on B
+  double *buf = (double *)evslcu_malloc(sizeof(double) * blk * 3);
+  double *raw = (double *)evslcu_malloc(sizeof(double) * (size_t)K * 3 * B);
+  double *nrm = (double *)evslcu_malloc(sizeof(double) * B);
+  double *part = (double *)evslcu_malloc(sizeof(double) * (size_t)std::max(3 * grid * B, 512 * B));
+  std::vector<double> hraw((size_t)K * 3 * B);
+  int rc = 0;
+  if (!buf || !raw || !nrm || !part) rc = EVSLCU_ERR_NOMEM;
+  double *V0 = buf, *W0 = buf + blk, *W1 = buf + 2 * blk;
+  if (!rc) {
+    dim3 g(std::min(grid_for(n), 512), B);
+    k_colsq_partial<<<g, kThreads, 0, stream()>>>(n, B, probes, part, counters() + CTR_COL, nrm);
+    count_launch();
+    rc = check_launch("k_colsq_partial");
+  }
+  if (!rc) {
+    k_interleave_scaled<<<grid_for(blk), kThreads, 0, stream()>>>(n, B, probes, nrm, V0);
+    count_launch();
+    rc = check_launch("k_interleave_scaled");
+  }
+  const CsrView A = csr_view(op->A);
+  const double nctr = -ctr;
+  double *W[2] = {W0, W1};
+  for (int k = 0; !rc && k < K; ++k) {
+    const double scal = (k == 0 ? 1.0 : 2.0) / wid;
+    const double *vk = (k == 0) ? V0 : W[(k - 1) % 2];
+    const double *vkm1 = (k == 0) ? nullptr : ((k == 1) ? V0 : W[k % 2]);
+    double *o = W[k % 2];
+    double *rr = raw + (size_t)k * 3 * B;
+    for (int p0 = 0; !rc && p0 < B; p0 += 32) {
+      const int nb = std::min(32, B - p0);
+      if (k == 0)
+        k_kpm_dbl<true><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+      else
+        k_kpm_dbl<false><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+      count_launch();
+      rc = check_launch("k_kpm_dbl");
+    }
+    if (!rc) {
+      k_kpm_reduce<<<(k == 0 ? 3 : 2) * B, kThreads, 0, stream()>>>(grid, part, rr);
+      count_launch();
+      rc = check_launch("k_kpm_reduce");
+    }
+  }
+  if (!rc) rc = evslcu_d2h(hraw.data(), raw, sizeof(double) * hraw.size());
+  if (!rc) {
+    // dots[(j-1)*B + p] = mu_j, j = 1..Mdeg
+    for (int p = 0; p < B; ++p) {
+      const double cc0 = hraw[2 * (size_t)B + p];  // <w_0, w_0>
+      const double mu1 = hraw[(size_t)B + p];      // <w_1, w_0>
+      for (int k = 0; k < K; ++k) {
+        const double a = hraw[(size_t)k * 3 * B + p], b = hraw[(size_t)k * 3 * B + B + p];
+        const int j1 = 2 * k + 1, j2 = 2 * k + 2;
+        dots[(size_t)(j1 - 1) * B + p] = (k == 0) ? mu1 : 2.0 * b - mu1;
+        if (j2 <= Mdeg) dots[(size_t)(j2 - 1) * B + p] = 2.0 * a - cc0;
+      }
+    }
+  }
+  evslcu_free(buf);
+  evslcu_free(raw);
+  evslcu_free(nrm);
+  evslcu_free(part);
+  return rc;
+}
+
 int evslcu_kpm_dots(const evslcu_op *op, int n, int Mdeg, int nvec, const double *probes, double ctr, double wid,
                     double *dots) {
   if (!op || !op->A) return fail(EVSLCU_ERR_STATE, "KPM needs a registered CSR matrix");
   if (nvec < 1 || nvec > 128 || Mdeg < 1 || n < 1) return fail(EVSLCU_ERR_ARG, "kpm: bad sizes");
+  if (g_kpm_doubling) return kpm_dots_doubling(op, n, Mdeg, nvec, probes, ctr, wid, dots);
   const int B = nvec;
   const size_t blk = (size_t)n * B;
   double *buf = (double *)evslcu_malloc(sizeof(double) * blk * 3);

@@ -250,6 +250,10 @@ int evslcu_mat_uses_patterns(const evslcu_mat *A);
  * rows of at most 8 or 16 stored entries (1, default) or the loop form (0).
  * Same arithmetic either way. */
 int evslcu_set_row_unroll(int on);
+/* KPM dots (evslcu_kpm_dots) through the Chebyshev product identities, two
+ * moments per block matrix product (1, default), or one dot with the probe
+ * per degree as the reference (0).  The moments agree to rounding. */
+int evslcu_set_kpm_doubling(int on);
 /* All k eigenvalues (ascending) of the symmetric tridiagonal matrix with
  * diagonal d[0..k) and off-diagonal e[0..k-1), all host arrays, computed on
  * the GPU by multisection on Sturm counts (one warp per eigenvalue);

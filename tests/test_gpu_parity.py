@@ -491,3 +491,25 @@ def test_long_rows_on_the_dictionary(gpu_lib):
             gpu_lib.free_pol(pol)
     finally:
         gpu_lib.set_filter_kernel(-1)
+
+
+@pytest.mark.parametrize("dims, M", [((30, 30, 30), 300), ((100, 100, 1), 500), ((17, 13, 11), 7)])
+def test_kpm_product_identities_match_direct_dots(gpu_lib, dims, M):
+    """KPM moments from the Chebyshev product identities (two moments per
+    block product) agree with the direct per-degree dots with the probes
+    within the moment bar (1e-12 of ||mu||_inf), odd and even counts."""
+    ia, ja, a = _lap(gpu_lib, *dims)
+    n = len(ia) - 1
+    hi = 12.0 if dims[2] > 1 else 8.0
+    probes = O.seeded_normal(n * 30, 77).reshape(30, n)
+    try:
+        out = {}
+        for dbl in (1, 0):
+            gpu_lib.lib.evslcu_set_kpm_doubling(dbl)
+            out[dbl] = gpu_lib.kpmdos_probes(M, 1, probes, [0.6, 1.2, 0.0, hi])
+        mu1, ec1 = out[1]
+        mu0, ec0 = out[0]
+        assert np.max(np.abs(mu1 - mu0)) <= 1e-12 * np.max(np.abs(mu0))
+        assert abs(ec1 - ec0) <= 1e-10 * max(abs(ec0), 1.0)
+    finally:
+        gpu_lib.lib.evslcu_set_kpm_doubling(1)
