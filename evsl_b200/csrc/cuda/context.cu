@@ -149,6 +149,8 @@ int evslcu_finish(void) {
     g_l2_owner = nullptr;
     cudaGetLastError();
   }
+  evslcu_kpm_release();
+  evslcu_trid_release();
   cudaFree(g_ctx.partials);
   cudaFree(g_ctx.counters);
   cudaFree(g_ctx.scalars);

@@ -614,7 +614,7 @@ __global__ void __launch_bounds__(kThreads)
 // part[(s * B + p0 + lane) * gridDim.x + block] and k_kpm_reduce adds them
 // up, so the summation order does not depend on B or on the slicing.
 template <bool FIRST>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     k_kpm_dbl(CsrView A, int B, int p0, int nb, const double *__restrict__ vk, const double *vkm1, double *out,
               double scal, double nctr, double *part) {
   constexpr int NS = FIRST ? 3 : 2;
@@ -1229,6 +1229,14 @@ int evslcu_cheb_update(int n, int k, double t, double s, double cc, double *vkp1
 }
 
 static int g_kpm_doubling = 1;
+static double *g_kpm_ws = nullptr;  // cached KPM workspace (product-identity path)
+static size_t g_kpm_ws_cap = 0;
+
+void evslcu_kpm_release(void) {
+  evslcu_free(g_kpm_ws);
+  g_kpm_ws = nullptr;
+  g_kpm_ws_cap = 0;
+}
 
 int evslcu_set_kpm_doubling(int on) {
   g_kpm_doubling = on ? 1 : 0;
@@ -1244,13 +1252,23 @@ static int kpm_dots_doubling(const evslcu_op *op, int n, int Mdeg, int nvec, con
   const int K = (Mdeg + 1) / 2;
   const size_t blk = (size_t)n * B;
   const int grid = kpm_grid(n);  // a function of n only: the summation order does not depend on B
-  double *buf = (double *)evslcu_malloc(sizeof(double) * blk * 3);
-  double *raw = (double *)evslcu_malloc(sizeof(double) * (size_t)K * 3 * B);
-  double *nrm = (double *)evslcu_malloc(sizeof(double) * B);
-  double *part = (double *)evslcu_malloc(sizeof(double) * (size_t)std::max(3 * grid * B, 512 * B));
+  // one cached workspace (grows, never shrinks): repeated DOS estimates do
+  // not allocate, and no free synchronises the device between them
+  const size_t n_buf = blk * 3, n_raw = (size_t)K * 3 * B, n_nrm = (size_t)B,
+               n_part = (size_t)std::max(3 * grid * B, 512 * B);
+  const size_t need = n_buf + n_raw + n_nrm + n_part + 4 * 32;
+  if (need > g_kpm_ws_cap) {
+    evslcu_free(g_kpm_ws);
+    g_kpm_ws = (double *)evslcu_malloc(sizeof(double) * need);
+    g_kpm_ws_cap = g_kpm_ws ? need : 0;
+  }
+  double *buf = g_kpm_ws;
+  double *raw = buf ? buf + (n_buf + 31) / 32 * 32 : nullptr;
+  double *nrm = raw ? raw + (n_raw + 31) / 32 * 32 : nullptr;
+  double *part = nrm ? nrm + (n_nrm + 31) / 32 * 32 : nullptr;
   std::vector<double> hraw((size_t)K * 3 * B);
   int rc = 0;
-  if (!buf || !raw || !nrm || !part) rc = EVSLCU_ERR_NOMEM;
+  if (!buf) rc = fail(EVSLCU_ERR_NOMEM, "kpm: out of device memory");
   double *V0 = buf, *W0 = buf + blk, *W1 = buf + 2 * blk;
   if (!rc) {
     dim3 g(std::min(grid_for(n), 512), B);
@@ -1301,10 +1319,6 @@ static int kpm_dots_doubling(const evslcu_op *op, int n, int Mdeg, int nvec, con
       }
     }
   }
-  evslcu_free(buf);
-  evslcu_free(raw);
-  evslcu_free(nrm);
-  evslcu_free(part);
   return rc;
 }
 

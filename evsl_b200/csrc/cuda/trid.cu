@@ -80,6 +80,12 @@ using namespace evslcu;
 
 extern "C" {
 
+void evslcu_trid_release(void) {
+  evslcu_free(g_trid_buf);
+  g_trid_buf = nullptr;
+  g_trid_cap = 0;
+}
+
 int evslcu_trid_eigvals(int k, const double *d, const double *e, double *w) {
   if (k <= 0) return 0;
   if (!d || !w || (k > 1 && !e)) return fail(EVSLCU_ERR_ARG, "evslcu_trid_eigvals: bad arguments");

@@ -254,6 +254,9 @@ int evslcu_set_row_unroll(int on);
  * moments per block matrix product (1, default), or one dot with the probe
  * per degree as the reference (0).  The moments agree to rounding. */
 int evslcu_set_kpm_doubling(int on);
+/* Free the cached KPM and tridiagonal workspaces (evslcu_finish calls them). */
+void evslcu_kpm_release(void);
+void evslcu_trid_release(void);
 /* All k eigenvalues (ascending) of the symmetric tridiagonal matrix with
  * diagonal d[0..k) and off-diagonal e[0..k-1), all host arrays, computed on
  * the GPU by multisection on Sturm counts (one warp per eigenvalue);
