@@ -608,95 +608,139 @@ __global__ void __launch_bounds__(kThreads)
 // product identities T_2k = 2 T_k^2 - T_0 and T_2k+1 = 2 T_k+1 T_k - T_1):
 // per probe, <w_k+1, w_k+1> and <w_k+1, w_k> (and <w_0, w_0> at the first
 // step).  No pass over the probes per degree, and ceil(M/2) products give M
-// moments.  One launch handles probes p0 .. p0+nb-1 (nb <= 32, lane = probe)
-// of the interleaved [n][B] block; rows as in k_kpm (warps over groups of
-// kKpmRows rows, grid a function of n only).  Block sums go to
-// part[(s * B + p0 + lane) * gridDim.x + block] and k_kpm_reduce adds them
-// up, so the summation order does not depend on B or on the slicing.
-template <bool FIRST>
+// moments.
+//
+// One launch handles probes p0 .. p0+nb-1 (nb <= 32) of the interleaved
+// [n][B] block.  Each half-warp owns 4 consecutive rows per iteration (a warp
+// 8), each lane 2 probes of them; a half-warp loads its rows' entries once
+// (2 per lane, rows of at most 8 entries) and passes them round by shuffles,
+// so a row's gathers for both probes are in flight together.  VEC: the two
+// probes are read as one 16-byte access (B and p0 even).  Block sums go to
+// part[(s * B + p) * gridDim.x + block] and k_kpm_reduce adds them up.  The
+// rows a lane visits, and the order of every sum, depend on n and the grid
+// only -- not on B, nb or VEC -- so probe shards reproduce the full block.
+constexpr int kKpmHalfRows = 4;  // rows per half-warp and iteration
+
+template <bool FIRST, bool VEC>
 __global__ void __launch_bounds__(kThreads, 4)
     k_kpm_dbl(CsrView A, int B, int p0, int nb, const double *__restrict__ vk, const double *vkm1, double *out,
               double scal, double nctr, double *part) {
   constexpr int NS = FIRST ? 3 : 2;
-  __shared__ double sh[NS][kThreads / 32][32];
+  __shared__ double sh[NS][kThreads / 32][2][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nwarps_total = gridDim.x * (kThreads / 32);
-  const bool on = lane < nb;
-  const int p = p0 + lane;
-  double sum[NS];
+  const int h = lane >> 4, hl = lane & 15;
+  const int q = 2 * hl;  // first of this lane's two probes, relative to p0
+  const bool onA = q < nb, onB = q + 1 < nb;
+  const int pa = p0 + q;
+  const int rows_per_iter = gridDim.x * (kThreads / 32) * 2 * kKpmHalfRows;
+  double sum[NS][2];
 #pragma unroll
-  for (int s = 0; s < NS; ++s) sum[s] = 0.0;
-  for (int r0 = (blockIdx.x * (kThreads / 32) + warp) * kKpmRows; r0 < A.n; r0 += nwarps_total * kKpmRows) {
-    int b[kKpmRows], len[kKpmRows], maxlen = 0;
+  for (int s = 0; s < NS; ++s) sum[s][0] = sum[s][1] = 0.0;
+  for (int base = (blockIdx.x * (kThreads / 32) + warp) * 2 * kKpmHalfRows; base < A.n; base += rows_per_iter) {
+    const int r0 = base + h * kKpmHalfRows;  // this half-warp's first row
+    int b[kKpmHalfRows], len[kKpmHalfRows], mymax = 0;
 #pragma unroll
-    for (int i = 0; i < kKpmRows; ++i) {
+    for (int i = 0; i < kKpmHalfRows; ++i) {
       const int r = r0 + i;
       b[i] = (r < A.n) ? A.ia[r] : 0;
       len[i] = (r < A.n) ? A.ia[r + 1] - b[i] : 0;
-      maxlen = max(maxlen, len[i]);
+      mymax = max(mymax, len[i]);
     }
-    double acc[kKpmRows];
+    const int maxlen = __reduce_max_sync(0xffffffffu, mymax);
+    double acc[kKpmHalfRows][2];
 #pragma unroll
-    for (int i = 0; i < kKpmRows; ++i) acc[i] = 0.0;
+    for (int i = 0; i < kKpmHalfRows; ++i) acc[i][0] = acc[i][1] = 0.0;
     if (maxlen <= 8) {
-      // the 4 rows' entries in one warp load (lane = row * 8 + entry), then
-      // broadcast by shuffles: a row's gathers are in flight together
-      static_assert(kKpmRows * 8 == 32, "one entry per lane");
-      const int li = lane >> 3, lj = lane & 7;
-      double ae = 0.0;
-      int ce = 0;
-      if (lj < len[li]) {
-        ae = __ldg(A.a + b[li] + lj);
-        ce = __ldg(A.ja + b[li] + lj);
+      // entries e = i * 8 + j of the half-warp's 4 rows: e < 16 in slot 0 of
+      // half-lane e, e >= 16 in slot 1 of half-lane e - 16
+      double ae[2];
+      int ce[2];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int e = hl + 16 * t, i = e >> 3, j = e & 7;
+        const int lr = (i == 0) ? len[0] : (i == 1) ? len[1] : (i == 2) ? len[2] : len[3];
+        const int br = (i == 0) ? b[0] : (i == 1) ? b[1] : (i == 2) ? b[2] : b[3];
+        ae[t] = 0.0;
+        ce[t] = 0;
+        if (j < lr) {
+          ae[t] = __ldg(A.a + br + j);
+          ce[t] = __ldg(A.ja + br + j);
+        }
       }
 #pragma unroll
-      for (int i = 0; i < kKpmRows; ++i) {
-        double av[8], xv[8];
+      for (int i = 0; i < kKpmHalfRows; ++i) {
+        double xa[8], xb[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-          av[j] = __shfl_sync(0xffffffffu, ae, i * 8 + j);
-          const int cj = __shfl_sync(0xffffffffu, ce, i * 8 + j);
-          xv[j] = (on && j < len[i]) ? __ldg(vk + (long long)cj * B + p) : 0.0;
+          const int e = i * 8 + j;
+          const int cj = __shfl_sync(0xffffffffu, ce[e >> 4], e & 15, 16);
+          xa[j] = 0.0;
+          xb[j] = 0.0;
+          if (j < len[i]) {
+            const double *src = vk + (long long)cj * B + pa;
+            if (VEC && onB) {
+              const double2 v2 = __ldg(reinterpret_cast<const double2 *>(src));
+              xa[j] = v2.x;
+              xb[j] = v2.y;
+            } else {
+              if (onA) xa[j] = __ldg(src);
+              if (onB) xb[j] = __ldg(src + 1);
+            }
+          }
         }
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (j < len[i]) acc[i] = __dadd_rn(acc[i], __dmul_rn(av[j], xv[j]));
+        for (int j = 0; j < 8; ++j) {
+          const int e = i * 8 + j;
+          const double av = __shfl_sync(0xffffffffu, ae[e >> 4], e & 15, 16);
+          if (j < len[i]) {
+            acc[i][0] = __dadd_rn(acc[i][0], __dmul_rn(av, xa[j]));
+            acc[i][1] = __dadd_rn(acc[i][1], __dmul_rn(av, xb[j]));
+          }
+        }
       }
     } else {
       for (int j = 0; j < maxlen; ++j) {
 #pragma unroll
-        for (int i = 0; i < kKpmRows; ++i) {
+        for (int i = 0; i < kKpmHalfRows; ++i) {
           if (j < len[i]) {
             const double aj = __ldg(A.a + b[i] + j);
-            const long long cj = (long long)__ldg(A.ja + b[i] + j) * B;
-            if (on) acc[i] = __dadd_rn(acc[i], __dmul_rn(aj, __ldg(vk + cj + p)));
+            const double *src = vk + (long long)__ldg(A.ja + b[i] + j) * B + pa;
+            if (onA) acc[i][0] = __dadd_rn(acc[i][0], __dmul_rn(aj, __ldg(src)));
+            if (onB) acc[i][1] = __dadd_rn(acc[i][1], __dmul_rn(aj, __ldg(src + 1)));
           }
         }
       }
     }
 #pragma unroll
-    for (int i = 0; i < kKpmRows; ++i) {
+    for (int i = 0; i < kKpmHalfRows; ++i) {
       const int r = r0 + i;
-      if (r >= A.n || !on) continue;
-      const long long idx = (long long)r * B + p;
-      const double x = vk[idx];
-      double w = __dmul_rn(scal, __dadd_rn(acc[i], __dmul_rn(nctr, x)));
-      if (!FIRST) w = __dadd_rn(w, -vkm1[idx]);
-      out[idx] = w;
-      sum[0] += w * w;
-      sum[1] += w * x;
-      if (FIRST) sum[NS - 1] += x * x;
+      if (r >= A.n) continue;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        if (!(c == 0 ? onA : onB)) continue;
+        const long long idx = (long long)r * B + pa + c;
+        const double x = vk[idx];
+        double w = __dmul_rn(scal, __dadd_rn(acc[i][c], __dmul_rn(nctr, x)));
+        if (!FIRST) w = __dadd_rn(w, -vkm1[idx]);
+        out[idx] = w;
+        sum[0][c] += w * w;
+        sum[1][c] += w * x;
+        if (FIRST) sum[NS - 1][c] += x * x;
+      }
     }
   }
 #pragma unroll
-  for (int s = 0; s < NS; ++s) sh[s][warp][lane] = sum[s];
+  for (int s = 0; s < NS; ++s) {
+    sh[s][warp][h][q] = sum[s][0];
+    sh[s][warp][h][q + 1] = sum[s][1];
+  }
   __syncthreads();
-  for (int q = threadIdx.x; q < NS * 32; q += blockDim.x) {
-    const int s = q / 32, l = q % 32;
+  for (int t = threadIdx.x; t < NS * 32; t += blockDim.x) {
+    const int s = t / 32, l = t % 32;
     if (l >= nb) continue;
-    double t = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) t += sh[s][w][l];
-    part[((long long)s * B + p0 + l) * gridDim.x + blockIdx.x] = t;
+    double v = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) v += sh[s][w][0][l] + sh[s][w][1][l];
+    part[((long long)s * B + p0 + l) * gridDim.x + blockIdx.x] = v;
   }
 }
 
@@ -1292,10 +1336,15 @@ static int kpm_dots_doubling(const evslcu_op *op, int n, int Mdeg, int nvec, con
     double *rr = raw + (size_t)k * 3 * B;
     for (int p0 = 0; !rc && p0 < B; p0 += 32) {
       const int nb = std::min(32, B - p0);
-      if (k == 0)
-        k_kpm_dbl<true><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+      const bool vec = (B % 2 == 0);  // two probes per 16-byte access
+      if (k == 0 && vec)
+        k_kpm_dbl<true, true><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+      else if (k == 0)
+        k_kpm_dbl<true, false><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+      else if (vec)
+        k_kpm_dbl<false, true><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
       else
-        k_kpm_dbl<false><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+        k_kpm_dbl<false, false><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
       count_launch();
       rc = check_launch("k_kpm_dbl");
     }
