@@ -1199,3 +1199,33 @@ def kpm_raw_dots(Mdeg, probes, intv, ia, ja, a):
             vkm1, vk = vk, vkp1
             out[k, m] = float(np.dot(vk, v))
     return out
+
+
+def kpm_raw_dots_identities(Mdeg, probes, intv, ia, ja, a):
+    """The same raw KPM products through the Chebyshev product identities
+    (T_2k = 2 T_k^2 - T_0, T_2k+1 = 2 T_k+1 T_k - T_1): with w_j = T_j(A~) v,
+    mu_2k+2 = 2 <w_k+1, w_k+1> - <w_0, w_0> and mu_2k+1 = 2 <w_k+1, w_k> - mu_1
+    (mu_1 = <w_1, w_0>), from ceil(Mdeg/2) products -- the restatement of the
+    library's two-moments-per-step KPM, checked against kpm_raw_dots."""
+    lmin, lmax = intv[2], intv[3]
+    ctr = (lmax + lmin) / 2.0
+    wid = (lmax - lmin) / 2.0
+    probes = np.atleast_2d(probes)
+    K = (Mdeg + 1) // 2
+    out = np.zeros((Mdeg, probes.shape[0]))
+    for m, p in enumerate(probes):
+        v = p * (1.0 / np.linalg.norm(p))
+        c0 = float(np.dot(v, v))
+        wk, wkm1 = v.copy(), np.zeros_like(v)
+        mu1 = 0.0
+        for k in range(K):
+            scal = (1.0 if k == 0 else 2.0) / wid
+            w = scal * (csr_matvec(ia, ja, a, wk) + (-ctr) * wk) - wkm1
+            a_k, b_k = float(np.dot(w, w)), float(np.dot(w, wk))
+            if k == 0:
+                mu1 = b_k
+            out[2 * k, m] = mu1 if k == 0 else 2.0 * b_k - mu1
+            if 2 * k + 1 < Mdeg:
+                out[2 * k + 1, m] = 2.0 * a_k - c0
+            wkm1, wk = wk, w
+    return out

@@ -150,3 +150,16 @@ def test_reference_library_matches_restatement():
     y = R.chebav(pol, x)
     assert np.array_equal(y, O.cheb_av(O.find_pol(iv), ia, ja, a, x))
     R.free_pol(pol)
+
+
+@pytest.mark.parametrize("dims, M", [((12, 10, 9), 60), ((40, 40, 1), 31)])
+def test_kpm_product_identities_restatement(dims, M):
+    """The product-identity form of the KPM moments (two per matrix product)
+    equals the direct per-degree dots to rounding, odd and even counts."""
+    ia, ja, a = O.lap_csr(*dims)
+    n = len(ia) - 1
+    probes = O.seeded_normal(n * 4, 5).reshape(4, n)
+    iv = [0.6, 1.2, 0.0, 12.0 if dims[2] > 1 else 8.0]
+    d0 = O.kpm_raw_dots(M, probes, iv, ia, ja, a)
+    d1 = O.kpm_raw_dots_identities(M, probes, iv, ia, ja, a)
+    assert np.max(np.abs(d1 - d0)) <= 1e-12 * np.max(np.abs(d0))
