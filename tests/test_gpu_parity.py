@@ -493,15 +493,18 @@ def test_long_rows_on_the_dictionary(gpu_lib):
         gpu_lib.set_filter_kernel(-1)
 
 
-@pytest.mark.parametrize("dims, M", [((30, 30, 30), 300), ((100, 100, 1), 500), ((17, 13, 11), 7)])
-def test_kpm_product_identities_match_direct_dots(gpu_lib, dims, M):
+@pytest.mark.parametrize("dims, M, nvec", [((30, 30, 30), 300, 30), ((100, 100, 1), 500, 30), ((17, 13, 11), 7, 30),
+                                           ((20, 20, 20), 60, 64), ((20, 20, 20), 61, 45)])
+def test_kpm_product_identities_match_direct_dots(gpu_lib, dims, M, nvec):
     """KPM moments from the Chebyshev product identities (two moments per
     block product) agree with the direct per-degree dots with the probes
-    within the moment bar (1e-12 of ||mu||_inf), odd and even counts."""
+    within the moment bar (1e-12 of ||mu||_inf): odd and even moment counts,
+    and more than 32 probes (several 32-probe launches per step, with paired
+    16-byte loads for an even count and single loads for an odd one)."""
     ia, ja, a = _lap(gpu_lib, *dims)
     n = len(ia) - 1
     hi = 12.0 if dims[2] > 1 else 8.0
-    probes = O.seeded_normal(n * 30, 77).reshape(30, n)
+    probes = O.seeded_normal(n * nvec, 77).reshape(nvec, n)
     try:
         out = {}
         for dbl in (1, 0):
