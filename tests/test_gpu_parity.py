@@ -516,3 +516,42 @@ def test_kpm_product_identities_match_direct_dots(gpu_lib, dims, M, nvec):
         assert abs(ec1 - ec0) <= 1e-10 * max(abs(ec0), 1.0)
     finally:
         gpu_lib.lib.evslcu_set_kpm_doubling(1)
+
+
+def _lap9_csr(nx, ny):
+    """2-D 9-point stencil (8 on the diagonal, -1 to the 8 neighbours)."""
+    rows = []
+    for j in range(ny):
+        for i in range(nx):
+            cols, vals = [], []
+            for dj in (-1, 0, 1):
+                for di in (-1, 0, 1):
+                    ii, jj = i + di, j + dj
+                    if 0 <= ii < nx and 0 <= jj < ny:
+                        cols.append(jj * nx + ii)
+                        vals.append(8.0 if (di == 0 and dj == 0) else -1.0)
+            rows.append((cols, vals))
+    return _csr_from_rows(rows)
+
+
+@pytest.mark.parametrize("variant", range(7))
+def test_filter_kernels_on_nine_entry_rows(gpu_lib, variant):
+    """Rows of 9 stored entries take the 16-wide unrolled row products
+    (variants 1, 2 and 5) and every other form: each gives the reference's
+    filtered vector bit for bit."""
+    ia, ja, a = _lap9_csr(61, 47)
+    n = len(ia) - 1
+    gpu_lib.set_filter_kernel(variant)
+    try:
+        gpu_lib.set_csr(ia, ja, a)
+        assert gpu_lib.row_pattern_count() == 9
+        iv = [3.0, 4.0, -1.0, 17.0]
+        v = O.seeded_normal(n, 21)
+        pol = gpu_lib.find_pol(iv, max_deg=120)
+        y = gpu_lib.chebav(pol, v)
+        gpu_lib.free_pol(pol)
+        y_ref = O.cheb_av(O.find_pol(iv, max_deg=120), ia, ja, a, v)
+        assert np.array_equal(y, y_ref), (variant, np.max(np.abs(y - y_ref)))
+        assert np.array_equal(gpu_lib.matvec(v), O.csr_matvec(ia, ja, a, v))
+    finally:
+        gpu_lib.set_filter_kernel(-1)
