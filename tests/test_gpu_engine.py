@@ -362,3 +362,36 @@ def test_mixed_engine_filters_small_matrices_in_fp64(gpu_lib):
     assert np.array_equal(out[0]["lam"], out[1]["lam"])
     M.free()
     gpu_lib.free_pol(pol)
+
+
+def test_multi_filter_dictionary_with_double_table(gpu_lib):
+    """The multi-column dictionary kernels (variants 4, 5) on a table that
+    holds doubles (a diagonal shifted by 1e-9 every 7th row, so the values
+    are not floats): every variant gives the same bits as variant 0, in FP64
+    and FP32, and FP64 matches ChebAv column by column."""
+    ia, ja, a = O.lap_csr(22, 19, 17)
+    a = a.copy()
+    n = len(ia) - 1
+    for r in range(0, n, 7):
+        for j in range(ia[r], ia[r + 1]):
+            if ja[j] == r:
+                a[j] += 1e-9
+    gpu_lib.set_csr(ia, ja, a)
+    assert 0 < gpu_lib.row_pattern_count() <= 1024
+    pol = gpu_lib.find_pol([0.6, 0.9, 0.0, 12.0], max_deg=200)
+    try:
+        for prec in (E.PREC_FP64, E.PREC_MIXED):
+            for B in (1, 4, 16):
+                X = O.seeded_normal(n * B, 40 + B).reshape(B, n)
+                gpu_lib.set_filter_variant(0)
+                ref = gpu_lib.chebav_multi([pol] * B, X, prec)
+                for v in (1, 2, 3, 4, 5):
+                    gpu_lib.set_filter_variant(v)
+                    assert np.array_equal(gpu_lib.chebav_multi([pol] * B, X, prec), ref), (prec, B, v)
+                if prec == E.PREC_FP64:
+                    gpu_lib.set_filter_variant(-1)
+                    for c in range(B):
+                        assert np.array_equal(ref[c], gpu_lib.chebav(pol, X[c]))
+    finally:
+        gpu_lib.set_filter_variant(-1)
+        gpu_lib.free_pol(pol)
