@@ -40,6 +40,10 @@ MAXIT = 2000
 SEED = 1234
 METRIC = "eigenpairs/sec + p50/p99 slice latency at resid<=1e-8; filter SpMV GB/s vs HBM"
 UNIT = "eigenpairs/s"
+# Random sparse SPD matrix of the mixed-precision configuration: 2,000,000
+# rows, 16 seeded off-diagonal columns per row, symmetrised (~66M nonzeros).
+RSPD_N = 2_000_000
+RSPD_SEED = 3
 # Lanczos dimension of this request, as the GPU arm measures it (used only to
 # scale the CPU sample to a whole request; the recurrence is the same).
 REQUEST_LANCZOS_STEPS = 451
@@ -54,7 +58,7 @@ def parse():
     p.add_argument("--count", type=int, default=COUNT)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve", "lap3d-multifilter",
-                                          "lap3d-reorth", "lap3d-kpm"],
+                                          "lap3d-reorth", "lap3d-kpm", "rspd-filter"],
                    default="lap3d-slice",
                    help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark); "
                         "lap3d-batch: several slices through the request engine; serve: a Poisson request stream")
@@ -70,6 +74,9 @@ def parse():
                    help="lap3d-batch: also time ChebLanNr on the same slices one after another")
     p.add_argument("--serve-mix", choices=["default", "small"], default="default",
                    help="serve: 'small' draws the large-matrix requests on the 2-D 100x100 Laplacian only")
+    p.add_argument("--rspd-n", type=int, default=RSPD_N, help="rspd-filter: rows of the random SPD matrix")
+    p.add_argument("--sigma", type=int, default=-1,
+                   help="rspd-filter: SELL-C-sigma sort window (-1 automatic, 0 unsorted SELL-32)")
     p.add_argument("--ncols", type=int, default=16, help="lap3d-multifilter: columns")
     p.add_argument("--variant", type=int, default=-1, help="lap3d-multifilter: kernel variant (-1 autotuned)")
     p.add_argument("--sweep", action="store_true", help="lap3d-multifilter: every variant/width/precision once")
@@ -304,6 +311,8 @@ def run_ours(args):
         h2d = v0.nbytes
         d2h = m * NX * NY * NZ * 8 + 2 * m * 8
 
+    config1 = run_config1_ours(lib, lstream) if world == 1 else None
+
     # aggregate over ranks
     stats = torch.tensor([t_dev, float(found), sum(e2e_times), float(e2e_found)], dtype=torch.float64,
                          device="cuda")
@@ -369,6 +378,8 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
+        if config1 is not None:
+            result["config1"] = config1
         if world == 1 and not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(pol.deg, kdim, intv, found / args.steps, v0, nthreads=1)
     lib.free_pol(pol)
@@ -378,6 +389,100 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(result))
+
+
+# ---------------------------------------------------------------------------
+# config 1, run to completion by both arms: ChebLanNr over [0.6, 0.9] of the
+# 2-D Laplacian 100x100 (260 eigenpairs), find_pol damping 2, thresholds
+# 0.8 / 0.2, tol 1e-8, maxit 2000, seeded normal start vector
+# ---------------------------------------------------------------------------
+C1_DIMS = (100, 100, 1)
+C1_INTV = [0.6, 0.9, 0.0, 8.0]
+C1_SEED = 1234
+C1_STEPS = 3
+
+
+def run_config1_ours(lib, lstream):
+    """Config 1 on the GPU through ChebLanNr (the drop-in entry point):
+    device time of each complete solve (CUDA events on the library stream),
+    eigenpairs/s = 260 / median solve time; e2e adds the start vector's copy
+    in and the eigenvectors' copy out."""
+    import ctypes as C
+
+    import torch
+
+    from evsl_b200 import workloads as W
+
+    ia, ja, a = W.laplacian_csr(*C1_DIMS)
+    ev = W.laplacian_eigenvalues(*C1_DIMS)
+    exact = ev[(ev >= C1_INTV[0]) & (ev <= C1_INTV[1])]
+    lib.set_csr(ia, ja, a)
+    pol = lib.find_pol(C1_INTV, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+    v = np.random.default_rng(C1_SEED).standard_normal(len(ia) - 1)
+    v /= np.linalg.norm(v)
+    out = {"workload": "config 1: ChebLanNr FP64 over [0.6, 0.9] of the 2-D Laplacian 100x100, tol 1e-8, "
+                       "maxit 2000, complete solve per step", "steps": C1_STEPS, "filter_degree": int(pol.deg)}
+    times, e2e, oks = [], [], []
+    for i in range(1 + C1_STEPS):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lstream)
+        lam, Y, res = lib.cheblan_nr(C1_INTV, 2000, TOL, v, pol, want_vectors=True)
+        e1.record(lstream)
+        e1.synchronize()
+        t1 = time.perf_counter()
+        if i == 0:
+            continue  # warm-up (kernel choice by timing, workspace)
+        times.append(e0.elapsed_time(e1) / 1e3)
+        e2e.append(t1 - t0)
+        lam = np.sort(lam)
+        ok = len(lam) == len(exact) and np.max(np.abs(lam - exact)) <= 1e-10 * 8.0 and np.all(res < TOL)
+        oks.append(bool(ok))
+    lib.free_pol(pol)
+    t = statistics.median(times)
+    out.update({"value": len(exact) / t, "unit": UNIT, "ms_per_step": 1e3 * t, "eigenpairs": int(len(exact)),
+                "e2e": {"value": len(exact) / statistics.median(e2e), "unit": UNIT,
+                        "h2d_bytes_per_step": int(v.nbytes), "d2h_bytes_per_step": int(len(exact) * (v.nbytes + 16))},
+                "all_steps_ok": all(oks), "timing": "device time per complete solve (CUDA events), median"})
+    return out
+
+
+def run_config1_reference(nthreads):
+    """Config 1 by the reference CPU build, to completion, with all host
+    threads in the reference's own parallel pattern (TESTS/PLanR/
+    MMPLanR_omp.c:183-241: the interval cut into slices, one ChebLanNr per
+    slice per OpenMP thread).  Slices hold about equal numbers of
+    eigenvalues, with end points at gap midpoints of the analytic spectrum
+    (at least 10 eigenvalues per slice)."""
+    from evsl_b200 import workloads as W
+    from oracle import evsl_oracle as O
+
+    R = O.RefLib()
+    ia, ja, a = R.lap_csr(*C1_DIMS)
+    R.set_csr(ia, ja, a)
+    ev = W.laplacian_eigenvalues(*C1_DIMS)
+    inside = ev[(ev >= C1_INTV[0]) & (ev <= C1_INTV[1])]
+    ns = max(1, min(nthreads, len(inside) // 10))
+    cuts = [C1_INTV[0]]
+    for k in range(1, ns):
+        i = round(k * len(inside) / ns)
+        while i < len(inside) and inside[i] - inside[i - 1] < 1e-10:
+            i += 1
+        cuts.append(0.5 * (inside[i - 1] + inside[i]))
+    cuts.append(C1_INTV[1])
+    v = np.random.default_rng(C1_SEED).standard_normal(len(ia) - 1)
+    v /= np.linalg.norm(v)
+    r = R.slices_nr(np.array(cuts), C1_INTV[2], C1_INTV[3], 2000, TOL, v, damping=2, thresh_int=0.8,
+                    thresh_ext=0.2, max_deg=3000, nthreads=nthreads)
+    lam = np.sort(np.concatenate(r["evals"]))
+    ok = len(lam) == len(inside) and np.max(np.abs(lam - inside)) <= 1e-10 * 8.0
+    return {"workload": "config 1: ChebLanNr over [0.6, 0.9] of the 2-D Laplacian 100x100, tol 1e-8, complete "
+                        "solve", "value": len(lam) / r["wall"], "unit": UNIT, "wall_s": r["wall"],
+            "eigenpairs": int(len(lam)), "exact": int(len(inside)), "ok": bool(ok), "threads": nthreads,
+            "slices": ns, "slice_degrees": [int(d) for d in r["deg"]],
+            "sample": "one complete run (measured, not extrapolated): %d slices on %d OpenMP threads" % (ns, nthreads)}
 
 
 # ---------------------------------------------------------------------------
@@ -410,6 +515,7 @@ def cpu_baseline(deg, kdim, intv, pairs_per_request, v0, nthreads=1):
     request_s = (kdim + 1) * rpol.deg * per_degree
     R.free_pol(rpol)
     return {"value": nthreads * pairs_per_request / request_s, "unit": UNIT, "cores": nthreads, "kind": "reference",
+            "extrapolated": True,
             "sample": f"{nthreads} thread(s) x reference ChebAv truncated to {SAMPLE_DEG} of {deg} degrees on the "
                       f"same matrix and filter ({wall:.2f} s); request = ({kdim}+1) x degree-{deg} filter "
                       f"applications, extrapolated"}
@@ -457,12 +563,17 @@ def run_reference(args):
         "config": {"workload": "lap3d-slice (same request as the GPU arm)", "interval": intv[:2],
                    "filter_degree": int(rpol.deg), "lanczos_steps": kdim,
                    "parallelism": f"{nthreads} concurrent requests (one per host thread)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "reference",
+        "extrapolated": True,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "reference", "extrapolated": True,
                          "sample": f"{nthreads} threads x reference ChebAv truncated to {SAMPLE_DEG} of "
                                    f"{rpol.deg} degrees per step; request = ({kdim}+1) filter applications"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     R.free_pol(rpol)
+    try:
+        out["config1"] = run_config1_reference(nthreads)
+    except Exception as e:  # the main line stands without it
+        out["config1"] = {"unavailable": str(e)}
     print(json.dumps(out))
 
 
@@ -527,6 +638,112 @@ def run_filter(args):
                                    "avg_launch_us": 1e6 * sec / launches},
                       "gpu_launches": launches, "clocks": clocks}))
     lib.free_pol(pol)
+
+
+def run_rspd_filter(args):
+    """rspd-filter: the filter kernel alone on the random sparse SPD matrix of
+    the mixed-precision configuration (n = 2,000,000, 16 seeded off-diagonal
+    columns per row, symmetrised: ~66M nonzeros of unequal row lengths, no
+    stencil structure, far larger than L2), stored as SELL-C-sigma.
+
+    --precision mixed: the FP32 filter (values and recurrence in float, FMA
+    accumulation; the multi-column kernel with one column).  Per-degree
+    device time = (time of a degree-400 filter - time of a degree-40 filter)
+    / 360, CUDA events on the library stream around evslx_chebav_multi on
+    device-resident vectors, median of K steps.
+    --precision fp64: ChebAv (the drop-in FP64 single-vector filter),
+    device time of every filter application from CUDA events, averaged over
+    its degree launches.
+
+    Algorithmic bytes per degree (the SpMV + Chebyshev update, no padding,
+    no chunk tables, no gathers counted): nnz (s_v + 4) + 4 (n + 1) + 5 n s_x
+    with s_v = s_x = 4 (FP32) or 8 (FP64)."""
+    import ctypes as C
+
+    import torch
+
+    import evsl_b200 as E
+    from evsl_b200 import workloads as W
+
+    n = args.rspd_n
+    t0 = time.time()
+    ia, ja, a = W.random_spd_csr(n, 16, RSPD_SEED)
+    glo, ghi = W.gershgorin_bounds(ia, ja, a)
+    gen_s = time.time() - t0
+    nnz = int(ia[-1])
+    lib = E.Library()
+    lib.set_sell_sigma(args.sigma)
+    lib.set_csr(ia, ja, a)
+    del ja, a
+    sigma, stored, stored_plain = lib.matrix_sell_layout()
+    iv = [glo + 0.3 * (ghi - glo), glo + 0.32 * (ghi - glo), glo, ghi]
+    fp32 = args.precision == "mixed"
+    sx = 4 if fp32 else 8
+    abytes = nnz * (sx + 4) + 4.0 * (n + 1) + 5.0 * n * sx
+    v0 = np.random.default_rng(RSPD_SEED).standard_normal(n)
+    dv = E.DeviceBuffer.from_host(lib.lib, v0)
+    dy = E.DeviceBuffer(lib.lib, 8 * n)
+    lstream = torch.cuda.ExternalStream(lib.stream_handle())
+    sampler = ClockSampler(rank_info()[2])
+    if fp32:
+        p_hi = lib.find_pol(iv, deg=400)
+        p_lo = lib.find_pol(iv, deg=40)
+
+        def timed(pol):
+            arr = (E.PolParams * 1)(pol)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(lstream)
+            lib._check(lib.lib.evslx_chebav_multi(1, arr, dv.ptr, dy.ptr, E.PREC_MIXED), "evslx_chebav_multi")
+            e1.record(lstream)
+            e1.synchronize()
+            return e0.elapsed_time(e1) / 1e3
+
+        for _ in range(args.warmup):
+            timed(p_hi)
+            timed(p_lo)
+        sampler.start()
+        per = []
+        for _ in range(args.steps):
+            per.append((timed(p_hi) - timed(p_lo)) / (p_hi.deg - p_lo.deg))
+        clocks = sampler.stop()
+        t = statistics.median(per)
+        launches = args.steps * (p_hi.deg + p_lo.deg + 4)
+        kernel = "k_mf_step<float,1>"
+        lib.free_pol(p_lo)
+    else:
+        p_hi = lib.find_pol(iv, deg=400)
+        dw = E.DeviceBuffer(lib.lib, 16 * n)
+        for _ in range(args.warmup):
+            lib._check(lib.lib.ChebAv(C.byref(p_hi), dv.ptr, dy.ptr, dw.ptr), "ChebAv")
+        lib.filter_profile(True)
+        sampler.start()
+        for _ in range(args.steps):
+            lib._check(lib.lib.ChebAv(C.byref(p_hi), dv.ptr, dy.ptr, dw.ptr), "ChebAv")
+        sec, byt, launches, calls = lib.filter_stats()
+        clocks = sampler.stop()
+        lib.filter_profile(False)
+        t = sec / launches
+        kernel = "k_cheb"
+    peak, kind = measured_peak_hbm()
+    gbs = abytes / t / 1e9
+    traffic = profiled_traffic(kernel, "rspd-filter-" + ("fp32" if fp32 else "fp64"))
+    print(json.dumps({
+        "metric": "filter SpMV GB/s", "value": gbs, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t * p_hi.deg, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if fp32 else "f64",
+        "data": "synthetic (random sparse SPD, seeded; inputs larger than L2)",
+        "config": {"workload": "rspd-filter: %s filter, degree %d, random sparse SPD n=%d, nnz=%d"
+                               % ("FP32" if fp32 else "FP64", p_hi.deg, n, nnz),
+                   "storage": {"sigma": sigma, "stored_slots": stored, "stored_slots_unsorted": stored_plain,
+                               "padding": stored / nnz - 1.0},
+                   "us_per_degree": 1e6 * t, "algorithmic_bytes_per_degree": abytes,
+                   "generate_s": round(gen_s, 1), "bounds": [glo, ghi]},
+        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": gbs, "peak": peak, "peak_kind": kind,
+                     "unit": "GB/s", "frac": gbs / peak, "traffic": traffic,
+                     "frac_dram": (traffic / t / 1e9 / peak) if traffic else None},
+        "gpu_launches": launches, "clocks": clocks}))
+    lib.free_pol(p_hi)
 
 
 def run_multifilter(args):
@@ -962,6 +1179,8 @@ def main():
         run_reorth(args)
     elif args.workload == "lap3d-kpm":
         run_kpm(args)
+    elif args.workload == "rspd-filter":
+        run_rspd_filter(args)
     else:
         run_ours(args)
 

@@ -265,6 +265,9 @@ def load():
         "evslx_set_filter_rows_per_thread": ([C.c_int], C.c_int),
         "evslx_set_matrix_compression": ([C.c_int], C.c_int),
         "evslx_matrix_storage": ([_ip, _ip], C.c_int),
+        "evslx_set_sell_sigma": ([C.c_int], C.c_int),
+        "evslx_set_wait_limit": ([C.c_ulonglong], C.c_int),
+        "evslx_matrix_sell_layout": ([_ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
         "evslx_read_coo_MM": ([C.c_char_p, C.c_int, C.c_int, C.POINTER(CooMat)], C.c_int),
         "evslx_coo_to_csr_device": ([C.c_int, C.POINTER(CooMat), C.c_int, C.POINTER(CsrMat)], C.c_int),
         "cooMat_to_csrMat": ([C.c_int, C.POINTER(CooMat), C.POINTER(CsrMat)], C.c_int),
@@ -588,6 +591,22 @@ class Library:
         vb, ib = C.c_int(), C.c_int()
         self._check(self.lib.evslx_matrix_storage(C.byref(vb), C.byref(ib)), "evslx_matrix_storage")
         return vb.value, ib.value
+
+    def set_wait_limit(self, polls):
+        """Polls before a device-side wait gives up (0: the defaults)."""
+        self._check(self.lib.evslx_set_wait_limit(int(polls)), "evslx_set_wait_limit")
+
+    def set_sell_sigma(self, sigma):
+        """SELL-C-sigma row sort window for matrices registered afterwards: -1
+        automatic (default), 0 never, or a power of two from 32 to 4096."""
+        self._check(self.lib.evslx_set_sell_sigma(int(sigma)), "evslx_set_sell_sigma")
+
+    def matrix_sell_layout(self):
+        """(sort window in use or 0, stored slots, slots of the unsorted layout)."""
+        sg, st, su = C.c_int(), C.c_longlong(), C.c_longlong()
+        self._check(self.lib.evslx_matrix_sell_layout(C.byref(sg), C.byref(st), C.byref(su)),
+                    "evslx_matrix_sell_layout")
+        return sg.value, st.value, su.value
 
     def set_spmv_kernel(self, which):
         self._check(self.lib.evslx_set_spmv_kernel(which), "evslx_set_spmv_kernel")

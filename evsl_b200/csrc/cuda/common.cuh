@@ -15,6 +15,8 @@ int fail(int code, const char *fmt, ...);
 int check_launch(const char *what);
 void count_launch(uint64_t k = 1);
 int sm_count();
+// The device the library was started on (its stream and memory live there).
+int lib_device();
 
 // Scratch for grid-wide reductions: partial sums (one slot per block) and
 // "last block" counters.  Kernels on the single library stream run one after

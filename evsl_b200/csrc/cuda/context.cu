@@ -34,6 +34,7 @@ unsigned int *counters() { return g_ctx.counters; }
 double *dev_scratch_scalars() { return g_ctx.scalars; }
 unsigned int *barrier_area() { return g_ctx.barrier; }
 int sm_count() { return g_ctx.sms; }
+int lib_device() { return g_ctx.device; }
 void count_launch(uint64_t k) { g_launches += k; }
 
 int fail(int code, const char *fmt, ...) {

@@ -26,6 +26,9 @@ using namespace evslcu;
 namespace {
 
 constexpr unsigned long long kBarrierSpinLimit = 1ull << 26;
+// Polls a block of the single-launch filter makes at a grid barrier before
+// it gives up (evslcu_set_wait_limit; 0 restores kBarrierSpinLimit).
+unsigned long long g_barrier_polls = kBarrierSpinLimit;
 
 // ---------------------------------------------------------------------------
 // profiling of filter applications
@@ -93,11 +96,11 @@ __device__ __forceinline__ unsigned ld_volatile(const unsigned *p) { return *(co
 // kBarGroup blocks, each counter on its own 128-byte line); the last block
 // of a group arrives on the top-level counter; the last group bumps the
 // generation word that every block polls.  Polling is tight for the first
-// spins and then backs off; after kBarrierSpinLimit polls the block records
-// an error and the whole grid leaves the kernel.
+// spins and then backs off; after `limit` polls (kBarrierSpinLimit unless
+// set lower) the block records an error and the whole grid leaves the kernel.
 constexpr int kBarGroup = 16;
 
-__device__ __forceinline__ bool grid_barrier(unsigned *area, int *err) {
+__device__ __forceinline__ bool grid_barrier(unsigned *area, int *err, unsigned long long limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -124,7 +127,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *area, int *err) {
       unsigned long long spins = 0;
       while (ld_volatile(gen) == my) {
         ++spins;
-        if (spins > kBarrierSpinLimit) {
+        if (spins > limit) {
           atomicExch(err, 1);
           ok = 0;
           break;
@@ -156,6 +159,7 @@ struct PersistArgs {
   double *dot_out;
   unsigned *bar;
   int *err;
+  unsigned long long polls;  // barrier wait limit
 };
 
 // Per-row state lives in dynamic shared memory: for slot i of thread t,
@@ -177,14 +181,15 @@ __global__ void __launch_bounds__(NT) k_filter_persistent(VIEW A, PersistArgs P,
     double *out = ((k - 1) & 1) ? P.W1 : P.W0;
     for (int i = 0; i < S; ++i) {
       const int c = gwarp + i * nwarps;
-      const int r = c * 32 + lane;
-      if (c < P.nchunks && r < A.n) {
+      const int sl = c * 32 + lane;
+      if (c < P.nchunks && sl < A.n) {
+        const int r = row_of(A, sl);
         double acc, xv;
         if (k == 1) {
-          acc = row_dot<false>(A, r, x);
+          acc = row_dot<false>(A, sl, x);
           xv = __ldg(x + r);
         } else {
-          acc = row_dot<true>(A, r, x);
+          acc = row_dot<true>(A, sl, x);
           xv = __ldcg(x + r);
         }
         double w = __dmul_rn(t, __dadd_rn(acc, __dmul_rn(P.ncc, xv)));
@@ -195,13 +200,14 @@ __global__ void __launch_bounds__(NT) k_filter_persistent(VIEW A, PersistArgs P,
         vs[i * NT + tid] = xv;
       }
     }
-    if (k < P.deg && !grid_barrier(P.bar, P.err)) return;
+    if (k < P.deg && !grid_barrier(P.bar, P.err, P.polls)) return;
   }
   double dsum = 0.0;
   for (int i = 0; i < S; ++i) {
     const int c = gwarp + i * nwarps;
-    const int r = c * 32 + lane;
-    if (c < P.nchunks && r < A.n) {
+    const int sl = c * 32 + lane;
+    if (c < P.nchunks && sl < A.n) {
+      const int r = row_of(A, sl);
       double yy = ys[i * NT + tid];
       if (P.zold) yy = __dadd_rn(yy, __dmul_rn(P.nbeta, P.zold[r]));
       P.y[r] = yy;
@@ -289,9 +295,17 @@ int evslcu_filter_error(void) {
   int *err = (int *)(counters() + 10);
   if (evslcu_d2h(&h, err, sizeof(int))) return EVSLCU_ERR_CUDA;
   if (h) {
-    evslcu_memset(err, 0, sizeof(int));
-    return fail(EVSLCU_ERR_TIMEOUT, "a grid barrier of the filter kernel did not complete within its bound");
+    // blocks that gave up left before the final reduction: clear every
+    // counter (all are zero between kernels) along with the flag
+    evslcu_memset(counters(), 0, sizeof(unsigned) * kNumCounters);
+    return fail(EVSLCU_ERR_TIMEOUT, "a wait of the filter kernel did not complete within its bound");
   }
+  return 0;
+}
+
+int evslcu_set_wait_limit(unsigned long long polls) {
+  g_barrier_polls = polls ? polls : kBarrierSpinLimit;
+  set_wave_wait_limit(polls);
   return 0;
 }
 
@@ -314,7 +328,7 @@ int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, dou
   }
   bool launched = false;
   int rc = 0;
-  if (A->wave && A->kernel == 0 && deg >= 2) {
+  if (A->wave && A->kernel == 0 && !A->perm && deg >= 2) {
     rc = chebav_wave((evslcu_mat *)A, mu, deg, cc, dd, v, y, work);
     if (!rc) rc = evslcu_filter_error();
     if (!rc && epi) rc = launch_lan_epi(n, epi, y);
@@ -352,6 +366,7 @@ int evslcu_chebav(const evslcu_op *op, const double *mu, int deg, double cc, dou
     P.dot_out = epi ? epi->dot_out : nullptr;
     P.bar = barrier_area();
     P.err = (int *)(counters() + 10);
+    P.polls = g_barrier_polls;
     if (evslcu_mat_uses_patterns(A))
       rc = A->pat_f32 ? launch_persistent(pat_pview(A), A->nchunks, P, &launched)
                       : launch_persistent(pat_view(A), A->nchunks, P, &launched);

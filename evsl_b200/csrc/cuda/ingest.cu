@@ -256,28 +256,69 @@ __global__ void k_csr_check_entries(int n, const int *ia, const int *ja, const d
   if ((threadIdx.x & 31) == 0) atomicMax(&flags[4], bw);
 }
 
-__global__ void k_chunk_width(int n, int nch, const int *ia, int *cw, long long *csize) {
+// Width of each chunk: its longest row (slot s holds row perm[s], or row s
+// when perm is null).
+__global__ void k_chunk_width(int n, int nch, const int *ia, const int *perm, int *cw, long long *csize) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nch; c += gridDim.x * blockDim.x) {
     int w = 0;
-    const int r1 = min(n, 32 * c + 32);
-    for (int r = 32 * c; r < r1; ++r) w = max(w, ia[r + 1] - ia[r]);
+    const int s1 = min(n, 32 * c + 32);
+    for (int s = 32 * c; s < s1; ++s) {
+      const int r = perm ? perm[s] : s;
+      w = max(w, ia[r + 1] - ia[r]);
+    }
     cw[c] = w;
     csize[c] = 32LL * w;
   }
 }
 
+// SELL-C-sigma row order: one block per window of W consecutive rows (W a
+// power of two, at most 4096) sorts the window's rows by length, longest
+// first, ties in row order, with a bitonic network on 64-bit keys
+// (0x7fffffff - length, position in the window) in shared memory; slot
+// w0 + i then holds row perm[w0 + i].  Positions past the last row carry the
+// largest key and sort to the end.
+template <int W>
+__global__ void __launch_bounds__(1024) k_sigma_sort(int n, const int *ia, int *perm) {
+  __shared__ unsigned long long key[W];
+  const int w0 = blockIdx.x * W;
+  for (int i = threadIdx.x; i < W; i += blockDim.x) {
+    const int r = w0 + i;
+    key[i] = (r < n) ? ((unsigned long long)(0x7fffffff - (ia[r + 1] - ia[r])) << 32) | (unsigned)i : ~0ULL;
+  }
+  __syncthreads();
+  for (int k = 2; k <= W; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < W; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long x = key[i], y = key[ixj];
+          if ((x > y) == ((i & k) == 0)) {
+            key[i] = y;
+            key[ixj] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = threadIdx.x; i < W; i += blockDim.x)
+    if (w0 + i < n) perm[w0 + i] = w0 + (int)(key[i] & 0xffffffffu);
+}
+
 // Thread per (chunk, lane) slot; entry j of lane l at cptr[c] + 32 j + l.
-// Padding: value 0 in the row's own column (adds 0 * x[r]).
+// Padding: value 0 in the row's own column (adds 0 * x[r]).  Slot s holds
+// row perm[s] (row s when perm is null); slots past the last row are all
+// padding and point at row 0.
 template <class VT, class IT>
-__global__ void k_sell_fill(int n, int nch, const int *ia, const int *ja, const double *a, const long long *cptr,
-                            const int *cw, IT *scol, VT *sval) {
+__global__ void k_sell_fill(int n, int nch, const int *ia, const int *ja, const double *a, const int *perm,
+                            const long long *cptr, const int *cw, IT *scol, VT *sval) {
   const long long slots = 32LL * nch;
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += (long long)gridDim.x * blockDim.x) {
     const int c = (int)(s >> 5), l = (int)(s & 31);
-    const int r = 32 * c + l;
-    const int len = (r < n) ? ia[r + 1] - ia[r] : 0;
-    const int rr = (r < n) ? r : 0;
-    const int beg = (r < n) ? ia[r] : 0;
+    const bool live = s < n;
+    const int r = live ? (perm ? perm[s] : (int)s) : 0;
+    const int len = live ? ia[r + 1] - ia[r] : 0;
+    const int rr = r;
+    const int beg = live ? ia[r] : 0;
     for (int j = 0; j < cw[c]; ++j) {
       const long long p = cptr[c] + 32LL * j + l;
       const int col = (j < len) ? ja[beg + j] : rr;
@@ -515,9 +556,32 @@ int build_patterns_device(evslcu_mat *M) {
   return 0;
 }
 
-// Builds the SELL-32 copy of M's device CSR (M->n, M->nnz, M->ia/ja/a set)
-// after validating it.  allow_compress: use the compressed formats when the
-// values and columns allow it.
+// Window of the SELL-C-sigma length sort: -1 automatic (kSigmaAuto rows
+// when the plain layout pads more than kSigmaTrigger times the entries),
+// 0 never, otherwise that window (a power of two from 32 to 4096) always.
+int g_sell_sigma = -1;
+constexpr int kSigmaAuto = 4096;
+constexpr double kSigmaTrigger = 1.10;
+
+int launch_sigma_sort(int n, int sigma, const int *ia, int *perm) {
+  const int nwin = (int)(((long long)n + sigma - 1) / sigma);
+  switch (sigma) {
+    case 32: k_sigma_sort<32><<<nwin, 32, 0, stream()>>>(n, ia, perm); break;
+    case 64: k_sigma_sort<64><<<nwin, 64, 0, stream()>>>(n, ia, perm); break;
+    case 128: k_sigma_sort<128><<<nwin, 128, 0, stream()>>>(n, ia, perm); break;
+    case 256: k_sigma_sort<256><<<nwin, 256, 0, stream()>>>(n, ia, perm); break;
+    case 512: k_sigma_sort<512><<<nwin, 512, 0, stream()>>>(n, ia, perm); break;
+    case 1024: k_sigma_sort<1024><<<nwin, 1024, 0, stream()>>>(n, ia, perm); break;
+    case 2048: k_sigma_sort<2048><<<nwin, 1024, 0, stream()>>>(n, ia, perm); break;
+    case 4096: k_sigma_sort<4096><<<nwin, 1024, 0, stream()>>>(n, ia, perm); break;
+    default: return fail(EVSLCU_ERR_ARG, "SELL sort window must be a power of two from 32 to 4096 (got %d)", sigma);
+  }
+  return launched("k_sigma_sort");
+}
+
+// Builds the SELL-C-sigma copy of M's device CSR (M->n, M->nnz, M->ia/ja/a
+// set) after validating it.  allow_compress: use the compressed formats when
+// the values and columns allow it.
 int build_sell_device(evslcu_mat *M, int allow_compress) {
   const int n = M->n;
   int *flags = (int *)evslcu_malloc(sizeof(int) * 5);
@@ -555,12 +619,49 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
     evslcu_free(csize);
     return fail(EVSLCU_ERR_NOMEM, "SELL build: out of device memory");
   }
-  k_chunk_width<<<grid_for(nch), kThreads, 0, stream()>>>(n, nch, M->ia, M->cw, csize);
+  k_chunk_width<<<grid_for(nch), kThreads, 0, stream()>>>(n, nch, M->ia, nullptr, M->cw, csize);
   rc = launched("k_chunk_width");
   if (!rc) rc = scan_exclusive<long long, long long>(csize, nch, M->cptr);
-  evslcu_free(csize);
   long long padded = 0;
   if (!rc) rc = evslcu_d2h(&padded, M->cptr + nch, sizeof(long long));
+  M->padded_plain = padded;
+  // SELL-C-sigma: sort the rows of each window by length when the chunks of
+  // the plain layout carry much padding, and keep the order when it cuts
+  // the stored slots by at least 5%.
+  const int sigma = g_sell_sigma < 0 ? kSigmaAuto : g_sell_sigma;
+  const bool try_sort = sigma > 0 && (g_sell_sigma > 0 || (double)padded > kSigmaTrigger * (double)std::max(M->nnz, 1LL));
+  if (!rc && try_sort) {
+    int *perm = (int *)evslcu_malloc(sizeof(int) * 32 * (size_t)nch);
+    if (!perm) rc = fail(EVSLCU_ERR_NOMEM, "SELL build: out of device memory (row order)");
+    if (!rc) rc = evslcu_memset(perm, 0, sizeof(int) * 32 * (size_t)nch);
+    if (!rc) rc = launch_sigma_sort(n, sigma, M->ia, perm);
+    long long *cptr2 = nullptr;
+    int *cw2 = nullptr;
+    if (!rc) {
+      cptr2 = (long long *)evslcu_malloc(sizeof(long long) * (nch + 1));
+      cw2 = (int *)evslcu_malloc(sizeof(int) * nch);
+      if (!cptr2 || !cw2) rc = fail(EVSLCU_ERR_NOMEM, "SELL build: out of device memory");
+    }
+    if (!rc) {
+      k_chunk_width<<<grid_for(nch), kThreads, 0, stream()>>>(n, nch, M->ia, perm, cw2, csize);
+      rc = launched("k_chunk_width");
+    }
+    if (!rc) rc = scan_exclusive<long long, long long>(csize, nch, cptr2);
+    long long padded2 = 0;
+    if (!rc) rc = evslcu_d2h(&padded2, cptr2 + nch, sizeof(long long));
+    if (!rc && (g_sell_sigma > 0 || (double)padded2 < 0.95 * (double)padded)) {
+      std::swap(M->cptr, cptr2);
+      std::swap(M->cw, cw2);
+      M->perm = perm;
+      perm = nullptr;
+      M->sigma = sigma;
+      padded = padded2;
+    }
+    evslcu_free(perm);
+    evslcu_free(cptr2);
+    evslcu_free(cw2);
+  }
+  evslcu_free(csize);
   if (rc) return rc;
   // uniform chunk width: the filter kernels compute row offsets instead of
   // loading them (one dependent load less per row)
@@ -592,16 +693,16 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
   M->sval = (char *)M->sell_block + colbytes;
   const int g = grid_for(32LL * nch);
   if (M->vfmt && M->ifmt)
-    k_sell_fill<float, short><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->cptr, M->cw,
+    k_sell_fill<float, short><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->perm, M->cptr, M->cw,
                                                             (short *)M->scol, (float *)M->sval);
   else if (M->vfmt)
-    k_sell_fill<float, int><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->cptr, M->cw,
+    k_sell_fill<float, int><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->perm, M->cptr, M->cw,
                                                           (int *)M->scol, (float *)M->sval);
   else if (M->ifmt)
-    k_sell_fill<double, short><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->cptr, M->cw,
+    k_sell_fill<double, short><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->perm, M->cptr, M->cw,
                                                              (short *)M->scol, (double *)M->sval);
   else
-    k_sell_fill<double, int><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->cptr, M->cw,
+    k_sell_fill<double, int><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->perm, M->cptr, M->cw,
                                                            (int *)M->scol, (double *)M->sval);
   return launched("k_sell_fill");
 }
@@ -611,6 +712,21 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
 using namespace evslcu;
 
 extern "C" {
+
+int evslcu_set_sell_sigma(int sigma) {
+  if (sigma < -1 || (sigma > 0 && (sigma < 32 || sigma > 4096 || (sigma & (sigma - 1)))))
+    return fail(EVSLCU_ERR_ARG, "SELL sort window must be -1 (automatic), 0 (off) or a power of two from 32 to 4096");
+  g_sell_sigma = sigma;
+  return 0;
+}
+
+int evslcu_mat_sell_layout(const evslcu_mat *A, int *sigma, long long *padded, long long *padded_plain) {
+  if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
+  if (sigma) *sigma = A->perm ? A->sigma : 0;
+  if (padded) *padded = A->padded;
+  if (padded_plain) *padded_plain = A->padded_plain;
+  return 0;
+}
 
 int evslcu_coo_to_csr(int n, long long nnz, const int *ir, const int *jc, const double *vv, int base, int **ia_out,
                       int **ja_out, double **a_out) {

@@ -153,8 +153,9 @@ __global__ void __launch_bounds__(kThreads)
   const long long total = (long long)npad * TPR;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
-    const int r = (int)(g / TPR), q = (int)(g % TPR);
-    const bool live = r < A.n;
+    const int sl = (int)(g / TPR), q = (int)(g % TPR);
+    const bool live = sl < A.n;
+    const int r = live ? row_of(A, sl) : 0;  // the row stored in slot sl
     const int cb = q * CPT;
     // this row's own values first: independent of the gathers below, so
     // their latency overlaps with them
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int c = 0; c < CPT; ++c) acc[c] = (VT)0;
     long long p;
     int w;
-    row_start(A, r, p, w);
+    row_start(A, sl, p, w);
     if constexpr (COOP) {
       // TPR entries per batch: thread q loads entry j0 + q of its row, the
       // row's threads exchange them, then gather and accumulate in order
@@ -199,29 +200,44 @@ __global__ void __launch_bounds__(kThreads)
       }
     } else {
       // U stored entries at a time: their gathers are in flight together,
-      // then accumulated in order j = 0, 1, ...  Slots past the row's width
-      // act as 0 * x[r].
-      constexpr int U = 4;
-      for (int j = 0; j < w; j += U, p += 32 * U) {
-        VT v[U];
-        int col[U];
+      // then accumulated in order j = 0, 1, ...; the next U entries of the
+      // stored matrix are loaded while the gathers are outstanding, so the
+      // streamed matrix loads do not wait behind the gathers.  Slots past
+      // the row's width act as 0 * x[r].  One column with 32-byte parts
+      // (variant 1; the same split as variant 0 at B = 1) takes 8 entries
+      // per batch instead of 4.
+      constexpr int U = (B == 1 && CPTB == 32) ? 8 : 4;
+      VT v[U];
+      int col[U];
+      auto fetch = [&](int j0, long long pp, VT(&vv)[U], int(&cc)[U]) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          if (live && j + u < w) {
-            v[u] = (VT)__ldg(A.val + p + 32 * u);
-            col[u] = decode_col(__ldg(A.col + p + 32 * u), r);
+          if (live && j0 + u < w) {
+            vv[u] = (VT)__ldg(A.val + pp + 32 * u);
+            cc[u] = decode_col(__ldg(A.col + pp + 32 * u), r);
           } else {
-            v[u] = (VT)0;
-            col[u] = live ? r : 0; /* rows past n gather row 0, unused */
+            vv[u] = (VT)0;
+            cc[u] = live ? r : 0; /* rows past n gather row 0, unused */
           }
         }
+      };
+      fetch(0, p, v, col);
+      for (int j = 0; j < w; j += U, p += 32 * U) {
         VT x[U][CPT];
 #pragma unroll
         for (int u = 0; u < U; ++u) load_row<VT, CPT>(vk + (long long)col[u] * B + cb, x[u]);
+        VT vn[U];
+        int cn[U];
+        fetch(j + U, p + 32 * U, vn, cn);
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
           for (int c = 0; c < CPT; ++c) acc[c] = fmadd(v[u], x[u][c], acc[c]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          v[u] = vn[u];
+          col[u] = cn[u];
+        }
       }
     }
     if (!live) continue;
@@ -565,8 +581,7 @@ int autotune(evslcu_mat *A, int fp32, int B) {
               default: return mf_step<float, 16>(A, view, v, k, (const float *)P, (const float *)W0, (float *)W1, (float *)Y, (const float *)cf);
             }
           };
-          rc = A->ifmt ? go(SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals, A->ellw})
-                       : go(SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals, A->ellw});
+          rc = A->ifmt ? go(sell_view_vals<float, short>(A, vals)) : go(sell_view_vals<float, int>(A, vals));
         } else {
           rc = with_view(A, [&](auto view) -> int {
             if constexpr (std::is_same<decltype(view), CsrView>::value) {
@@ -632,10 +647,10 @@ int mf_sequence(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_co
       const float *cf = (const float *)coef + off;
       const void *vals = (A->vfmt == 1) ? A->sval : A->sval32;
       if (A->ifmt)
-        rc = mf_dispatch<float>(A, SellT<float, short>{n, A->cptr, A->cw, (const short *)A->scol, (const float *)vals, A->ellw},
+        rc = mf_dispatch<float>(A, sell_view_vals<float, short>(A, vals),
                                 variant_of(A, 1, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
       else
-        rc = mf_dispatch<float>(A, SellT<float, int>{n, A->cptr, A->cw, (const int *)A->scol, (const float *)vals, A->ellw},
+        rc = mf_dispatch<float>(A, sell_view_vals<float, int>(A, vals),
                                 variant_of(A, 1, B), B, gc, md, cf, xt, yt, P, W0, W1, Y, nlaunch);
     } else {
       double *P = (double *)w, *W0 = (double *)(w + blk), *W1 = (double *)(w + 2 * blk), *Y = (double *)(w + 3 * blk);

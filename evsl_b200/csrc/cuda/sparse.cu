@@ -289,7 +289,8 @@ namespace {
 
 template <class M>
 __global__ void __launch_bounds__(kThreads) k_spmv(M A, const double *__restrict__ x, double *__restrict__ y) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) y[r] = row_dot<false>(A, r, x);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += gridDim.x * blockDim.x)
+    y[row_of(A, s)] = row_dot<false>(A, s, x);
 }
 
 // One Chebyshev degree step k (FIRST: k == 1; EPI: k == deg, Lanczos epilogue).
@@ -309,10 +310,11 @@ __global__ void __launch_bounds__(kThreads)
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   asm volatile("griddepcontrol.wait;" ::: "memory");
   double dsum = 0.0;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) {
+  for (int sl = blockIdx.x * blockDim.x + threadIdx.x; sl < A.n; sl += gridDim.x * blockDim.x) {
+    const int r = row_of(A, sl);  // slot sl holds row r (sigma-sorted SELL storage), else r == sl
     const double xm1 = FIRST ? 0.0 : vkm1[r];
     const double yo = FIRST ? 0.0 : y[r];
-    const double acc = row_dot_any<WMAX, false>(A, r, vk);
+    const double acc = row_dot_any<WMAX, false>(A, sl, vk);
     const double x = vk[r];
     // vkp1 = A vk; vkp1 += (-cc) vk; vkp1 *= t; vkp1 += (-1) vkm1
     double w = __dmul_rn(t, __dadd_rn(acc, __dmul_rn(ncc, x)));
@@ -352,14 +354,14 @@ __global__ void __launch_bounds__(kThreads)
   const int nwt = gridDim.x * (kThreads / 32);
   const int npairs = (A.n + 63) / 64;
   for (int pr = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); pr < npairs; pr += nwt) {
-    const int r0 = pr * 64 + lane;
-    const bool has1 = (pr * 64 + 32) < A.n;
+    const int s0 = pr * 64 + lane;
+    const bool has0 = s0 < A.n, has1 = s0 + 32 < A.n;
     double acc[2];
-    row_dot2<false>(A, r0, has1, vk, acc[0], acc[1]);
+    row_dot2<false>(A, s0, has0, has1, vk, acc[0], acc[1]);
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int r = r0 + 32 * h;
-      if (r < A.n) {
+      if (h == 0 ? has0 : has1) {
+        const int r = row_of(A, s0 + 32 * h);
         const double x = vk[r];
         double w = __dmul_rn(t, __dadd_rn(acc[h], __dmul_rn(ncc, x)));
         if (!FIRST) w = __dadd_rn(w, -vkm1[r]);
@@ -847,9 +849,10 @@ __global__ void k_kpm_accumulate(int Mdeg, int nvec, const double *jac, const do
 constexpr size_t kNoAllocDoubles = (size_t)1 << 22;
 static __device__ __align__(256) double g_kpm_noalloc_scratch[kNoAllocDoubles];
 
-// Device address of the scratch array, looked up once per device.
-constexpr int kMaxDevices = 64;
-double *g_noalloc_ptr[kMaxDevices] = {};
+// Device address of the scratch array on the library's device, looked up
+// once (again only if a later EVSLStart picks another device).
+double *g_noalloc_ptr = nullptr;
+int g_noalloc_dev = -1;
 
 }  // namespace
 
@@ -1219,6 +1222,7 @@ void evslcu_mat_destroy(evslcu_mat *M) {
   }
   evslcu_free(M->cptr);
   evslcu_free(M->cw);
+  evslcu_free(M->perm);
   evslcu_mat_l2_persist(M, 0);
   evslcu_free(M->sell_block);
   evslcu_free(M->wave_ctl);
@@ -1475,19 +1479,27 @@ int evslcu_kpm_noalloc(const evslcu_op *op, int n, int Mdeg, int nvec, const dou
                 "allocation-free kpmdos needs %zu doubles of scratch (3*n*nvec + Mdeg*nvec + ...) but the fixed "
                 "scratch holds %zu (32 MiB); use kpmdos/evslx_kpmdos_probes for this size",
                 need, kNoAllocDoubles);
-  // set-up, once per device, with that device current
+  // The library's stream and the caller's probes live on the device the
+  // library was started on; the scratch address is only valid there, so the
+  // calling thread must have that device current.
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return fail(EVSLCU_ERR_ARG, "device ordinal %d out of range", dev);
-  if (!g_noalloc_ptr[dev]) {
+  if (dev != lib_device())
+    return fail(EVSLCU_ERR_STATE,
+                "allocation-free kpmdos called with device %d current; the library runs on device %d (make it "
+                "current in this thread first)",
+                dev, lib_device());
+  // set-up, once per device, with that device current
+  if (!g_noalloc_ptr || g_noalloc_dev != dev) {
     double *ptr = nullptr;
     e = cudaGetSymbolAddress((void **)&ptr, g_kpm_noalloc_scratch);
     if (e != cudaSuccess || !ptr)
       return fail(EVSLCU_ERR_CUDA, "cudaGetSymbolAddress of the KPM scratch failed: %s", cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = ptr;
+    g_noalloc_ptr = ptr;
+    g_noalloc_dev = dev;
   }
-  double *base = g_noalloc_ptr[dev];
+  double *base = g_noalloc_ptr;
   unsigned int *ctrs = (unsigned int *)base;  // first 64 doubles: counters
   const int B = nvec;
   const int G = kpm_grid(n);

@@ -4,10 +4,17 @@
 
 #include "common.cuh"
 
-// Prepared matrix.  The filter uses SELL-32: rows in chunks of 32, entries of
-// a chunk stored column-major (entry j of lane l at cptr[c] + 32 j + l),
-// chunks padded to their longest row with zero values pointing at the row
-// itself.  Storage is compressed losslessly when the matrix allows it:
+// Prepared matrix.  The filter uses SELL-C-sigma with C = 32: rows in chunks
+// of 32 slots, entries of a chunk stored column-major (entry j of slot l at
+// cptr[c] + 32 j + l), chunks padded to their longest row with zero values
+// pointing at the row itself.  When the row lengths vary (general sparse
+// matrices), the rows of each window of sigma consecutive rows are sorted by
+// length (longest first) before they are cut into chunks, so that the rows
+// of a chunk have nearly equal lengths and padding is small; perm[s] is then
+// the row stored in slot s (a permutation inside each window).  Vectors stay
+// in the original row order: a kernel reads and writes row perm[s] for slot
+// s.  Each row's entries keep their CSR order, so row sums are unchanged.
+// Storage is compressed losslessly when the matrix allows it:
 //   vfmt 1: values stored as float because every value is exactly a float;
 //   ifmt 1: columns stored as int16 offsets from the row (|col-row| < 32768).
 // Every variant multiplies in FP64 in the same order, so results are
@@ -35,6 +42,9 @@ struct evslcu_mat {
   long long bandwidth = 0;  // max |col - row| over the stored entries
   int ellw = 0;             // > 0: every SELL-32 chunk has this width
   int maxw = 0;             // widest SELL-32 chunk
+  int *perm = nullptr;      // slot -> row when the rows are sigma-sorted (null: slot s holds row s)
+  int sigma = 0;            // window of the length sort (0: rows in their original order)
+  long long padded_plain = 0;  // stored slots the unsorted SELL-32 layout would need
   int wave = 0;             // 1: pipelined single-launch filter (wavefilter.cu)
   unsigned *wave_ctl = nullptr;
   size_t wave_ctl_words = 0;
@@ -78,17 +88,28 @@ struct SellT {
   const IT *__restrict__ col;
   const VT *__restrict__ val;
   int ellw;  // > 0: every chunk has this width (offsets computed, not loaded)
+  const int *__restrict__ perm;  // slot -> row (null: identity)
 };
 
-// Start of row r's entries and the width of its chunk.
+// The row stored in slot s (the views without a slot order map s to s).
 template <class VT, class IT>
-__device__ __forceinline__ void row_start(const SellT<VT, IT> &A, int r, long long &p, int &w) {
-  const int c = r >> 5;
+__device__ __forceinline__ int row_of(const SellT<VT, IT> &A, int s) {
+  return A.perm ? __ldg(A.perm + s) : s;
+}
+template <class V>
+__device__ __forceinline__ int row_of(const V &, int s) {
+  return s;
+}
+
+// Start of slot s's entries and the width of its chunk.
+template <class VT, class IT>
+__device__ __forceinline__ void row_start(const SellT<VT, IT> &A, int s, long long &p, int &w) {
+  const int c = s >> 5;
   if (A.ellw > 0) {
     w = A.ellw;
-    p = (long long)c * 32 * A.ellw + (r & 31);
+    p = (long long)c * 32 * A.ellw + (s & 31);
   } else {
-    p = A.cptr[c] + (r & 31);
+    p = A.cptr[c] + (s & 31);
     w = A.cw[c];
   }
 }
@@ -110,33 +131,64 @@ __device__ __forceinline__ double ldx(const double *p) {
   return __ldg(p);
 }
 
-// Row r of A times x, summed left to right with rounded multiply and add.
+// The row in slot s of A times x, summed left to right with rounded multiply
+// and add.  Entries are taken 4 at a time with their gathers in flight
+// together, and the next 4 stored entries are loaded while those gathers are
+// outstanding; the sum is still formed entry by entry in row order.
 template <bool COHERENT, class VT, class IT>
-__device__ __forceinline__ double row_dot(const SellT<VT, IT> &A, int r, const double *x) {
+__device__ __forceinline__ double row_dot(const SellT<VT, IT> &A, int s, const double *x) {
+  constexpr int U = 4;
   long long p;
   int w;
-  row_start(A, r, p, w);
+  row_start(A, s, p, w);
+  const int r = row_of(A, s);
+  VT v[U];
+  int col[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u)
+    if (u < w) {
+      v[u] = __ldg(A.val + p + 32 * u);
+      col[u] = decode_col(__ldg(A.col + p + 32 * u), r);
+    }
   double acc = 0.0;
-#pragma unroll 4
-  for (int j = 0; j < w; ++j, p += 32) {
-    const double v = (double)__ldg(A.val + p);
-    const int col = decode_col(__ldg(A.col + p), r);
-    acc = __dadd_rn(acc, __dmul_rn(v, ldx<COHERENT>(x + col)));
+  for (int j = 0; j < w; j += U, p += 32 * U) {
+    double g[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (j + u < w) g[u] = ldx<COHERENT>(x + col[u]);
+    VT vn[U];
+    int cn[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (j + U + u < w) {
+        vn[u] = __ldg(A.val + p + 32 * (U + u));
+        cn[u] = decode_col(__ldg(A.col + p + 32 * (U + u)), r);
+      }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (j + u < w) acc = __dadd_rn(acc, __dmul_rn((double)v[u], g[u]));
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      v[u] = vn[u];
+      col[u] = cn[u];
+    }
   }
   return acc;
 }
 
-// Rows r0 and r1 = r0 + 32 (same lane of chunks c and c+1) with their loads
+// Slots s0 and s0 + 32 (same lane of chunks c and c+1) with their loads
 // interleaved: two independent dependency chains per thread.  Each row is
-// still summed left to right, so results equal row_dot's.
+// still summed left to right, so results equal row_dot's.  A slot past the
+// last row (has0 / has1 false) reads nothing and gives 0.
 template <bool COHERENT, class VT, class IT>
-__device__ __forceinline__ void row_dot2(const SellT<VT, IT> &A, int r0, bool has1, const double *x, double &acc0,
-                                         double &acc1) {
-  long long p0, p1 = 0;
-  int w0, w1 = 0;
-  row_start(A, r0, p0, w0);
-  if (has1) row_start(A, r0 + 32, p1, w1);
-  const int r1 = r0 + 32;
+__device__ __forceinline__ void row_dot2(const SellT<VT, IT> &A, int s0, bool has0, bool has1, const double *x,
+                                         double &acc0, double &acc1) {
+  long long p0 = 0, p1 = 0;
+  int w0 = 0, w1 = 0;
+  if (has0) row_start(A, s0, p0, w0);
+  if (has1) row_start(A, s0 + 32, p1, w1);
+  const int r0 = has0 ? row_of(A, s0) : 0;
+  const int r1 = has1 ? row_of(A, s0 + 32) : 0;
   acc0 = 0.0;
   acc1 = 0.0;
   const int wm = w0 > w1 ? w0 : w1;
@@ -155,12 +207,13 @@ __device__ __forceinline__ void row_dot2(const SellT<VT, IT> &A, int r0, bool ha
   }
 }
 
-// Calls f(value, column) for the entries of row r, left to right.
+// Calls f(value, column) for the entries of the row in slot s, left to right.
 template <class VT, class IT, class F>
-__device__ __forceinline__ void row_for_each(const SellT<VT, IT> &A, int r, F &&f) {
+__device__ __forceinline__ void row_for_each(const SellT<VT, IT> &A, int s, F &&f) {
   long long p;
   int w;
-  row_start(A, r, p, w);
+  row_start(A, s, p, w);
+  const int r = row_of(A, s);
   for (int j = 0; j < w; ++j, p += 32) f((double)__ldg(A.val + p), decode_col(__ldg(A.col + p), r));
 }
 
@@ -226,10 +279,11 @@ __device__ __forceinline__ double row_dot_w(const PatView &A, int r, const doubl
 }
 
 template <int WMAX, bool COHERENT, class VT, class IT>
-__device__ __forceinline__ double row_dot_w(const SellT<VT, IT> &A, int r, const double *x) {
+__device__ __forceinline__ double row_dot_w(const SellT<VT, IT> &A, int s, const double *x) {
   long long p;
   int w;
-  row_start(A, r, p, w);
+  row_start(A, s, p, w);
+  const int r = row_of(A, s);
   VT v[WMAX];
   double g[WMAX];
 #pragma unroll
@@ -323,7 +377,13 @@ inline PatView pat_view(const evslcu_mat *A) {
 
 template <class VT, class IT>
 inline SellT<VT, IT> sell_view(const evslcu_mat *A) {
-  return SellT<VT, IT>{A->n, A->cptr, A->cw, (const IT *)A->scol, (const VT *)A->sval, A->ellw};
+  return SellT<VT, IT>{A->n, A->cptr, A->cw, (const IT *)A->scol, (const VT *)A->sval, A->ellw, A->perm};
+}
+
+// The same storage with the values read from another array (the FP32 copy).
+template <class VT, class IT>
+inline SellT<VT, IT> sell_view_vals(const evslcu_mat *A, const void *vals) {
+  return SellT<VT, IT>{A->n, A->cptr, A->cw, (const IT *)A->scol, (const VT *)vals, A->ellw, A->perm};
 }
 
 inline CsrView csr_view(const evslcu_mat *A) { return CsrView{A->n, A->ia, A->ja, A->a}; }
@@ -338,6 +398,8 @@ inline int with_view(const evslcu_mat *A, F &&f) {
   return f(sell_view<float, short>(A));
 }
 
+// Wait limit of the pipelined filter's dependency waits (0: default).
+void set_wave_wait_limit(unsigned long long polls);
 // Pipelined single-launch filter (wavefilter.cu); work: 2n doubles.
 int chebav_wave(evslcu_mat *A, const double *mu, int deg, double cc, double dd, const double *v, double *y,
                 double *work);

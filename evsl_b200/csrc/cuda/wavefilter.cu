@@ -31,6 +31,7 @@ namespace {
 constexpr int kWaveThreads = 256;
 constexpr int kWaveRows = 2048;  // rows per tile (8 per thread)
 constexpr unsigned kWaveSpinLimit = 1u << 22;
+unsigned g_wave_polls = kWaveSpinLimit;  // polls per dependency wait
 
 struct WaveArgs {
   int n, T, delta, deg;
@@ -43,6 +44,7 @@ struct WaveArgs {
   unsigned *abort_flag;
   int *err;
   unsigned *done;  // done[t] = last step published for tile t
+  unsigned polls;  // dependency wait limit
 };
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(kWaveThreads) k_filter_wave(SellT<VT, IT> A, W
         if (tt <= hi) {
           unsigned spins = 0;
           while (ld_acquire(P.done + tt) < (unsigned)(s - 1)) {
-            if (++spins > kWaveSpinLimit || *(volatile unsigned *)P.abort_flag) {
+            if (++spins > P.polls || *(volatile unsigned *)P.abort_flag) {
               ok = 0;
               break;
             }
@@ -145,10 +147,16 @@ int launch_wave(const SellT<VT, IT> &A, const WaveArgs &P) {
 
 }  // namespace
 
+void set_wave_wait_limit(unsigned long long polls) {
+  g_wave_polls = (polls == 0 || polls > kWaveSpinLimit) ? kWaveSpinLimit : (unsigned)polls;
+}
+
 // Filter application through the pipelined kernel (the matrix must use the
-// SELL-32 storage).  work: 2n doubles.
+// SELL-32 storage with rows in their original order: a tile's dependencies
+// are computed from row numbers).  work: 2n doubles.
 int chebav_wave(evslcu_mat *A, const double *mu, int deg, double cc, double dd, const double *v, double *y,
                 double *work) {
+  if (A->perm) return fail(EVSLCU_ERR_ARG, "the pipelined filter needs the unsorted SELL-32 row order");
   const int n = A->n;
   const int T = (n + kWaveRows - 1) / kWaveRows;
   const size_t need = 8 + (size_t)T;  // 2 words of counter, abort flag, padding, then done[]
@@ -188,6 +196,7 @@ int chebav_wave(evslcu_mat *A, const double *mu, int deg, double cc, double dd, 
   P.abort_flag = A->wave_ctl + 2;
   P.err = (int *)(counters() + 10);
   P.done = A->wave_ctl + 8;
+  P.polls = g_wave_polls;
   if (A->vfmt == 0 && A->ifmt == 0)
     return launch_wave(sell_view<double, int>(A), P);
   if (A->vfmt == 0 && A->ifmt == 1)

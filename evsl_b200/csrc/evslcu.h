@@ -232,10 +232,21 @@ void *evslcu_stream_handle(void);
 /* Non-zero (EVSLCU_ERR_TIMEOUT) if a bounded grid barrier of the filter
  * kernel gave up since the last check; clears the flag.  Synchronous. */
 int evslcu_filter_error(void);
+/* Polls a device-side wait makes before giving up with EVSLCU_ERR_TIMEOUT:
+ * the grid barrier of the single-launch filter and the dependency waits of
+ * the pipelined filter.  0 restores the defaults (2^26 and 2^22 polls). */
+int evslcu_set_wait_limit(unsigned long long polls);
 /* Lossless compression of the SELL copy (values as float when all are exactly
  * floats, columns as int16 offsets when they fit); applies to matrices
  * created afterwards.  Default on. */
 int evslcu_set_compression(int on);
+/* Row order of the SELL copy: -1 automatic (rows sorted by length inside
+ * windows of 4096 when that cuts the padded slots), 0 never, or a window (a
+ * power of two from 32 to 4096) always.  Matrices registered afterwards. */
+int evslcu_set_sell_sigma(int sigma);
+/* The sort window in use (0: rows in their original order) and the stored
+ * slots with and without the sort. */
+int evslcu_mat_sell_layout(const evslcu_mat *A, int *sigma, long long *padded, long long *padded_plain);
 int evslcu_mat_storage(const evslcu_mat *A, int *vfmt, int *ifmt);
 /* Row-pattern dictionary: built at registration when the rows take at most
  * 1024 distinct (value, column - row) sequences (default on; applies to

@@ -585,6 +585,15 @@ int evslx_set_filter_persistent(int on) {
 
 int evslx_set_matrix_compression(int on) { return from_cu(evslcu_set_compression(on)); }
 
+int evslx_set_sell_sigma(int sigma) { return from_cu(evslcu_set_sell_sigma(sigma)); }
+
+int evslx_set_wait_limit(unsigned long long polls) { return from_cu(evslcu_set_wait_limit(polls)); }
+
+int evslx_matrix_sell_layout(int *sigma, long long *stored, long long *stored_unsorted) {
+  if (!evslh.mat) return evsl_seterr(EVSLX_ERR_STATE, "no registered CSR matrix");
+  return from_cu(evslcu_mat_sell_layout(evslh.mat, sigma, stored, stored_unsorted));
+}
+
 int evslx_matrix_storage(int *value_bytes, int *index_bytes) {
   int vf = 0, xf = 0;
   if (!evslh.mat) return evsl_seterr(EVSLX_ERR_STATE, "no registered CSR matrix");

@@ -74,42 +74,41 @@ def random_spd_csr(n: int, offdiag: int = 16, seed: int = 0):
     `offdiag` column indices uniformly (seeded), values U(-1, 1); the matrix
     is symmetrised as (M + M^T)/2 and each diagonal entry set to the row's
     absolute off-diagonal sum plus U(0, 1) (strict diagonal dominance).
-    Returns (ia, ja, a) with sorted rows and duplicates summed."""
+    Returns (ia, ja, a) with sorted rows and duplicates summed (in the order
+    of the stable sort of (row, column) keys)."""
     rng = np.random.default_rng(seed)
     rows = np.repeat(np.arange(n, dtype=np.int64), offdiag)
     cols = rng.integers(0, n, size=n * offdiag, dtype=np.int64)
     vals = rng.uniform(-1.0, 1.0, size=n * offdiag)
     keep = rows != cols
     rows, cols, vals = rows[keep], cols[keep], vals[keep]
-    r = np.concatenate([rows, cols])
-    c = np.concatenate([cols, rows])
+    key = np.concatenate([rows * n + cols, cols * n + rows])
     v = np.concatenate([vals, vals]) * 0.5
-    key = r * n + c
+    del rows, cols, vals
     order = np.argsort(key, kind="stable")
     key, v = key[order], v[order]
-    uk, start = np.unique(key, return_index=True)
-    v = np.add.reduceat(v, start)
-    r, c = uk // n, uk % n
-    rowsum = np.zeros(n)
-    np.add.at(rowsum, r, np.abs(v))
-    diag = rowsum + rng.uniform(0.0, 1.0, size=n)
-    r = np.concatenate([r, np.arange(n, dtype=np.int64)])
-    c = np.concatenate([c, np.arange(n, dtype=np.int64)])
-    v = np.concatenate([v, diag])
-    order = np.lexsort((c, r))
-    r, c, v = r[order], c[order], v[order]
+    del order
+    if np.any(key[1:] == key[:-1]):
+        start = np.flatnonzero(np.concatenate([[True], key[1:] != key[:-1]]))
+        v = np.add.reduceat(v, start)
+        key = key[start]
+    r = key // n
+    c = key - r * n
+    diag = np.bincount(r, weights=np.abs(v), minlength=n) + rng.uniform(0.0, 1.0, size=n)
+    # the diagonal entry goes between the row's columns below and above it
+    pos = np.searchsorted(key, np.arange(n, dtype=np.int64) * (n + 1))
+    c = np.insert(c, pos, np.arange(n, dtype=np.int64))
+    v = np.insert(v, pos, diag)
     ia = np.zeros(n + 1, dtype=np.int64)
-    np.add.at(ia, r + 1, 1)
-    return np.cumsum(ia).astype(np.int32), c.astype(np.int32), v
+    np.cumsum(np.bincount(r, minlength=n) + 1, out=ia[1:])
+    return ia.astype(np.int32), c.astype(np.int32), v
 
 
 def gershgorin_bounds(ia, ja, a):
     """[min(d_i - r_i), max(d_i + r_i)] over the rows (contains the spectrum)."""
     n = len(ia) - 1
     rows = np.repeat(np.arange(n), np.diff(ia))
-    diag = np.zeros(n)
-    absum = np.zeros(n)
     on = rows == ja
-    np.add.at(diag, rows[on], a[on])
-    np.add.at(absum, rows[~on], np.abs(a[~on]))
+    diag = np.bincount(rows[on], weights=a[on], minlength=n)
+    absum = np.bincount(rows[~on], weights=np.abs(a[~on]), minlength=n)
     return float(np.min(diag - absum)), float(np.max(diag + absum))

@@ -23,6 +23,7 @@ extern "C" {
 #define EVSLX_ERR_NOMEM (-102)
 #define EVSLX_ERR_NODEV (-103)
 #define EVSLX_ERR_STATE (-104)
+#define EVSLX_ERR_TIMEOUT (-105) /* a bounded device-side wait gave up */
 #define EVSLX_ERR_UNSUPPORTED (-106)
 #define EVSLX_ERR_NUMERIC (-107)
 
@@ -48,8 +49,11 @@ int evslx_kpmdos_probes(int Mdeg, int damping, int nvec, double *intv, const dou
  * run: a serving process that reserves the GPU's memory up front (resident
  * matrices and Lanczos bases under a fixed HBM budget) cannot let a density-
  * of-states request call cudaMalloc/cudaFree, which would break the budget
- * and synchronise the device in the middle of other requests.  Results are
- * the same as evslx_kpmdos_probes.
+ * and synchronise the device in the middle of other requests.  Results agree
+ * with evslx_kpmdos_probes to rounding (within 1e-12 of max |mu|, normwise):
+ * this entry point forms one dot product with the probes per degree, while
+ * evslx_kpmdos_probes by default takes two moments per block step from the
+ * Chebyshev product identities.
  *
  * All device scratch (block vectors, dot products, partial sums, counters)
  * lives in one fixed 32 MiB array inside the library's device image, which
@@ -57,8 +61,13 @@ int evslx_kpmdos_probes(int Mdeg, int damping, int nvec, double *intv, const dou
  * 1 <= nvec <= 128, 1 <= Mdeg <= EVSLX_NOALLOC_KPM_MAX_DEG, and
  * 3*n*nvec + Mdeg*nvec + (partial sums) must fit the array (about
  * n*nvec <= 1.3 million); larger sizes return EVSLX_ERR_ARG with a message.
- * The first call on each device looks up the array's device address
+ * The calling thread must have the library's device (the one current at
+ * EVSLStart) current; another device is rejected with EVSLX_ERR_STATE.  The
+ * first call on that device looks up the array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The damping factors and sine differences are formed on the calling
+ * thread's stack: 16*Mdeg bytes, 64 KiB at the largest Mdeg, which a thread
+ * with a small stack must allow for.
  * Every call uses the same array and keeps the previous call's contents
  * (the reduction counters are cleared at the start of each call), so calls
  * that overlap on the GPU -- from several host threads, or enqueued on
@@ -109,11 +118,33 @@ int evslx_set_filter_block(int threads);
  * from the row when they fit.  Applies to matrices registered afterwards;
  * default on.  Results are identical either way. */
 int evslx_set_matrix_compression(int on);
+/* SELL-C-sigma row order of the stored matrix (C = 32).  sigma -1 (default):
+ * when the chunks of 32 consecutive rows would carry more than 10% padding
+ * (rows of unequal length, as in general sparse matrices), the rows of each
+ * window of 4096 consecutive rows are sorted by length before they are cut
+ * into chunks, and the sorted order is kept when it stores at least 5% fewer
+ * slots; 0: never sort; a power of two from 32 to 4096: always sort with that
+ * window.  Vectors stay in the caller's row order and every row is summed in
+ * its CSR order, so results are identical either way.  Applies to matrices
+ * registered afterwards.  (Replaces the cuSPARSE CSR descriptor of
+ * SRC/spmat.c:529-621; the CSR matvec SRC/spmat.c:257-298 is the arithmetic.) */
+int evslx_set_sell_sigma(int sigma);
+/* Layout of the registered matrix: the sort window in use (0: rows in their
+ * original order), the stored slots (entries plus padding) and the slots the
+ * unsorted layout would store. */
+int evslx_matrix_sell_layout(int *sigma, long long *stored, long long *stored_unsorted);
 /* Run each filter application as one pipelined launch: rows in tiles, work
  * items (degree, tile) handed out in order, a tile's degree k waiting only
  * for degree k-1 of the tiles its rows reach (bounded waits).  Results are
  * bitwise those of the per-degree launches. */
 int evslx_set_filter_wave(int on);
+/* Every device-side wait is bounded: a block of the single-launch filter
+ * gives up at a grid barrier after 2^26 polls (about 2 s), a tile of the
+ * pipelined filter after 2^22 polls on a dependency; the call then returns
+ * EVSLX_ERR_TIMEOUT and the library stays usable.  This sets both limits
+ * (0 restores the defaults); a very small limit makes the waits run out,
+ * which tests of the failure path use. */
+int evslx_set_wait_limit(unsigned long long polls);
 
 /* Keep the registered matrix's stored arrays resident in L2 (a persisting
  * access-policy window on the library stream with this process's persisting

@@ -2,10 +2,16 @@
 library (oracle/_ref/libevsl_ref.so, built by `make -C oracle` from the
 reference sources).  Run from the repository root:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # evsl_ref_golden.npz
+    python tests/golden/make_golden.py scale    # evsl_ref_golden_scale.npz
 
 Every input is seeded; probe and start vectors are injected into the
-reference through its rand_double_device hook (oracle/ref_hooks.c).
+reference through its rand_double_device hook (oracle/ref_hooks.c).  The
+`scale` fixtures hold reference results at the benchmark configurations'
+sizes (minutes of reference CPU time): kpmdos on the 3-D Laplacian 100^3 with
+300 moments and 30 probes, and on the 2-million-row random SPD matrix with 100
+moments and 8 Gaussian probes; ChebLanNr on a 20,000-row matrix from the
+same random SPD generator with its exact eigenvalues from a dense solve.
 """
 import gzip
 import os
@@ -20,7 +26,16 @@ from oracle import evsl_oracle as O  # noqa: E402
 
 OUT = os.path.join(ROOT, "tests", "golden")
 MM_DIR = os.path.join(OUT, "mm")
-REF_MATRICES = "/root/reference/EVSL_1.1.1/MATRICES"
+REF_ROOT = os.environ.get("EVSL_REFERENCE", "/root/reference/EVSL_1.1.1")
+REF_MATRICES = os.path.join(REF_ROOT, "MATRICES")
+
+# Scale fixtures: (name, value) of the seeds and sizes the GPU tests repeat.
+SCALE = {
+    "kpm100_dims": (100, 100, 100), "kpm100_M": 300, "kpm100_nvec": 30, "kpm100_seed": 41,
+    "kpm100_intv": (0.6, 1.2, 0.0, 12.0),
+    "rspd_n": 20000, "rspd_seed": 33, "rspd_vseed": 34, "rspd_lo_index": 1000, "rspd_count": 50,
+    "rspd2m_n": 2000000, "rspd2m_seed": 3, "rspd2m_M": 100, "rspd2m_nvec": 8, "rspd2m_pseed": 45,
+}
 
 
 def _fmt(v, rng):
@@ -225,5 +240,74 @@ def main():
     print("wrote", os.path.join(OUT, "evsl_ref_golden.npz"), "keys:", len(out))
 
 
+def main_scale():
+    import time
+
+    from evsl_b200 import workloads as W
+
+    R = O.RefLib()
+    S = SCALE
+    out = {k: np.array(v) for k, v in S.items()}
+    # ---- kpmdos at the config-2 settings: 3-D Laplacian 100^3, 300 moments,
+    #      Jackson damping, 30 seeded Rademacher probes ------------------------
+    t = time.time()
+    ia, ja, a = R.lap_csr(*S["kpm100_dims"])
+    R.set_csr(ia, ja, a)
+    n = len(ia) - 1
+    probes = O.seeded_rademacher(S["kpm100_nvec"], n, S["kpm100_seed"])
+    rc, mu, ec = R.kpmdos(S["kpm100_M"], 1, probes, list(S["kpm100_intv"]))
+    assert rc == 0
+    out["kpm100_mu"], out["kpm100_ecnt"] = mu, np.array([ec])
+    del probes
+    print(f"kpm100: ecnt {ec:.3f} ({time.time() - t:.0f} s)", flush=True)
+    # ---- ChebLanNr on a 20,000-row random SPD matrix (the config-3 generator):
+    #      50 eigenvalues from the 1000th up, end points at gap midpoints of the
+    #      dense spectrum, bounds just outside the extreme eigenvalues ------------
+    t = time.time()
+    ia, ja, a = W.random_spd_csr(S["rspd_n"], 16, S["rspd_seed"])
+    n = len(ia) - 1
+    M = np.zeros((n, n))
+    rows = np.repeat(np.arange(n), np.diff(ia))
+    M[rows, ja] = a
+    ev = np.linalg.eigvalsh(M)
+    del M
+    i0, i1 = S["rspd_lo_index"], S["rspd_lo_index"] + S["rspd_count"]
+    lo, hi = float(ev[0] - 0.01), float(ev[-1] + 0.01)
+    iv = [0.5 * (ev[i0 - 1] + ev[i0]), 0.5 * (ev[i1 - 1] + ev[i1]), lo, hi]
+    out["rspd_intv"] = np.array(iv)
+    out["rspd_exact"] = ev[i0:i1]
+    out["rspd_extremes"] = np.array([ev[0], ev[-1]])
+    R.set_csr(ia, ja, a)
+    rc, pol = R.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2)
+    v = O.seeded_normal(n, S["rspd_vseed"])
+    rc, (lam, Wv, res) = R.cheblan_nr(iv, 3000, 1e-8, v, pol)
+    assert rc == 0
+    out["rspd_lam"] = np.sort(lam)
+    out["rspd_res_max"] = np.array([res.max()])
+    out["rspd_deg"] = np.array([R.pol_dict(pol)["deg"]])
+    R.free_pol(pol)
+    print(f"rspd: {len(lam)} eigenvalues (exact {i1 - i0}), degree {out['rspd_deg'][0]}, "
+          f"{time.time() - t:.0f} s", flush=True)
+    # ---- kpmdos on the 2-million-row random SPD matrix: 100 moments, Jackson,
+    #      8 seeded Gaussian probes, Gershgorin bounds -------------------------------
+    t = time.time()
+    ia, ja, a = W.random_spd_csr(S["rspd2m_n"], 16, S["rspd2m_seed"])
+    n = len(ia) - 1
+    glo, ghi = W.gershgorin_bounds(ia, ja, a)
+    R.set_csr(ia, ja, a)
+    probes = O.seeded_normal(n * S["rspd2m_nvec"], S["rspd2m_pseed"]).reshape(S["rspd2m_nvec"], n)
+    iv = [glo + 0.3 * (ghi - glo), glo + 0.35 * (ghi - glo), glo, ghi]
+    rc, mu, ec = R.kpmdos(S["rspd2m_M"], 1, probes, iv)
+    assert rc == 0
+    out["rspd2m_intv"], out["rspd2m_mu"], out["rspd2m_ecnt"] = np.array(iv), mu, np.array([ec])
+    print(f"rspd2m: nnz {ia[-1]}, bounds [{glo:.3f}, {ghi:.3f}], ecnt {ec:.1f} ({time.time() - t:.0f} s)",
+          flush=True)
+    np.savez_compressed(os.path.join(OUT, "evsl_ref_golden_scale.npz"), **out)
+    print("wrote", os.path.join(OUT, "evsl_ref_golden_scale.npz"), "keys:", len(out))
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "scale":
+        main_scale()
+    else:
+        main()

@@ -112,3 +112,43 @@ def test_cheb_si_edge_cases(gpu_lib):
     lam, Y, res = gpu_lib.cheb_si(4, [9.0, 10.0, 0.0, 8.0], 50, 1e-8, V0, pol)
     assert len(lam) == 0
     gpu_lib.free_pol(pol)
+
+
+@pytest.mark.parametrize("mode", ["persistent", "wave"])
+def test_bounded_waits_time_out_and_library_recovers(gpu_lib, mode):
+    """Failure path of the device-side waits: with a wait limit of one poll,
+    the grid barriers of the single-launch filter (or the dependency waits of
+    the pipelined filter) give up; the call returns EVSLX_ERR_TIMEOUT (-105),
+    every block leaves, and afterwards -- default limits restored -- the
+    same filter gives the reference's vector bit for bit."""
+    import evsl_b200 as E
+
+    ia, ja, a = O.lap_csr(60, 50, 40)
+    n = len(ia) - 1
+    iv = [0.6, 1.2, 0.0, 12.0]
+    v = O.seeded_normal(n, 3)
+    y_ref = O.cheb_av(O.find_pol(iv, deg=40), ia, ja, a, v)
+    gpu_lib.set_csr(ia, ja, a)
+    pol = gpu_lib.find_pol(iv, deg=40)
+    on = (gpu_lib.set_filter_persistent if mode == "persistent" else gpu_lib.set_filter_wave)
+    try:
+        on(True)
+        gpu_lib.set_wait_limit(1)
+        codes = []
+        for _ in range(3):
+            try:
+                gpu_lib.chebav(pol, v)
+                codes.append(0)
+            except E.EvslError as e:
+                codes.append(-105 if "returned -105" in str(e) else str(e))
+                assert "within its bound" in gpu_lib.last_error()
+        assert -105 in codes, codes
+        assert all(c in (0, -105) for c in codes), codes
+        gpu_lib.set_wait_limit(0)
+        assert np.array_equal(gpu_lib.chebav(pol, v), y_ref)
+        on(False)
+        assert np.array_equal(gpu_lib.chebav(pol, v), y_ref)
+    finally:
+        gpu_lib.set_wait_limit(0)
+        on(False)
+        gpu_lib.free_pol(pol)

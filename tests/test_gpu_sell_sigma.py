@@ -1,0 +1,166 @@
+"""SELL-C-sigma storage and the general sparse matrices it is for.
+
+The random sparse SPD generator of the mixed-precision configuration (16
+seeded off-diagonal columns per row, symmetrised, diagonally dominant) gives
+rows of 18-54 entries; chunks of 32 consecutive rows then carry ~27% padding,
+and sorting the rows of each window by length (SELL-C-sigma) removes almost
+all of it.  The sort only moves rows between slots: every row keeps its CSR
+order, vectors keep the caller's order, so every filter and matvec result is
+bitwise the reference's CPU arithmetic (SRC/spmat.c:257-298 matvec_csr,
+SRC/chebpoly.c:519-598 ChebAv), whatever the window.
+
+Tolerances: bitwise for SpMV, ChebAv and the FP64 multi-column filter;
+FP32 filter 1e-4 relative to the FP64 result (degree 60); eigenvalues within
+1e-10 x spectral width (FP64) and 1e-8 x width (mixed) of the reference build's
+and the dense solver's, counts exact, residuals below tol.
+"""
+import numpy as np
+import pytest
+
+import evsl_b200 as E
+from evsl_b200 import workloads as W
+from oracle import evsl_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def rspd():
+    # 20,013 rows: not a multiple of 32 nor of any sort window
+    ia, ja, a = W.random_spd_csr(20013, 16, 33)
+    return ia, ja, a
+
+
+def _register(lib, sigma, ia, ja, a):
+    lib.set_sell_sigma(sigma)
+    try:
+        lib.set_csr(ia, ja, a)
+    finally:
+        lib.set_sell_sigma(-1)
+    return lib.matrix_sell_layout()
+
+
+def test_sigma_layout_choice(gpu_lib, rspd):
+    ia, ja, a = rspd
+    nnz = int(ia[-1])
+    sigma, stored, plain = _register(gpu_lib, -1, ia, ja, a)
+    assert sigma == 4096
+    assert plain > 1.2 * nnz and stored < 1.01 * nnz
+    sigma, stored0, plain0 = _register(gpu_lib, 0, ia, ja, a)
+    assert sigma == 0 and stored0 == plain0 == plain
+    # a Laplacian's chunks are already full: the automatic choice keeps them
+    sigma, stored, plain = _register(gpu_lib, -1, *O.lap_csr(17, 13, 11))
+    assert sigma == 0 and stored == plain
+    with pytest.raises(E.EvslError):
+        gpu_lib.set_sell_sigma(48)
+
+
+@pytest.mark.parametrize("sigma", [-1, 0, 32, 256, 2048])
+def test_sigma_spmv_and_filter_bitwise(gpu_lib, rspd, sigma):
+    ia, ja, a = rspd
+    n = len(ia) - 1
+    _register(gpu_lib, sigma, ia, ja, a)
+    x = O.seeded_normal(n, 5)
+    assert np.array_equal(gpu_lib.matvec(x), O.csr_matvec(ia, ja, a, x))
+    lo, hi = W.gershgorin_bounds(ia, ja, a)
+    iv = [lo + 0.3 * (hi - lo), lo + 0.33 * (hi - lo), lo, hi]
+    pol = gpu_lib.find_pol(iv, deg=60)
+    y_ref = O.cheb_av(O.find_pol(iv, deg=60), ia, ja, a, x)
+    try:
+        assert np.array_equal(gpu_lib.chebav(pol, x), y_ref)
+        # two rows per thread and the single-launch cooperative filter
+        gpu_lib.lib.evslx_set_filter_rows_per_thread(2)
+        assert np.array_equal(gpu_lib.chebav(pol, x), y_ref)
+        gpu_lib.lib.evslx_set_filter_rows_per_thread(1)
+        gpu_lib.set_filter_persistent(True)
+        assert np.array_equal(gpu_lib.chebav(pol, x), y_ref)
+        gpu_lib.set_filter_persistent(False)
+        # the multi-column filter: FP64 bitwise per column, FP32 close
+        X = np.stack([x, O.seeded_normal(n, 6), O.seeded_normal(n, 7)])
+        Y64 = gpu_lib.chebav_multi([pol] * 3, X, E.PREC_FP64)
+        assert np.array_equal(Y64[0], y_ref)
+        for c in (1, 2):
+            assert np.array_equal(Y64[c], O.cheb_av(O.find_pol(iv, deg=60), ia, ja, a, X[c]))
+        Y32 = gpu_lib.chebav_multi([pol] * 3, X, E.PREC_MIXED)
+        assert np.max(np.abs(Y32 - Y64)) <= 1e-4 * np.max(np.abs(Y64))
+    finally:
+        gpu_lib.lib.evslx_set_filter_rows_per_thread(1)
+        gpu_lib.set_filter_persistent(False)
+        gpu_lib.free_pol(pol)
+
+
+def test_sigma_irregular_and_empty_rows(gpu_lib):
+    """Rows of 0..70 entries (empty rows included), int16 column offsets
+    and float values (compressed storage) and the plain forms, every sort
+    window: the matvec and the filter stay bitwise."""
+    rng = np.random.default_rng(12)
+    n = 3001
+    rows = []
+    for r in range(n):
+        k = 0 if r % 17 == 0 else 1 + (r * 37) % 70
+        c = np.unique(np.clip(r + rng.integers(-3000, 3000, k), 0, n - 1)) if k else np.zeros(0, np.int64)
+        rows.append((c, rng.integers(-8, 9, len(c)).astype(np.float64)))
+    ia = np.zeros(n + 1, dtype=np.int32)
+    ia[1:] = np.cumsum([len(c) for c, _ in rows])
+    ja = np.concatenate([c for c, _ in rows]).astype(np.int32)
+    a = np.concatenate([v for _, v in rows])
+    x = O.seeded_normal(n, 8)
+    iv = [0.1, 0.3, -600.0, 600.0]
+    y_ref = O.cheb_av(O.find_pol(iv, deg=25), ia, ja, a, x)
+    for comp in (True, False):
+        gpu_lib.set_matrix_compression(comp)
+        try:
+            for sigma in (-1, 0, 32, 4096):
+                got, stored, plain = _register(gpu_lib, sigma, ia, ja, a)
+                assert got == sigma if sigma >= 0 else got in (0, 4096)
+                assert stored <= plain or got == sigma
+                assert gpu_lib.matrix_storage() == ((4, 2) if comp else (8, 4))
+                assert np.array_equal(gpu_lib.matvec(x), O.csr_matvec(ia, ja, a, x)), (comp, sigma)
+                pol = gpu_lib.find_pol(iv, deg=25)
+                assert np.array_equal(gpu_lib.chebav(pol, x), y_ref), (comp, sigma)
+                gpu_lib.free_pol(pol)
+        finally:
+            gpu_lib.set_matrix_compression(True)
+
+
+@pytest.fixture(scope="module")
+def golden_scale():
+    import os
+
+    return np.load(os.path.join(os.path.dirname(__file__), "golden", "evsl_ref_golden_scale.npz"))
+
+
+def test_cheblan_nr_random_spd_matches_reference(gpu_lib, golden_scale):
+    """ChebLanNr on a 20,000-row matrix of the random SPD generator (the
+    mixed-precision configuration's matrix at reduced size), 50 eigenvalues
+    from the 1000th up, against the reference build fed the same start
+    vector and the dense solver's eigenvalues: FP64 drop-in path (SELL-C-sigma
+    storage) and the mixed-precision engine (FP32 filter, FP64 refinement)."""
+    G = golden_scale
+    ia, ja, a = W.random_spd_csr(int(G["rspd_n"]), 16, int(G["rspd_seed"]))
+    n = len(ia) - 1
+    iv = list(G["rspd_intv"])
+    width = iv[3] - iv[2]
+    exact = G["rspd_exact"]
+    sigma, _, _ = _register(gpu_lib, -1, ia, ja, a)
+    assert sigma == 4096
+    pol = gpu_lib.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2)
+    assert pol.deg == int(G["rspd_deg"][0])
+    v = O.seeded_normal(n, int(G["rspd_vseed"]))
+    lam, Y, res = gpu_lib.cheblan_nr(iv, 3000, 1e-8, v, pol, want_vectors=False)
+    lam = np.sort(lam)
+    assert len(lam) == len(exact) == len(G["rspd_lam"])
+    assert np.max(np.abs(lam - G["rspd_lam"])) <= 1e-10 * width
+    assert np.max(np.abs(lam - exact)) <= 1e-10 * width
+    assert np.all(res < 1e-8)
+    gpu_lib.set_mixed_min_rows(0)
+    try:
+        (lam2, Y2, res2), = gpu_lib.cheblan_nr_batch([iv], 3000, 1e-8, v, [pol], precision=E.PREC_MIXED,
+                                                    want_vectors=False)
+    finally:
+        gpu_lib.set_mixed_min_rows(131072)
+    lam2 = np.sort(lam2)
+    assert len(lam2) == len(exact)
+    assert np.max(np.abs(lam2 - exact)) <= 1e-8 * width
+    assert np.all(res2 < 1e-8)
+    gpu_lib.free_pol(pol)

@@ -36,12 +36,9 @@ def _kpm(lib, fn, Mdeg, damping, nvec, intv, dprobes):
     return rc, mu, ec.value
 
 
-def test_noalloc_kpm_matches_allocating_entry_point(gpu_lib):
-    ia, ja, a = O.lap_csr(30, 30, 4)
-    gpu_lib.set_csr(ia, ja, a)
-    n = len(ia) - 1
-    nvec, Mdeg, intv = 24, 120, [0.8, 2.5, 0.0, 12.0]
-    probes = O.seeded_rademacher(nvec, n, 13)
+def _check_twice(gpu_lib, nvec, Mdeg, intv, seed):
+    n = gpu_lib.n
+    probes = O.seeded_rademacher(nvec, n, seed)
     dprobes = evsl_b200.DeviceBuffer.from_host(gpu_lib.lib, probes)
     rc, mu_ref, ec_ref = _kpm(gpu_lib.lib, gpu_lib.lib.evslx_kpmdos_probes, Mdeg, 1, nvec, intv, dprobes)
     assert rc == 0, gpu_lib.last_error()
@@ -50,6 +47,37 @@ def test_noalloc_kpm_matches_allocating_entry_point(gpu_lib):
         assert rc == 0, gpu_lib.last_error()
         assert np.max(np.abs(mu - mu_ref)) <= 1e-12 * np.max(np.abs(mu_ref))
         assert abs(ec - ec_ref) <= 1e-10 * abs(ec_ref)
+
+
+@pytest.mark.parametrize("nvec", [24, 64, 100, 128])
+def test_noalloc_kpm_matches_allocating_entry_point(gpu_lib, nvec):
+    """Up to 32, 64 and 128 probes per launch (the three kernel forms)."""
+    ia, ja, a = O.lap_csr(30, 30, 4)
+    gpu_lib.set_csr(ia, ja, a)
+    _check_twice(gpu_lib, nvec, 120, [0.8, 2.5, 0.0, 12.0], 13)
+
+
+def test_noalloc_kpm_just_under_its_scratch(gpu_lib):
+    """The largest 2-D grid whose scratch need fits the fixed array at 128
+    probes: it runs and matches; one row more per column is rejected."""
+    need = gpu_lib.lib.evslcu_kpm_noalloc_need
+    need.argtypes = [C.c_int, C.c_int, C.c_int]
+    need.restype = C.c_size_t
+    cap_fn = gpu_lib.lib.evslcu_kpm_noalloc_capacity
+    cap_fn.restype = C.c_size_t
+    cap = cap_fn()
+    nx, Mdeg, nvec = 100, 60, 128
+    ny = max(k for k in range(1, 200) if need(nx * k, Mdeg, nvec) <= cap)
+    assert need(nx * ny, Mdeg, nvec) > 0.98 * cap and need(nx * (ny + 1), Mdeg, nvec) > cap
+    ia, ja, a = O.lap_csr(nx, ny, 1)
+    gpu_lib.set_csr(ia, ja, a)
+    _check_twice(gpu_lib, nvec, Mdeg, [0.8, 2.5, 0.0, 8.0], 14)
+    ia, ja, a = O.lap_csr(nx, ny + 1, 1)
+    gpu_lib.set_csr(ia, ja, a)
+    dprobes = evsl_b200.DeviceBuffer(gpu_lib.lib, 8 * nx * (ny + 1) * nvec)
+    rc, mu, ec = _kpm(gpu_lib.lib, gpu_lib.lib.evslx_kpmdos_probes_noalloc, Mdeg, 1, nvec, [0.8, 2.5, 0.0, 8.0],
+                      dprobes)
+    assert rc != 0 and "scratch" in gpu_lib.last_error()
 
 
 def test_noalloc_kpm_rejects_sizes_beyond_its_scratch(gpu_lib):
