@@ -709,7 +709,7 @@ def run_rspd_filter(args):
         clocks = sampler.stop()
         t = statistics.median(per)
         launches = args.steps * (p_hi.deg + p_lo.deg + 4)
-        kernel = "k_mf_step<float,1>"
+        kernel = "k_mf_panel<float>" if lib.tuned_filter_variant(E.PREC_MIXED, 1) == 6 else "k_mf_step<float,1>"
         lib.free_pol(p_lo)
     else:
         p_hi = lib.find_pol(iv, deg=400)
@@ -724,7 +724,7 @@ def run_rspd_filter(args):
         clocks = sampler.stop()
         lib.filter_profile(False)
         t = sec / launches
-        kernel = "k_cheb"
+        kernel = "k_cheb_panel" if lib.filter_kernel()[0] == 7 else "k_cheb"
     peak, kind = measured_peak_hbm()
     gbs = abytes / t / 1e9
     traffic = profiled_traffic(kernel, "rspd-filter-" + ("fp32" if fp32 else "fp64"))
@@ -736,7 +736,10 @@ def run_rspd_filter(args):
         "config": {"workload": "rspd-filter: %s filter, degree %d, random sparse SPD n=%d, nnz=%d"
                                % ("FP32" if fp32 else "FP64", p_hi.deg, n, nnz),
                    "storage": {"sigma": sigma, "stored_slots": stored, "stored_slots_unsorted": stored_plain,
-                               "padding": stored / nnz - 1.0},
+                               "padding": stored / nnz - 1.0,
+                               "panel_layout": dict(zip(("rows_per_block", "panel_width", "bytes"),
+                                                        lib.matrix_panel_layout(fp32)))},
+                   "kernel_times_us": (lib.filter_kernel()[1] if not fp32 else None),
                    "us_per_degree": 1e6 * t, "algorithmic_bytes_per_degree": abytes,
                    "generate_s": round(gen_s, 1), "bounds": [glo, ghi]},
         "roofline": {"bound": "hbm", "kernel": kernel, "achieved": gbs, "peak": peak, "peak_kind": kind,

@@ -267,6 +267,8 @@ def load():
         "evslx_matrix_storage": ([_ip, _ip], C.c_int),
         "evslx_set_sell_sigma": ([C.c_int], C.c_int),
         "evslx_set_wait_limit": ([C.c_ulonglong], C.c_int),
+        "evslx_set_panel_filter": ([C.c_int, C.c_int], C.c_int),
+        "evslx_matrix_panel_layout": ([C.c_int, _ip, _ip, C.POINTER(C.c_longlong)], C.c_int),
         "evslx_matrix_sell_layout": ([_ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
         "evslx_read_coo_MM": ([C.c_char_p, C.c_int, C.c_int, C.POINTER(CooMat)], C.c_int),
         "evslx_coo_to_csr_device": ([C.c_int, C.POINTER(CooMat), C.c_int, C.POINTER(CsrMat)], C.c_int),
@@ -558,7 +560,7 @@ class Library:
         return int(self.lib.evslx_row_pattern_count())
 
     FILTER_KERNELS = ("sell-loop", "sell-unrolled", "pattern-global-unrolled", "pattern-global-loop",
-                      "pattern-constant-loop", "pattern-constant-unrolled", "pattern-constant-rowdesc")
+                      "pattern-constant-loop", "pattern-constant-unrolled", "pattern-constant-rowdesc", "panel")
 
     def set_filter_kernel(self, variant):
         """Force a single-vector filter kernel (index or name), or -1/None for timed selection."""
@@ -570,9 +572,9 @@ class Library:
 
     def filter_kernel(self):
         """(chosen variant or -1, {variant name: measured us per degree step}) of the registered matrix."""
-        us = (C.c_double * 7)()
+        us = (C.c_double * 8)()
         v = int(self.lib.evslx_filter_kernel(us))
-        return v, {self.FILTER_KERNELS[i]: us[i] for i in range(7) if us[i] > 0}
+        return v, {self.FILTER_KERNELS[i]: us[i] for i in range(8) if us[i] > 0}
 
     def filter_kernel_grid(self):
         """Blocks per degree step chosen with the filter kernel (0: one row per thread)."""
@@ -595,6 +597,17 @@ class Library:
     def set_wait_limit(self, polls):
         """Polls before a device-side wait gives up (0: the defaults)."""
         self._check(self.lib.evslx_set_wait_limit(int(polls)), "evslx_set_wait_limit")
+
+    def set_panel_filter(self, on, min_rows=0):
+        """Build (default) or skip the column-panel layout of large general matrices."""
+        self._check(self.lib.evslx_set_panel_filter(1 if on else 0, int(min_rows)), "evslx_set_panel_filter")
+
+    def matrix_panel_layout(self, fp32=False):
+        """(rows per block, panel width, device bytes) of the panel layout (zeros if none)."""
+        r, w, b = C.c_int(), C.c_int(), C.c_longlong()
+        self._check(self.lib.evslx_matrix_panel_layout(1 if fp32 else 0, C.byref(r), C.byref(w), C.byref(b)),
+                    "evslx_matrix_panel_layout")
+        return r.value, w.value, b.value
 
     def set_sell_sigma(self, sigma):
         """SELL-C-sigma row sort window for matrices registered afterwards: -1

@@ -135,8 +135,10 @@ struct Split {
 // (0..3, SELL-32), or the row-pattern dictionary with 16- or 32-byte parts
 // (4, 5).  -1: each matrix uses the variant the autotuner measured fastest
 // for it (per precision and block width); 0..5: that variant everywhere.
+// Variant 6: one column on the column-panel layout (panel.cu), x staged
+// through shared memory; built for large general matrices.
 static int g_mf_variant = -1;
-constexpr int kMfVariants = 6;
+constexpr int kMfVariants = 7;
 
 // One degree of the recurrence for all columns: thread (row r, part q)
 // handles columns q*CPT .. q*CPT+CPT-1 of row r.  Rows run over the padded
@@ -379,6 +381,9 @@ int mf_step(const evslcu_mat *M, const SellT<AV, IT> &A, int variant, int k, con
     case 1: return mf_step_v<VT, B, 32, false>(A, k, vk, vkm1, out, y, coef);
     case 2: return mf_step_v<VT, B, 16, true>(A, k, vk, vkm1, out, y, coef);
     case 3: return mf_step_v<VT, B, 32, true>(A, k, vk, vkm1, out, y, coef);
+    case 6:
+      if constexpr (B == 1) return panel_mf_step<VT>(M, k, vk, vkm1, out, y, coef);
+      return fail(EVSLCU_ERR_ARG, "filter variant 6 takes one column");
     case 4:
     case 5:
       if (!mf_pattern_ok(M)) return fail(EVSLCU_ERR_ARG, "filter variant %d needs the row-pattern dictionary", variant);
@@ -561,9 +566,12 @@ int autotune(evslcu_mat *A, int fp32, int B) {
   cudaEventCreate(&e1);
   float best = 1e30f;
   int bestv = 0;
+  if (B == 1 && panel_candidate(A) && !(fp32 ? A->pn32 : A->pn64) && panel_build(A, fp32))
+    cudaGetLastError();  // without the panel layout the SELL kernels serve
   for (int v = 0; !rc && v < kMfVariants; ++v) {
     if (g_mf_variant >= 0 && v != g_mf_variant) continue;  // a forced variant is only timed
-    if (v >= 4 && !mf_pattern_ok(A)) continue;
+    if ((v == 4 || v == 5) && !mf_pattern_ok(A)) continue;
+    if (v == 6 && !(B == 1 && (fp32 ? A->pn32 : A->pn64))) continue;
     float ms = 0.0f;
     for (int rep = 0; !rc && rep < 2; ++rep) {
       cudaEventRecord(e0, stream());
@@ -787,7 +795,7 @@ int evslcu_filter_plan_run(evslcu_filter_plan *P, const double *const *x, double
 int evslcu_filter_plan_columns(const evslcu_filter_plan *P) { return P ? P->ncols : 0; }
 
 int evslcu_set_filter_variant(int v) {
-  if (v < -1 || v >= kMfVariants) return fail(EVSLCU_ERR_ARG, "filter variant must be -1 (tuned) or 0..5");
+  if (v < -1 || v >= kMfVariants) return fail(EVSLCU_ERR_ARG, "filter variant must be -1 (tuned) or 0..6");
   g_mf_variant = v;
   return 0;
 }

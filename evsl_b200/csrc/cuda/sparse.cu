@@ -914,7 +914,7 @@ int evslcu::chebav_user_matvec(const evslcu_op *op, const double *mu, int deg, d
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr int kChebVariants = 7;
+constexpr int kChebVariants = 8;
 int g_cheb_force = -1;
 
 bool cheb_variant_ok(const evslcu_mat *A, int v) {
@@ -929,6 +929,7 @@ bool cheb_variant_ok(const evslcu_mat *A, int v) {
     case 4: return pconst;
     case 5: return pconst && unroll_width(A->pat_maxlen) > 0;
     case 6: return pconst && A->pat_desc;
+    case 7: return A->pn64 != nullptr;
     default: return false;
   }
 }
@@ -952,6 +953,11 @@ int launch_variant(const evslcu_mat *A, int v, bool first, bool epi, const doubl
       if (A->pat_f32)
         return launch_cheb_step(pat_pview(A), n, wmax, first, epi, vk, vkm1, out, y, t, ncc, s, mu0, ep);
       return launch_cheb_step(pat_view(A), n, wmax, first, epi, vk, vkm1, out, y, t, ncc, s, mu0, ep);
+    }
+    case 7: {
+      const bool e = epi && ep;
+      return panel_cheb_step(A, first, e, vk, vkm1, out, y, t, ncc, s, mu0, e ? ep->zold : nullptr,
+                             e ? ep->nbeta : 0.0, e ? ep->dotv : nullptr, e ? ep->dot_out : nullptr);
     }
     case 6:
       if (A->pat_f32)
@@ -988,7 +994,7 @@ float time_variant(const evslcu_mat *A, int v, int g, double *scr, cudaEvent_t e
 // Times every allowed variant on zero-filled scratch vectors and keeps the
 // fastest in A->cheb_variant, then its best grid limit in A->cheb_grid.
 int tune_cheb(evslcu_mat *A) {
-  static const int pref[kChebVariants] = {4, 6, 2, 3, 1, 0, 5};
+  static const int pref[kChebVariants] = {4, 6, 2, 3, 1, 0, 5, 7};
   int fallback = 0;
   for (int v : pref)
     if (cheb_variant_ok(A, v)) {
@@ -999,6 +1005,8 @@ int tune_cheb(evslcu_mat *A) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(stream(), &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return fallback;
   const int n = A->n;
+  // large general matrices also get the column-panel layout, timed with the rest
+  if (panel_candidate(A) && !A->pn64 && panel_build(A, 0)) cudaGetLastError();  // without it the SELL kernels serve
   double *scr = (double *)evslcu_malloc(sizeof(double) * 3 * (size_t)n);
   if (!scr) return fallback;
   int best = fallback;
@@ -1042,6 +1050,10 @@ int tune_cheb(evslcu_mat *A) {
 int cheb_variant(const evslcu_mat *A_) {
   evslcu_mat *A = const_cast<evslcu_mat *>(A_);
   if (A->kernel != 0) return -1;
+  if (g_cheb_force == 7 && panel_candidate(A) && !A->pn64) {
+    const int prc = panel_build(A, 0);
+    if (prc) return prc;
+  }
   if (g_cheb_force >= 0) return cheb_variant_ok(A, g_cheb_force) ? g_cheb_force : -2;
   if (A->cheb_variant >= 0 && cheb_variant_ok(A, A->cheb_variant)) return A->cheb_variant;
   const int v = tune_cheb(A);
@@ -1223,6 +1235,7 @@ void evslcu_mat_destroy(evslcu_mat *M) {
   evslcu_free(M->cptr);
   evslcu_free(M->cw);
   evslcu_free(M->perm);
+  panel_free(M);
   evslcu_mat_l2_persist(M, 0);
   evslcu_free(M->sell_block);
   evslcu_free(M->wave_ctl);

@@ -19,6 +19,8 @@
 //   ifmt 1: columns stored as int16 offsets from the row (|col-row| < 32768).
 // Every variant multiplies in FP64 in the same order, so results are
 // identical bit for bit across variants.
+struct evslcu_panels;  // column-panel layout (panel.cu)
+
 struct evslcu_mat {
   int n = 0;
   long long nnz = 0;
@@ -65,8 +67,10 @@ struct evslcu_mat {
   int pat_chdr = -1;   // first header there
   unsigned *pat_desc = nullptr;  // per row: (first pool entry << 8) | count, when in the pool
   int use_pat = 0;     // 1: the FP64 single-vector filter and SpMV read the dictionary
+  evslcu_panels *pn64 = nullptr;  // column-panel layout for the FP64 kernels (large general matrices)
+  evslcu_panels *pn32 = nullptr;  // the same for the FP32 kernels
   int cheb_variant = -1;      // single-vector filter kernel chosen by timing (-1: not yet)
-  float cheb_us[7] = {0, 0, 0, 0, 0, 0, 0};  // measured time per degree step of each variant
+  float cheb_us[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // measured time per degree step of each variant
   int cheb_grid = 0;                      // tuned block limit per degree step (0: one row per thread)
   float cheb_best_us = 0.0f;              // time per degree step of the chosen variant and grid
 };
@@ -397,6 +401,17 @@ inline int with_view(const evslcu_mat *A, F &&f) {
   if (A->vfmt == 1 && A->ifmt == 0) return f(sell_view<float, int>(A));
   return f(sell_view<float, short>(A));
 }
+
+// Column-panel layout (panel.cu): x staged through shared memory panel by
+// panel, for large matrices whose gathers miss every cache line.
+bool panel_candidate(const evslcu_mat *M);
+int panel_build(evslcu_mat *M, int fp32);
+void panel_free(evslcu_mat *M);
+int panel_cheb_step(const evslcu_mat *M, bool first, bool epi, const double *vk, const double *vkm1, double *out,
+                    double *y, double t, double ncc, double s, double mu0, const double *zold, double nbeta,
+                    const double *dotv, double *dout);
+template <class VT>
+int panel_mf_step(const evslcu_mat *M, int k, const VT *vk, const VT *vkm1, VT *out, VT *y, const VT *coef);
 
 // Wait limit of the pipelined filter's dependency waits (0: default).
 void set_wave_wait_limit(unsigned long long polls);

@@ -494,11 +494,18 @@ int evslx_set_filter_kernel(int variant) { return from_cu(evslcu_set_cheb_varian
 int evslx_filter_kernel_grid(void) { return evslh.mat ? evslcu_mat_cheb_grid(evslh.mat) : 0; }
 
 int evslx_filter_kernel(double *us) {
-  float f[7] = {0, 0, 0, 0, 0, 0, 0};
+  float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const int v = evslh.mat ? evslcu_mat_cheb_variant(evslh.mat, f) : -1;
   if (us)
-    for (int i = 0; i < 7; ++i) us[i] = f[i];
+    for (int i = 0; i < 8; ++i) us[i] = f[i];
   return v;
+}
+
+int evslx_set_panel_filter(int on, int min_rows) { return from_cu(evslcu_set_panels(on, min_rows)); }
+
+int evslx_matrix_panel_layout(int fp32, int *rows_per_block, int *panel_width, long long *bytes) {
+  if (!evslh.mat) return evsl_seterr(EVSLX_ERR_STATE, "no registered CSR matrix");
+  return from_cu(evslcu_mat_panel_layout(evslh.mat, fp32, rows_per_block, panel_width, bytes));
 }
 
 int evslx_set_l2_resident(int on) {

@@ -169,15 +169,34 @@ int evslx_row_pattern_count(void);
  * fastest; 0..6 forces one: 0/1 SELL-32 with looped/unrolled row products,
  * 2/3 pattern table in global memory unrolled/looped, 4/5 pattern table in
  * constant memory looped/unrolled, 6 constant-memory table addressed by a
- * 4-byte descriptor per row (2-6 need the row-pattern dictionary, 4-6 its
- * table in the constant pool; filtering fails with EVSLX_ERR_ARG when the
- * forced variant is not available).  Every variant gives the same result
+ * 4-byte descriptor per row, 7 the column-panel layout (2-6 need the
+ * row-pattern dictionary, 4-6 its table in the constant pool, 7 the panel
+ * layout; filtering fails with EVSLX_ERR_ARG when the forced variant is not
+ * available).  Every variant gives the same result
  * bit for bit. */
 int evslx_set_filter_kernel(int variant);
 /* The registered matrix's chosen variant (-1: not chosen yet) and, when us is
- * not NULL, us[0..6] = measured microseconds per degree step of each variant
- * timed (0: not timed). */
+ * not NULL, us[0..7] = measured microseconds per degree step of each variant
+ * timed (0: not timed).  Variant 7 is the column-panel kernel (see
+ * evslx_set_panel_filter). */
 int evslx_filter_kernel(double *us);
+/* Column-panel filter for large general sparse matrices (no counterpart in
+ * the reference, whose SpMV is the CSR matvec SRC/spmat.c:257-298 or
+ * cuSPARSE, :529-621).  On a matrix whose rows have unequal lengths (SELL-C-
+ * sigma sorted) and at least min_rows rows (default 2^18), the first filter
+ * call also builds a layout in which each thread block owns a block of rows
+ * and walks the columns in panels: each panel of x is copied into shared
+ * memory and the block's entries in that panel are multiplied from there, so
+ * the random gathers read shared memory instead of one cache line each.
+ * Every row is still summed left to right in CSR order: results are
+ * bitwise those of the other FP64 kernels.  The timing-based kernel choice
+ * (single vector: variant 7; multi-column filter at one column: variant 6)
+ * uses it where it is faster.  on = 0 stops building it; min_rows <= 0 keeps
+ * the current minimum. */
+int evslx_set_panel_filter(int on, int min_rows);
+/* The registered matrix's panel layout for the FP64 (fp32 = 0) or FP32
+ * kernels: rows per block, panel width and device bytes (zeros if none). */
+int evslx_matrix_panel_layout(int fp32, int *rows_per_block, int *panel_width, long long *bytes);
 /* Blocks per degree step chosen with that variant (0: one row per thread;
  * otherwise rows go round a grid-stride loop of that many blocks). */
 int evslx_filter_kernel_grid(void);

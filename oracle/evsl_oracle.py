@@ -1201,6 +1201,61 @@ def kpm_raw_dots(Mdeg, probes, intv, ia, ja, a):
     return out
 
 
+def kpm_raw_dots_exact(Mdeg, probes, intv, ia, ja, a):
+    """kpm_raw_dots with each dot product (T_{k+1}(A~) v_m) . v_m of the
+    reference's FP64 vectors accumulated in extended precision (numpy
+    longdouble: 64-bit significand products and sums) and rounded once: the
+    dots of the reference's own recurrence without the rounding error of a
+    sequential FP64 sum over n terms (SRC/spslice.c:101-125 forms them with
+    one FP64 ddot per degree)."""
+    lmin, lmax = intv[2], intv[3]
+    ctr = (lmax + lmin) / 2.0
+    wid = (lmax - lmin) / 2.0
+    probes = np.atleast_2d(probes)
+    out = np.zeros((Mdeg, probes.shape[0]))
+    for m, p in enumerate(probes):
+        v = p * (1.0 / np.linalg.norm(p))
+        vl = v.astype(np.longdouble)
+        vk = v.copy()
+        vkm1 = np.zeros_like(v)
+        for k in range(Mdeg):
+            vkp1 = csr_matvec(ia, ja, a, vk)
+            scal = (1.0 if k == 0 else 2.0) / wid
+            vkp1 = vkp1 + (-ctr) * vk
+            vkp1 = scal * vkp1
+            vkp1 = vkp1 + (-1.0) * vkm1
+            vkm1, vk = vk, vkp1
+            out[k, m] = float(np.sum(vk.astype(np.longdouble) * vl))
+    return out
+
+
+def kpm_moments_from_dots(Mdeg, damping, n, intv, dots):
+    """The accumulation of kpmdos (SRC/spslice.c:101-148) from raw dots
+    (Mdeg x nvec), in the reference's probe-major order."""
+    lmin, lmax = intv[2], intv[3]
+    aa = max(intv[0], lmin)
+    bb = min(intv[1], lmax)
+    ctr = (lmax + lmin) / 2.0
+    wid = (lmax - lmin) / 2.0
+    beta1 = math.acos(max(-1.0 + DBL_EPS, (aa - ctr) / wid))
+    beta2 = math.acos(min(1.0 - DBL_EPS, (bb - ctr) / wid))
+    jac = dampcf(Mdeg, damping)
+    jac[0] = 1.0
+    mu = np.zeros(Mdeg + 1)
+    tcnt = 0.0
+    nvec = dots.shape[1]
+    for m in range(nvec):
+        mu[0] += jac[0]
+        tcnt -= jac[0] * (beta2 - beta1)
+        for k in range(Mdeg):
+            k1 = k + 1
+            t = 2 * jac[k1] * float(dots[k, m])
+            mu[k1] += t
+            tcnt -= t * (math.sin(k1 * beta2) - math.sin(k1 * beta1)) / k1
+    t = 1.0 / (nvec * np.pi)
+    return mu * t, tcnt * t * n
+
+
 def kpm_raw_dots_identities(Mdeg, probes, intv, ia, ja, a):
     """The same raw KPM products through the Chebyshev product identities
     (T_2k = 2 T_k^2 - T_0, T_2k+1 = 2 T_k+1 T_k - T_1): with w_j = T_j(A~) v,

@@ -4,6 +4,7 @@ reference sources).  Run from the repository root:
 
     python tests/golden/make_golden.py          # evsl_ref_golden.npz
     python tests/golden/make_golden.py scale    # evsl_ref_golden_scale.npz
+    python tests/golden/make_golden.py scale-exact   # (re)adds its exact-dot KPM moments
 
 Every input is seeded; probe and start vectors are injected into the
 reference through its rand_double_device hook (oracle/ref_hooks.c).  The
@@ -240,6 +241,38 @@ def main():
     print("wrote", os.path.join(OUT, "evsl_ref_golden.npz"), "keys:", len(out))
 
 
+def _exact_dots_worker(args):
+    Mdeg, probes, intv, dims = args
+    ia, ja, a = O.lap_csr(*dims)
+    return O.kpm_raw_dots_exact(Mdeg, probes, intv, ia, ja, a)
+
+
+def main_scale_exact():
+    """Adds to the scale fixtures the KPM moments of the 3-D Laplacian 100^3
+    case computed from the reference's own FP64 recurrence with every dot
+    product accumulated in extended precision (oracle kpm_raw_dots_exact):
+    the reference's moments without the rounding of its sequential FP64 dot
+    over 10^6 terms, which for Rademacher probes (equal |v_i|) is systematic
+    and reaches ~1.5e-12 of max |mu|."""
+    import multiprocessing as mp
+
+    path = os.path.join(OUT, "evsl_ref_golden_scale.npz")
+    out = dict(np.load(path))
+    S = SCALE
+    dims = S["kpm100_dims"]
+    n = dims[0] * dims[1] * dims[2]
+    probes = O.seeded_rademacher(S["kpm100_nvec"], n, S["kpm100_seed"])
+    jobs = [(S["kpm100_M"], probes[m:m + 1], list(S["kpm100_intv"]), dims) for m in range(S["kpm100_nvec"])]
+    with mp.get_context("spawn").Pool(6) as pool:
+        dots = np.concatenate(pool.map(_exact_dots_worker, jobs), axis=1)
+    mu, ec = O.kpm_moments_from_dots(S["kpm100_M"], 1, n, list(S["kpm100_intv"]), dots)
+    out["kpm100_mu_exactdot"], out["kpm100_ecnt_exactdot"] = mu, np.array([ec])
+    ref = out["kpm100_mu"]
+    print("reference vs exact-dot moments: normwise %.2e" % (np.max(np.abs(ref - mu)) / np.max(np.abs(mu))))
+    np.savez_compressed(path, **out)
+    print("wrote", path, "keys:", len(out))
+
+
 def main_scale():
     import time
 
@@ -309,5 +342,8 @@ def main_scale():
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "scale":
         main_scale()
+        main_scale_exact()
+    elif len(sys.argv) > 1 and sys.argv[1] == "scale-exact":
+        main_scale_exact()
     else:
         main()

@@ -15,6 +15,15 @@ Bars: ||mu - mu_ref||_inf <= 1e-12 ||mu_ref||_inf (normwise), and per moment
 level of the dot products, |mu_ref,k| >= 1e-3 ||mu_ref||_inf (below it the
 reference's own sequential dots carry errors of that relative size);
 ecnt 1e-10 relative.  Both errors are printed.
+
+For the Rademacher probes on 10^6 rows the reference's own moments are off
+by ~1.5e-12 of max |mu|: every probe entry has the same magnitude, so the
+rounding of its sequential FP64 dot over 10^6 terms is systematic.  That
+case is therefore judged against the moments of the reference's own FP64
+recurrence with every dot accumulated in extended precision (the
+`exactdot` fixture): the library must be within the bars of those, and its
+distance to the reference's printed moments must not exceed the reference's
+own distance to them by more than 1e-13 of max |mu|.
 """
 import os
 
@@ -51,12 +60,17 @@ def test_kpm_config2_settings_match_reference(gpu_lib, G, doubling):
         mu, ec = gpu_lib.kpmdos_probes(int(G["kpm100_M"]), 1, probes, list(G["kpm100_intv"]))
     finally:
         gpu_lib.lib.evslcu_set_kpm_doubling(1)
-    ref = G["kpm100_mu"]
-    normwise, rel, nbig = _moment_errors(mu, ref)
-    print(f"kpm 100^3 ({'product identities' if doubling else 'direct dots'}): normwise {normwise:.2e}, "
-          f"per-moment relative {rel:.2e} over {nbig} of {len(ref)} moments")
+    ref, exact = G["kpm100_mu"], G["kpm100_mu_exactdot"]
+    normwise, rel, nbig = _moment_errors(mu, exact)
+    ref_norm, ref_rel, _ = _moment_errors(ref, exact)
+    print(f"kpm 100^3 ({'product identities' if doubling else 'direct dots'}) vs exact-dot moments: normwise "
+          f"{normwise:.2e}, per-moment relative {rel:.2e} over {nbig} of {len(ref)} moments; the reference "
+          f"itself: {ref_norm:.2e} / {ref_rel:.2e}; library vs reference {_moment_errors(mu, ref)[0]:.2e}")
     assert normwise <= 1e-12
     assert rel <= 1e-12
+    scale = np.max(np.abs(exact))
+    assert np.max(np.abs(mu - ref)) <= np.max(np.abs(ref - exact)) + 1e-13 * scale
+    assert abs(ec - G["kpm100_ecnt_exactdot"][0]) <= 1e-10 * abs(G["kpm100_ecnt_exactdot"][0])
     assert abs(ec - G["kpm100_ecnt"][0]) <= 1e-10 * abs(G["kpm100_ecnt"][0])
 
 

@@ -105,7 +105,7 @@ def test_sigma_irregular_and_empty_rows(gpu_lib):
     ja = np.concatenate([c for c, _ in rows]).astype(np.int32)
     a = np.concatenate([v for _, v in rows])
     x = O.seeded_normal(n, 8)
-    iv = [0.1, 0.3, -600.0, 600.0]
+    iv = [-50.0, 50.0, -600.0, 600.0]
     y_ref = O.cheb_av(O.find_pol(iv, deg=25), ia, ja, a, x)
     for comp in (True, False):
         gpu_lib.set_matrix_compression(comp)
@@ -164,3 +164,63 @@ def test_cheblan_nr_random_spd_matches_reference(gpu_lib, golden_scale):
     assert np.max(np.abs(lam2 - exact)) <= 1e-8 * width
     assert np.all(res2 < 1e-8)
     gpu_lib.free_pol(pol)
+
+
+@pytest.mark.parametrize("case", ["rspd", "irregular"])
+def test_panel_filter_bitwise(gpu_lib, rspd, case):
+    """The column-panel kernels (x staged through shared memory panel by
+    panel), built here on small matrices by lowering their row threshold:
+    several row blocks and panels, odd n (unaligned Lanczos basis columns),
+    empty rows.  FP64: the single-vector kernel (variant 7) and the
+    multi-column kernel at one column (variant 6) give the reference's
+    filtered vector bit for bit, and ChebLanNr gives the same eigenvalues bit
+    for bit as with the SELL kernel; FP32 agrees to 1e-4."""
+    if case == "rspd":
+        ia, ja, a = rspd
+    else:
+        rng = np.random.default_rng(21)
+        n = 6007
+        rows = []
+        for r in range(n):
+            k = 0 if r % 13 == 0 else 1 + (r * 29) % 45
+            c = np.unique(rng.integers(0, n, k)) if k else np.zeros(0, np.int64)
+            c = np.unique(np.concatenate([c, [r]])) if k else c
+            rows.append((c, np.where(c == r, 60.0, rng.uniform(-1, 1, len(c)))))
+        ia = np.zeros(n + 1, dtype=np.int32)
+        ia[1:] = np.cumsum([len(c) for c, _ in rows])
+        ja = np.concatenate([c for c, _ in rows]).astype(np.int32)
+        a = np.concatenate([v for _, v in rows])
+    n = len(ia) - 1
+    lo, hi = W.gershgorin_bounds(ia, ja, a)
+    iv = [lo + 0.3 * (hi - lo), lo + 0.34 * (hi - lo), lo, hi]
+    x = O.seeded_normal(n, 9)
+    y_ref = O.cheb_av(O.find_pol(iv, deg=40), ia, ja, a, x)
+    gpu_lib.set_panel_filter(True, 1000)
+    try:
+        for variant in (7, 0):
+            gpu_lib.set_filter_kernel(variant)
+            _register(gpu_lib, 256, ia, ja, a)
+            pol = gpu_lib.find_pol(iv, deg=40)
+            y = gpu_lib.chebav(pol, x)
+            assert np.array_equal(y, y_ref), (variant, np.max(np.abs(y - y_ref)))
+            if variant == 7:
+                R, Wd, nbytes = gpu_lib.matrix_panel_layout(False)
+                assert R > 0 and 0 < Wd < n and nbytes > 0, (R, Wd)
+                lam7 = gpu_lib.cheblan_nr(iv, 600, 1e-8, x, pol, want_vectors=False)[0]
+            else:
+                lam0 = gpu_lib.cheblan_nr(iv, 600, 1e-8, x, pol, want_vectors=False)[0]
+            gpu_lib.free_pol(pol)
+        assert len(lam7) > 0 and np.array_equal(lam7, lam0)
+        gpu_lib.set_filter_kernel(-1)
+        pol = gpu_lib.find_pol(iv, deg=40)
+        gpu_lib.set_filter_variant(6)
+        Y64 = gpu_lib.chebav_multi([pol], x[None, :], E.PREC_FP64)
+        assert np.array_equal(Y64[0], y_ref)
+        Y32 = gpu_lib.chebav_multi([pol], x[None, :], E.PREC_MIXED)
+        assert gpu_lib.matrix_panel_layout(True)[0] > 0
+        assert np.max(np.abs(Y32[0] - y_ref)) <= 1e-4 * np.max(np.abs(y_ref))
+        gpu_lib.free_pol(pol)
+    finally:
+        gpu_lib.set_filter_variant(-1)
+        gpu_lib.set_filter_kernel(-1)
+        gpu_lib.set_panel_filter(True, 1 << 18)
