@@ -673,6 +673,8 @@ def run_rspd_filter(args):
     nnz = int(ia[-1])
     lib = E.Library()
     lib.set_sell_sigma(args.sigma)
+    lib.set_filter_kernel(None if args.filter_kernel == "auto" else args.filter_kernel)
+    lib.set_filter_variant(args.variant)
     lib.set_csr(ia, ja, a)
     del ja, a
     sigma, stored, stored_plain = lib.matrix_sell_layout()

@@ -267,7 +267,7 @@ def load():
         "evslx_matrix_storage": ([_ip, _ip], C.c_int),
         "evslx_set_sell_sigma": ([C.c_int], C.c_int),
         "evslx_set_wait_limit": ([C.c_ulonglong], C.c_int),
-        "evslx_set_panel_filter": ([C.c_int, C.c_int], C.c_int),
+        "evslx_set_panel_filter": ([C.c_int, C.c_int, C.c_int], C.c_int),
         "evslx_matrix_panel_layout": ([C.c_int, _ip, _ip, C.POINTER(C.c_longlong)], C.c_int),
         "evslx_matrix_sell_layout": ([_ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
         "evslx_read_coo_MM": ([C.c_char_p, C.c_int, C.c_int, C.POINTER(CooMat)], C.c_int),
@@ -598,9 +598,10 @@ class Library:
         """Polls before a device-side wait gives up (0: the defaults)."""
         self._check(self.lib.evslx_set_wait_limit(int(polls)), "evslx_set_wait_limit")
 
-    def set_panel_filter(self, on, min_rows=0):
+    def set_panel_filter(self, on, min_rows=0, max_width=0):
         """Build (default) or skip the column-panel layout of large general matrices."""
-        self._check(self.lib.evslx_set_panel_filter(1 if on else 0, int(min_rows)), "evslx_set_panel_filter")
+        self._check(self.lib.evslx_set_panel_filter(1 if on else 0, int(min_rows), int(max_width)),
+                    "evslx_set_panel_filter")
 
     def matrix_panel_layout(self, fp32=False):
         """(rows per block, panel width, device bytes) of the panel layout (zeros if none)."""

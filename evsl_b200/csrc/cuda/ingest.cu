@@ -556,11 +556,11 @@ int build_patterns_device(evslcu_mat *M) {
   return 0;
 }
 
-// Window of the SELL-C-sigma length sort: -1 automatic (kSigmaAuto rows
+// Window of the SELL-C-sigma length sort: -1 automatic (g_sigma_auto rows
 // when the plain layout pads more than kSigmaTrigger times the entries),
 // 0 never, otherwise that window (a power of two from 32 to 4096) always.
 int g_sell_sigma = -1;
-constexpr int kSigmaAuto = 4096;
+int g_sigma_auto = 256;
 constexpr double kSigmaTrigger = 1.10;
 
 int launch_sigma_sort(int n, int sigma, const int *ia, int *perm) {
@@ -628,7 +628,7 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
   // SELL-C-sigma: sort the rows of each window by length when the chunks of
   // the plain layout carry much padding, and keep the order when it cuts
   // the stored slots by at least 5%.
-  const int sigma = g_sell_sigma < 0 ? kSigmaAuto : g_sell_sigma;
+  const int sigma = g_sell_sigma < 0 ? g_sigma_auto : g_sell_sigma;
   const bool try_sort = sigma > 0 && (g_sell_sigma > 0 || (double)padded > kSigmaTrigger * (double)std::max(M->nnz, 1LL));
   if (!rc && try_sort) {
     int *perm = (int *)evslcu_malloc(sizeof(int) * 32 * (size_t)nch);

@@ -289,9 +289,10 @@ int evslcu_set_cheb_max_grid(int blocks);
 /* A's chosen variant (-1: not chosen yet) and, in us[0..6], the measured
  * microseconds per degree step of each variant timed (0: not timed). */
 int evslcu_mat_cheb_variant(const evslcu_mat *A, float *us);
-/* Column-panel layout for large general matrices (panel.cu): on/off and the
- * fewest rows for which it is built (0 keeps the current minimum, 2^18). */
-int evslcu_set_panels(int on, int min_rows);
+/* Column-panel layout for large general matrices (panel.cu): on/off, the
+ * fewest rows for which it is built (0 keeps the current minimum, 2^18) and
+ * the widest panel tried (0 keeps the current width, 16384 columns). */
+int evslcu_set_panels(int on, int min_rows, int max_width);
 /* Rows per block, panel width and device bytes of the matrix's panel layout
  * for the FP64 (fp32 = 0) or FP32 kernels (zeros when not built). */
 int evslcu_mat_panel_layout(const evslcu_mat *A, int fp32, int *rows_per_block, int *panel_width,

@@ -501,7 +501,9 @@ int evslx_filter_kernel(double *us) {
   return v;
 }
 
-int evslx_set_panel_filter(int on, int min_rows) { return from_cu(evslcu_set_panels(on, min_rows)); }
+int evslx_set_panel_filter(int on, int min_rows, int max_width) {
+  return from_cu(evslcu_set_panels(on, min_rows, max_width));
+}
 
 int evslx_matrix_panel_layout(int fp32, int *rows_per_block, int *panel_width, long long *bytes) {
   if (!evslh.mat) return evsl_seterr(EVSLX_ERR_STATE, "no registered CSR matrix");

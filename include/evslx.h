@@ -185,15 +185,18 @@ int evslx_filter_kernel(double *us);
  * cuSPARSE, :529-621).  On a matrix whose rows have unequal lengths (SELL-C-
  * sigma sorted) and at least min_rows rows (default 2^18), the first filter
  * call also builds a layout in which each thread block owns a block of rows
- * and walks the columns in panels: each panel of x is copied into shared
- * memory and the block's entries in that panel are multiplied from there, so
- * the random gathers read shared memory instead of one cache line each.
+ * and walks the columns in panels: each panel of x and the block's entries in
+ * it are copied into shared memory by TMA bulk copies through a multi-stage
+ * ring (a producer warp runs ahead of the warps that multiply), so the random
+ * gathers read shared memory instead of one cache line each.
  * Every row is still summed left to right in CSR order: results are
  * bitwise those of the other FP64 kernels.  The timing-based kernel choice
  * (single vector: variant 7; multi-column filter at one column: variant 6)
  * uses it where it is faster.  on = 0 stops building it; min_rows <= 0 keeps
- * the current minimum. */
-int evslx_set_panel_filter(int on, int min_rows);
+ * the current minimum; max_width > 0 caps the panel width (columns, at least
+ * 512; default 16384), max_width <= 0 keeps the current cap.  Applies to
+ * layouts built afterwards. */
+int evslx_set_panel_filter(int on, int min_rows, int max_width);
 /* The registered matrix's panel layout for the FP64 (fp32 = 0) or FP32
  * kernels: rows per block, panel width and device bytes (zeros if none). */
 int evslx_matrix_panel_layout(int fp32, int *rows_per_block, int *panel_width, long long *bytes);
