@@ -241,7 +241,7 @@ int evslcu_set_wait_limit(unsigned long long polls);
  * created afterwards.  Default on. */
 int evslcu_set_compression(int on);
 /* Row order of the SELL copy: -1 automatic (rows sorted by length inside
- * windows of 4096 when that cuts the padded slots), 0 never, or a window (a
+ * windows of 256 when that cuts the padded slots), 0 never, or a window (a
  * power of two from 32 to 4096) always.  Matrices registered afterwards. */
 int evslcu_set_sell_sigma(int sigma);
 /* The sort window in use (0: rows in their original order) and the stored

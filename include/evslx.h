@@ -121,7 +121,7 @@ int evslx_set_matrix_compression(int on);
 /* SELL-C-sigma row order of the stored matrix (C = 32).  sigma -1 (default):
  * when the chunks of 32 consecutive rows would carry more than 10% padding
  * (rows of unequal length, as in general sparse matrices), the rows of each
- * window of 4096 consecutive rows are sorted by length before they are cut
+ * window of 256 consecutive rows are sorted by length before they are cut
  * into chunks, and the sorted order is kept when it stores at least 5% fewer
  * slots; 0: never sort; a power of two from 32 to 4096: always sort with that
  * window.  Vectors stay in the caller's row order and every row is summed in
