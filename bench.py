@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--count", type=int, default=COUNT)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve", "lap3d-multifilter",
-                                          "lap3d-reorth", "lap3d-kpm", "rspd-filter"],
+                                          "lap3d-reorth", "lap3d-kpm", "rspd-filter", "dgemm"],
                    default="lap3d-slice",
                    help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark); "
                         "lap3d-batch: several slices through the request engine; serve: a Poisson request stream")
@@ -77,6 +77,8 @@ def parse():
     p.add_argument("--rspd-n", type=int, default=RSPD_N, help="rspd-filter: rows of the random SPD matrix")
     p.add_argument("--sigma", type=int, default=-1,
                    help="rspd-filter: SELL-C-sigma sort window (-1 automatic, 0 unsorted SELL-32)")
+    p.add_argument("--gemm", default="1000000,1000,256",
+                   help="dgemm: n,K,m of the Ritz product V(n x K) Y(K x m)")
     p.add_argument("--ncols", type=int, default=16, help="lap3d-multifilter: columns")
     p.add_argument("--variant", type=int, default=-1, help="lap3d-multifilter: kernel variant (-1 autotuned)")
     p.add_argument("--sweep", action="store_true", help="lap3d-multifilter: every variant/width/precision once")
@@ -780,6 +782,69 @@ def run_rspd_filter(args):
     lib.free_pol(p_hi)
 
 
+def run_dgemm(args):
+    """dgemm: the FP64 Ritz product U = V(:, 1:K) Y of ChebLanNr
+    (SRC/cheblanNr.c:333-399) through evsl_dgemm_device, V n x K and Y K x m
+    column-major, device-resident seeded operands.  Device time per GEMM from
+    CUDA events on the library stream, median of K steps; FP64 TFLOP/s =
+    2 n K m / time, against the FP64 peak measured on this GPU by the
+    library's probe (FMA chains and mma.sync f64 chains in registers)."""
+    import ctypes as C
+
+    import torch
+
+    import evsl_b200 as E
+
+    n, K, m = (int(x) for x in args.gemm.split(","))
+    lib = E.Library()
+    lib.lib.evslcu_fp64_probe.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    dfma, dmma = C.c_double(), C.c_double()
+    lib._check(lib.lib.evslcu_fp64_probe(C.byref(dfma), C.byref(dmma)), "evslcu_fp64_probe")
+    peak = max(dfma.value, dmma.value)
+    g = torch.Generator(device="cuda").manual_seed(SEED)
+    V = torch.randn(K, n, dtype=torch.float64, device="cuda", generator=g)  # column-major n x K
+    Y = torch.randn(m, K, dtype=torch.float64, device="cuda", generator=g)  # column-major K x m
+    U = torch.zeros(m, n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    lstream = torch.cuda.ExternalStream(lib.stream_handle())
+    ci = lambda v: C.byref(C.c_int(v))  # noqa: E731
+    cd = lambda v: C.byref(C.c_double(v))  # noqa: E731
+
+    def gemm():
+        lib.lib.evsl_dgemm_device(b"N", b"N", ci(n), ci(m), ci(K), cd(1.0), C.c_void_p(V.data_ptr()), ci(n),
+                                  C.c_void_p(Y.data_ptr()), ci(K), cd(0.0), C.c_void_p(U.data_ptr()), ci(n))
+
+    for _ in range(args.warmup):
+        gemm()
+    sampler = ClockSampler(rank_info()[2])
+    sampler.start()
+    times = []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lstream)
+        gemm()
+        e1.record(lstream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    clocks = sampler.stop()
+    t = statistics.median(times)
+    tf = 2.0 * n * K * m / t / 1e12
+    # spot check of one output column against torch
+    j = m // 2
+    err = (U[j] - V.t() @ Y[j]).abs().max().item() / max(1e-300, (V.t() @ Y[j]).abs().max().item())
+    print(json.dumps({
+        "metric": "FP64 GEMM TFLOP/s (Ritz product)", "value": tf, "unit": "TFLOP/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded normal operands)",
+        "config": {"workload": "dgemm: U = V(:,1:K) Y, n=%d K=%d m=%d" % (n, K, m), "check_rel_err": err},
+        "roofline": {"bound": "fp64", "kernel": "k_dgemm_nn128", "achieved": tf, "peak": peak,
+                     "peak_kind": "measured on this GPU (FMA %.1f, mma.sync f64 %.1f TFLOP/s)" % (dfma.value,
+                                                                                               dmma.value),
+                     "unit": "TFLOP/s", "frac": tf / peak},
+        "clocks": clocks}))
+
+
 def run_multifilter(args):
     """lap3d-multifilter: the multi-column filter kernel alone on the 3-D
     Laplacian 100^3, `--ncols` columns with the slice request's polynomial
@@ -1215,6 +1280,8 @@ def main():
         run_kpm(args)
     elif args.workload == "rspd-filter":
         run_rspd_filter(args)
+    elif args.workload == "dgemm":
+        run_dgemm(args)
     else:
         run_ours(args)
 

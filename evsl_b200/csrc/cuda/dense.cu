@@ -239,6 +239,127 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// ---------------------------------------------------------------------------
+// GEMM C = alpha A B + beta C (A m x k, B k x n, column-major) for the Ritz
+// vectors V(:, 1:K) Y and the other tall products: 128 x 128 tiles, 16-deep
+// k slices double-buffered in shared memory by cp.async, 256 threads in 8
+// warps of 64 x 32, 8 x 8 accumulators per thread, FP64 FMA.  Each C entry
+// is the FMA chain over k = 0, 1, ... from 0, then alpha acc (+ beta C), as
+// k_dgemm computes it, so both kernels give the same bits.  Needs A, B and
+// their leading dimensions 16-byte aligned (the caller checks).
+//
+// Thread (lane l of warp w): warp tile rows 64 (w % 2) .. +63, columns
+// 32 (w / 2) .. +31; the thread's rows are 2 (l % 8) + 16 q + {0, 1}
+// (q = 0..3) and its columns l / 8 + 4 j (j = 0..7), so that a warp's
+// shared-memory reads of A (16-byte pairs) and of B (one double per column,
+// B tile rows padded to 18 doubles) fall in distinct banks.
+// ---------------------------------------------------------------------------
+constexpr int GT = 128, GK = 16, GKP = 18;  // tile, k slice, padded B row (doubles)
+constexpr size_t kGemmSmem = 2 * (size_t)(GK * GT + GT * GKP) * sizeof(double);
+
+__device__ __forceinline__ void cpa16(void *dst, const void *src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cpa8(void *dst, const void *src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+// A pair of doubles into 16-byte aligned shared memory: one 16-byte copy
+// when the source pair is 16-byte aligned (AL), else two 8-byte copies.
+// bytes: 16 (both in range), 8 (only the first), 0 (neither; zero fill).
+template <bool AL>
+__device__ __forceinline__ void cp_pair(double *dst, const double *src, const double *base, int bytes) {
+  if (AL) {
+    cpa16(dst, bytes ? src : base, bytes);
+  } else {
+    cpa8(dst, bytes ? src : base, bytes >= 8 ? 8 : 0);
+    cpa8(dst + 1, bytes == 16 ? src + 1 : base, bytes == 16 ? 8 : 0);
+  }
+}
+
+template <bool A16, bool B16>
+__global__ void __launch_bounds__(256, 1)
+    k_dgemm_nn128(int m, int n, int k, double alpha, const double *__restrict__ A, long long lda,
+                  const double *__restrict__ B, long long ldb, double beta, double *C, long long ldc) {
+  extern __shared__ __align__(16) double gsm[];
+  // stage st: A slice at gsm + st GK GT ([k][m]); B slice at gsm + 2 GK GT + st GT GKP ([n][k])
+  double *const sA0 = gsm;
+  double *const sB0 = gsm + 2 * GK * GT;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int m0 = blockIdx.x * GT, n0 = blockIdx.y * GT;
+  const int wm = 64 * (warp & 1), wn = 32 * (warp >> 1);
+  const int tx = lane & 7, ty = lane >> 3;
+  auto load = [&](int st, int k0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = tid + 256 * i;
+      // A: k row kk = c / 64, pair p = c % 64 -> rows m0 + 2p, +1
+      const int kk = c >> 6, pa = c & 63;
+      const int gr = m0 + 2 * pa, gk = k0 + kk;
+      int bytes = 0;
+      if (gk < k) bytes = (gr + 1 < m) ? 16 : ((gr < m) ? 8 : 0);
+      cp_pair<A16>(sA0 + st * (GK * GT) + kk * GT + 2 * pa, A + (long long)gk * lda + gr, A, bytes);
+      // B: column nn = c / 8, pair q = c % 8 -> k0 + 2q, +1
+      const int nn = c >> 3, q = c & 7;
+      const int gc = n0 + nn, gk2 = k0 + 2 * q;
+      int bb = 0;
+      if (gc < n) bb = (gk2 + 1 < k) ? 16 : ((gk2 < k) ? 8 : 0);
+      cp_pair<B16>(sB0 + st * (GT * GKP) + nn * GKP + 2 * q, B + (long long)gc * ldb + gk2, B, bb);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  const int nk = (k + GK - 1) / GK;
+  load(0, 0);
+  for (int t = 0; t < nk; ++t) {
+    const int st = t & 1;
+    if (t + 1 < nk) {
+      load(st ^ 1, (t + 1) * GK);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    const double *a_s = sA0 + st * (GK * GT) + wm + 2 * tx;
+    const double *b_s = sB0 + st * (GT * GKP) + (wn + ty) * GKP;
+#pragma unroll
+    for (int kk = 0; kk < GK; ++kk) {
+      double a[8], b[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double2 v = *reinterpret_cast<const double2 *>(a_s + kk * GT + 16 * q);
+        a[2 * q] = v.x;
+        a[2 * q + 1] = v.y;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = b_s[4 * j * GKP + kk];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int gn = n0 + wn + ty + 4 * j;
+    if (gn >= n) continue;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int gm = m0 + wm + 2 * tx + 16 * (i >> 1) + (i & 1);
+      if (gm < m) {
+        double *c = C + (long long)gn * ldc + gm;
+        *c = (beta == 0.0) ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*c);
+      }
+    }
+  }
+}
+
 // C = sum over slabs of part (slab stride m*n, ld m) scaled: C = S + beta C
 __global__ void k_splitk_reduce(int m, int n, int slabs, const double *part, double beta, double *C, long long ldc) {
   const long long total = (long long)m * n;
@@ -420,11 +541,107 @@ int evslcu_dgemv(char trans, int m, int n, double alpha, const double *A, long l
   return 0;
 }
 
+// FP64 throughput probe (the roofline's FP64 peak): chains of FMA on each
+// thread, and chains of mma.sync m8n8k4 f64 on each warp, registers only;
+// every thread writes one value so the work is kept.  out: blocks x 256.
+__global__ void __launch_bounds__(256) k_probe_dfma(int iters, double seed, double *out) {
+  double a[8];
+  const double b = seed * 0.5 + 1.0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) a[i] = seed + i;
+  for (int it = 0; it < iters; ++it)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = fma(a[i], b, 1e-9);
+  double s = 0.0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) s += a[i];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(256) k_probe_dmma(int iters, double seed, double *out) {
+  double c[8][2];
+  const double a = seed + threadIdx.x * 1e-3, b = seed - threadIdx.x * 1e-3;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) c[i][0] = c[i][1] = 0.0;
+  for (int it = 0; it < iters; ++it)
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                   : "+d"(c[i][0]), "+d"(c[i][1])
+                   : "d"(a), "d"(b));
+  double s = 0.0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) s += c[i][0] + c[i][1];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+static int g_dgemm_tiled = 1;
+
+int evslcu_fp64_probe(double *dfma_tflops, double *dmma_tflops) {
+  const int blocks = 4 * sm_count(), iters = 1 << 14;
+  double *out = (double *)evslcu_malloc(sizeof(double) * (size_t)blocks * 256);
+  if (!out) return EVSLCU_ERR_NOMEM;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float ms[2] = {0.f, 0.f};
+  int rc = 0;
+  for (int rep = 0; rep < 2 && !rc; ++rep)
+    for (int which = 0; which < 2 && !rc; ++which) {
+      cudaEventRecord(e0, stream());
+      if (which == 0)
+        k_probe_dfma<<<blocks, 256, 0, stream()>>>(iters, 1.0, out);
+      else
+        k_probe_dmma<<<blocks, 256, 0, stream()>>>(iters, 1.0, out);
+      count_launch();
+      cudaEventRecord(e1, stream());
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(EVSLCU_ERR_CUDA, "fp64 probe failed");
+      if (!rc) rc = check_launch("fp64 probe");
+      if (!rc) cudaEventElapsedTime(&ms[which], e0, e1);
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  evslcu_free(out);
+  if (rc) return rc;
+  const double threads = (double)blocks * 256;
+  if (dfma_tflops) *dfma_tflops = 2.0 * 8 * iters * threads / (ms[0] * 1e-3) / 1e12;
+  if (dmma_tflops) *dmma_tflops = 2.0 * 256 * 8 * iters * (threads / 32) / (ms[1] * 1e-3) / 1e12;
+  return 0;
+}
+
+int evslcu_set_dgemm_tiled(int on) {
+  g_dgemm_tiled = on ? 1 : 0;
+  return 0;
+}
+
 int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const double *A, long long lda,
                  const double *B, long long ldb, double beta, double *C, long long ldc) {
   if (m <= 0 || n <= 0) return 0;
   const bool TA = (ta == 'T' || ta == 't'), TB = (tb == 'T' || tb == 't');
   cudaStream_t st = stream();
+  // tall products (Ritz vectors V Y, block updates): the 128 x 128 kernel
+  if (!TA && !TB && g_dgemm_tiled && m >= 2 * GT && n >= 32 && k >= GK &&
+      ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 7) == 0) {
+    const bool a16 = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (lda & 1) == 0;
+    const bool b16 = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (ldb & 1) == 0;
+    auto go = [&](auto fn) -> int {
+      static bool smem_set[4] = {false, false, false, false};
+      const int idx = (a16 ? 2 : 0) + (b16 ? 1 : 0);
+      if (!smem_set[idx]) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+        if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "dgemm: shared memory limit: %s", cudaGetErrorString(e));
+        smem_set[idx] = true;
+      }
+      dim3 g((m + GT - 1) / GT, (n + GT - 1) / GT);
+      fn<<<g, 256, kGemmSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+      count_launch();
+      return check_launch("k_dgemm_nn128");
+    };
+    if (a16 && b16) return go(k_dgemm_nn128<true, true>);
+    if (a16) return go(k_dgemm_nn128<true, false>);
+    if (b16) return go(k_dgemm_nn128<false, true>);
+    return go(k_dgemm_nn128<false, false>);
+  }
   const int gm = (m + BM - 1) / BM, gn = (n + BN - 1) / BN;
   // Long inner dimension with few output tiles (V^T W): split K into slabs
   // computed in parallel, then summed in slab order (deterministic).

@@ -152,6 +152,12 @@ int evslcu_cgs_dgks(int n, int k, int imax, const double *Q, long long ldq, doub
 int evslcu_dgemv(char trans, int m, int n, double alpha, const double *A, long long lda,
                  const double *x, double beta, double *y);
 /* C = alpha * op(A) op(B) + beta * C, column-major; op = 'N' or 'T'. */
+/* 1 (default): tall no-transpose products with 16-byte aligned operands use
+ * the 128 x 128 tiled GEMM; 0: always the 64 x 64 kernel (same results). */
+int evslcu_set_dgemm_tiled(int on);
+/* FP64 throughput of this GPU (TFLOP/s): FMA chains per thread and
+ * mma.sync m8n8k4 f64 chains per warp, registers only (the FP64 roofline). */
+int evslcu_fp64_probe(double *dfma_tflops, double *dmma_tflops);
 int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const double *A,
                  long long lda, const double *B, long long ldb, double beta, double *C,
                  long long ldc);
