@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--count", type=int, default=COUNT)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve", "lap3d-multifilter",
-                                          "lap3d-reorth", "lap3d-kpm", "rspd-filter", "dgemm"],
+                                          "lap3d-reorth", "lap3d-kpm", "rspd-filter", "dgemm", "batch-uneven"],
                    default="lap3d-slice",
                    help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark); "
                         "lap3d-batch: several slices through the request engine; serve: a Poisson request stream")
@@ -77,6 +77,7 @@ def parse():
     p.add_argument("--rspd-n", type=int, default=RSPD_N, help="rspd-filter: rows of the random SPD matrix")
     p.add_argument("--sigma", type=int, default=-1,
                    help="rspd-filter: SELL-C-sigma sort window (-1 automatic, 0 unsorted SELL-32)")
+    p.add_argument("--instances", type=int, default=128, help="batch-uneven: independent Laplacians")
     p.add_argument("--gemm", default="1000000,1000,256",
                    help="dgemm: n,K,m of the Ritz product V(n x K) Y(K x m)")
     p.add_argument("--ncols", type=int, default=16, help="lap3d-multifilter: columns")
@@ -1029,6 +1030,139 @@ def _slice_plan(ev, start, nslices, count):
     return out
 
 
+def uneven_instances(count, seed=4, nmin=1e3, nmax=2e5):
+    """The batched-instances configuration: `count` independent 2-D / 3-D
+    Dirichlet Laplacians with n log-uniform in [nmin, nmax] (grid dims from
+    the seed), each with an interval of 20-80 eigenvalues of its analytic
+    spectrum starting at a seeded point of [0.3, 1.5], end points at gap
+    midpoints.  Returns a list of (dims, intv, exact eigenvalues)."""
+    from evsl_b200 import workloads as W
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        nn = int(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+        if i % 2 == 0:
+            s = max(int(round(np.sqrt(nn))), 10)
+            dims, hi = (s, s + i % 3, 1), 8.0
+        else:
+            s = max(int(round(nn ** (1 / 3))), 8)
+            dims, hi = (s, s + 1, s), 12.0
+        ev = W.laplacian_eigenvalues(*dims)
+        a0, b0, cnt = W.gap_interval(ev, float(rng.uniform(0.3, 1.5)), int(rng.integers(20, 81)))
+        out.append((dims, [a0, b0, 0.0, hi], ev[(ev >= a0) & (ev <= b0)]))
+    return out
+
+
+def run_batch_uneven(args):
+    """batch-uneven: `--instances` (default 128) independent Laplacians of
+    uneven size (n log-uniform in [10^3, 2*10^5]), each with its own interval
+    of 20-80 eigenvalues and its own find_pol degree, all submitted to one
+    request engine (one slot per instance: every tick filters all slots --
+    the slots of one matrix share multi-column launches, captured as CUDA
+    graphs -- and advances every slot's Lanczos step).  One step = the whole
+    batch; counts checked against the analytic spectra, residuals < tol.
+    --compare-sequential also times the FP64 drop-in ChebLanNr on the same
+    instances one after another."""
+    import torch
+
+    import evsl_b200 as E
+    from evsl_b200 import workloads as W
+
+    lib = E.Library()
+    inst = uneven_instances(args.instances)
+    mats, pols, vs = [], [], []
+    for i, (dims, iv, _) in enumerate(inst):
+        ia, ja, a = W.laplacian_csr(*dims)
+        mats.append(lib.matrix(ia, ja, a))
+        lib.set_csr(ia, ja, a)
+        pols.append(lib.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000))
+        v = np.random.default_rng(SEED + i).standard_normal(len(ia) - 1)
+        vs.append(v / np.linalg.norm(v))
+    prec = E.PREC_MIXED if args.precision == "mixed" else E.PREC_FP64
+    lstream = torch.cuda.ExternalStream(lib.stream_handle())
+    maxit = 1000
+
+    def one_batch():
+        eng = lib.engine(len(inst), precision=prec)
+        for i, (dims, iv, _) in enumerate(inst):
+            eng.submit_slice(mats[i], iv, pols[i], maxit, TOL, vs[i], i)
+        eng.run()
+        out = {}
+        while True:
+            r = eng.pop()
+            if r is None:
+                break
+            out[int(r["tag"])] = r
+        eng.free()
+        return out
+
+    for _ in range(args.warmup):
+        one_batch()
+    sampler = ClockSampler(rank_info()[2])
+    sampler.start()
+    launches0 = lib.launch_count()
+    times, found, ok, lat, max_err, max_res, bad = [], 0, True, [], 0.0, 0.0, []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lstream)
+        res = one_batch()
+        e1.record(lstream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+        for i, (dims, iv, exact) in enumerate(inst):
+            r = res[i]
+            good = r["rc"] == 0 and r["nev"] == len(exact) and bool(np.all(r["res"] < TOL))
+            if good:
+                err = float(np.max(np.abs(np.sort(r["lam"]) - exact)))
+                max_err = max(max_err, err)
+                max_res = max(max_res, float(np.max(r["res"])))
+                good = err <= 1e-8 * iv[3]
+            if not good:
+                bad.append({"instance": i, "dims": dims, "found": int(r["nev"]), "exact": int(len(exact))})
+            ok = ok and good
+            found += r["nev"]
+            lat.append(1e3 * (r["t_finish"] - r["t_submit"]))
+    launches = lib.launch_count() - launches0
+    clocks = sampler.stop()
+    t = sum(times)
+    seq = None
+    if args.compare_sequential:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        nseq, tseq = 0, 0.0
+        for i, (dims, iv, _) in enumerate(inst):
+            ia, ja, a = W.laplacian_csr(*dims)
+            lib.set_csr(ia, ja, a)
+            e0.record(lstream)
+            lam, _, _ = lib.cheblan_nr(iv, maxit, TOL, vs[i], pols[i], want_vectors=False)
+            e1.record(lstream)
+            e1.synchronize()
+            tseq += e0.elapsed_time(e1) / 1e3
+            nseq += len(lam)
+        seq = {"eigenpairs": nseq, "seconds": tseq, "eigenpairs_per_s": nseq / tseq,
+               "engine_speedup": (found / t) / (nseq / tseq)}
+    sizes = [int(np.prod(d)) for d, _, _ in inst]
+    print(json.dumps({
+        "metric": METRIC, "value": found / t, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 filter + f64" if prec == E.PREC_MIXED else "f64",
+        "data": "synthetic (2-D/3-D Dirichlet Laplacians, seeded sizes, intervals and start vectors)",
+        "config": {"workload": "batch-uneven: %d Laplacians, n log-uniform in [1e3, 2e5] (sum %d rows), 20-80 "
+                               "eigenvalues each, one engine, %s" % (len(inst), sum(sizes), args.precision),
+                   "filter_degrees": [int(p.deg) for p in pols], "n": sizes, "tol": TOL, "maxit": maxit},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "sequential_chebLanNr_same_instances": seq,
+        "accuracy": {"max_abs_eig_err_vs_analytic": max_err, "max_residual": max_res,
+                     "bar": "counts exact, |err| <= 1e-8 x width, residual < 1e-8", "failures": bad[:10]},
+        "all_steps_ok": bool(ok), "gpu_launches": int(launches), "clocks": clocks}))
+    for p in pols:
+        lib.free_pol(p)
+    for M in mats:
+        M.free()
+
+
 def run_batch(args):
     """lap3d-batch: `--slices` slices of `--count` eigenvalues above 0.6 on the
     3-D Laplacian 100^3 solved together by the request engine (one Lanczos
@@ -1282,6 +1416,8 @@ def main():
         run_rspd_filter(args)
     elif args.workload == "dgemm":
         run_dgemm(args)
+    elif args.workload == "batch-uneven":
+        run_batch_uneven(args)
     else:
         run_ours(args)
 
