@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--count", type=int, default=COUNT)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve", "lap3d-multifilter",
-                                          "lap3d-reorth", "lap3d-kpm", "rspd-filter", "dgemm", "batch-uneven"],
+                                          "lap3d-reorth", "lap3d-kpm", "rspd-filter", "dgemm", "batch-uneven", "rspd-kpm"],
                    default="lap3d-slice",
                    help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark); "
                         "lap3d-batch: several slices through the request engine; serve: a Poisson request stream")
@@ -968,6 +968,59 @@ def run_reorth(args):
     lib.free_pol(pol)
 
 
+def run_rspd_kpm(args):
+    """rspd-kpm: kpmdos on the 2-million-row random sparse SPD matrix with the
+    mixed-precision configuration's settings: 64 seeded Gaussian probes (drawn
+    on the host, normalised inside as the reference does), 500 moments,
+    Jackson damping, Gershgorin bounds; device time of the block recurrence
+    (CUDA events around the KPM kernels).  Algorithmic bytes per block step
+    as in lap3d-kpm (CSR 12 B per nonzero + 4 B per row, 3 probe vectors)."""
+    import ctypes as C
+
+    import evsl_b200
+    from evsl_b200 import workloads as W
+
+    n = args.rspd_n
+    ia, ja, a = W.random_spd_csr(n, 16, RSPD_SEED)
+    glo, ghi = W.gershgorin_bounds(ia, ja, a)
+    nnz = int(ia[-1])
+    lib = evsl_b200.Library()
+    lib.lib.evslx_last_kpm_seconds.restype = C.c_double
+    lib.set_csr(ia, ja, a)
+    del ja, a
+    B = args.kpm_probes if args.kpm_probes != 30 else 64
+    M = args.kpm_moments if args.kpm_moments != 300 else 500
+    probes = np.random.default_rng(RSPD_SEED).standard_normal((B, n))
+    iv = [glo + 0.3 * (ghi - glo), glo + 0.35 * (ghi - glo), glo, ghi]
+    for _ in range(args.warmup):
+        lib.kpmdos_probes(M, 1, probes, iv)
+    sampler = ClockSampler(rank_info()[2])
+    sampler.start()
+    secs = []
+    for _ in range(args.steps):
+        mu, ec = lib.kpmdos_probes(M, 1, probes, iv)
+        secs.append(lib.lib.evslx_last_kpm_seconds())
+    clocks = sampler.stop()
+    t = statistics.median(secs)
+    steps = (M + 1) // 2
+    abytes = steps * (12.0 * nnz + 4.0 * (n + 1) + 3 * 8.0 * n * B)
+    peak, kind = measured_peak_hbm()
+    gbs = abytes / t / 1e9
+    print(json.dumps({
+        "metric": "KPM moments/s", "value": M / t, "unit": "moments/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (random sparse SPD, seeded Gaussian probes)",
+        "config": {"workload": "rspd-kpm: kpmdos, %d probes, %d moments, random sparse SPD n=%d nnz=%d"
+                               % (B, M, n, nnz), "block_steps": steps, "us_per_block_step": 1e6 * t / steps,
+                   "ecount": ec},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "peak_kind": kind, "unit": "GB/s",
+                     "frac": gbs / peak, "algorithmic_bytes": abytes,
+                     "note": "every stored entry gathers 8 B per probe from a random row of the probe block "
+                             "(n x 32 x 8 B per launch = 512 MB, larger than L2): nnz x probes x 8 B of gather "
+                             "traffic per step on top of the formula's bytes"},
+        "clocks": clocks}))
+
+
 def run_kpm(args):
     """lap3d-kpm: kpmdos on the 3-D Laplacian 100^3 with the config-2
     settings (30 Rademacher probes, 300 moments, Jackson damping; `--kpm-probes`,
@@ -1418,6 +1471,8 @@ def main():
         run_dgemm(args)
     elif args.workload == "batch-uneven":
         run_batch_uneven(args)
+    elif args.workload == "rspd-kpm":
+        run_rspd_kpm(args)
     else:
         run_ours(args)
 
