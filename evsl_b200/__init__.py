@@ -296,6 +296,8 @@ def load():
         "evslx_engine_pop_result": ([C.c_void_p, C.POINTER(EvslxResult)], C.c_int),
         "evslx_result_free": ([C.POINTER(EvslxResult)], None),
         "evslx_engine_use_graphs": ([C.c_void_p, C.c_int], None),
+        "evslx_engine_use_batch": ([C.c_void_p, C.c_int, C.c_int], None),
+        "evslx_engine_batched_columns": ([C.c_void_p], C.c_uint64),
         "evslx_set_mixed_min_rows": ([C.c_int], None),
         "evslx_set_filter_variant": ([C.c_int], C.c_int),
         "evslx_set_l2_resident": ([C.c_int], C.c_int),
@@ -420,6 +422,12 @@ class Engine:
 
     def bytes_in_use(self):
         return self.lib.evslx_engine_bytes_in_use(self.ptr)
+
+    def use_batch(self, on, max_rows=0):
+        self.lib.evslx_engine_use_batch(self.ptr, 1 if on else 0, int(max_rows))
+
+    def batched_columns(self):
+        return int(self.lib.evslx_engine_batched_columns(self.ptr))
 
     def use_graphs(self, on):
         self.lib.evslx_engine_use_graphs(self.ptr, 1 if on else 0)

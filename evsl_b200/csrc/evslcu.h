@@ -183,6 +183,25 @@ typedef struct {
   const double *x;
   double *y;
 } evslcu_filter_col;
+/* One column of a batched filter over many matrices (mmfilter.cu): y =
+ * p(A) x with the polynomial's coefficients on the device (deg + 1) and a
+ * device workspace w of 2 n doubles. */
+typedef struct {
+  const evslcu_mat *A;
+  const double *mu;
+  int deg;
+  double cc, dd;
+  const double *x;
+  double *y;
+  double *w;
+} evslcu_batch_col;
+/* Device bytes of the batch's column table (ncols columns, total_rows rows). */
+size_t evslcu_filter_batch_table_bytes(int ncols, long long total_rows);
+/* Filters ncols columns of possibly different matrices, one launch per
+ * degree for all columns whose degree reaches it; each column's y equals
+ * ChebAv of that column bit for bit.  table: device memory of at least
+ * evslcu_filter_batch_table_bytes(...) bytes. */
+int evslcu_filter_batch(int ncols, const evslcu_batch_col *cols, void *table, size_t table_bytes);
 size_t evslcu_filter_columns_work(int n, int fp32, int ncols);
 int evslcu_filter_columns(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_col *cols, void *work,
                           size_t work_bytes);

@@ -66,6 +66,7 @@ typedef struct req_s {
   int maxit;
   double tol;
   double *vinit; /* device copy */
+  double *mu_dev; /* device copy of pol.mu (batched filters) */
   uint64_t seed;
   int Mdeg, damping, nvec;
   double t_submit;
@@ -86,6 +87,7 @@ typedef struct {
 typedef struct {
   req_t *req;
   double *V, *cgsw, *vrand;
+  double *bw; /* 2n recurrence workspace of the batched filter */
   double *dT, *eT, *EvalT;
   int k, phase, nwn, restarts;
   double beta, wn, tr0;
@@ -118,6 +120,13 @@ struct evslx_engine {
   int use_graphs;
   uint64_t ticks, plan_builds;
   uint64_t width_hist[5]; /* filter groups launched, by block width 1, 2, 4, 8, 16 */
+  /* batched filter: one-column FP64 groups of matrices with at most
+   * batch_max_rows rows, filtered together (one launch per degree) */
+  int use_batch, batch_max_rows;
+  evslcu_batch_col *bcols;
+  void *btab;
+  size_t btab_bytes;
+  uint64_t batched_columns;
 };
 
 /* ---------------------------------------------------------------------------
@@ -204,8 +213,11 @@ evslx_engine *evslx_engine_create(int max_slots, size_t hbm_budget, int precisio
   E->gstart = (int *)malloc(sizeof(int) * ((size_t)max_slots + 1));
   E->plans = (plan_cache_t *)calloc((size_t)max_slots, sizeof(plan_cache_t));
   E->use_graphs = 1;
+  E->use_batch = 1;
+  E->batch_max_rows = 1 << 18;
+  E->bcols = (evslcu_batch_col *)malloc(sizeof(evslcu_batch_col) * (size_t)max_slots);
   if (!E->slots || !E->ds || !E->hs || !E->cols || !E->colslot || !E->xs || !E->ys || !E->uidbuf || !E->plans ||
-      !E->gbest || !E->gcut || !E->gstart) {
+      !E->gbest || !E->gcut || !E->gstart || !E->bcols) {
     evsl_seterr(EVSLX_ERR_NOMEM, "evslx_engine_create: out of memory");
     evslx_engine_free(E);
     return NULL;
@@ -217,6 +229,7 @@ static void req_free(req_t *r) {
   if (!r) return;
   free(r->pol.mu);
   evslcu_free(r->vinit);
+  evslcu_free(r->mu_dev);
   free(r);
 }
 
@@ -224,6 +237,7 @@ static void slot_release(evslx_engine *E, slot_t *s) {
   evslcu_free(s->V);
   evslcu_free(s->cgsw);
   evslcu_free(s->vrand);
+  evslcu_free(s->bw);
   free(s->dT);
   free(s->eT);
   free(s->EvalT);
@@ -259,6 +273,8 @@ void evslx_engine_free(evslx_engine *E) {
   evslcu_free(E->ds);
   free(E->hs);
   evslcu_free(E->fwork);
+  evslcu_free(E->btab);
+  free(E->bcols);
   for (int i = 0; i < E->nplans; i++) {
     evslcu_filter_plan_destroy(E->plans[i].plan);
     free(E->plans[i].uids);
@@ -278,6 +294,14 @@ void evslx_engine_free(evslx_engine *E) {
 void evslx_engine_use_graphs(evslx_engine *E, int on) {
   if (E) E->use_graphs = on ? 1 : 0;
 }
+
+void evslx_engine_use_batch(evslx_engine *E, int on, int max_rows) {
+  if (!E) return;
+  E->use_batch = on ? 1 : 0;
+  if (max_rows > 0) E->batch_max_rows = max_rows;
+}
+
+uint64_t evslx_engine_batched_columns(const evslx_engine *E) { return E ? E->batched_columns : 0; }
 
 uint64_t evslx_engine_plan_builds(const evslx_engine *E) { return E ? E->plan_builds : 0; }
 
@@ -416,7 +440,7 @@ int evslx_engine_submit_slice(evslx_engine *E, evslx_matrix *M, const double *in
     req_free(r);
     return evsl_seterr(rc, "%s", evslcu_errstr());
   }
-  r->bytes = sizeof(double) * ((size_t)n * ((size_t)r->maxit + 3) + evslcu_cgs_work_size(n, r->maxit + 1));
+  r->bytes = sizeof(double) * ((size_t)n * ((size_t)r->maxit + 5) + evslcu_cgs_work_size(n, r->maxit + 1));
   r->t_submit = evsl_timer();
   r->uid = ++E->next_uid;
   enqueue(E, r);
@@ -542,12 +566,18 @@ static int admit(evslx_engine *E) {
     s->V = (double *)evslcu_malloc(sizeof(double) * (size_t)n * ((size_t)r->maxit + 1));
     s->cgsw = (double *)evslcu_malloc(sizeof(double) * evslcu_cgs_work_size(n, r->maxit + 1));
     s->vrand = (double *)evslcu_malloc(sizeof(double) * (size_t)n);
+    s->bw = (double *)evslcu_malloc(sizeof(double) * 2 * (size_t)n);
+    r->mu_dev = (double *)evslcu_malloc(sizeof(double) * ((size_t)r->pol.deg + 1));
+    if (r->mu_dev && evslcu_h2d(r->mu_dev, r->pol.mu, sizeof(double) * ((size_t)r->pol.deg + 1))) {
+      evslcu_free(r->mu_dev);
+      r->mu_dev = NULL;
+    }
     s->dT = (double *)malloc(sizeof(double) * (size_t)r->maxit);
     s->eT = (double *)malloc(sizeof(double) * (size_t)r->maxit);
     s->EvalT = (double *)malloc(sizeof(double) * (size_t)r->maxit);
     s->phase = PH_START;
     s->t_start = evsl_timer();
-    if (!s->V || !s->cgsw || !s->vrand || !s->dT || !s->eT || !s->EvalT) {
+    if (!s->V || !s->cgsw || !s->vrand || !s->bw || !r->mu_dev || !s->dT || !s->eT || !s->EvalT) {
       evslx_result out;
       memset(&out, 0, sizeof(out));
       out.tag = r->tag;
@@ -788,6 +818,11 @@ int evslx_engine_step(evslx_engine *E) {
    * captured multi-column filter. */
   for (int i = 0; i < E->nplans; i++) E->plans[i].used = 0;
   for (int i = 0; i < E->max_slots; i++) E->colslot[i] = -1;
+  int nbatch = 0;
+  long long batch_rows = 0;
+  evslx_matrix *batch_M = NULL;
+  evslcu_filter_col batch_col;
+  uint64_t batch_uid = 0;
   for (int i = 0; i < E->max_slots; i++) {
     slot_t *s0 = &E->slots[i];
     if (!s0->req || E->colslot[i] >= 0) continue;
@@ -831,6 +866,26 @@ int evslx_engine_step(evslx_engine *E) {
       E->uidbuf[b2 + 1] = uv;
     }
     if (fp32 && (rc = evslcu_mat_prepare_fp32(M->mat))) return evsl_seterr(rc, "%s", evslcu_errstr());
+    /* a lone FP64 column of a small matrix joins the batched filter: the
+     * columns of all such matrices advance one degree per launch together */
+    if (E->use_batch && nc == 1 && !fp32 && M->op.n <= E->batch_max_rows) {
+      slot_t *t = &E->slots[i];
+      evslcu_batch_col *b = &E->bcols[nbatch++];
+      b->A = M->mat;
+      b->mu = t->req->mu_dev;
+      b->deg = E->cols[0].deg;
+      b->cc = E->cols[0].cc;
+      b->dd = E->cols[0].dd;
+      b->x = E->cols[0].x;
+      b->y = E->cols[0].y;
+      b->w = t->bw;
+      batch_rows += M->op.n;
+      batch_M = M;
+      batch_col = E->cols[0];
+      batch_uid = E->uidbuf[0];
+      evslstat.n_polAv += nc;
+      continue;
+    }
     /* groups: contiguous runs of the degree-sorted columns chosen to minimise
      * sum over groups of (largest degree) x (measured time of one degree step
      * at that width) -- the autotuner's timings for this matrix */
@@ -883,6 +938,20 @@ int evslx_engine_step(evslx_engine *E) {
       if ((rc = run_group_filter(E, M, g1 - g0, E->cols + g0, E->uidbuf + g0, fp32))) return rc;
     }
     evslstat.n_polAv += nc;
+  }
+  if (nbatch == 1) {
+    /* a batch of one: the single-vector filter (its kernel tuned for the matrix) */
+    if ((rc = run_group_filter(E, batch_M, 1, &batch_col, &batch_uid, 0))) return rc;
+  } else if (nbatch > 1) {
+    const size_t need = evslcu_filter_batch_table_bytes(nbatch, batch_rows);
+    if (need > E->btab_bytes) {
+      evslcu_free(E->btab);
+      E->btab = evslcu_malloc(need);
+      E->btab_bytes = E->btab ? need : 0;
+      if (!E->btab) return evsl_seterr(EVSLX_ERR_NOMEM, "engine: out of device memory (batch table)");
+    }
+    if ((rc = evslcu_filter_batch(nbatch, E->bcols, E->btab, E->btab_bytes))) return evsl_seterr(rc, "%s", evslcu_errstr());
+    E->batched_columns += (uint64_t)nbatch;
   }
   /* drop the captured filters no group used in this tick */
   for (int i = 0; i < E->nplans;) {

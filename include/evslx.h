@@ -299,6 +299,17 @@ void evslx_set_mixed_min_rows(int rows);
 /* Filters run as captured CUDA graphs, rebuilt when the set of requests on
  * a matrix changes (default on); plan_builds counts the captures. */
 void evslx_engine_use_graphs(evslx_engine *E, int on);
+/* Batched filter of the engine (default on, max_rows 2^18): every tick, the
+ * lone FP64 columns of matrices with at most max_rows rows (independent
+ * instances, small serving requests) are filtered together, one launch per
+ * degree for all of them, instead of one launch per degree per matrix; each
+ * column's result is bit for bit the single-vector filter's.  max_rows <= 0
+ * keeps the current limit.  No counterpart in the reference, whose drivers
+ * solve slices one after another (TESTS/PLanR/MMPLanR_omp.c:183-241 runs
+ * them on OpenMP threads). */
+void evslx_engine_use_batch(evslx_engine *E, int on, int max_rows);
+/* Columns filtered through the batched filter so far. */
+uint64_t evslx_engine_batched_columns(const evslx_engine *E);
 uint64_t evslx_engine_plan_builds(const evslx_engine *E);
 /* Filter groups launched so far, by block width 1, 2, 4, 8, 16 (a group of
  * one FP64 column runs the single-vector filter). */

@@ -395,3 +395,52 @@ def test_multi_filter_dictionary_with_double_table(gpu_lib):
     finally:
         gpu_lib.set_filter_variant(-1)
         gpu_lib.free_pol(pol)
+
+
+def test_engine_batched_filter_is_bitwise_the_per_matrix_filter(gpu_lib):
+    """The engine's batched filter (the lone FP64 columns of all small
+    matrices advanced one degree per launch together) gives every instance
+    the same eigenvalues, bit for bit, as filtering each matrix on its own."""
+    rng = np.random.default_rng(8)
+    mats, pols, subs = [], [], []
+    for i in range(10):
+        nn = int(np.exp(rng.uniform(np.log(500), np.log(2e4))))
+        if i % 2 == 0:
+            s = max(int(round(np.sqrt(nn))), 10)
+            dims, hi = (s, s + 1, 1), 8.0
+        else:
+            s = max(int(round(nn ** (1 / 3))), 8)
+            dims, hi = (s, s, s + 1), 12.0
+        ia, ja, a = O.lap_csr(*dims)
+        ev = np.sort(W.laplacian_eigenvalues(*dims))
+        a0, b0, cnt = W.gap_interval(ev, float(rng.uniform(0.4, 1.2)), int(rng.integers(15, 40)))
+        iv = [a0, b0, 0.0, hi]
+        M = gpu_lib.matrix(ia, ja, a)
+        pol = gpu_lib.find_pol(iv)
+        mats.append(M)
+        pols.append(pol)
+        subs.append((M, iv, pol, O.seeded_normal(len(ia) - 1, 30 + i), i, len(ev[(ev >= a0) & (ev <= b0)])))
+    out = {}
+    for batch in (True, False):
+        eng = gpu_lib.engine(len(subs), precision=E.PREC_FP64)
+        eng.use_batch(batch)
+        for M, iv, pol, v, tag, _ in subs:
+            eng.submit_slice(M, iv, pol, 1500, 1e-8, v, tag)
+        eng.run()
+        res = {}
+        while True:
+            r = eng.pop()
+            if r is None:
+                break
+            res[r["tag"]] = r
+        assert (eng.batched_columns() > 0) == batch
+        eng.free()
+        out[batch] = res
+    for _, _, _, _, tag, cnt in subs:
+        a, b = out[True][tag], out[False][tag]
+        assert a["rc"] == b["rc"] == 0 and a["nev"] == b["nev"] == cnt
+        assert np.array_equal(a["lam"], b["lam"]) and np.array_equal(a["res"], b["res"])
+    for M in mats:
+        M.free()
+    for p in pols:
+        gpu_lib.free_pol(p)
