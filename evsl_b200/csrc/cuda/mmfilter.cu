@@ -1,8 +1,9 @@
 // Filters of many slices on many matrices in one launch per degree: the
 // batched form of ChebAv (SRC/chebpoly.c:519-598) for the request engine.
 //
-// A batch is a list of columns, each with its own matrix (the device CSR of a
-// registered matrix), polynomial (degree, coefficients on the device, cc,
+// A batch is a list of columns, each with its own matrix (a registered
+// matrix, read through its SELL-C-sigma copy), polynomial (degree,
+// coefficients on the device, cc,
 // dd), input and output vectors and a 2n recurrence workspace.  Degree k is
 // one launch for every column whose degree is at least k: the columns are
 // sorted by degree, largest first, so those are a prefix of the list, and the
@@ -11,10 +12,10 @@
 // batched-instances configuration, small serving requests) then cost one
 // launch per degree of the batch instead of one per degree per instance.
 //
-// Each row is the CSR row summed left to right with rounded multiply and
-// add, and the three-term update is the single-vector kernel's: every
-// column's output equals ChebAv of that column bit for bit, whatever else is
-// in the batch.
+// Each row is read through the matrix's SELL-C-sigma copy and summed left to
+// right with rounded multiply and add, and the three-term update is the
+// single-vector kernel's: every column's output equals ChebAv of that column
+// bit for bit, whatever else is in the batch.
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -25,16 +26,28 @@
 namespace evslcu {
 namespace {
 
+// One column of the batch.  The matrix is read through its SELL-C-sigma copy
+// (coalesced chunks, compressed values / column offsets where lossless);
+// fmt = 2 * (values stored as float) + (columns stored as int16 offsets).
 struct MMItem {
-  const int *ia, *ja;
-  const double *a;
+  const long long *cptr;
+  const int *cw;
+  const void *scol, *sval;
+  const int *perm;
   const double *mu;  // device, deg + 1
   const double *x;
   double *y;
   double *w;  // 2n
   double t1, t2, ncc;
-  int n, deg, block0, pad;
+  int n, deg, block0, fmt, ellw, pad;
 };
+
+template <class VT, class IT>
+__device__ __forceinline__ double mm_row(const MMItem &I, int s, const double *x) {
+  const SellT<VT, IT> A{I.n, I.cptr, I.cw, (const IT *)I.scol, (const VT *)I.sval, I.ellw, I.perm};
+  return row_dot<false>(A, s, x);
+}
+__device__ __forceinline__ int mm_row_of(const MMItem &I, int s) { return I.perm ? __ldg(I.perm + s) : s; }
 
 constexpr int kMMThreads = 256;
 
@@ -45,8 +58,9 @@ __global__ void __launch_bounds__(kMMThreads) k_mm_cheb(const MMItem *__restrict
   asm volatile("griddepcontrol.wait;" ::: "memory");
   const MMItem &I = items[__ldg(blk_item + blockIdx.x)];
   const int n = I.n;
-  const int r = (blockIdx.x - I.block0) * kMMThreads + threadIdx.x;
-  if (k > I.deg || r >= n) return;
+  const int sl = (blockIdx.x - I.block0) * kMMThreads + threadIdx.x;  // SELL slot
+  if (k > I.deg || sl >= n) return;
+  const int r = mm_row_of(I, sl);
   double *W0 = I.w, *W1 = I.w + n;
   const double *vk = FIRST ? I.x : (((k - 2) & 1) ? W1 : W0);
   const double *vkm1 = FIRST ? nullptr : ((k == 2) ? I.x : (((k - 1) & 1) ? W1 : W0));
@@ -56,8 +70,13 @@ __global__ void __launch_bounds__(kMMThreads) k_mm_cheb(const MMItem *__restrict
   const double xm1 = FIRST ? 0.0 : vkm1[r];
   double *y = I.y;
   const double yo = FIRST ? 0.0 : y[r];
-  const CsrView A{n, I.ia, I.ja, I.a};
-  const double acc = row_dot<false>(A, r, vk);
+  double acc;
+  switch (I.fmt) {
+    case 0: acc = mm_row<double, int>(I, sl, vk); break;
+    case 1: acc = mm_row<double, short>(I, sl, vk); break;
+    case 2: acc = mm_row<float, int>(I, sl, vk); break;
+    default: acc = mm_row<float, short>(I, sl, vk); break;
+  }
   const double x = vk[r];
   double w = __dmul_rn(t, __dadd_rn(acc, __dmul_rn(I.ncc, x)));
   if (!FIRST) w = __dadd_rn(w, -xm1);
@@ -119,9 +138,13 @@ int evslcu_filter_batch(int ncols, const evslcu_batch_col *cols, void *table, si
       return fail(EVSLCU_ERR_ARG, "filter_batch: bad column %d", order[i]);
     const int n = c.A->n;
     MMItem &I = items[i];
-    I.ia = c.A->ia;
-    I.ja = c.A->ja;
-    I.a = c.A->a;
+    I.cptr = c.A->cptr;
+    I.cw = c.A->cw;
+    I.scol = c.A->scol;
+    I.sval = c.A->sval;
+    I.perm = c.A->perm;
+    I.fmt = 2 * (c.A->vfmt ? 1 : 0) + (c.A->ifmt ? 1 : 0);
+    I.ellw = c.A->ellw;
     I.mu = c.mu;
     I.x = c.x;
     I.y = c.y;
