@@ -75,6 +75,9 @@ def parse():
     p.add_argument("--serve-mix", choices=["default", "small"], default="default",
                    help="serve: 'small' draws the large-matrix requests on the 2-D 100x100 Laplacian only")
     p.add_argument("--rspd-n", type=int, default=RSPD_N, help="rspd-filter: rows of the random SPD matrix")
+    p.add_argument("--rspd-ncols", default="1",
+                   help="rspd-filter: columns filtered together (> 1: the multi-column block filter, "
+                        "FP64 or FP32 by --precision); a comma-separated list prints one line per width")
     p.add_argument("--sigma", type=int, default=-1,
                    help="rspd-filter: SELL-C-sigma sort window (-1 automatic, 0 unsorted SELL-32)")
     p.add_argument("--instances", type=int, default=128, help="batch-uneven: independent Laplacians")
@@ -679,8 +682,12 @@ def run_rspd_filter(args):
     device time of every filter application from CUDA events, averaged over
     its degree launches.
 
+    --rspd-ncols B > 1: the block filter (evslx_chebav_multi with B columns,
+    each with the same degree-400 polynomial; FP64 or FP32 by --precision),
+    per-degree time from the same degree-400 minus degree-40 difference.
+
     Algorithmic bytes per degree (the SpMV + Chebyshev update, no padding,
-    no chunk tables, no gathers counted): nnz (s_v + 4) + 4 (n + 1) + 5 n s_x
+    no chunk tables, no gathers counted): nnz (s_v + 4) + 4 (n + 1) + 5 B n s_x
     with s_v = s_x = 4 (FP32) or 8 (FP64)."""
     import ctypes as C
 
@@ -703,24 +710,38 @@ def run_rspd_filter(args):
     del ja, a
     sigma, stored, stored_plain = lib.matrix_sell_layout()
     iv = [glo + 0.3 * (ghi - glo), glo + 0.32 * (ghi - glo), glo, ghi]
+    for B in [max(1, int(b)) for b in str(args.rspd_ncols).split(",")]:
+        _rspd_filter_width(args, lib, B, n, nnz, iv, (sigma, stored, stored_plain), gen_s, glo, ghi)
+
+
+def _rspd_filter_width(args, lib, B, n, nnz, iv, layout, gen_s, glo, ghi):
+    """One rspd-filter line: the filter of B columns on the registered matrix."""
+    import ctypes as C
+
+    import torch
+
+    import evsl_b200 as E
+
+    sigma, stored, stored_plain = layout
     fp32 = args.precision == "mixed"
     sx = 4 if fp32 else 8
-    abytes = nnz * (sx + 4) + 4.0 * (n + 1) + 5.0 * n * sx
-    v0 = np.random.default_rng(RSPD_SEED).standard_normal(n)
+    abytes = nnz * (sx + 4) + 4.0 * (n + 1) + 5.0 * B * n * sx
+    v0 = np.random.default_rng(RSPD_SEED).standard_normal((B, n))
     dv = E.DeviceBuffer.from_host(lib.lib, v0)
-    dy = E.DeviceBuffer(lib.lib, 8 * n)
+    dy = E.DeviceBuffer(lib.lib, 8 * n * B)
     lstream = torch.cuda.ExternalStream(lib.stream_handle())
     sampler = ClockSampler(rank_info()[2])
-    if fp32:
+    if fp32 or B > 1:
         p_hi = lib.find_pol(iv, deg=400)
         p_lo = lib.find_pol(iv, deg=40)
+        prec = E.PREC_MIXED if fp32 else E.PREC_FP64
 
         def timed(pol):
-            arr = (E.PolParams * 1)(pol)
+            arr = (E.PolParams * B)(*([pol] * B))
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(lstream)
-            lib._check(lib.lib.evslx_chebav_multi(1, arr, dv.ptr, dy.ptr, E.PREC_MIXED), "evslx_chebav_multi")
+            lib._check(lib.lib.evslx_chebav_multi(B, arr, dv.ptr, dy.ptr, prec), "evslx_chebav_multi")
             e1.record(lstream)
             e1.synchronize()
             return e0.elapsed_time(e1) / 1e3
@@ -735,7 +756,11 @@ def run_rspd_filter(args):
         clocks = sampler.stop()
         t = statistics.median(per)
         launches = args.steps * (p_hi.deg + p_lo.deg + 4)
-        kernel = "k_mf_panel<float>" if lib.tuned_filter_variant(E.PREC_MIXED, 1) == 6 else "k_mf_step<float,1>"
+        bw = 1
+        while bw < B:
+            bw *= 2
+        kernel = ("k_mf_panel<float>" if fp32 and B == 1 and lib.tuned_filter_variant(E.PREC_MIXED, 1) == 6
+                  else "k_mf_step<%s,%d>" % ("float" if fp32 else "double", bw))
         lib.free_pol(p_lo)
     else:
         p_hi = lib.find_pol(iv, deg=400)
@@ -756,29 +781,36 @@ def run_rspd_filter(args):
     traffic = profiled_traffic(kernel, "rspd-filter-" + ("fp32" if fp32 else "fp64"))
     if traffic:
         traffic *= nnz / 33.0e6  # captured at n = 10^6 (33M stored entries); traffic grows with the entries
+    # one gather per stored entry brings B * s_x bytes; a 128-byte line carries up to 128 of them
+    gathers_per_entry = max(1.0, B * sx / 128.0)
+    gather_us = nnz * gathers_per_entry / (sm_count() * 1.965e9) * 1e6
     print(json.dumps({
         "metric": "filter SpMV GB/s", "value": gbs, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t * p_hi.deg, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if fp32 else "f64",
         "data": "synthetic (random sparse SPD, seeded; inputs larger than L2)",
-        "config": {"workload": "rspd-filter: %s filter, degree %d, random sparse SPD n=%d, nnz=%d"
-                               % ("FP32" if fp32 else "FP64", p_hi.deg, n, nnz),
+        "config": {"workload": "rspd-filter: %s filter, %d column%s, degree %d, random sparse SPD n=%d, nnz=%d"
+                               % ("FP32" if fp32 else "FP64", B, "" if B == 1 else "s", p_hi.deg, n, nnz),
+                   "columns": B, "us_per_column_degree": 1e6 * t / B,
                    "storage": {"sigma": sigma, "stored_slots": stored, "stored_slots_unsorted": stored_plain,
                                "padding": stored / nnz - 1.0,
                                "panel_layout": dict(zip(("rows_per_block", "panel_width", "bytes"),
                                                         lib.matrix_panel_layout(fp32)))},
-                   "kernel_times_us": (lib.filter_kernel()[1] if not fp32 else None),
+                   "kernel_times_us": (lib.filter_kernel()[1] if not fp32 and B == 1 else None),
                    "us_per_degree": 1e6 * t, "algorithmic_bytes_per_degree": abytes,
                    "generate_s": round(gen_s, 1), "bounds": [glo, ghi]},
         "roofline": {"bound": "hbm", "kernel": kernel, "achieved": gbs, "peak": peak, "peak_kind": kind,
                      "unit": "GB/s", "frac": gbs / peak, "traffic": traffic,
                      "frac_dram": (traffic / t / 1e9 / peak) if traffic else None,
-                     "gather_bound_us": nnz / (sm_count() * 1.965e9) * 1e6,
-                     "frac_of_gather_bound": (nnz / (sm_count() * 1.965e9)) / t,
-                     "note": "every stored entry gathers x[col] from its own cache line (random columns, x far "
-                             "larger than L1): one L1TEX wavefront per entry; ncu shows L1TEX at 90-94% of peak "
-                             "and DRAM at 24-33%, so the gather rate (one line per clock per SM), not HBM, bounds "
-                             "the kernel; gather_bound_us = nnz / (SMs x 1.965 GHz)"},
+                     "gather_bound_us": gather_us,
+                     "hbm_bound_us": abytes / (peak * 1e9) * 1e6,
+                     "frac_of_gather_bound": gather_us / 1e6 / t,
+                     "note": "every stored entry gathers x[col] (B values) from its own cache line (random "
+                             "columns, x far larger than L1): one L1TEX wavefront per entry and 128 bytes; ncu "
+                             "shows L1TEX at 90-94% of peak and DRAM at 24-33% for one column, so the gather "
+                             "rate (one line per clock per SM), not HBM, bounds the single-vector kernel; "
+                             "gather_bound_us = nnz x max(1, B s_x / 128) / (SMs x 1.965 GHz); with B columns "
+                             "each line carries B values and the bound moves to HBM once hbm_bound_us exceeds it"},
         "gpu_launches": launches, "clocks": clocks}))
     lib.free_pol(p_hi)
 
