@@ -29,6 +29,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB_PATH = os.path.join(_HERE, "_ref", "libevsl_ref.so")
 
+EVSL_PI = 3.14159265358979323846  # INC/evsl.h:22
 DBL_EPS = np.finfo(np.float64).eps
 EVSL_DBL_EPS_MULT = 10  # INC/evsl.h:27
 ORTH_TOL = 1e-14  # INC/internal_header.h:21
@@ -453,28 +454,41 @@ def csr_matvec(ia, ja, a, x):
     return y
 
 
+def _trig(fn, j0, j1, th):
+    """fn(j * th) for j = j0 .. j1-1 through the C library's sin / cos (the
+    functions the reference calls; numpy's vectorised ones may round the last
+    bit differently)."""
+    return np.array([fn(j * th) for j in range(j0, j1)], dtype=np.float64)
+
+
+def _seqsum(t):
+    """Left-to-right sum (the reference's loops), not numpy's pairwise sum."""
+    return float(np.cumsum(t)[-1]) if len(t) else 0.0
+
+
 def dampcf(m, damping):
     """Damping coefficients jac[0..m] (SRC/chebpoly.c:39-66)."""
     jac = np.empty(m + 1)
     jac[0] = 0.5
+    if m < 1:
+        return jac
     k = np.arange(1, m + 1, dtype=np.float64)
     if damping == 0:
         jac[1:] = 1.0
     elif damping == 1:
-        thetJ = np.pi / (m + 2.0)
+        thetJ = EVSL_PI / (m + 2.0)
         a1 = 1.0 / (m + 2.0)
         a2 = math.sin(thetJ)
-        jac[1:] = a1 * np.sin((k + 1) * thetJ) / a2 + (1 - (k + 1) * a1) * np.cos(k * thetJ)
+        jac[1:] = a1 * _trig(math.sin, 2, m + 2, thetJ) / a2 + (1 - (k + 1) * a1) * _trig(math.cos, 1, m + 1, thetJ)
     else:
-        thetL = np.pi / (m + 1.0)
-        jac[1:] = np.sin(k * thetL) / (k * thetL)
+        thetL = EVSL_PI / (m + 1.0)
+        jac[1:] = _trig(math.sin, 1, m + 1, thetL) / (k * thetL)
     return jac
 
 
 def _dif_eval(v, m, thc, jac):
-    """sum_j v_j cos(j thc) jac_j (SRC/chebpoly.c:78-84)."""
-    j = np.arange(m + 1)
-    return float(np.sum(v[:m + 1] * np.cos(j * thc) * jac[:m + 1]))
+    """sum_j v_j cos(j thc) jac_j, summed left to right (SRC/chebpoly.c:78-84)."""
+    return _seqsum(v[:m + 1] * _trig(math.cos, 0, m + 1, thc) * jac[:m + 1])
 
 
 def _chebx_pltd(m, mu, x):
@@ -502,10 +516,10 @@ def _rootchb(m, v, jac, tha, thb):
     fa = _dif_eval(v, m, tha, jac)
     if fa > 0 or fb < 0:
         return False, None, thc
-    j = np.arange(1, m + 1)
+    j = np.arange(1, m + 1, dtype=np.float64)
     for _ in range(max_iter + 1):
         fval = _dif_eval(v, m, thc, jac)
-        d = float(np.sum(jac[1:m + 1] * j * np.sin(j * thc) * v[1:m + 1]))
+        d = _seqsum(jac[1:m + 1] * j * _trig(math.sin, 1, m + 1, thc) * v[1:m + 1])
         thN = thc + fval / d
         if abs(fval) < tol_bal or abs(thc - thN) < DBL_EPS * abs(thc):
             break
@@ -519,7 +533,7 @@ def _rootchb(m, v, jac, tha, thb):
                 thN = 0.5 * (thc + thb)
             tha = thc
             thc = thN
-    mu = np.cos(np.arange(m + 1) * thc) * jac[:m + 1]
+    mu = _trig(math.cos, 0, m + 1, thc) * jac[:m + 1]
     return True, mu, thc
 
 
@@ -616,8 +630,7 @@ def find_pol(intv, *, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=10000, 
         thresh = -1
         max_deg = deg
     v = np.zeros(max_deg + 1)
-    j = np.arange(min_deg)
-    v[:min_deg] = np.cos(j * thb) - np.cos(j * tha)
+    v[:min_deg] = _trig(math.cos, 0, min_deg, thb) - _trig(math.cos, 0, min_deg, tha)
     mu = None
     t = 0.0
     vals = np.array([np.nan, np.nan])

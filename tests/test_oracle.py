@@ -163,3 +163,27 @@ def test_kpm_product_identities_restatement(dims, M):
     d0 = O.kpm_raw_dots(M, probes, iv, ia, ja, a)
     d1 = O.kpm_raw_dots_identities(M, probes, iv, ia, ja, a)
     assert np.max(np.abs(d1 - d0)) <= 1e-12 * np.max(np.abs(d0))
+
+
+@pytest.mark.skipif(not HAVE_REF, reason="reference build not present")
+def test_find_pol_restatement_bitwise_on_random_intervals():
+    """The restated filter design equals the reference build's bit for bit
+    on seeded random mid-spectrum intervals, all three dampings, designed
+    and forced degrees: its sines, cosines and sums are taken in the
+    reference's scalar order (C library trigonometry, left-to-right sums)."""
+    R = O.RefLib()
+    rng = np.random.default_rng(17)
+    for i in range(40):
+        x = np.sort(rng.uniform(0.05, 0.95, 2))
+        lo, hi = -3.0 + rng.uniform(), 9.0 + rng.uniform()
+        iv = [lo + x[0] * (hi - lo), lo + x[1] * (hi - lo), lo, hi]
+        # a forced degree at or above the design loop's starting degree 2 + 0.5 / (half-width in [-1, 1])
+        dmin = int(2 + 0.5 / ((x[1] - x[0]) * 2.0)) + 1
+        kw = dict(damping=int(i % 3), max_deg=400, deg=(0 if i % 2 else int(rng.integers(dmin, dmin + 120))))
+        rc, pol = R.find_pol(iv, **kw)
+        ref = R.pol_dict(pol)
+        R.free_pol(pol)
+        got = O.find_pol(iv, **kw)
+        assert rc == 0 and got["deg"] == ref["deg"] and got["type"] == ref["type"], (i, iv, kw)
+        assert np.array_equal(got["mu"], ref["mu"]), (i, iv, kw)
+        assert got["gam"] == ref["gam"] and got["bar"] == ref["bar"], (i, iv, kw)
