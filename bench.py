@@ -75,6 +75,11 @@ def parse():
     p.add_argument("--serve-mix", choices=["default", "small"], default="default",
                    help="serve: 'small' draws the large-matrix requests on the 2-D 100x100 Laplacian only")
     p.add_argument("--rspd-n", type=int, default=RSPD_N, help="rspd-filter: rows of the random SPD matrix")
+    p.add_argument("--kpm-split", type=int, choices=[-1, 0, 1], default=-1,
+                   help="rspd-kpm: KPM block step on the column-split copy: -1 automatic, 0 off, 1 on")
+    p.add_argument("--split-range-mb", type=float, default=0.0,
+                   help="rspd-filter / rspd-kpm: MiB of block rows one column range of the column-split copy "
+                        "gathers from (0: the library default)")
     p.add_argument("--rspd-ncols", default="1",
                    help="rspd-filter: columns filtered together (> 1: the multi-column block filter, "
                         "FP64 or FP32 by --precision); a comma-separated list prints one line per width")
@@ -706,6 +711,7 @@ def run_rspd_filter(args):
     lib.set_sell_sigma(args.sigma)
     lib.set_filter_kernel(None if args.filter_kernel == "auto" else args.filter_kernel)
     lib.set_filter_variant(args.variant)
+    lib.set_split_range_bytes(int(args.split_range_mb * (1 << 20)))
     lib.set_csr(ia, ja, a)
     del ja, a
     sigma, stored, stored_plain = lib.matrix_sell_layout()
@@ -792,6 +798,7 @@ def _rspd_filter_width(args, lib, B, n, nnz, iv, layout, gen_s, glo, ghi):
         "config": {"workload": "rspd-filter: %s filter, %d column%s, degree %d, random sparse SPD n=%d, nnz=%d"
                                % ("FP32" if fp32 else "FP64", B, "" if B == 1 else "s", p_hi.deg, n, nnz),
                    "columns": B, "us_per_column_degree": 1e6 * t / B,
+                   "tuned_variant": lib.tuned_filter_variant(E.PREC_MIXED if fp32 else E.PREC_FP64, B),
                    "storage": {"sigma": sigma, "stored_slots": stored, "stored_slots_unsorted": stored_plain,
                                "padding": stored / nnz - 1.0,
                                "panel_layout": dict(zip(("rows_per_block", "panel_width", "bytes"),
@@ -1018,6 +1025,9 @@ def run_rspd_kpm(args):
     nnz = int(ia[-1])
     lib = evsl_b200.Library()
     lib.lib.evslx_last_kpm_seconds.restype = C.c_double
+    lib.set_split_range_bytes(int(args.split_range_mb * (1 << 20)))
+    lib.lib.evslcu_set_kpm_split.argtypes = [C.c_int]
+    lib.lib.evslcu_set_kpm_split(args.kpm_split)
     lib.set_csr(ia, ja, a)
     del ja, a
     B = args.kpm_probes if args.kpm_probes != 30 else 64
@@ -1044,6 +1054,7 @@ def run_rspd_kpm(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (random sparse SPD, seeded Gaussian probes)",
         "config": {"workload": "rspd-kpm: kpmdos, %d probes, %d moments, random sparse SPD n=%d nnz=%d"
                                % (B, M, n, nnz), "block_steps": steps, "us_per_block_step": 1e6 * t / steps,
+                   "kpm_split": args.kpm_split, "split_range_mb": args.split_range_mb,
                    "ecount": ec},
         "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "peak_kind": kind, "unit": "GB/s",
                      "frac": gbs / peak, "algorithmic_bytes": abytes,

@@ -300,6 +300,7 @@ def load():
         "evslx_engine_batched_columns": ([C.c_void_p], C.c_uint64),
         "evslx_set_mixed_min_rows": ([C.c_int], None),
         "evslx_set_filter_variant": ([C.c_int], C.c_int),
+        "evslx_set_split_range_bytes": ([C.c_longlong], C.c_int),
         "evslx_set_l2_resident": ([C.c_int], C.c_int),
         "evslx_set_row_patterns": ([C.c_int], C.c_int),
         "evslx_row_pattern_count": ([], C.c_int),
@@ -731,6 +732,11 @@ class Library:
 
     def tuned_filter_variant(self, precision, ncols):
         return self.lib.evslx_tuned_filter_variant(precision, ncols)
+
+    def set_split_range_bytes(self, nbytes):
+        """Bytes of block rows one column range of filter variant 7 gathers
+        from (0: the default)."""
+        self._check(self.lib.evslx_set_split_range_bytes(int(nbytes)), "evslx_set_split_range_bytes")
 
     def matrix(self, ia, ja, a):
         return Matrix(self.lib, ia, ja, a)

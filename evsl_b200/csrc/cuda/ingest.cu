@@ -256,15 +256,27 @@ __global__ void k_csr_check_entries(int n, const int *ia, const int *ja, const d
   if ((threadIdx.x & 31) == 0) atomicMax(&flags[4], bw);
 }
 
+// Row lengths of the sort and chunk-width kernels: a CSR row's, or an
+// explicit per-row count (the rows' entries in one column range).
+struct LenCsr {
+  const int *ia;
+  __device__ __forceinline__ int operator()(int r) const { return ia[r + 1] - ia[r]; }
+};
+struct LenArr {
+  const int *len;
+  __device__ __forceinline__ int operator()(int r) const { return len[r]; }
+};
+
 // Width of each chunk: its longest row (slot s holds row perm[s], or row s
 // when perm is null).
-__global__ void k_chunk_width(int n, int nch, const int *ia, const int *perm, int *cw, long long *csize) {
+template <class L>
+__global__ void k_chunk_width(int n, int nch, L len, const int *perm, int *cw, long long *csize) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nch; c += gridDim.x * blockDim.x) {
     int w = 0;
     const int s1 = min(n, 32 * c + 32);
     for (int s = 32 * c; s < s1; ++s) {
       const int r = perm ? perm[s] : s;
-      w = max(w, ia[r + 1] - ia[r]);
+      w = max(w, len(r));
     }
     cw[c] = w;
     csize[c] = 32LL * w;
@@ -277,13 +289,13 @@ __global__ void k_chunk_width(int n, int nch, const int *ia, const int *perm, in
 // (0x7fffffff - length, position in the window) in shared memory; slot
 // w0 + i then holds row perm[w0 + i].  Positions past the last row carry the
 // largest key and sort to the end.
-template <int W>
-__global__ void __launch_bounds__(1024) k_sigma_sort(int n, const int *ia, int *perm) {
+template <int W, class L>
+__global__ void __launch_bounds__(1024) k_sigma_sort(int n, L len, int *perm) {
   __shared__ unsigned long long key[W];
   const int w0 = blockIdx.x * W;
   for (int i = threadIdx.x; i < W; i += blockDim.x) {
     const int r = w0 + i;
-    key[i] = (r < n) ? ((unsigned long long)(0x7fffffff - (ia[r + 1] - ia[r])) << 32) | (unsigned)i : ~0ULL;
+    key[i] = (r < n) ? ((unsigned long long)(0x7fffffff - len(r)) << 32) | (unsigned)i : ~0ULL;
   }
   __syncthreads();
   for (int k = 2; k <= W; k <<= 1)
@@ -328,6 +340,55 @@ __global__ void k_sell_fill(int n, int nch, const int *ia, const int *ja, const 
       else
         scol[p] = (IT)col;
       sval[p] = (VT)v;
+    }
+  }
+}
+
+// ---- column-split copy (multi-column filter on large general matrices) -----
+//
+// Range p of the columns is [p * width, (p + 1) * width).  For each row the
+// entries of every range form one run of its CSR entries, because the row's
+// columns increase; beg/len (P x n, range-major) hold each run.
+
+// Walks each row once, recording where every range's run starts and how long
+// it is, and flags rows whose columns do not increase.
+__global__ void k_xs_bounds(int n, const int *ia, const int *ja, int P, int width, int *beg, int *len, int *bad) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int hi = ia[r + 1];
+    int j = ia[r], prev = -1;
+    bool ok = true;
+    for (int p = 0; p < P; ++p) {
+      const long long lim = (long long)(p + 1) * width;
+      const int b = j;
+      while (j < hi) {
+        const int c = ja[j];
+        if (c <= prev) ok = false;
+        if (c >= lim) break;
+        prev = c;
+        ++j;
+      }
+      beg[(size_t)p * n + r] = b;
+      len[(size_t)p * n + r] = j - b;
+    }
+    if (!ok) atomicExch(bad, 1);
+  }
+}
+
+// Thread per (chunk, lane) slot of one range; entry j of lane l at
+// cptr[c] + 32 j + l.  Padding slots get column -1 (the filter skips them).
+__global__ void k_xs_fill(int n, int nch, const int *beg, const int *len, const int *ja, const double *a,
+                          const int *perm, const long long *cptr, const int *cw, int *col, double *val) {
+  const long long slots = 32LL * nch;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(s >> 5), l = (int)(s & 31);
+    const bool live = s < n;
+    const int r = live ? perm[s] : 0;
+    const int ln = live ? len[r] : 0;
+    const int b = live ? beg[r] : 0;
+    for (int j = 0; j < cw[c]; ++j) {
+      const long long p = cptr[c] + 32LL * j + l;
+      col[p] = (j < ln) ? ja[b + j] : -1;
+      val[p] = (j < ln) ? a[b + j] : 0.0;
     }
   }
 }
@@ -563,17 +624,18 @@ int g_sell_sigma = -1;
 int g_sigma_auto = 256;
 constexpr double kSigmaTrigger = 1.10;
 
-int launch_sigma_sort(int n, int sigma, const int *ia, int *perm) {
+template <class L>
+int launch_sigma_sort(int n, int sigma, L len, int *perm) {
   const int nwin = (int)(((long long)n + sigma - 1) / sigma);
   switch (sigma) {
-    case 32: k_sigma_sort<32><<<nwin, 32, 0, stream()>>>(n, ia, perm); break;
-    case 64: k_sigma_sort<64><<<nwin, 64, 0, stream()>>>(n, ia, perm); break;
-    case 128: k_sigma_sort<128><<<nwin, 128, 0, stream()>>>(n, ia, perm); break;
-    case 256: k_sigma_sort<256><<<nwin, 256, 0, stream()>>>(n, ia, perm); break;
-    case 512: k_sigma_sort<512><<<nwin, 512, 0, stream()>>>(n, ia, perm); break;
-    case 1024: k_sigma_sort<1024><<<nwin, 1024, 0, stream()>>>(n, ia, perm); break;
-    case 2048: k_sigma_sort<2048><<<nwin, 1024, 0, stream()>>>(n, ia, perm); break;
-    case 4096: k_sigma_sort<4096><<<nwin, 1024, 0, stream()>>>(n, ia, perm); break;
+    case 32: k_sigma_sort<32><<<nwin, 32, 0, stream()>>>(n, len, perm); break;
+    case 64: k_sigma_sort<64><<<nwin, 64, 0, stream()>>>(n, len, perm); break;
+    case 128: k_sigma_sort<128><<<nwin, 128, 0, stream()>>>(n, len, perm); break;
+    case 256: k_sigma_sort<256><<<nwin, 256, 0, stream()>>>(n, len, perm); break;
+    case 512: k_sigma_sort<512><<<nwin, 512, 0, stream()>>>(n, len, perm); break;
+    case 1024: k_sigma_sort<1024><<<nwin, 1024, 0, stream()>>>(n, len, perm); break;
+    case 2048: k_sigma_sort<2048><<<nwin, 1024, 0, stream()>>>(n, len, perm); break;
+    case 4096: k_sigma_sort<4096><<<nwin, 1024, 0, stream()>>>(n, len, perm); break;
     default: return fail(EVSLCU_ERR_ARG, "SELL sort window must be a power of two from 32 to 4096 (got %d)", sigma);
   }
   return launched("k_sigma_sort");
@@ -619,7 +681,7 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
     evslcu_free(csize);
     return fail(EVSLCU_ERR_NOMEM, "SELL build: out of device memory");
   }
-  k_chunk_width<<<grid_for(nch), kThreads, 0, stream()>>>(n, nch, M->ia, nullptr, M->cw, csize);
+  k_chunk_width<<<grid_for(nch), kThreads, 0, stream()>>>(n, nch, LenCsr{M->ia}, nullptr, M->cw, csize);
   rc = launched("k_chunk_width");
   if (!rc) rc = scan_exclusive<long long, long long>(csize, nch, M->cptr);
   long long padded = 0;
@@ -634,7 +696,7 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
     int *perm = (int *)evslcu_malloc(sizeof(int) * 32 * (size_t)nch);
     if (!perm) rc = fail(EVSLCU_ERR_NOMEM, "SELL build: out of device memory (row order)");
     if (!rc) rc = evslcu_memset(perm, 0, sizeof(int) * 32 * (size_t)nch);
-    if (!rc) rc = launch_sigma_sort(n, sigma, M->ia, perm);
+    if (!rc) rc = launch_sigma_sort(n, sigma, LenCsr{M->ia}, perm);
     long long *cptr2 = nullptr;
     int *cw2 = nullptr;
     if (!rc) {
@@ -643,7 +705,7 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
       if (!cptr2 || !cw2) rc = fail(EVSLCU_ERR_NOMEM, "SELL build: out of device memory");
     }
     if (!rc) {
-      k_chunk_width<<<grid_for(nch), kThreads, 0, stream()>>>(n, nch, M->ia, perm, cw2, csize);
+      k_chunk_width<<<grid_for(nch), kThreads, 0, stream()>>>(n, nch, LenCsr{M->ia}, perm, cw2, csize);
       rc = launched("k_chunk_width");
     }
     if (!rc) rc = scan_exclusive<long long, long long>(csize, nch, cptr2);
@@ -705,6 +767,86 @@ int build_sell_device(evslcu_mat *M, int allow_compress) {
     k_sell_fill<double, int><<<g, kThreads, 0, stream()>>>(n, nch, M->ia, M->ja, M->a, M->perm, M->cptr, M->cw,
                                                            (int *)M->scol, (double *)M->sval);
   return launched("k_sell_fill");
+}
+
+// Column-split copy: P ranges of `width` columns, each a SELL-C-sigma with a
+// 256-row sort window over the rows' lengths in that range.
+int build_xsplit_device(evslcu_mat *M, int P, int width, evslcu_xsplit *X) {
+  const int n = M->n, nch = (n + 31) / 32;
+  if (P < 1 || P > evslcu_xsplit::kMaxRanges || width < 1 || (long long)P * width < n)
+    return fail(EVSLCU_ERR_ARG, "column-split copy: bad range count %d or width %d", P, width);
+  int *beg = (int *)evslcu_malloc(sizeof(int) * (size_t)P * n);
+  int *len = (int *)evslcu_malloc(sizeof(int) * (size_t)P * n);
+  int *bad = (int *)evslcu_malloc(sizeof(int));
+  long long *csize = (long long *)evslcu_malloc(sizeof(long long) * (size_t)nch);
+  int rc = (beg && len && bad && csize) ? 0 : fail(EVSLCU_ERR_NOMEM, "column-split copy: out of device memory");
+  if (!rc) rc = evslcu_memset(bad, 0, sizeof(int));
+  if (!rc) {
+    k_xs_bounds<<<grid_for(n), kThreads, 0, stream()>>>(n, M->ia, M->ja, P, width, beg, len, bad);
+    rc = launched("k_xs_bounds");
+  }
+  int hbad = 0;
+  if (!rc) rc = evslcu_d2h(&hbad, bad, sizeof(int));
+  if (!rc && hbad) {
+    M->xs_bad = 1;
+    rc = fail(EVSLCU_ERR_ARG, "column-split copy needs strictly increasing column indices in every row");
+  }
+  X->P = P;
+  X->width = width;
+  X->nch = nch;
+  X->slots = 0;
+  for (int p = 0; !rc && p < P; ++p) {
+    const LenArr lp{len + (size_t)p * n};
+    X->perm[p] = (int *)evslcu_malloc(sizeof(int) * 32 * (size_t)nch);
+    X->cw[p] = (int *)evslcu_malloc(sizeof(int) * (size_t)nch);
+    X->cptr[p] = (long long *)evslcu_malloc(sizeof(long long) * ((size_t)nch + 1));
+    if (!X->perm[p] || !X->cw[p] || !X->cptr[p]) rc = fail(EVSLCU_ERR_NOMEM, "column-split copy: out of device memory");
+    if (!rc) rc = evslcu_memset(X->perm[p], 0, sizeof(int) * 32 * (size_t)nch);
+    if (!rc) rc = launch_sigma_sort(n, 256, lp, X->perm[p]);
+    if (!rc) {
+      k_chunk_width<<<grid_for(nch), kThreads, 0, stream()>>>(n, nch, lp, X->perm[p], X->cw[p], csize);
+      rc = launched("k_chunk_width");
+    }
+    if (!rc) rc = scan_exclusive<long long, long long>(csize, nch, X->cptr[p]);
+    long long sp = 0;
+    if (!rc) rc = evslcu_d2h(&sp, X->cptr[p] + nch, sizeof(long long));
+    if (!rc) {
+      const size_t cap = (size_t)std::max(sp, 1LL);
+      X->col[p] = (int *)evslcu_malloc(sizeof(int) * cap);
+      X->val[p] = (double *)evslcu_malloc(sizeof(double) * cap);
+      if (!X->col[p] || !X->val[p]) rc = fail(EVSLCU_ERR_NOMEM, "column-split copy: out of device memory");
+    }
+    if (!rc) {
+      k_xs_fill<<<grid_for(32LL * nch), kThreads, 0, stream()>>>(n, nch, beg + (size_t)p * n, len + (size_t)p * n,
+                                                                M->ja, M->a, X->perm[p], X->cptr[p], X->cw[p],
+                                                                X->col[p], X->val[p]);
+      rc = launched("k_xs_fill");
+    }
+    X->slots += sp;
+  }
+  evslcu_free(beg);
+  evslcu_free(len);
+  evslcu_free(bad);
+  evslcu_free(csize);
+  return rc;
+}
+
+void xsplit_free(evslcu_mat *M) {
+  for (evslcu_xsplit *&X : M->xs) {
+    if (!X) continue;
+    for (int p = 0; p < evslcu_xsplit::kMaxRanges; ++p) {
+      evslcu_free(X->cptr[p]);
+      evslcu_free(X->cw[p]);
+      evslcu_free(X->perm[p]);
+      evslcu_free(X->col[p]);
+      evslcu_free(X->val[p]);
+      evslcu_free(X->val32[p]);
+    }
+    delete X;
+    X = nullptr;
+  }
+  evslcu_free(M->xs_acc);
+  M->xs_acc = nullptr;
 }
 
 }  // namespace evslcu

@@ -27,62 +27,84 @@ namespace {
 
 constexpr int kMaxB = 16;
 
+// Loads by cache policy: 0 read-only path, 1 L2 only (data this launch
+// sequence writes), 2 streaming (evict first: read once, keeps L2 for the
+// gathered vector).
+template <int MODE, class T>
+__device__ __forceinline__ T ldm(const T *p) {
+  if constexpr (MODE == 0) return __ldg(p);
+  else if constexpr (MODE == 1) return __ldcg(p);
+  else return __ldcs(p);
+}
+
 // Contiguous B-value loads/stores of a row of an interleaved block, as
 // 16-byte (or 8-byte) vector accesses unpacked into registers.
-template <bool CG, class VT, int B>
+template <int MODE, class VT, int B>
 __device__ __forceinline__ void load_row_impl(const VT *p, VT (&x)[B]) {
   if constexpr (std::is_same<VT, float>::value && B % 4 == 0) {
 #pragma unroll
     for (int i = 0; i < B / 4; ++i) {
-      const float4 f = CG ? __ldcg(reinterpret_cast<const float4 *>(p) + i) : __ldg(reinterpret_cast<const float4 *>(p) + i);
+      const float4 f = ldm<MODE>(reinterpret_cast<const float4 *>(p) + i);
       x[4 * i] = f.x;
       x[4 * i + 1] = f.y;
       x[4 * i + 2] = f.z;
       x[4 * i + 3] = f.w;
     }
   } else if constexpr (std::is_same<VT, float>::value && B == 2) {
-    const float2 f = CG ? __ldcg(reinterpret_cast<const float2 *>(p)) : __ldg(reinterpret_cast<const float2 *>(p));
+    const float2 f = ldm<MODE>(reinterpret_cast<const float2 *>(p));
     x[0] = f.x;
     x[1] = f.y;
   } else if constexpr (std::is_same<VT, double>::value && B % 2 == 0) {
 #pragma unroll
     for (int i = 0; i < B / 2; ++i) {
-      const double2 f =
-          CG ? __ldcg(reinterpret_cast<const double2 *>(p) + i) : __ldg(reinterpret_cast<const double2 *>(p) + i);
+      const double2 f = ldm<MODE>(reinterpret_cast<const double2 *>(p) + i);
       x[2 * i] = f.x;
       x[2 * i + 1] = f.y;
     }
   } else {
 #pragma unroll
-    for (int c = 0; c < B; ++c) x[c] = CG ? __ldcg(p + c) : __ldg(p + c);
+    for (int c = 0; c < B; ++c) x[c] = ldm<MODE>(p + c);
   }
 }
 
 template <class VT, int B>
 __device__ __forceinline__ void load_row(const VT *p, VT (&x)[B]) {
-  load_row_impl<false, VT, B>(p, x);
+  load_row_impl<0, VT, B>(p, x);
 }
 
 // Same for data this launch sequence writes (L2 only, no read-only path).
 template <class VT, int B>
 __device__ __forceinline__ void load_row_cg(const VT *p, VT (&x)[B]) {
-  load_row_impl<true, VT, B>(p, x);
+  load_row_impl<1, VT, B>(p, x);
 }
 
+// Same, streaming (evict first).
 template <class VT, int B>
+__device__ __forceinline__ void load_row_cs(const VT *p, VT (&x)[B]) {
+  load_row_impl<2, VT, B>(p, x);
+}
+
+// Stores by cache policy: CS = streaming (evict first).
+template <bool CS, class T>
+__device__ __forceinline__ void stm(T *p, T v) {
+  if constexpr (CS) __stcs(p, v);
+  else *p = v;
+}
+
+template <class VT, int B, bool CS = false>
 __device__ __forceinline__ void store_row(VT *p, const VT (&x)[B]) {
   if constexpr (std::is_same<VT, float>::value && B % 4 == 0) {
 #pragma unroll
     for (int i = 0; i < B / 4; ++i)
-      reinterpret_cast<float4 *>(p)[i] = make_float4(x[4 * i], x[4 * i + 1], x[4 * i + 2], x[4 * i + 3]);
+      stm<CS>(reinterpret_cast<float4 *>(p) + i, make_float4(x[4 * i], x[4 * i + 1], x[4 * i + 2], x[4 * i + 3]));
   } else if constexpr (std::is_same<VT, float>::value && B == 2) {
-    *reinterpret_cast<float2 *>(p) = make_float2(x[0], x[1]);
+    stm<CS>(reinterpret_cast<float2 *>(p), make_float2(x[0], x[1]));
   } else if constexpr (std::is_same<VT, double>::value && B % 2 == 0) {
 #pragma unroll
-    for (int i = 0; i < B / 2; ++i) reinterpret_cast<double2 *>(p)[i] = make_double2(x[2 * i], x[2 * i + 1]);
+    for (int i = 0; i < B / 2; ++i) stm<CS>(reinterpret_cast<double2 *>(p) + i, make_double2(x[2 * i], x[2 * i + 1]));
   } else {
 #pragma unroll
-    for (int c = 0; c < B; ++c) p[c] = x[c];
+    for (int c = 0; c < B; ++c) stm<CS>(p + c, x[c]);
   }
 }
 
@@ -136,9 +158,11 @@ struct Split {
 // (4, 5).  -1: each matrix uses the variant the autotuner measured fastest
 // for it (per precision and block width); 0..5: that variant everywhere.
 // Variant 6: one column on the column-panel layout (panel.cu), x staged
-// through shared memory; built for large general matrices.
+// through shared memory; built for large general matrices.  Variant 7: 2-16
+// columns on the column-split copy (ranges of columns whose rows of the
+// block fit in L2), for large general matrices whose block does not.
 static int g_mf_variant = -1;
-constexpr int kMfVariants = 7;
+constexpr int kMfVariants = 8;
 
 // One degree of the recurrence for all columns: thread (row r, part q)
 // handles columns q*CPT .. q*CPT+CPT-1 of row r.  Rows run over the padded
@@ -275,6 +299,187 @@ int mf_step_v(const SellT<AV, IT> &A, int k, const VT *vk, const VT *vkm1, VT *o
   return check_launch("k_mf_step");
 }
 
+// ---- column-split filter (variant 7) -------------------------------------
+//
+// On a large general matrix the gathers x[col] of a degree step land on
+// random rows of the whole block; once the block (n x B values) is larger
+// than L2 most of them miss L2 and each stored entry costs a DRAM line.  The
+// column-split copy (evslcu_xsplit) cuts the columns into ranges whose rows
+// of x fit in L2, and a degree step runs one launch per range: the range's
+// rows of x stay in L2 while every row adds the products of its entries in
+// that range to its running sum, which is carried from range to range in a
+// partial-sum block (read and written with streaming hints, like the stored
+// matrix, so that L2 keeps the gathered rows).  The last range applies the
+// three-term update of k_mf_step.  Ranges follow the columns and each range
+// keeps the CSR order, so every row is summed in its CSR order: FP64 columns
+// equal ChebAv bit for bit; padding slots (column -1) are skipped.
+size_t g_xs_range_bytes = (size_t)40 << 20;  // gathered rows of x per range
+
+template <class VT, int B, bool PFIRST, bool PLAST, bool FIRST>
+__global__ void __launch_bounds__(kThreads)
+    k_xs_step(XsRange<VT> A, const VT *__restrict__ vk, const VT *vkm1, VT *out, VT *__restrict__ y, VT *part,
+              const VT *__restrict__ coef) {
+  // 16-byte column parts: the TPR threads of a row gather its B values with
+  // one warp instruction (one L1 wavefront per gathered row, the bound on
+  // random columns)
+  constexpr int CPT = Split<VT, B, 16>::CPT, TPR = Split<VT, B, 16>::TPR;
+  constexpr int U = 4;
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const int npad = (A.n + 31) & ~31;
+  const long long total = (long long)npad * TPR;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+    const int sl = (int)(g / TPR), q = (int)(g % TPR);
+    const bool live = sl < A.n;
+    const int r = live ? __ldg(A.perm + sl) : 0;
+    const int cb = q * CPT;
+    const long long base = (long long)r * B + cb;
+    VT acc[CPT], xr[CPT], yv[CPT], vm[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] = (VT)0;
+    if (!PFIRST && live) load_row_cs<VT, CPT>(part + base, acc);
+    if (PLAST && live) {
+      load_row<VT, CPT>(vk + base, xr);
+      load_row_cs<VT, CPT>(y + base, yv);
+      if (!FIRST) load_row_cs<VT, CPT>(vkm1 + base, vm);
+    }
+    const int ch = sl >> 5;
+    long long p = __ldg(A.cptr + ch) + (sl & 31);
+    const int w = __ldg(A.cw + ch);
+    VT v[U];
+    int col[U];
+    auto fetch = [&](int j0, long long pp, VT(&vv)[U], int(&cc)[U]) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (live && j0 + u < w) {
+          vv[u] = __ldcs(A.val + pp + 32 * u);
+          cc[u] = __ldcs(A.col + pp + 32 * u);
+        } else {
+          vv[u] = (VT)0;
+          cc[u] = -1;
+        }
+      }
+    };
+    fetch(0, p, v, col);
+    for (int j = 0; j < w; j += U, p += 32 * U) {
+      VT x[U][CPT];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (col[u] >= 0) {
+          load_row<VT, CPT>(vk + (long long)col[u] * B + cb, x[u]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) x[u][c] = (VT)0;
+        }
+      }
+      VT vn[U];
+      int cn[U];
+      fetch(j + U, p + 32 * U, vn, cn);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (col[u] >= 0) {
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) acc[c] = fmadd(v[u], x[u][c], acc[c]);
+        }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        v[u] = vn[u];
+        col[u] = cn[u];
+      }
+    }
+    if (!live) continue;
+    if constexpr (!PLAST) {
+      store_row<VT, CPT, true>(part + base, acc);
+    } else {
+      VT wv[CPT];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const VT *cf = coef + kCoef * (cb + c);
+        VT t = mul(__ldg(cf), add(acc[c], mul(__ldg(cf + 1), xr[c])));
+        if (!FIRST) t = add(t, -vm[c]);
+        wv[c] = t;
+        if (__ldg(cf + 3) != (VT)0) yv[c] = add(yv[c], mul(__ldg(cf + 2), t));
+      }
+      store_row<VT, CPT>(out + base, wv);
+      store_row<VT, CPT, true>(y + base, yv);
+    }
+  }
+}
+
+// Ranges of the column-split copy for a B-column block: the fewest (a power
+// of two up to 32) whose rows of x fit g_xs_range_bytes -- one when the
+// whole block fits (the kernel then only adds streaming cache hints and
+// skips padding); 0 when 32 ranges are not enough.
+inline int xs_ranges_rows(const evslcu_mat *M, size_t row) {
+  for (int P = 1; P <= evslcu_xsplit::kMaxRanges; P *= 2)
+    if ((((size_t)M->n + P - 1) / P) * row <= g_xs_range_bytes) return P;
+  return 0;
+}
+inline int xs_ranges(const evslcu_mat *M, int fp32, int B) {
+  return xs_ranges_rows(M, (size_t)B * (fp32 ? sizeof(float) : sizeof(double)));
+}
+inline int xs_slot(int P) { return P <= 1 ? 0 : P <= 2 ? 1 : P <= 4 ? 2 : P <= 8 ? 3 : P <= 16 ? 4 : 5; }
+
+// The column-split copy a (precision, width) uses, or null when it has none
+// (not applicable or not built).
+inline const evslcu_xsplit *xs_of(const evslcu_mat *M, int fp32, int B) {
+  const int P = xs_ranges(M, fp32, B);
+  if (!P) return nullptr;
+  const evslcu_xsplit *X = M->xs[xs_slot(P)];
+  if (!X || (fp32 && !X->val32[0])) return nullptr;
+  return X;
+}
+
+template <class VT, int B, bool PF, bool PL>
+cudaError_t xs_launch(cudaLaunchConfig_t &cfg, bool first, const XsRange<VT> &R, const VT *vk, const VT *vkm1, VT *out,
+                      VT *y, VT *part, const VT *coef) {
+  return first ? cudaLaunchKernelEx(&cfg, k_xs_step<VT, B, PF, PL, true>, R, vk, vkm1, out, y, part, coef)
+               : cudaLaunchKernelEx(&cfg, k_xs_step<VT, B, PF, PL, false>, R, vk, vkm1, out, y, part, coef);
+}
+
+template <class VT, int B>
+int xs_step(const evslcu_mat *M, int k, const VT *vk, const VT *vkm1, VT *out, VT *y, const VT *coef) {
+  constexpr bool F32 = std::is_same<VT, float>::value;
+  const evslcu_xsplit *X = xs_of(M, F32 ? 1 : 0, B);
+  if constexpr (B == 1) {
+    return fail(EVSLCU_ERR_ARG, "filter variant 7 takes 2 to 16 columns");
+  } else {
+    if (!X || !M->xs_acc) return fail(EVSLCU_ERR_ARG, "filter variant 7 needs a column-split copy for this width");
+    constexpr int TPR = Split<VT, B, 16>::TPR;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid_for((long long)((M->n + 31) & ~31) * TPR, kThreads, 1 << 20));
+    cfg.blockDim = dim3(kThreads);
+    cfg.stream = stream();
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    VT *part = (VT *)M->xs_acc;
+    for (int p = 0; p < X->P; ++p) {
+      const VT *val;
+      if constexpr (F32) val = X->val32[p];
+      else val = X->val[p];
+      const XsRange<VT> R{M->n, X->cptr[p], X->cw[p], X->col[p], val, X->perm[p]};
+      const bool first = (k == 1);
+      cudaError_t e;
+      if (X->P == 1)
+        e = xs_launch<VT, B, true, true>(cfg, first, R, vk, vkm1, out, y, part, coef);
+      else if (p == 0)
+        e = xs_launch<VT, B, true, false>(cfg, first, R, vk, vkm1, out, y, part, coef);
+      else if (p == X->P - 1)
+        e = xs_launch<VT, B, false, true>(cfg, first, R, vk, vkm1, out, y, part, coef);
+      else
+        e = xs_launch<VT, B, false, false>(cfg, first, R, vk, vkm1, out, y, part, coef);
+      if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "column-split filter launch failed: %s", cudaGetErrorString(e));
+      int rc = check_launch("k_xs_step");
+      if (rc) return rc;
+    }
+    return 0;
+  }
+}
+
 // One table entry of a row pattern: the value as a double and the column
 // offset from the row.
 __device__ __forceinline__ void pat_entry(const PatPView &A, int idx, double &v, int &off) {
@@ -384,6 +589,7 @@ int mf_step(const evslcu_mat *M, const SellT<AV, IT> &A, int variant, int k, con
     case 6:
       if constexpr (B == 1) return panel_mf_step<VT>(M, k, vk, vkm1, out, y, coef);
       return fail(EVSLCU_ERR_ARG, "filter variant 6 takes one column");
+    case 7: return xs_step<VT, B>(M, k, vk, vkm1, out, y, coef);
     case 4:
     case 5:
       if (!mf_pattern_ok(M)) return fail(EVSLCU_ERR_ARG, "filter variant %d needs the row-pattern dictionary", variant);
@@ -394,6 +600,12 @@ int mf_step(const evslcu_mat *M, const SellT<AV, IT> &A, int variant, int k, con
                         : mf_step_pat_v<VT, B, 32>(pat_view(M), k, vk, vkm1, out, y, coef);
     default: return mf_step_v<VT, B, 16, false>(A, k, vk, vkm1, out, y, coef);
   }
+}
+
+// Kernel launches of one degree step: one, or one per column range
+// (variant 7).
+inline int launches_per_step(const evslcu_mat *M, int fp32, int B, int variant) {
+  return (variant == 7) ? std::max(1, xs_ranges(M, fp32, B)) : 1;
 }
 
 // Number of VT values of the coefficient table of one group.
@@ -442,7 +654,7 @@ int mf_group(const evslcu_mat *M, const SellT<AV, IT> &A, int variant, int ncols
     k_mf_unpack<VT, B><<<g, kThreads, 0, stream()>>>(n, ncols, Y, ytab);
     rc = check_launch("k_mf_unpack");
   }
-  *nlaunch += maxdeg + 2;
+  *nlaunch += maxdeg * launches_per_step(M, std::is_same<VT, float>::value ? 1 : 0, B, variant) + 2;
   return rc;
 }
 
@@ -547,6 +759,67 @@ int variant_of(const evslcu_mat *A, int fp32, int B) {
   return v >= 0 ? v : 0;
 }
 
+constexpr int kXsMinRows = 1 << 18;
+
+// Builds the column-split copy a (precision, width) would use, with its FP32
+// values and the shared partial-sum block, when the matrix is a candidate:
+// SELL storage, no row-pattern dictionary in use, rows with increasing
+// columns, at least kXsMinRows rows.  0 when the copy is there afterwards
+// (or not applicable).
+int xs_build(evslcu_mat *A, int P);
+
+int xs_prepare(evslcu_mat *A, int fp32, int B) {
+  if (A->kernel != 0 || A->xs_bad || mf_pattern_ok(A) || !A->ia) return 0;
+  // the copy costs another stored matrix: only large matrices get one, unless
+  // the variant is forced
+  if (A->n < kXsMinRows && g_mf_variant != 7) return 0;
+  const int P = xs_ranges(A, fp32, B);
+  if (!P) return 0;
+  int rc = xs_build(A, P);
+  if (rc) return rc;
+  evslcu_xsplit *X = A->xs[xs_slot(P)];
+  if (fp32 && !X->val32[0]) {
+    for (int p = 0; p < X->P; ++p) {
+      long long sp = 0;
+      rc = evslcu_d2h(&sp, X->cptr[p] + X->nch, sizeof(long long));
+      if (rc) return rc;
+      X->val32[p] = (float *)evslcu_malloc(sizeof(float) * (size_t)std::max(sp, 1LL));
+      if (!X->val32[p]) return fail(EVSLCU_ERR_NOMEM, "column-split filter: out of device memory (FP32 values)");
+      k_to_float<<<grid_for(std::max(sp, 1LL)), kThreads, 0, stream()>>>(sp, X->val[p], X->val32[p]);
+      count_launch();
+      if ((rc = check_launch("k_to_float"))) return rc;
+    }
+  }
+  return 0;
+}
+
+// Builds (once) the copy with P ranges and the shared partial-sum block.
+int xs_build(evslcu_mat *A, int P) {
+  evslcu_xsplit *&X = A->xs[xs_slot(P)];
+  if (!X) {
+    evslcu_xsplit *nx = new evslcu_xsplit();
+    const int width = (int)(((long long)A->n + P - 1) / P);
+    int rc = build_xsplit_device(A, P, width, nx);
+    if (rc) {
+      for (int p = 0; p < evslcu_xsplit::kMaxRanges; ++p) {
+        evslcu_free(nx->cptr[p]);
+        evslcu_free(nx->cw[p]);
+        evslcu_free(nx->perm[p]);
+        evslcu_free(nx->col[p]);
+        evslcu_free(nx->val[p]);
+      }
+      delete nx;
+      return rc;
+    }
+    X = nx;
+  }
+  if (!A->xs_acc) {
+    A->xs_acc = evslcu_malloc(sizeof(double) * kMaxB * (size_t)A->n);
+    if (!A->xs_acc) return fail(EVSLCU_ERR_NOMEM, "column-split filter: out of device memory (partial sums)");
+  }
+  return 0;
+}
+
 // Autotuner: times every kernel variant for this matrix, precision and block
 // width on a few degree steps (CUDA events on the library stream, zero
 // vectors) and records the fastest in the matrix.  Runs once per
@@ -568,10 +841,12 @@ int autotune(evslcu_mat *A, int fp32, int B) {
   int bestv = 0;
   if (B == 1 && panel_candidate(A) && !(fp32 ? A->pn32 : A->pn64) && panel_build(A, fp32))
     cudaGetLastError();  // without the panel layout the SELL kernels serve
+  if (B > 1 && xs_prepare(A, fp32, B)) cudaGetLastError();  // without the split copy the SELL kernels serve
   for (int v = 0; !rc && v < kMfVariants; ++v) {
     if (g_mf_variant >= 0 && v != g_mf_variant) continue;  // a forced variant is only timed
     if ((v == 4 || v == 5) && !mf_pattern_ok(A)) continue;
     if (v == 6 && !(B == 1 && (fp32 ? A->pn32 : A->pn64))) continue;
+    if (v == 7 && !(B > 1 && xs_of(A, fp32, B))) continue;
     float ms = 0.0f;
     for (int rep = 0; !rc && rep < 2; ++rep) {
       cudaEventRecord(e0, stream());
@@ -605,7 +880,7 @@ int autotune(evslcu_mat *A, int fp32, int B) {
             }
           });
         }
-        count_launch();
+        count_launch(launches_per_step(A, fp32, B, v));
       }
       cudaEventRecord(e1, stream());
       if (cudaEventSynchronize(e1) != cudaSuccess) rc = fail(EVSLCU_ERR_CUDA, "filter autotune: timing failed");
@@ -687,6 +962,22 @@ int check_cols(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_col
 }
 
 }  // namespace
+
+// The column-split copy for blocks of row_bytes bytes per row (built on first
+// use, with the shared partial-sum block of n x 16 doubles); null when the
+// matrix has none (fewer than kXsMinRows rows unless any_size, no SELL
+// storage, a row-pattern dictionary in use, decreasing columns in a row, or
+// 32 ranges are not enough).
+const evslcu_xsplit *xsplit_for(evslcu_mat *A, size_t row_bytes, bool any_size) {
+  if (A->kernel != 0 || A->xs_bad || mf_pattern_ok(A) || !A->ia || (A->n < kXsMinRows && !any_size)) return nullptr;
+  const int P = xs_ranges_rows(A, row_bytes);
+  if (!P || xs_build(A, P)) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return A->xs[xs_slot(P)];
+}
+
 }  // namespace evslcu
 
 struct evslcu_filter_plan {
@@ -795,12 +1086,18 @@ int evslcu_filter_plan_run(evslcu_filter_plan *P, const double *const *x, double
 int evslcu_filter_plan_columns(const evslcu_filter_plan *P) { return P ? P->ncols : 0; }
 
 int evslcu_set_filter_variant(int v) {
-  if (v < -1 || v >= kMfVariants) return fail(EVSLCU_ERR_ARG, "filter variant must be -1 (tuned) or 0..6");
+  if (v < -1 || v >= kMfVariants) return fail(EVSLCU_ERR_ARG, "filter variant must be -1 (tuned) or 0..7");
   g_mf_variant = v;
   return 0;
 }
 
 int evslcu_get_filter_variant(void) { return g_mf_variant; }
+
+int evslcu_set_xs_range_bytes(long long bytes) {
+  if (bytes < 0) return fail(EVSLCU_ERR_ARG, "split range bytes must be >= 0");
+  g_xs_range_bytes = bytes ? (size_t)bytes : ((size_t)40 << 20);
+  return 0;
+}
 
 int evslcu_mat_filter_variant(const evslcu_mat *A, int fp32, int B) {
   return A ? A->mf_variant[fp32 ? 1 : 0][log2_width(B)] : -1;

@@ -746,6 +746,152 @@ __global__ void __launch_bounds__(kThreads, 4)
   }
 }
 
+// The same KPM block step on the column-split copy of a large general
+// matrix, for 8 probes p0 .. p0+nb-1 at a time.  With random columns the
+// gathers of k_kpm_dbl land on random rows of the whole probe block, most of
+// which miss L2; here the columns are cut into ranges whose rows of the
+// 8 probes (64 bytes each) fit in L2, one launch per range, each row's
+// running sum carried from range to range in xpart ([n][8], streaming
+// loads and stores).  The last range forms w_k+1 and the per-probe sums
+// <w_k+1, w_k+1>, <w_k+1, w_k> (and <w_0, w_0> first) into part, laid out as
+// k_kpm_dbl's so that k_kpm_reduce adds them up.  Four threads per row, two
+// probes each (one 16-byte access when VEC); a probe's sums run over the
+// rows in an order fixed by n and the grid, not by the other probes.
+constexpr int kKpmChunk = 8;
+
+template <bool PFIRST, bool PLAST, bool FIRST, bool VEC>
+__global__ void __launch_bounds__(kThreads)
+    k_kpm_xs(XsRange<double> A, int B, int p0, int nb, const double *__restrict__ vk, const double *vkm1,
+             double *out, double scal, double nctr, double *xpart, double *part) {
+  constexpr int TPR = kKpmChunk / 2, U = 4;
+  constexpr int NS = FIRST ? 3 : 2;
+  __shared__ double sh[NS][kThreads / 32][kKpmChunk];
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int q = lane & (TPR - 1);
+  const bool onA = 2 * q < nb, onB = 2 * q + 1 < nb;
+  double sum[NS][2];
+#pragma unroll
+  for (int t = 0; t < NS; ++t) sum[t][0] = sum[t][1] = 0.0;
+  const int npad = (A.n + 31) & ~31;
+  const long long total = (long long)npad * TPR;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  auto ld2 = [&](const double *src, double &a, double &b, bool cs) {
+    if (VEC && onB) {
+      const double2 v = cs ? __ldcs(reinterpret_cast<const double2 *>(src)) : __ldg(reinterpret_cast<const double2 *>(src));
+      a = v.x;
+      b = v.y;
+    } else {
+      a = onA ? (cs ? __ldcs(src) : __ldg(src)) : 0.0;
+      b = onB ? (cs ? __ldcs(src + 1) : __ldg(src + 1)) : 0.0;
+    }
+  };
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+    const int sl = (int)(g / TPR);
+    const bool live = sl < A.n;
+    const int r = live ? __ldg(A.perm + sl) : 0;
+    const long long base = (long long)r * B + p0 + 2 * q;
+    double* const xp = xpart + (long long)r * kKpmChunk + 2 * q;
+    double acc0 = 0.0, acc1 = 0.0;
+    if (!PFIRST && live) {
+      const double2 v = __ldcs(reinterpret_cast<const double2 *>(xp));
+      acc0 = v.x;
+      acc1 = v.y;
+    }
+    double x0 = 0.0, x1 = 0.0, m0 = 0.0, m1 = 0.0;
+    if (PLAST && live) {
+      ld2(vk + base, x0, x1, false);
+      if (!FIRST) ld2(vkm1 + base, m0, m1, true);
+    }
+    const int ch = sl >> 5;
+    long long p = __ldg(A.cptr + ch) + (sl & 31);
+    const int w = __ldg(A.cw + ch);
+    double v[U];
+    int col[U];
+    auto fetch = [&](int j0, long long pp, double(&vv)[U], int(&cc)[U]) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (live && j0 + u < w) {
+          vv[u] = __ldcs(A.val + pp + 32 * u);
+          cc[u] = __ldcs(A.col + pp + 32 * u);
+        } else {
+          vv[u] = 0.0;
+          cc[u] = -1;
+        }
+      }
+    };
+    fetch(0, p, v, col);
+    for (int j = 0; j < w; j += U, p += 32 * U) {
+      double g0[U], g1[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        g0[u] = g1[u] = 0.0;
+        if (col[u] >= 0) ld2(vk + (long long)col[u] * B + p0 + 2 * q, g0[u], g1[u], false);
+      }
+      double vn[U];
+      int cn[U];
+      fetch(j + U, p + 32 * U, vn, cn);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (col[u] >= 0) {
+          acc0 = __dadd_rn(acc0, __dmul_rn(v[u], g0[u]));
+          acc1 = __dadd_rn(acc1, __dmul_rn(v[u], g1[u]));
+        }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        v[u] = vn[u];
+        col[u] = cn[u];
+      }
+    }
+    if (!live) continue;
+    if (!PLAST) {
+      __stcs(reinterpret_cast<double2 *>(xp), make_double2(acc0, acc1));
+      continue;
+    }
+    double w0 = __dmul_rn(scal, __dadd_rn(acc0, __dmul_rn(nctr, x0)));
+    double w1 = __dmul_rn(scal, __dadd_rn(acc1, __dmul_rn(nctr, x1)));
+    if (!FIRST) {
+      w0 = __dadd_rn(w0, -m0);
+      w1 = __dadd_rn(w1, -m1);
+    }
+    if (onA) out[base] = w0;
+    if (onB) out[base + 1] = w1;
+    sum[0][0] += w0 * w0;
+    sum[0][1] += w1 * w1;
+    sum[1][0] += w0 * x0;
+    sum[1][1] += w1 * x1;
+    if (FIRST) {
+      sum[NS - 1][0] += x0 * x0;
+      sum[NS - 1][1] += x1 * x1;
+    }
+  }
+  if constexpr (PLAST) {
+    // lanes q, q+4, ..., q+28 hold the same probes: fixed butterfly over them
+#pragma unroll
+    for (int t = 0; t < NS; ++t)
+#pragma unroll
+      for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int o = TPR; o < 32; o <<= 1) sum[t][c] += __shfl_xor_sync(0xffffffffu, sum[t][c], o);
+    if (lane < TPR) {
+#pragma unroll
+      for (int t = 0; t < NS; ++t) {
+        sh[t][warp][2 * q] = sum[t][0];
+        sh[t][warp][2 * q + 1] = sum[t][1];
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < NS * kKpmChunk; t += blockDim.x) {
+      const int s = t / kKpmChunk, l = t % kKpmChunk;
+      if (l >= nb) continue;
+      double acc = 0.0;
+      for (int wi = 0; wi < kThreads / 32; ++wi) acc += sh[s][wi][l];
+      part[((long long)s * B + p0 + l) * gridDim.x + blockIdx.x] = acc;
+    }
+  }
+}
+
 // raw[q] = sum over the nb block partials of sum q (block q; fixed order).
 __global__ void __launch_bounds__(kThreads) k_kpm_reduce(int nb, const double *__restrict__ part, double *raw) {
   __shared__ double sh[kThreads / 32];
@@ -1236,6 +1382,7 @@ void evslcu_mat_destroy(evslcu_mat *M) {
   evslcu_free(M->cw);
   evslcu_free(M->perm);
   panel_free(M);
+  xsplit_free(M);
   evslcu_mat_l2_persist(M, 0);
   evslcu_free(M->sell_block);
   evslcu_free(M->wave_ctl);
@@ -1290,6 +1437,74 @@ int evslcu_cheb_update(int n, int k, double t, double s, double cc, double *vkp1
 }
 
 static int g_kpm_doubling = 1;
+static int g_kpm_split = -1;  // -1: automatic, 0: never, 1: whenever the matrix has a column-split copy
+
+// The column-split copy the KPM block step runs on, or null for k_kpm_dbl:
+// automatically for matrices whose columns reach far from the diagonal (the
+// gathers of one step then spread over the whole probe block), whatever the
+// probe count, so that probe shards take the same path as the full block.
+static const evslcu_xsplit *kpm_split_copy(const evslcu_op *op) {
+  if (g_kpm_split == 0 || !op->A) return nullptr;
+  evslcu_mat *M = const_cast<evslcu_mat *>(op->A);
+  if (g_kpm_split < 0 && M->bandwidth < (1 << 17)) return nullptr;
+  return xsplit_for(M, sizeof(double) * kKpmChunk, g_kpm_split == 1);
+}
+
+}  // extern "C"
+
+namespace evslcu {
+
+template <bool PF, bool PL, bool FIRST>
+static cudaError_t kpm_xs_launch(int grid, bool vec, const XsRange<double> &R, int B, int p0, int nb, const double *vk,
+                                 const double *vkm1, double *o, double scal, double nctr, double *xpart, double *part) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.stream = stream();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return vec ? cudaLaunchKernelEx(&cfg, k_kpm_xs<PF, PL, FIRST, true>, R, B, p0, nb, vk, vkm1, o, scal, nctr, xpart, part)
+             : cudaLaunchKernelEx(&cfg, k_kpm_xs<PF, PL, FIRST, false>, R, B, p0, nb, vk, vkm1, o, scal, nctr, xpart, part);
+}
+
+// One KPM block step of all probes on the column-split copy X: per chunk of 8
+// probes, one launch per column range.
+static int kpm_xs_step(const evslcu_mat *M, const evslcu_xsplit *X, int grid, int B, bool first, const double *vk,
+                       const double *vkm1, double *o, double scal, double nctr, double *part) {
+  const bool vec = (B % 2 == 0);
+  double *xpart = (double *)M->xs_acc;
+  for (int p0 = 0; p0 < B; p0 += kKpmChunk) {
+    const int nb = std::min(kKpmChunk, B - p0);
+    for (int p = 0; p < X->P; ++p) {
+      const XsRange<double> R{M->n, X->cptr[p], X->cw[p], X->col[p], X->val[p], X->perm[p]};
+      const bool pf = (p == 0), pl = (p == X->P - 1);
+      cudaError_t e;
+      if (pf && pl)
+        e = first ? kpm_xs_launch<true, true, true>(grid, vec, R, B, p0, nb, vk, vkm1, o, scal, nctr, xpart, part)
+                  : kpm_xs_launch<true, true, false>(grid, vec, R, B, p0, nb, vk, vkm1, o, scal, nctr, xpart, part);
+      else if (pf)
+        e = kpm_xs_launch<true, false, false>(grid, vec, R, B, p0, nb, vk, vkm1, o, scal, nctr, xpart, part);
+      else if (pl)
+        e = first ? kpm_xs_launch<false, true, true>(grid, vec, R, B, p0, nb, vk, vkm1, o, scal, nctr, xpart, part)
+                  : kpm_xs_launch<false, true, false>(grid, vec, R, B, p0, nb, vk, vkm1, o, scal, nctr, xpart, part);
+      else
+        e = kpm_xs_launch<false, false, false>(grid, vec, R, B, p0, nb, vk, vkm1, o, scal, nctr, xpart, part);
+      if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "KPM launch failed: %s", cudaGetErrorString(e));
+      count_launch();
+      int rc = check_launch("k_kpm_xs");
+      if (rc) return rc;
+    }
+  }
+  return 0;
+}
+
+}  // namespace evslcu
+
+extern "C" {
+
 static double *g_kpm_ws = nullptr;  // cached KPM workspace (product-identity path)
 static size_t g_kpm_ws_cap = 0;
 
@@ -1301,6 +1516,12 @@ void evslcu_kpm_release(void) {
 
 int evslcu_set_kpm_doubling(int on) {
   g_kpm_doubling = on ? 1 : 0;
+  return 0;
+}
+
+int evslcu_set_kpm_split(int mode) {
+  if (mode < -1 || mode > 1) return fail(EVSLCU_ERR_ARG, "KPM split mode must be -1, 0 or 1");
+  g_kpm_split = mode;
   return 0;
 }
 
@@ -1345,13 +1566,15 @@ static int kpm_dots_doubling(const evslcu_op *op, int n, int Mdeg, int nvec, con
   const CsrView A = csr_view(op->A);
   const double nctr = -ctr;
   double *W[2] = {W0, W1};
+  const evslcu_xsplit *X = rc ? nullptr : kpm_split_copy(op);
   for (int k = 0; !rc && k < K; ++k) {
     const double scal = (k == 0 ? 1.0 : 2.0) / wid;
     const double *vk = (k == 0) ? V0 : W[(k - 1) % 2];
     const double *vkm1 = (k == 0) ? nullptr : ((k == 1) ? V0 : W[k % 2]);
     double *o = W[k % 2];
     double *rr = raw + (size_t)k * 3 * B;
-    for (int p0 = 0; !rc && p0 < B; p0 += 32) {
+    if (X) rc = kpm_xs_step(op->A, X, grid, B, k == 0, vk, vkm1, o, scal, nctr, part);
+    for (int p0 = 0; !X && !rc && p0 < B; p0 += 32) {
       const int nb = std::min(32, B - p0);
       const bool vec = (B % 2 == 0);  // two probes per 16-byte access
       if (k == 0 && vec)

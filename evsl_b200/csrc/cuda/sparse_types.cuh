@@ -21,6 +21,32 @@
 // identical bit for bit across variants.
 struct evslcu_panels;  // column-panel layout (panel.cu)
 
+// Column-split SELL-C-sigma copy for the multi-column filter on large
+// general matrices (built by build_xsplit_device, ingest.cu).  The columns
+// are cut into P >= 1 ranges of `width` consecutive columns; range p holds, for
+// every row, the row's entries whose column lies in the range, in CSR order,
+// stored as its own SELL-C-sigma (chunks of 32 slots, rows of each 256-row
+// window sorted by their length in this range, slot -> row map perm).
+// Padding slots carry column -1 and are skipped.  A degree step of a
+// B-column block then runs range by range: the rows of x a range gathers
+// from (width x B values) stay in L2 while the range is processed, and each
+// row's running sum is carried from range to range in a partial-sum block.
+// Ranges are visited in column order and the entries of a range in CSR
+// order, so each row is still summed left to right in its CSR order.
+struct evslcu_xsplit {
+  static constexpr int kMaxRanges = 32;
+  int P = 0;
+  int width = 0;  // columns per range (the last one may be shorter)
+  int nch = 0;    // chunks per range
+  long long slots = 0;  // stored slots over all ranges
+  long long *cptr[kMaxRanges] = {};  // nch + 1 chunk offsets of each range
+  int *cw[kMaxRanges] = {};          // chunk widths
+  int *perm[kMaxRanges] = {};        // slot -> row (32 nch entries)
+  int *col[kMaxRanges] = {};         // column of each stored slot (-1: padding)
+  double *val[kMaxRanges] = {};      // value of each stored slot
+  float *val32[kMaxRanges] = {};     // FP32 copy, made on first FP32 use
+};
+
 struct evslcu_mat {
   int n = 0;
   long long nnz = 0;
@@ -69,6 +95,9 @@ struct evslcu_mat {
   int use_pat = 0;     // 1: the FP64 single-vector filter and SpMV read the dictionary
   evslcu_panels *pn64 = nullptr;  // column-panel layout for the FP64 kernels (large general matrices)
   evslcu_panels *pn32 = nullptr;  // the same for the FP32 kernels
+  evslcu_xsplit *xs[6] = {};      // column-split copies with 1, 2, 4, 8, 16, 32 ranges (null: not built)
+  void *xs_acc = nullptr;         // partial-sum block of the column-split filter (n x 16 doubles)
+  int xs_bad = 0;                 // 1: no column-split copy (a row's columns are not increasing)
   int cheb_variant = -1;      // single-vector filter kernel chosen by timing (-1: not yet)
   float cheb_us[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // measured time per degree step of each variant
   int cheb_grid = 0;                      // tuned block limit per degree step (0: one row per thread)
@@ -83,6 +112,26 @@ int build_sell_device(evslcu_mat *M, int allow_compress);
 // Builds M's row-pattern dictionary when its rows take at most 1024
 // distinct forms; leaves M->pat_id null otherwise (ingest.cu).
 int build_patterns_device(evslcu_mat *M);
+// Builds M's column-split copy with P column ranges of `width` columns into X
+// (ingest.cu).  Fails with EVSLCU_ERR_ARG, and sets M->xs_bad, when a row's
+// column indices are not strictly increasing.
+int build_xsplit_device(evslcu_mat *M, int P, int width, evslcu_xsplit *X);
+void xsplit_free(evslcu_mat *M);
+// The column-split copy for blocks of row_bytes bytes per row, built on first
+// use (multifilter.cu); null when the matrix has none (or is smaller than
+// the size worth a copy, unless any_size).
+const evslcu_xsplit *xsplit_for(evslcu_mat *M, size_t row_bytes, bool any_size = false);
+
+// One column range of a column-split copy, as the kernels read it.
+template <class VT>
+struct XsRange {
+  int n;
+  const long long *__restrict__ cptr;
+  const int *__restrict__ cw;
+  const int *__restrict__ col;
+  const VT *__restrict__ val;
+  const int *__restrict__ perm;
+};
 
 template <class VT, class IT>
 struct SellT {

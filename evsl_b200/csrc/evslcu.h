@@ -216,10 +216,15 @@ int evslcu_filter_plan_run(evslcu_filter_plan *P, const double *const *x, double
 int evslcu_filter_plan_columns(const evslcu_filter_plan *P);
 /* Multi-column kernel variant (0..3): bit 0 = 32-byte column parts per
  * thread (else 16), bit 1 = rows' stored entries loaded cooperatively;
+ * 4, 5: row-pattern dictionary; 6: column panels (one column); 7: the
+ * column-split copy (2-16 columns);
  * -1 (default): per matrix, precision and block width, the variant an
  * autotuner measured fastest (timed once, on first use). */
 int evslcu_set_filter_variant(int v);
 int evslcu_get_filter_variant(void);
+/* Bytes of block rows one column range of the column-split filter
+ * (variant 7) gathers from; 0: the default (40 MiB). */
+int evslcu_set_xs_range_bytes(long long bytes);
 /* Variant the autotuner chose for A (fp32, block width B), -1 if untuned. */
 int evslcu_mat_filter_variant(const evslcu_mat *A, int fp32, int B);
 /* Measured device time (µs) of one degree step of the multi-column filter on
@@ -290,6 +295,12 @@ int evslcu_set_row_unroll(int on);
  * moments per block matrix product (1, default), or one dot with the probe
  * per degree as the reference (0).  The moments agree to rounding. */
 int evslcu_set_kpm_doubling(int on);
+/* KPM block step of the product-identity form on the column-split copy of
+ * the matrix (8 probes at a time, one launch per column range): -1
+ * (default) for large matrices whose columns reach far from the diagonal,
+ * 0 never, 1 whenever the matrix can have a copy.  The moments agree to
+ * rounding. */
+int evslcu_set_kpm_split(int mode);
 /* Free the cached KPM and tridiagonal workspaces (evslcu_finish calls them). */
 void evslcu_kpm_release(void);
 void evslcu_trid_release(void);

@@ -1132,6 +1132,11 @@ int evslx_set_filter_variant(int v) {
 
 int evslx_get_filter_variant(void) { return evslcu_get_filter_variant(); }
 
+int evslx_set_split_range_bytes(long long bytes) {
+  int rc = evslcu_set_xs_range_bytes(bytes);
+  return rc ? evsl_seterr(rc, "%s", evslcu_errstr()) : 0;
+}
+
 int evslx_tuned_filter_variant(int precision, int ncols) {
   if (evsl_require_operator() || !evsl_op()->A) return -1;
   int B = 1;

@@ -333,11 +333,28 @@ int evslx_chebav_multi(int ncols, const polparams *pols, const double *X, double
  * 4, 5 -- the row-pattern dictionary (see evslx_set_row_patterns), 16- or
  * 32-byte column parts; filtering fails with EVSLX_ERR_ARG when the matrix
  * has none;
+ * 6 -- one column on the column-panel layout (large general matrices);
+ * 7 -- 2 to 16 columns on the column-split copy: the columns are cut into
+ * ranges whose rows of the block fit in L2 (see
+ * evslx_set_split_range_bytes), a degree step runs range by range and
+ * carries each row's running sum between ranges (one range when the whole
+ * block fits); streaming cache hints keep the gathered rows in L2.  Tried by
+ * the autotuner on matrices of at least 2^18 rows (it costs another stored
+ * copy of the matrix).
+ * Rows are summed in their CSR order and padding is skipped, so FP64
+ * columns equal ChebAv bit for bit.  Needs increasing column indices in
+ * every row; filtering fails with EVSLX_ERR_ARG when the matrix or width
+ * has no such copy;
  * -1 (default) -- autotuned: the first filter on a matrix with a given
  * precision and block width times the variants available for it on a few
  * degree steps and keeps the fastest for that matrix. */
 int evslx_set_filter_variant(int v);
 int evslx_get_filter_variant(void);
+/* Bytes of the block's rows one column range of filter variant 7 may
+ * gather from (default 40 MiB, about a third of the B200's L2; 0 restores
+ * it).  Widths whose block fits in this many bytes run as one range.  Applies
+ * to matrices whose filter is tuned afterwards. */
+int evslx_set_split_range_bytes(long long bytes);
 /* The variant tuned for the registered matrix (-1: not tuned yet). */
 int evslx_tuned_filter_variant(int precision, int ncols);
 

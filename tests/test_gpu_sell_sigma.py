@@ -224,3 +224,120 @@ def test_panel_filter_bitwise(gpu_lib, rspd, case):
         gpu_lib.set_filter_variant(-1)
         gpu_lib.set_filter_kernel(-1)
         gpu_lib.set_panel_filter(True, 1 << 18, 16384)
+
+
+@pytest.mark.parametrize("ncols, range_kib", [(2, 128), (3, 128), (8, 128), (16, 128), (4, 0)])
+def test_column_split_filter_bitwise(gpu_lib, rspd, ncols, range_kib):
+    """Filter variant 7 (the column-split copy: column ranges whose rows of
+    the block fit a byte budget, each row's running sum carried from range to
+    range) on the random SPD matrix, with the budget lowered to 128 KiB so
+    that this 20,013-row matrix is cut into 2 to 32 ranges at every width,
+    and with the default budget (one range).  Columns
+    with their own polynomials (degrees 24-45, some masked early): FP64 is the
+    reference's ChebAv of each column bit for bit (rows summed in CSR order,
+    padding skipped); FP32 equals the SELL kernel's FP32 result (same fused
+    multiply-adds in the same order) and is within 1e-4 of FP64."""
+    ia, ja, a = rspd
+    n = len(ia) - 1
+    lo, hi = W.gershgorin_bounds(ia, ja, a)
+    ivs = [[lo + (0.2 + 0.03 * c) * (hi - lo), lo + (0.25 + 0.03 * c) * (hi - lo), lo, hi] for c in range(ncols)]
+    degs = [24 + (7 * c) % 22 for c in range(ncols)]
+    X = np.stack([O.seeded_normal(n, 40 + c) for c in range(ncols)])
+    refs = [O.cheb_av(O.find_pol(ivs[c], deg=degs[c]), ia, ja, a, X[c]) for c in range(ncols)]
+    pols = [gpu_lib.find_pol(ivs[c], deg=degs[c]) for c in range(ncols)]
+    gpu_lib.set_split_range_bytes(range_kib << 10)
+    try:
+        _register(gpu_lib, -1, ia, ja, a)
+        gpu_lib.set_filter_variant(7)
+        Y64 = gpu_lib.chebav_multi(pols, X, E.PREC_FP64)
+        for c in range(ncols):
+            assert np.array_equal(Y64[c], refs[c]), (c, np.max(np.abs(Y64[c] - refs[c])))
+        Y32 = gpu_lib.chebav_multi(pols, X, E.PREC_MIXED)
+        assert np.max(np.abs(Y32 - Y64)) <= 1e-4 * np.max(np.abs(Y64))
+        gpu_lib.set_filter_variant(0)
+        assert np.array_equal(gpu_lib.chebav_multi(pols, X, E.PREC_MIXED), Y32)
+        # tuned on a freshly registered matrix: whichever variant wins, FP64 stays bitwise
+        gpu_lib.set_filter_variant(-1)
+        _register(gpu_lib, -1, ia, ja, a)
+        Y = gpu_lib.chebav_multi(pols, X, E.PREC_FP64)
+        assert all(np.array_equal(Y[c], refs[c]) for c in range(ncols))
+    finally:
+        gpu_lib.set_filter_variant(-1)
+        gpu_lib.set_split_range_bytes(0)
+        for p in pols:
+            gpu_lib.free_pol(p)
+
+
+def test_column_split_needs_increasing_columns(gpu_lib):
+    """A row whose column indices are not increasing has no column-split
+    copy: forcing variant 7 fails with an error, the tuned filter serves it
+    with the SELL kernels in CSR order (bitwise the reference)."""
+    ia, ja, a = W.random_spd_csr(3001, 16, 35)
+    ja = ja.copy()
+    a = a.copy()
+    r = 17
+    ja[ia[r]:ia[r + 1]] = ja[ia[r]:ia[r + 1]][::-1].copy()
+    a[ia[r]:ia[r + 1]] = a[ia[r]:ia[r + 1]][::-1].copy()
+    n = len(ia) - 1
+    lo, hi = W.gershgorin_bounds(ia, ja, a)
+    iv = [lo + 0.3 * (hi - lo), lo + 0.35 * (hi - lo), lo, hi]
+    X = np.stack([O.seeded_normal(n, 50 + c) for c in range(4)])
+    pol = gpu_lib.find_pol(iv, deg=20)
+    ref = O.cheb_av(O.find_pol(iv, deg=20), ia, ja, a, X[0])
+    gpu_lib.set_split_range_bytes(16 << 10)
+    try:
+        _register(gpu_lib, -1, ia, ja, a)
+        gpu_lib.set_filter_variant(7)
+        with pytest.raises(E.EvslError):
+            gpu_lib.chebav_multi([pol] * 4, X, E.PREC_FP64)
+        gpu_lib.set_filter_variant(-1)
+        _register(gpu_lib, -1, ia, ja, a)
+        Y = gpu_lib.chebav_multi([pol] * 4, X, E.PREC_FP64)
+        assert np.array_equal(Y[0], ref)
+        assert gpu_lib.tuned_filter_variant(E.PREC_FP64, 4) != 7
+    finally:
+        gpu_lib.set_filter_variant(-1)
+        gpu_lib.set_split_range_bytes(0)
+        gpu_lib.free_pol(pol)
+
+
+@pytest.mark.parametrize("nvec", [12, 13])
+def test_kpm_on_column_split_copy(gpu_lib, rspd, nvec):
+    """The KPM block step on the column-split copy (8 probes at a time, one
+    launch per column range, running sums carried between ranges), forced on
+    the 20,013-row random SPD matrix with 128 KiB ranges: moments within 1e-12
+    (normwise, and per moment relative where |mu_k| >= 1e-3 max |mu|) of the
+    reference's direct per-degree recurrence restated in the oracle and of
+    the default kernel; even (16-byte loads) and odd probe counts; each
+    probe's dot products bitwise the same whichever probes share its block,
+    so probe shards reproduce the full block."""
+    import ctypes as C
+
+    ia, ja, a = rspd
+    n = len(ia) - 1
+    lo, hi = W.gershgorin_bounds(ia, ja, a)
+    iv = [lo + 0.3 * (hi - lo), lo + 0.36 * (hi - lo), lo, hi]
+    M = 60
+    probes = O.seeded_rademacher(nvec, n, 71)
+    mu_or, ec_or = O.kpmdos(M, 1, probes, iv, ia, ja, a)
+    _register(gpu_lib, -1, ia, ja, a)
+    mu_def, ec_def = gpu_lib.kpmdos_probes(M, 1, probes, iv)
+    gpu_lib.set_split_range_bytes(128 << 10)
+    gpu_lib.lib.evslcu_set_kpm_split.argtypes = [C.c_int]
+    try:
+        _register(gpu_lib, -1, ia, ja, a)
+        gpu_lib.lib.evslcu_set_kpm_split(1)
+        mu, ec = gpu_lib.kpmdos_probes(M, 1, probes, iv)
+        for ref in (mu_or, mu_def):
+            assert np.max(np.abs(mu - ref)) <= 1e-12 * np.max(np.abs(ref))
+            big = np.abs(ref) >= 1e-3 * np.max(np.abs(ref))
+            assert np.all(np.abs(mu - ref)[big] <= 1e-12 * np.abs(ref)[big])
+        assert abs(ec - ec_or) <= 1e-10 * abs(ec_or)
+        full = E.DeviceBuffer.from_host(gpu_lib.lib, probes)
+        dots = gpu_lib.kpm_dots(M, iv, full, nvec)
+        for a0, b0 in ((0, 5), (5, nvec)):
+            part = E.DeviceBuffer.from_host(gpu_lib.lib, np.ascontiguousarray(probes[a0:b0]))
+            assert np.array_equal(gpu_lib.kpm_dots(M, iv, part, b0 - a0), dots[:, a0:b0])
+    finally:
+        gpu_lib.lib.evslcu_set_kpm_split(-1)
+        gpu_lib.set_split_range_bytes(0)
