@@ -86,6 +86,8 @@ def parse():
     p.add_argument("--sigma", type=int, default=-1,
                    help="rspd-filter: SELL-C-sigma sort window (-1 automatic, 0 unsorted SELL-32)")
     p.add_argument("--instances", type=int, default=128, help="batch-uneven: independent Laplacians")
+    p.add_argument("--batch-persistent", type=int, choices=[0, 1], default=0,
+                   help="batch-uneven: the batched filter as one persistent launch (1) or one launch per degree (0)")
     p.add_argument("--gemm", default="1000000,1000,256",
                    help="dgemm: n,K,m of the Ritz product V(n x K) Y(K x m)")
     p.add_argument("--ncols", type=int, default=16, help="lap3d-multifilter: columns")
@@ -1166,6 +1168,7 @@ def run_batch_uneven(args):
     from evsl_b200 import workloads as W
 
     lib = E.Library()
+    lib.set_batch_persistent(bool(args.batch_persistent))
     inst = uneven_instances(args.instances)
     mats, pols, vs = [], [], []
     for i, (dims, iv, _) in enumerate(inst):
@@ -1178,6 +1181,7 @@ def run_batch_uneven(args):
     prec = E.PREC_MIXED if args.precision == "mixed" else E.PREC_FP64
     lstream = torch.cuda.ExternalStream(lib.stream_handle())
     maxit = 1000
+    phases = []
 
     def one_batch():
         eng = lib.engine(len(inst), precision=prec)
@@ -1190,6 +1194,7 @@ def run_batch_uneven(args):
             if r is None:
                 break
             out[int(r["tag"])] = r
+        phases.append(eng.phase_times())
         eng.free()
         return out
 
@@ -1247,9 +1252,11 @@ def run_batch_uneven(args):
         "data": "synthetic (2-D/3-D Dirichlet Laplacians, seeded sizes, intervals and start vectors)",
         "config": {"workload": "batch-uneven: %d Laplacians, n log-uniform in [1e3, 2e5] (sum %d rows), 20-80 "
                                "eigenvalues each, one engine, %s" % (len(inst), sum(sizes), args.precision),
+                   "batched_filter": "persistent" if args.batch_persistent else "one launch per degree",
                    "filter_degrees": [int(p.deg) for p in pols], "n": sizes, "tol": TOL, "maxit": maxit},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "sequential_chebLanNr_same_instances": seq,
+        "engine_phase_seconds_last_step": phases[-1] if phases else None,
         "accuracy": {"max_abs_eig_err_vs_analytic": max_err, "max_residual": max_res,
                      "bar": "counts exact, |err| <= 1e-8 x width, residual < 1e-8", "failures": bad[:10]},
         "all_steps_ok": bool(ok), "gpu_launches": int(launches), "clocks": clocks}))

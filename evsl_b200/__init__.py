@@ -297,6 +297,9 @@ def load():
         "evslx_result_free": ([C.POINTER(EvslxResult)], None),
         "evslx_engine_use_graphs": ([C.c_void_p, C.c_int], None),
         "evslx_engine_use_batch": ([C.c_void_p, C.c_int, C.c_int], None),
+        "evslx_set_batch_persistent": ([C.c_int], C.c_int),
+        "evslx_engine_use_batch_ops": ([C.c_void_p, C.c_int], None),
+        "evslx_engine_phase_times": ([C.c_void_p, _dp], None),
         "evslx_engine_batched_columns": ([C.c_void_p], C.c_uint64),
         "evslx_set_mixed_min_rows": ([C.c_int], None),
         "evslx_set_filter_variant": ([C.c_int], C.c_int),
@@ -417,6 +420,18 @@ class Engine:
 
     def run(self):
         self._check(self.lib.evslx_engine_run(self.ptr), "evslx_engine_run")
+
+    def use_batch_ops(self, on):
+        """The slots' Lanczos vector operations in one launch per operation
+        (True, default) or per slot (False)."""
+        self.lib.evslx_engine_use_batch_ops(self.ptr, 1 if on else 0)
+
+    def phase_times(self):
+        """Host seconds per step phase: filter issue, Lanczos issue, scalar wait,
+        host part, retirement."""
+        out = np.zeros(5)
+        self.lib.evslx_engine_phase_times(self.ptr, _d(out))
+        return dict(zip(("filter_issue", "lanczos_issue", "scalar_wait", "host", "retire"), out.tolist()))
 
     def pending(self):
         return self.lib.evslx_engine_pending(self.ptr)
@@ -732,6 +747,11 @@ class Library:
 
     def tuned_filter_variant(self, precision, ncols):
         return self.lib.evslx_tuned_filter_variant(precision, ncols)
+
+    def set_batch_persistent(self, on):
+        """The engines' batched filter as one persistent launch (True) or one
+        launch per degree (False, default)."""
+        self._check(self.lib.evslx_set_batch_persistent(1 if on else 0), "evslx_set_batch_persistent")
 
     def set_split_range_bytes(self, nbytes):
         """Bytes of block rows one column range of filter variant 7 gathers

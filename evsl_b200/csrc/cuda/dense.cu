@@ -60,39 +60,44 @@ constexpr int kGemvTRows = 1024;   // rows per chunk of the transposed product
 constexpr int kGemvTCols = 32;     // columns per block
 constexpr int kGemvNChunk = 2048;  // h values staged in shared memory at once
 
-// part[chunk * k + j] = sum over the chunk's rows of Q[r, j] * v[r]
-__global__ void __launch_bounds__(kThreads)
-    k_gemvT_partial(int n, int k, const double *__restrict__ Q, long long ld, const double *__restrict__ v,
-                    double *__restrict__ part, const double *state) {
-  if (state && state[2] != 0.0) return;
-  __shared__ double sv[kGemvTRows];
-  const int r0 = blockIdx.x * kGemvTRows;
+// part[chunk * k + j] = sum over the chunk's rows of Q[r, j] * v[r]; block
+// (bx, by) of the chunk x column-tile grid.  Shared by the single-vector
+// kernel and the engine's batched one, so both round alike.
+__device__ __forceinline__ void gemvT_partial_body(int n, int k, const double *__restrict__ Q, long long ld,
+                                                   const double *__restrict__ v, double *__restrict__ part, int bx,
+                                                   int by, double *sv) {
+  const int r0 = bx * kGemvTRows;
   const int rows = min(kGemvTRows, n - r0);
   for (int i = threadIdx.x; i < kGemvTRows; i += blockDim.x) sv[i] = (i < rows) ? v[r0 + i] : 0.0;
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int jj = warp; jj < kGemvTCols; jj += kThreads / 32) {
-    const int j = blockIdx.y * kGemvTCols + jj;
+    const int j = by * kGemvTCols + jj;
     if (j >= k) break;
     const double *q = Q + (long long)j * ld + r0;
     double acc = 0.0;
 #pragma unroll 8
     for (int i = lane; i < rows; i += 32) acc += __ldg(q + i) * sv[i];  // 32 loads per lane, unrolled
     acc = warp_sum(acc);
-    if (lane == 0) part[(long long)blockIdx.x * k + j] = acc;
+    if (lane == 0) part[(long long)bx * k + j] = acc;
   }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_gemvT_partial(int n, int k, const double *__restrict__ Q, long long ld, const double *__restrict__ v,
+                    double *__restrict__ part, const double *state) {
+  if (state && state[2] != 0.0) return;
+  __shared__ double sv[kGemvTRows];
+  gemvT_partial_body(n, k, Q, ld, v, part, blockIdx.x, blockIdx.y, sv);
 }
 
 // h[j] = alpha * sum_chunks part[chunk*k + j] (+ beta * h[j] when beta != 0).
 // Block of 256 threads = 8 warps per 32 columns: lane = column, warp w sums
 // chunks w, w+8, ...; the 8 warp sums are added in warp order (fixed order).
-__global__ void __launch_bounds__(256)
-    k_gemvT_reduce(int nchunks, int k, const double *part, double alpha, double beta, double *h,
-                   const double *state) {
-  if (state && state[2] != 0.0) return;
-  __shared__ double sh[8][33];
+__device__ __forceinline__ void gemvT_reduce_body(int nchunks, int k, const double *part, double alpha, double beta,
+                                                  double *h, int bx, double (*sh)[33]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int j = blockIdx.x * 32 + lane;
+  const int j = bx * 32 + lane;
   double s = 0.0;
   if (j < k)
     for (int c = warp; c < nchunks; c += 8) s += part[(long long)c * k + j];
@@ -106,17 +111,24 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+__global__ void __launch_bounds__(256)
+    k_gemvT_reduce(int nchunks, int k, const double *part, double alpha, double beta, double *h,
+                   const double *state) {
+  if (state && state[2] != 0.0) return;
+  __shared__ double sh[8][33];
+  gemvT_reduce_body(nchunks, k, part, alpha, beta, h, blockIdx.x, sh);
+}
+
 // v[r] <- v[r] + sum_j (alpha*h[j]) * Q[r, j], summed over j in order as the
 // reference dgemv('N') does.  With `state`, also computes ||v|| and applies
 // the DGKS decision of SRC/misc_la.c:246-250.
-__global__ void __launch_bounds__(kThreads)
-    k_gemvN(int n, int k, const double *__restrict__ Q, long long ld, const double *__restrict__ h, double alpha,
-            double *v, double *part, unsigned int *ctr, double *state) {
-  if (state && state[2] != 0.0) return;
-  __shared__ double sh_h[kGemvNChunk];
-  __shared__ double sh[kThreads / 32];
+// Rows bx*blockDim.x + threadIdx.x + i*gx*blockDim.x of the update; returns
+// this thread's sum of the new z^2.
+__device__ __forceinline__ double gemvN_body(int n, int k, const double *__restrict__ Q, long long ld,
+                                             const double *__restrict__ h, double alpha, double *v, int bx, int gx,
+                                             double *sh_h) {
   double nsum = 0.0;
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+  for (long long base = (long long)bx * blockDim.x; base < n; base += (long long)gx * blockDim.x) {
     const long long r = base + threadIdx.x;
     double z = (r < n) ? v[r] : 0.0;
     for (int j0 = 0; j0 < k; j0 += kGemvNChunk) {
@@ -144,19 +156,32 @@ __global__ void __launch_bounds__(kThreads)
       nsum += z * z;
     }
   }
+  return nsum;
+}
+
+// The DGKS decision of SRC/misc_la.c:246-250 from the new norm's square.
+__device__ __forceinline__ void dgks_decide(double t, double *state) {
+  const double nw = sqrt(t);
+  state[1] = nw;
+  if (nw > kEta * state[0])
+    state[2] = 1.0;
+  else
+    state[0] = nw;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_gemvN(int n, int k, const double *__restrict__ Q, long long ld, const double *__restrict__ h, double alpha,
+            double *v, double *part, unsigned int *ctr, double *state) {
+  if (state && state[2] != 0.0) return;
+  __shared__ double sh_h[kGemvNChunk];
+  __shared__ double sh[kThreads / 32];
+  double nsum = gemvN_body(n, k, Q, ld, h, alpha, v, blockIdx.x, gridDim.x, sh_h);
   if (state) {
     nsum = block_sum(nsum, sh);
     if (threadIdx.x == 0) part[blockIdx.x] = nsum;
     if (last_block(ctr)) {
       double t = reduce_partials(part, gridDim.x, ctr, sh);
-      if (threadIdx.x == 0) {
-        const double nw = sqrt(t);
-        state[1] = nw;
-        if (nw > kEta * state[0])
-          state[2] = 1.0;
-        else
-          state[0] = nw;
-      }
+      if (threadIdx.x == 0) dgks_decide(t, state);
     }
   }
 }
@@ -168,6 +193,167 @@ __global__ void k_cgs_init(double *state, const double *nrm) {
 }
 
 __global__ void k_copy_scalar(const double *src, double *dst) { *dst = *src; }
+
+// ---------------------------------------------------------------------------
+// The request engine's Lanczos step for many slots at once.  Every slot's
+// work is split into blocks exactly as the single-slot kernels split it (the
+// same grids, per slot), and a block finds its slot in a prefix table of
+// block counts, so each slot's arithmetic -- including every reduction
+// order -- is that of evslcu_axpy / evslcu_dot / evslcu_cgs_dgks on it alone.
+// Reductions that the single-slot kernels finish in their last block are
+// finished here by one block per slot in a separate launch, with the same
+// code and thread count.
+// ---------------------------------------------------------------------------
+struct LzSlot {
+  int n, kc;            // rows; basis columns orthogonalised against (k + 1)
+  int g_dot, nchunks;   // grids of the dot / norm and of the transposed GEMV
+  int ctiles, g_n;      // column tiles of the transposed GEMV; grid of the GEMV
+  double nbeta;         // -beta of the previous step (0 at k = 0: no update)
+  const double *V;      // basis, ld = n
+  const double *v;      // V(:, k)
+  const double *vprev;  // V(:, k-1), or null
+  double *z;            // V(:, k+1): the filtered vector, orthogonalised in place
+  double *ds;           // ds[0] = alpha, ds[1] = new norm
+  double *part;         // transposed GEMV partials (nchunks x kc), then h (kc), state (4)
+  double *npart;        // norm / dot partials (g_n >= g_dot entries)
+};
+enum { LZ_DOT = 0, LZ_T, LZ_TR, LZ_N, LZ_ONE, LZ_NPREF };
+
+__device__ __forceinline__ int lz_slot_of(const int *pre, int ns, int b) {
+  int lo = 0, hi = ns;  // pre[0] = 0 <= b < pre[ns]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pre[mid] <= b)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+__device__ __forceinline__ double *lz_h(const LzSlot &S) { return S.part + (size_t)S.nchunks * S.kc; }
+__device__ __forceinline__ double *lz_state(const LzSlot &S) { return lz_h(S) + S.kc; }
+
+// z -= beta v_prev (k > 0), then partial sums of z . v (k_axpy + k_dot)
+__global__ void __launch_bounds__(kThreads) k_lz_axpy_dot(const LzSlot *__restrict__ SS, const int *__restrict__ pre,
+                                                         int ns) {
+  __shared__ double sh[kThreads / 32];
+  const int si = lz_slot_of(pre, ns, blockIdx.x);
+  const LzSlot &S = SS[si];
+  const int b = blockIdx.x - pre[si];
+  double acc = 0.0;
+  for (int i = b * blockDim.x + threadIdx.x; i < S.n; i += S.g_dot * blockDim.x) {
+    double zi = S.z[i];
+    if (S.vprev) zi = __dadd_rn(zi, __dmul_rn(S.nbeta, S.vprev[i]));
+    S.z[i] = zi;
+    acc += zi * S.v[i];
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) S.npart[b] = acc;
+}
+
+// alpha = the sum of the dot partials (reduce_partials' order)
+__global__ void __launch_bounds__(kThreads) k_lz_alpha(const LzSlot *__restrict__ SS) {
+  __shared__ double sh[kThreads / 32];
+  const LzSlot &S = SS[blockIdx.x];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < S.g_dot; i += blockDim.x) s += __ldcg(S.npart + i);
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) S.ds[0] = s;
+}
+
+// z -= alpha v (k_axpy_ds), then partial sums of z . z (the norm of k_dot)
+__global__ void __launch_bounds__(kThreads) k_lz_axpy_nrm(const LzSlot *__restrict__ SS, const int *__restrict__ pre,
+                                                         int ns) {
+  __shared__ double sh[kThreads / 32];
+  const int si = lz_slot_of(pre, ns, blockIdx.x);
+  const LzSlot &S = SS[si];
+  const int b = blockIdx.x - pre[si];
+  const double c = -1.0 * __ldcg(S.ds);
+  double acc = 0.0;
+  for (int i = b * blockDim.x + threadIdx.x; i < S.n; i += S.g_dot * blockDim.x) {
+    const double zi = __dadd_rn(S.z[i], __dmul_rn(c, S.v[i]));
+    S.z[i] = zi;
+    acc += zi * zi;
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) S.npart[b] = acc;
+}
+
+// the starting norm of the Gram-Schmidt passes (k_cgs_init)
+__global__ void __launch_bounds__(kThreads) k_lz_cgs_init(const LzSlot *__restrict__ SS) {
+  __shared__ double sh[kThreads / 32];
+  const LzSlot &S = SS[blockIdx.x];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < S.g_dot; i += blockDim.x) s += __ldcg(S.npart + i);
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) {
+    double *st = lz_state(S);
+    st[0] = sqrt(s);
+    st[1] = 0.0;
+    st[2] = 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_lz_gemvT(const LzSlot *__restrict__ SS, const int *__restrict__ pre,
+                                                      int ns) {
+  __shared__ double sv[kGemvTRows];
+  const int si = lz_slot_of(pre, ns, blockIdx.x);
+  const LzSlot &S = SS[si];
+  if (lz_state(S)[2] != 0.0) return;
+  const int b = blockIdx.x - pre[si];
+  gemvT_partial_body(S.n, S.kc, S.V, S.n, S.z, S.part, b % S.nchunks, b / S.nchunks, sv);
+}
+
+__global__ void __launch_bounds__(256) k_lz_gemvT_reduce(const LzSlot *__restrict__ SS, const int *__restrict__ pre,
+                                                         int ns) {
+  __shared__ double sh[8][33];
+  const int si = lz_slot_of(pre, ns, blockIdx.x);
+  const LzSlot &S = SS[si];
+  if (lz_state(S)[2] != 0.0) return;
+  gemvT_reduce_body(S.nchunks, S.kc, S.part, 1.0, 0.0, lz_h(S), blockIdx.x - pre[si], sh);
+}
+
+__global__ void __launch_bounds__(kThreads) k_lz_gemvN(const LzSlot *__restrict__ SS, const int *__restrict__ pre,
+                                                      int ns) {
+  __shared__ double sh_h[kGemvNChunk];
+  __shared__ double sh[kThreads / 32];
+  const int si = lz_slot_of(pre, ns, blockIdx.x);
+  const LzSlot &S = SS[si];
+  if (lz_state(S)[2] != 0.0) return;
+  const int b = blockIdx.x - pre[si];
+  double nsum = gemvN_body(S.n, S.kc, S.V, S.n, lz_h(S), -1.0, S.z, b, S.g_n, sh_h);
+  nsum = block_sum(nsum, sh);
+  if (threadIdx.x == 0) S.npart[b] = nsum;
+}
+
+// the pass's norm and DGKS decision; the norm goes to ds[1]
+__global__ void __launch_bounds__(kThreads) k_lz_dgks(const LzSlot *__restrict__ SS) {
+  __shared__ double sh[kThreads / 32];
+  const LzSlot &S = SS[blockIdx.x];
+  double *st = lz_state(S);
+  if (st[2] != 0.0) return;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < S.g_n; i += blockDim.x) s += __ldcg(S.npart + i);
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) {
+    dgks_decide(s, st);
+    S.ds[1] = st[1];
+  }
+}
+
+// x_s *= a_s for a list of vectors (k_scal)
+struct LzScale {
+  int n, g;
+  double a;
+  double *x;
+};
+__global__ void __launch_bounds__(kThreads) k_lz_scal(const LzScale *__restrict__ SS, const int *__restrict__ pre,
+                                                     int ns) {
+  const int si = lz_slot_of(pre, ns, blockIdx.x);
+  const LzScale &S = SS[si];
+  const int b = blockIdx.x - pre[si];
+  for (int i = b * blockDim.x + threadIdx.x; i < S.n; i += S.g * blockDim.x) S.x[i] = __dmul_rn(S.a, S.x[i]);
+}
 
 // y = beta*y for the transposed GEMV when alpha == 0 etc. (rarely used)
 __global__ void k_scale_vec(int n, double beta, double *y) {
@@ -472,6 +658,155 @@ int evslcu_scal(int n, double a, double *x) {
 }
 
 int evslcu_copy(int n, const double *x, double *y) { return evslcu_d2d(y, x, sizeof(double) * (size_t)n); }
+
+// Host staging for the batched engine operations: pinned, so the copies of
+// the slot tables are asynchronous; one buffer per call site, rewritten only
+// once the event recorded after its last copy has completed.
+static void *g_lz_stage[2] = {nullptr, nullptr};
+static size_t g_lz_stage_cap[2] = {0, 0};
+static cudaEvent_t g_lz_evt[2] = {nullptr, nullptr};
+
+static void *lz_stage(int which, size_t bytes) {
+  if (g_lz_evt[which]) cudaEventSynchronize(g_lz_evt[which]);
+  if (bytes > g_lz_stage_cap[which]) {
+    if (g_lz_stage[which]) {
+      cudaStreamSynchronize(stream());
+      cudaFreeHost(g_lz_stage[which]);
+    }
+    g_lz_stage[which] = nullptr;
+    g_lz_stage_cap[which] = 0;
+    if (cudaMallocHost(&g_lz_stage[which], bytes) != cudaSuccess) {
+      cudaGetLastError();
+      g_lz_stage[which] = nullptr;
+      return nullptr;
+    }
+    g_lz_stage_cap[which] = bytes;
+  }
+  return g_lz_stage[which];
+}
+
+// Marks the end of the copy just issued from staging buffer `which`.
+static int lz_staged(int which) {
+  if (!g_lz_evt[which] && cudaEventCreateWithFlags(&g_lz_evt[which], cudaEventDisableTiming) != cudaSuccess)
+    return fail(EVSLCU_ERR_CUDA, "batched engine operations: event creation failed");
+  if (cudaEventRecord(g_lz_evt[which], stream()) != cudaSuccess)
+    return fail(EVSLCU_ERR_CUDA, "batched engine operations: event record failed");
+  return 0;
+}
+
+void evslcu_lz_release(void) {
+  for (int i = 0; i < 2; ++i) {
+    if (g_lz_evt[i]) {
+      cudaEventSynchronize(g_lz_evt[i]);
+      cudaEventDestroy(g_lz_evt[i]);
+    }
+    g_lz_evt[i] = nullptr;
+    if (g_lz_stage[i]) cudaFreeHost(g_lz_stage[i]);
+    g_lz_stage[i] = nullptr;
+    g_lz_stage_cap[i] = 0;
+  }
+}
+
+size_t evslcu_lz_scratch_doubles(void) { return (size_t)kMaxPartials; }
+
+size_t evslcu_lanczos_batch_table_bytes(int ns) {
+  return (sizeof(LzSlot) * (size_t)std::max(ns, 1) + 255) / 256 * 256 + sizeof(int) * LZ_NPREF * ((size_t)ns + 1);
+}
+
+int evslcu_lanczos_batch(int ns, const evslcu_lz_col *cols, int imax, void *table, size_t table_bytes) {
+  if (ns <= 0) return 0;
+  if (!cols || !table || table_bytes < evslcu_lanczos_batch_table_bytes(ns))
+    return fail(EVSLCU_ERR_ARG, "lanczos_batch: bad arguments");
+  const size_t sbytes = (sizeof(LzSlot) * (size_t)ns + 255) / 256 * 256;
+  const size_t bytes = evslcu_lanczos_batch_table_bytes(ns);
+  unsigned char *h = (unsigned char *)lz_stage(0, bytes);
+  if (!h) return fail(EVSLCU_ERR_NOMEM, "lanczos_batch: out of pinned host memory");
+  LzSlot *S = reinterpret_cast<LzSlot *>(h);
+  int *pre = reinterpret_cast<int *>(h + sbytes);
+  for (int q = 0; q < LZ_NPREF; ++q) pre[q * (ns + 1)] = 0;
+  for (int i = 0; i < ns; ++i) {
+    const evslcu_lz_col &c = cols[i];
+    if (c.n < 1 || c.k < 0 || !c.V || !c.ds || !c.cgsw || !c.npart)
+      return fail(EVSLCU_ERR_ARG, "lanczos_batch: bad column %d", i);
+    LzSlot &L = S[i];
+    L.n = c.n;
+    L.kc = c.k + 1;
+    L.g_dot = grid_for(c.n, kThreads, 1024);
+    L.nchunks = (c.n + kGemvTRows - 1) / kGemvTRows;
+    L.ctiles = (L.kc + kGemvTCols - 1) / kGemvTCols;
+    L.g_n = grid_for(c.n, kThreads, kMaxPartials);
+    L.nbeta = -c.beta;
+    L.V = c.V;
+    L.v = c.V + (size_t)c.k * c.n;
+    L.vprev = c.k > 0 ? c.V + (size_t)(c.k - 1) * c.n : nullptr;
+    L.z = c.V + (size_t)(c.k + 1) * c.n;
+    L.ds = c.ds;
+    L.part = c.cgsw;
+    L.npart = c.npart;
+    const int cnt[LZ_NPREF] = {L.g_dot, L.nchunks * L.ctiles, (L.kc + 31) / 32, L.g_n, 1};
+    for (int q = 0; q < LZ_NPREF; ++q) pre[q * (ns + 1) + i + 1] = pre[q * (ns + 1) + i] + cnt[q];
+  }
+  int rc = evslcu_h2d_async(table, h, bytes);
+  if (!rc) rc = lz_staged(0);
+  if (rc) return rc;
+  const LzSlot *dS = reinterpret_cast<const LzSlot *>(table);
+  const int *dpre = reinterpret_cast<const int *>(static_cast<unsigned char *>(table) + sbytes);
+  auto P = [&](int q) { return dpre + q * (ns + 1); };
+  auto G = [&](int q) { return pre[q * (ns + 1) + ns]; };
+  cudaStream_t st = stream();
+  k_lz_axpy_dot<<<G(LZ_DOT), kThreads, 0, st>>>(dS, P(LZ_DOT), ns);
+  EVSLCU_LAUNCH_CHECK("k_lz_axpy_dot");
+  k_lz_alpha<<<ns, kThreads, 0, st>>>(dS);
+  EVSLCU_LAUNCH_CHECK("k_lz_alpha");
+  k_lz_axpy_nrm<<<G(LZ_DOT), kThreads, 0, st>>>(dS, P(LZ_DOT), ns);
+  EVSLCU_LAUNCH_CHECK("k_lz_axpy_nrm");
+  k_lz_cgs_init<<<ns, kThreads, 0, st>>>(dS);
+  EVSLCU_LAUNCH_CHECK("k_lz_cgs_init");
+  for (int pass = 0; pass < imax; ++pass) {
+    k_lz_gemvT<<<G(LZ_T), kThreads, 0, st>>>(dS, P(LZ_T), ns);
+    EVSLCU_LAUNCH_CHECK("k_lz_gemvT");
+    k_lz_gemvT_reduce<<<G(LZ_TR), 256, 0, st>>>(dS, P(LZ_TR), ns);
+    EVSLCU_LAUNCH_CHECK("k_lz_gemvT_reduce");
+    k_lz_gemvN<<<G(LZ_N), kThreads, 0, st>>>(dS, P(LZ_N), ns);
+    EVSLCU_LAUNCH_CHECK("k_lz_gemvN");
+    k_lz_dgks<<<ns, kThreads, 0, st>>>(dS);
+    EVSLCU_LAUNCH_CHECK("k_lz_dgks");
+  }
+  return 0;
+}
+
+size_t evslcu_scal_batch_table_bytes(int ns) {
+  return (sizeof(LzScale) * (size_t)std::max(ns, 1) + 255) / 256 * 256 + sizeof(int) * ((size_t)ns + 1);
+}
+
+int evslcu_scal_batch(int ns, const int *n, double *const *x, const double *a, void *table, size_t table_bytes) {
+  if (ns <= 0) return 0;
+  if (!n || !x || !a || !table || table_bytes < evslcu_scal_batch_table_bytes(ns))
+    return fail(EVSLCU_ERR_ARG, "scal_batch: bad arguments");
+  const size_t sbytes = (sizeof(LzScale) * (size_t)ns + 255) / 256 * 256;
+  const size_t bytes = evslcu_scal_batch_table_bytes(ns);
+  unsigned char *h = (unsigned char *)lz_stage(1, bytes);
+  if (!h) return fail(EVSLCU_ERR_NOMEM, "scal_batch: out of pinned host memory");
+  LzScale *S = reinterpret_cast<LzScale *>(h);
+  int *pre = reinterpret_cast<int *>(h + sbytes);
+  pre[0] = 0;
+  for (int i = 0; i < ns; ++i) {
+    S[i].n = n[i];
+    S[i].g = grid_for(n[i]);
+    S[i].a = a[i];
+    S[i].x = x[i];
+    pre[i + 1] = pre[i] + S[i].g;
+  }
+  int rc = evslcu_h2d_async(table, h, bytes);
+  if (!rc) rc = lz_staged(1);
+  if (rc) return rc;
+  k_lz_scal<<<pre[ns], kThreads, 0, stream()>>>(reinterpret_cast<const LzScale *>(table),
+                                                reinterpret_cast<const int *>(static_cast<unsigned char *>(table) +
+                                                                              sbytes),
+                                                ns);
+  EVSLCU_LAUNCH_CHECK("k_lz_scal");
+  return 0;
+}
 
 size_t evslcu_cgs_work_size(int n, int k) {
   const size_t nchunks = ((size_t)n + kGemvTRows - 1) / kGemvTRows;

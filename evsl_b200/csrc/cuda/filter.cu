@@ -306,6 +306,7 @@ int evslcu_filter_error(void) {
 int evslcu_set_wait_limit(unsigned long long polls) {
   g_barrier_polls = polls ? polls : kBarrierSpinLimit;
   set_wave_wait_limit(polls);
+  set_batch_wait_limit(polls);
   return 0;
 }
 

@@ -464,6 +464,7 @@ int panel_mf_step(const evslcu_mat *M, int k, const VT *vk, const VT *vkm1, VT *
 
 // Wait limit of the pipelined filter's dependency waits (0: default).
 void set_wave_wait_limit(unsigned long long polls);
+void set_batch_wait_limit(unsigned long long polls);
 // Pipelined single-launch filter (wavefilter.cu); work: 2n doubles.
 int chebav_wave(evslcu_mat *A, const double *mu, int deg, double cc, double dd, const double *v, double *y,
                 double *work);

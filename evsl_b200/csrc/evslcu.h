@@ -202,6 +202,11 @@ size_t evslcu_filter_batch_table_bytes(int ncols, long long total_rows);
  * ChebAv of that column bit for bit.  table: device memory of at least
  * evslcu_filter_batch_table_bytes(...) bytes. */
 int evslcu_filter_batch(int ncols, const evslcu_batch_col *cols, void *table, size_t table_bytes);
+/* 1: the batched filter runs every degree of every column in one persistent
+ * launch (work items handed out in degree order, each waiting -- bounded --
+ * for its column's previous degree); 0 (default): one launch per degree.
+ * Same results bit for bit. */
+int evslcu_set_batch_persistent(int on);
 size_t evslcu_filter_columns_work(int n, int fp32, int ncols);
 int evslcu_filter_columns(const evslcu_mat *A, int fp32, int ncols, const evslcu_filter_col *cols, void *work,
                           size_t work_bytes);
@@ -301,6 +306,31 @@ int evslcu_set_kpm_doubling(int on);
  * 0 never, 1 whenever the matrix can have a copy.  The moments agree to
  * rounding. */
 int evslcu_set_kpm_split(int mode);
+/* The request engine's Lanczos step for many slots in a dozen launches:
+ * per slot, z = V(:,k+1) (the filtered vector) gets z -= beta V(:,k-1)
+ * (k > 0), alpha = z.V(:,k) into ds[0], z -= alpha V(:,k), then classical
+ * Gram-Schmidt with the DGKS test against V(:,0..k) (at most imax passes),
+ * the final norm into ds[1] -- the arithmetic, reduction orders included,
+ * of evslcu_axpy / evslcu_dot / evslcu_axpy_ds / evslcu_cgs_dgks on each
+ * slot alone.  cgsw: evslcu_cgs_work_size(n, k + 1) doubles; npart:
+ * evslcu_lz_scratch_doubles() doubles of device scratch per slot (distinct
+ * slots, distinct scratch).  table: device memory of
+ * evslcu_lanczos_batch_table_bytes(ns) bytes. */
+typedef struct {
+  int n, k;
+  double beta;
+  double *V;
+  double *ds;
+  double *cgsw;
+  double *npart;
+} evslcu_lz_col;
+size_t evslcu_lz_scratch_doubles(void);
+size_t evslcu_lanczos_batch_table_bytes(int ns);
+int evslcu_lanczos_batch(int ns, const evslcu_lz_col *cols, int imax, void *table, size_t table_bytes);
+/* x_i *= a_i (evslcu_scal) for ns vectors in one launch. */
+size_t evslcu_scal_batch_table_bytes(int ns);
+int evslcu_scal_batch(int ns, const int *n, double *const *x, const double *a, void *table, size_t table_bytes);
+void evslcu_lz_release(void);
 /* Free the cached KPM and tridiagonal workspaces (evslcu_finish calls them). */
 void evslcu_kpm_release(void);
 void evslcu_trid_release(void);

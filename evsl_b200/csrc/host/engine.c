@@ -41,6 +41,9 @@
  * treats columns independently and the reductions are per slot), so a
  * request's result is the same alone and in any mix of requests.
  */
+#define _POSIX_C_SOURCE 199309L
+#include <time.h>
+
 #include "internal.h"
 
 #define ENG_NTEST 30
@@ -127,6 +130,23 @@ struct evslx_engine {
   void *btab;
   size_t btab_bytes;
   uint64_t batched_columns;
+  /* batched Lanczos step: the vector operations of all slots in the Lanczos
+   * phase as one launch per operation (evslcu_lanczos_batch), and the
+   * normalisations of all continuing slots as one launch */
+  int use_batch_ops;
+  evslcu_lz_col *lzcols;
+  double *lz_npart; /* max_slots x evslcu_lz_scratch_doubles() */
+  void *lztab;
+  size_t lztab_bytes;
+  int *sc_n;
+  double **sc_x;
+  double *sc_a;
+  void *sctab;
+  size_t sctab_bytes;
+  /* host wall-clock seconds per phase of engine_step (no device syncs added):
+   * [0] admission and filter issue, [1] Lanczos-step issue, [2] the wait for
+   * the scalars' copy (device backlog), [3] host part, [4] retirement */
+  double phase_s[5];
 };
 
 /* ---------------------------------------------------------------------------
@@ -216,8 +236,19 @@ evslx_engine *evslx_engine_create(int max_slots, size_t hbm_budget, int precisio
   E->use_batch = 1;
   E->batch_max_rows = 1 << 18;
   E->bcols = (evslcu_batch_col *)malloc(sizeof(evslcu_batch_col) * (size_t)max_slots);
+  E->use_batch_ops = 1;
+  E->lzcols = (evslcu_lz_col *)malloc(sizeof(evslcu_lz_col) * (size_t)max_slots);
+  E->sc_n = (int *)malloc(sizeof(int) * (size_t)max_slots);
+  E->sc_x = (double **)malloc(sizeof(double *) * (size_t)max_slots);
+  E->sc_a = (double *)malloc(sizeof(double) * (size_t)max_slots);
+  E->lztab_bytes = evslcu_lanczos_batch_table_bytes(max_slots);
+  E->sctab_bytes = evslcu_scal_batch_table_bytes(max_slots);
+  E->lztab = evslcu_malloc(E->lztab_bytes);
+  E->sctab = evslcu_malloc(E->sctab_bytes);
+  E->lz_npart = (double *)evslcu_malloc(sizeof(double) * evslcu_lz_scratch_doubles() * (size_t)max_slots);
   if (!E->slots || !E->ds || !E->hs || !E->cols || !E->colslot || !E->xs || !E->ys || !E->uidbuf || !E->plans ||
-      !E->gbest || !E->gcut || !E->gstart || !E->bcols) {
+      !E->gbest || !E->gcut || !E->gstart || !E->bcols || !E->lzcols || !E->sc_n || !E->sc_x || !E->sc_a ||
+      !E->lztab || !E->sctab || !E->lz_npart) {
     evsl_seterr(EVSLX_ERR_NOMEM, "evslx_engine_create: out of memory");
     evslx_engine_free(E);
     return NULL;
@@ -275,6 +306,13 @@ void evslx_engine_free(evslx_engine *E) {
   evslcu_free(E->fwork);
   evslcu_free(E->btab);
   free(E->bcols);
+  free(E->lzcols);
+  free(E->sc_n);
+  free(E->sc_x);
+  free(E->sc_a);
+  evslcu_free(E->lztab);
+  evslcu_free(E->sctab);
+  evslcu_free(E->lz_npart);
   for (int i = 0; i < E->nplans; i++) {
     evslcu_filter_plan_destroy(E->plans[i].plan);
     free(E->plans[i].uids);
@@ -293,6 +331,12 @@ void evslx_engine_free(evslx_engine *E) {
 
 void evslx_engine_use_graphs(evslx_engine *E, int on) {
   if (E) E->use_graphs = on ? 1 : 0;
+}
+
+int evslx_set_batch_persistent(int on) { return evslcu_set_batch_persistent(on); }
+
+void evslx_engine_use_batch_ops(evslx_engine *E, int on) {
+  if (E) E->use_batch_ops = on ? 1 : 0;
 }
 
 void evslx_engine_use_batch(evslx_engine *E, int on, int max_rows) {
@@ -807,8 +851,19 @@ static int retire(evslx_engine *E, slot_t *s, int kdim, int rc_in) {
 }
 
 /* one tick: admit, filter every active slot, Lanczos step, tests, retire */
+static double eng_clock(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+void evslx_engine_phase_times(const evslx_engine *E, double out[5]) {
+  for (int i = 0; i < 5; i++) out[i] = E ? E->phase_s[i] : 0.0;
+}
+
 int evslx_engine_step(evslx_engine *E) {
   if (!E) return evsl_seterr(EVSLX_ERR_ARG, "evslx_engine_step: null engine");
+  double tph = eng_clock();
   int rc = admit(E);
   if (rc) return rc;
   if (E->nactive == 0) return evslx_engine_pending(E);
@@ -964,7 +1019,13 @@ int evslx_engine_step(evslx_engine *E) {
     E->plans[i] = E->plans[--E->nplans];
     memset(&E->plans[E->nplans], 0, sizeof(plan_cache_t));
   }
+  {
+    const double t = eng_clock();
+    E->phase_s[0] += t - tph;
+    tph = t;
+  }
   /* 2. device part of the Lanczos step */
+  int nlz = 0;
   for (int i = 0; i < E->max_slots; i++) {
     slot_t *s = &E->slots[i];
     if (!s->req) continue;
@@ -973,6 +1034,15 @@ int evslx_engine_step(evslx_engine *E) {
     double *ds = E->ds + ENG_NSCAL * (size_t)i;
     if (s->phase == PH_START) {
       if ((rc = evslcu_nrm2(n, s->V, ds + 1)) || (rc = evslcu_scal_inv_ds(n, ds + 1, s->V))) break;
+    } else if (s->phase == PH_LANCZOS && E->use_batch_ops) {
+      evslcu_lz_col *c = &E->lzcols[nlz++];
+      c->n = n;
+      c->k = s->k;
+      c->beta = s->beta;
+      c->V = s->V;
+      c->ds = ds;
+      c->cgsw = s->cgsw;
+      c->npart = E->lz_npart + evslcu_lz_scratch_doubles() * (size_t)i;
     } else if (s->phase == PH_LANCZOS) {
       double *v = s->V + (size_t)s->k * n_l, *z = v + n_l;
       if (s->k > 0 && (rc = evslcu_axpy(n, -s->beta, v - n_l, z))) break;
@@ -986,11 +1056,23 @@ int evslx_engine_step(evslx_engine *E) {
         break;
     }
   }
+  if (!rc && nlz > 0) rc = evslcu_lanczos_batch(nlz, E->lzcols, EVSL_NGS_MAX, E->lztab, E->lztab_bytes);
   if (rc) return evsl_seterr(rc, "%s", evslcu_errstr());
+  {
+    const double t = eng_clock();
+    E->phase_s[1] += t - tph;
+    tph = t;
+  }
   /* 3. one copy of every slot's scalars */
   if ((rc = evslcu_d2h(E->hs, E->ds, sizeof(double) * ENG_NSCAL * (size_t)E->max_slots)))
     return evsl_seterr(rc, "%s", evslcu_errstr());
+  {
+    const double t = eng_clock();
+    E->phase_s[2] += t - tph;
+    tph = t;
+  }
   /* 4. host part of the step */
+  int nsc = 0;
   for (int i = 0; i < E->max_slots; i++) {
     slot_t *s = &E->slots[i];
     if (!s->req) continue;
@@ -1016,8 +1098,14 @@ int evslx_engine_step(evslx_engine *E) {
         continue;
       }
       s->beta = beta;
-      if ((rc = evslcu_scal(n, 1.0 / beta, s->V + (size_t)(s->k + 1) * (size_t)n)))
+      if (E->use_batch_ops) {
+        E->sc_n[nsc] = n;
+        E->sc_x[nsc] = s->V + (size_t)(s->k + 1) * (size_t)n;
+        E->sc_a[nsc] = 1.0 / beta;
+        nsc++;
+      } else if ((rc = evslcu_scal(n, 1.0 / beta, s->V + (size_t)(s->k + 1) * (size_t)n))) {
         return evsl_seterr(rc, "%s", evslcu_errstr());
+      }
       s->eT[s->k] = beta;
       step_done = 1;
     } else {
@@ -1039,11 +1127,21 @@ int evslx_engine_step(evslx_engine *E) {
     }
     if (!finished && k + 1 >= r->maxit) finished = 1;
     if (finished) {
+      const double tr = eng_clock();
+      /* the queued normalisations first: retiring releases this slot's basis */
+      if (nsc > 0 && (rc = evslcu_scal_batch(nsc, E->sc_n, E->sc_x, E->sc_a, E->sctab, E->sctab_bytes)))
+        return evsl_seterr(rc, "%s", evslcu_errstr());
+      nsc = 0;
       if ((rc = retire(E, s, kdim, 0))) return rc;
+      E->phase_s[4] += eng_clock() - tr;
+      tph += eng_clock() - tr;  /* keep retirement out of the host-part time */
     } else {
       s->k = k + 1;
     }
   }
+  if (nsc > 0 && (rc = evslcu_scal_batch(nsc, E->sc_n, E->sc_x, E->sc_a, E->sctab, E->sctab_bytes)))
+    return evsl_seterr(rc, "%s", evslcu_errstr());
+  E->phase_s[3] += eng_clock() - tph;
   E->ticks++;
   return evslx_engine_pending(E);
 }

@@ -308,6 +308,24 @@ void evslx_engine_use_graphs(evslx_engine *E, int on);
  * solve slices one after another (TESTS/PLanR/MMPLanR_omp.c:183-241 runs
  * them on OpenMP threads). */
 void evslx_engine_use_batch(evslx_engine *E, int on, int max_rows);
+/* 1 (default): the vector operations of the Lanczos steps of all slots run
+ * together, one launch per operation for every slot (the same arithmetic,
+ * reductions included, as each slot's own launches); 0: each slot's own
+ * launches. */
+void evslx_engine_use_batch_ops(evslx_engine *E, int on);
+/* The batched filter's form, for every engine: 0 (default) one launch per
+ * degree for all its columns; 1 one persistent launch for all degrees (work
+ * items -- degree, block of a column -- handed out in degree order, each
+ * waiting, with the bound of evslx_set_wait_limit, for its column's previous
+ * degree; a wait that runs out makes the engine step return
+ * EVSLX_ERR_TIMEOUT).  Results are the same bit for bit. */
+int evslx_set_batch_persistent(int on);
+/* Host wall-clock seconds the engine's steps spent so far in: [0] admission
+ * and issuing the filters, [1] issuing the rest of the Lanczos steps, [2]
+ * waiting for the step's scalars (the device's backlog), [3] the host part
+ * (tridiagonal tests, restarts), [4] retiring finished requests.  No
+ * synchronisation is added to measure them. */
+void evslx_engine_phase_times(const evslx_engine *E, double out[5]);
 /* Columns filtered through the batched filter so far. */
 uint64_t evslx_engine_batched_columns(const evslx_engine *E);
 uint64_t evslx_engine_plan_builds(const evslx_engine *E);

@@ -397,10 +397,12 @@ def test_multi_filter_dictionary_with_double_table(gpu_lib):
         gpu_lib.free_pol(pol)
 
 
-def test_engine_batched_filter_is_bitwise_the_per_matrix_filter(gpu_lib):
+@pytest.mark.parametrize("persistent", [False, True])
+def test_engine_batched_filter_is_bitwise_the_per_matrix_filter(gpu_lib, persistent):
     """The engine's batched filter (the lone FP64 columns of all small
-    matrices advanced one degree per launch together) gives every instance
-    the same eigenvalues, bit for bit, as filtering each matrix on its own."""
+    matrices advanced one degree per launch together, or all degrees in one
+    persistent launch) gives every instance the same eigenvalues, bit for
+    bit, as filtering each matrix on its own."""
     rng = np.random.default_rng(8)
     mats, pols, subs = [], [], []
     for i in range(10):
@@ -424,9 +426,13 @@ def test_engine_batched_filter_is_bitwise_the_per_matrix_filter(gpu_lib):
     for batch in (True, False):
         eng = gpu_lib.engine(len(subs), precision=E.PREC_FP64)
         eng.use_batch(batch)
+        gpu_lib.set_batch_persistent(persistent)
         for M, iv, pol, v, tag, _ in subs:
             eng.submit_slice(M, iv, pol, 1500, 1e-8, v, tag)
-        eng.run()
+        try:
+            eng.run()
+        finally:
+            gpu_lib.set_batch_persistent(False)
         res = {}
         while True:
             r = eng.pop()
@@ -446,7 +452,7 @@ def test_engine_batched_filter_is_bitwise_the_per_matrix_filter(gpu_lib):
         gpu_lib.free_pol(p)
 
 
-def test_engine_batched_uneven_instances_full_scale(gpu_lib):
+def test_engine_batched_uneven_instances_full_scale(gpu_lib, persistent=False):
     """The batched-instances configuration at full scale: 128 independent
     2-D / 3-D Laplacians, n log-uniform in [1e3, 2e5] (4.85 million rows in
     all), each with its own interval of 20-80 eigenvalues (end points at gap
@@ -457,6 +463,7 @@ def test_engine_batched_uneven_instances_full_scale(gpu_lib):
     import bench
 
     inst = bench.uneven_instances(128)
+    gpu_lib.set_batch_persistent(persistent)
     eng = gpu_lib.engine(len(inst), precision=E.PREC_FP64)
     mats, pols = [], []
     for i, (dims, iv, _) in enumerate(inst):
@@ -467,7 +474,10 @@ def test_engine_batched_uneven_instances_full_scale(gpu_lib):
         mats.append(M)
         pols.append(pol)
         eng.submit_slice(M, iv, pol, 1000, 1e-8, O.seeded_normal(len(ia) - 1, 100 + i), i)
-    eng.run()
+    try:
+        eng.run()
+    finally:
+        gpu_lib.set_batch_persistent(False)
     seen = 0
     while True:
         r = eng.pop()
@@ -480,6 +490,111 @@ def test_engine_batched_uneven_instances_full_scale(gpu_lib):
         seen += 1
     assert seen == len(inst) and eng.batched_columns() > 0
     eng.free()
+    for M in mats:
+        M.free()
+    for p in pols:
+        gpu_lib.free_pol(p)
+
+
+def test_engine_persistent_batch_wait_times_out_and_recovers(gpu_lib):
+    """Failure path of the persistent batched filter's dependency waits: with
+    a limit of one poll a wait gives up, the engine step returns
+    EVSLX_ERR_TIMEOUT (-105) with every block gone; with the default limit
+    restored a new engine solves the same requests exactly."""
+    rng = np.random.default_rng(9)
+    subs, mats, pols = [], [], []
+    for i in range(6):
+        dims = (40 + 3 * i, 41, 1)
+        ia, ja, a = O.lap_csr(*dims)
+        ev = np.sort(W.laplacian_eigenvalues(*dims))
+        a0, b0, cnt = W.gap_interval(ev, float(rng.uniform(0.5, 1.0)), 20)
+        iv = [a0, b0, 0.0, 8.0]
+        M = gpu_lib.matrix(ia, ja, a)
+        pol = gpu_lib.find_pol(iv)
+        mats.append(M)
+        pols.append(pol)
+        subs.append((M, iv, pol, O.seeded_normal(len(ia) - 1, 60 + i), i, len(ev[(ev >= a0) & (ev <= b0)])))
+    gpu_lib.set_batch_persistent(True)
+    try:
+        gpu_lib.set_wait_limit(1)
+        eng = gpu_lib.engine(len(subs), precision=E.PREC_FP64)
+        for M, iv, pol, v, tag, _ in subs:
+            eng.submit_slice(M, iv, pol, 1500, 1e-8, v, tag)
+        with pytest.raises(E.EvslError) as err:
+            eng.run()
+        assert "returned -105" in str(err.value) and "ran out of polls" in gpu_lib.last_error()
+        eng.free()
+        gpu_lib.set_wait_limit(0)
+        eng = gpu_lib.engine(len(subs), precision=E.PREC_FP64)
+        for M, iv, pol, v, tag, _ in subs:
+            eng.submit_slice(M, iv, pol, 1500, 1e-8, v, tag)
+        eng.run()
+        seen = 0
+        while True:
+            r = eng.pop()
+            if r is None:
+                break
+            cnt = subs[r["tag"]][5]
+            assert r["rc"] == 0 and r["nev"] == cnt and np.all(r["res"] < 1e-8)
+            seen += 1
+        assert seen == len(subs) and eng.batched_columns() > 0
+        eng.free()
+    finally:
+        gpu_lib.set_wait_limit(0)
+        gpu_lib.set_batch_persistent(False)
+        for M in mats:
+            M.free()
+        for p in pols:
+            gpu_lib.free_pol(p)
+
+
+@pytest.mark.parametrize("precision", [E.PREC_FP64, E.PREC_MIXED])
+def test_engine_batched_lanczos_ops_are_bitwise_per_slot(gpu_lib, precision):
+    """The engine's Lanczos vector operations for all slots in one launch per
+    operation (evslcu_lanczos_batch: every slot split into blocks as its own
+    launches split it, reductions in the same order) give every request the
+    same eigenvalues, residuals and step counts, bit for bit, as each slot's
+    own launches -- with lone columns of several matrices, several slices of
+    one matrix (multi-column groups) and the mixed-precision refinement."""
+    rng = np.random.default_rng(12)
+    mats, pols, subs = [], [], []
+    specs = [((30, 31, 1), 8.0), ((14, 15, 16), 12.0), ((52, 50, 1), 8.0), ((70, 71, 1), 8.0)]
+    for i, (dims, hi) in enumerate(specs):
+        ia, ja, a = O.lap_csr(*dims)
+        ev = np.sort(W.laplacian_eigenvalues(*dims))
+        M = gpu_lib.matrix(ia, ja, a)
+        mats.append(M)
+        for j in range(2 if i == 3 else 1):
+            a0, b0, cnt = W.gap_interval(ev, float(rng.uniform(0.4, 1.2)), int(rng.integers(12, 30)))
+            iv = [a0, b0, 0.0, hi]
+            pol = gpu_lib.find_pol(iv)
+            pols.append(pol)
+            subs.append((M, iv, pol, O.seeded_normal(len(ia) - 1, 80 + 10 * i + j), len(subs),
+                         len(ev[(ev >= a0) & (ev <= b0)])))
+    gpu_lib.set_mixed_min_rows(0)
+    out = {}
+    try:
+        for batched in (True, False):
+            eng = gpu_lib.engine(len(subs), precision=precision)
+            eng.use_batch_ops(batched)
+            for M, iv, pol, v, tag, _ in subs:
+                eng.submit_slice(M, iv, pol, 1500, 1e-8, v, tag)
+            eng.run()
+            res = {}
+            while True:
+                r = eng.pop()
+                if r is None:
+                    break
+                res[r["tag"]] = r
+            eng.free()
+            out[batched] = res
+    finally:
+        gpu_lib.set_mixed_min_rows(131072)
+    for _, _, _, _, tag, cnt in subs:
+        a, b = out[True][tag], out[False][tag]
+        assert a["rc"] == b["rc"] == 0 and a["nev"] == b["nev"] == cnt
+        assert a["lanczos_steps"] == b["lanczos_steps"]
+        assert np.array_equal(a["lam"], b["lam"]) and np.array_equal(a["res"], b["res"])
     for M in mats:
         M.free()
     for p in pols:
