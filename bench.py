@@ -58,7 +58,8 @@ def parse():
     p.add_argument("--count", type=int, default=COUNT)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", choices=["lap3d-slice", "lap3d-filter", "lap3d-batch", "serve", "lap3d-multifilter",
-                                          "lap3d-reorth", "lap3d-kpm", "rspd-filter", "dgemm", "batch-uneven", "rspd-kpm"],
+                                          "lap3d-reorth", "lap3d-kpm", "rspd-filter", "dgemm", "batch-uneven", "rspd-kpm",
+                                          "block-cgs", "lap3d-pipeline"],
                    default="lap3d-slice",
                    help="lap3d-filter: only the filter p(A)v of the same request (kernel micro-benchmark); "
                         "lap3d-batch: several slices through the request engine; serve: a Poisson request stream")
@@ -75,6 +76,8 @@ def parse():
     p.add_argument("--serve-mix", choices=["default", "small"], default="default",
                    help="serve: 'small' draws the large-matrix requests on the 2-D 100x100 Laplacian only")
     p.add_argument("--rspd-n", type=int, default=RSPD_N, help="rspd-filter: rows of the random SPD matrix")
+    p.add_argument("--grid", type=int, default=50,
+                   help="lap3d-pipeline: the 3-D Laplacian's grid points per side")
     p.add_argument("--kpm-split", type=int, choices=[-1, 0, 1], default=-1,
                    help="rspd-kpm: KPM block step on the column-split copy: -1 automatic, 0 off, 1 on")
     p.add_argument("--split-range-mb", type=float, default=0.0,
@@ -887,6 +890,153 @@ def run_dgemm(args):
         "clocks": clocks}))
 
 
+def run_pipeline(args):
+    """lap3d-pipeline: the drop-in slicing pipeline of the reference's
+    Laplacian driver (TESTS/PLanN/LapPLanN.c:10-283) with the drop-in slicing
+    configuration's settings on a `--grid`^3 3-D Laplacian (default 50^3 =
+    125,000 rows; the configuration's 100^3 takes hours per step): kpmdos over
+    [0.6, 1.2] (300 moments, Jackson damping, 30 seeded Rademacher probes),
+    spslicer into 8 slices (npts = 10 ecount), then per slice find_pol
+    (damping 2, thresholds 0.8 / 0.2) and ChebLanNr (tol 1e-8) from a seeded
+    normal start vector.  One step = the whole pipeline; every slice's count
+    is checked against the analytic spectrum and every residual against tol.
+    Device time per phase from CUDA events on the library stream (the
+    slicer's host time by the wall clock)."""
+    import torch
+
+    import evsl_b200 as E
+    from evsl_b200 import workloads as W
+
+    nx = args.grid
+    lib = E.Library()
+    ia, ja, a = W.laplacian_csr(nx, nx, nx)
+    n = len(ia) - 1
+    lib.set_csr(ia, ja, a)
+    ev = W.laplacian_eigenvalues(nx, nx, nx)
+    intv = [0.6, 1.2, 0.0, 12.0]
+    probes = np.random.default_rng(SEED).choice(np.array([-1.0, 1.0]), size=(30, n))
+    v0 = np.random.default_rng(SEED + 1).standard_normal(n)
+    v0 /= np.linalg.norm(v0)
+    lstream = torch.cuda.ExternalStream(lib.stream_handle())
+    nexact_total = int(np.count_nonzero((ev >= intv[0]) & (ev <= intv[1])))
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lstream)
+        out = fn()
+        e1.record(lstream)
+        e1.synchronize()
+        return out, e0.elapsed_time(e1) / 1e3
+
+    def pipeline():
+        (mu, ecnt), t_kpm = timed(lambda: lib.kpmdos_probes(300, 1, probes, intv))
+        w0 = time.time()
+        rc, sli = lib.spslicer(mu, intv, 8, int(10 * ecnt))
+        t_sli = time.time() - w0
+        if rc != 0:
+            raise RuntimeError("spslicer returned %d" % rc)
+        slices = []
+        for i in range(8):
+            iv = [float(sli[i]), float(sli[i + 1]), 0.0, 12.0]
+            exact = int(np.count_nonzero((ev >= iv[0]) & (ev <= iv[1])))
+            pol = lib.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2)
+            maxit = max(2000, 8 * exact)
+            (lam, _, res), t = timed(lambda: lib.cheblan_nr(iv, maxit, TOL, v0, pol, want_vectors=False))
+            kdim, ncand = lib.last_solve_info()
+            slices.append({"interval": iv[:2], "degree": int(pol.deg), "found": int(len(lam)), "exact": exact,
+                           "max_res": float(np.max(res)) if len(res) else 0.0, "seconds": t,
+                           "lanczos_steps": int(kdim), "ritz_candidates": int(ncand)})
+            lib.free_pol(pol)
+        return {"kpm_s": t_kpm, "ecount": float(ecnt), "slicer_s": t_sli, "slices": slices}
+
+    for _ in range(args.warmup):
+        pipeline()
+    sampler = ClockSampler(rank_info()[2])
+    sampler.start()
+    runs = [pipeline() for _ in range(args.steps)]
+    clocks = sampler.stop()
+    tot = [r["kpm_s"] + r["slicer_s"] + sum(x["seconds"] for x in r["slices"]) for r in runs]
+    found = [sum(x["found"] for x in r["slices"]) for r in runs]
+    ok = all(all(x["found"] == x["exact"] and x["max_res"] < TOL for x in r["slices"]) for r in runs)
+    t = statistics.median(tot)
+    last = runs[-1]
+    print(json.dumps({
+        "metric": METRIC, "value": found[-1] / tot[-1], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (3-D Dirichlet Laplacian, seeded probes and start)",
+        "config": {"workload": "lap3d-pipeline: kpmdos (300 moments, 30 Rademacher probes) + spslicer (8 slices) + "
+                               "8 x ChebLanNr over [0.6, 1.2] of the 3-D Laplacian %d^3 (n=%d)" % (nx, n, ),
+                   "eigenvalues_in_interval": nexact_total, "kpm_s": last["kpm_s"], "ecount": last["ecount"],
+                   "slicer_s": last["slicer_s"], "slices": last["slices"]},
+        "all_steps_ok": bool(ok), "clocks": clocks}))
+
+
+def run_block_cgs(args):
+    """block-cgs: the blocked Gram-Schmidt of the mixed-precision refinement
+    (evslcu_block_cgs2: two passes of GEMM projections against the earlier
+    blocks, CGS + DGKS inside each block of b columns) on a seeded n x m
+    block, `--gemm n,m,b`.  Device time per call from CUDA events on the
+    library stream, median of K steps (the block is re-seeded between calls,
+    outside the timed region).  FP64 flops counted: the GEMMs, 8 n c0 nb per
+    block (two passes of W_prev^T W_b and W_b -= W_prev H), against the FP64
+    peak measured by the library's probe."""
+    import ctypes as C
+
+    import torch
+
+    import evsl_b200 as E
+
+    n, m, b = (int(x) for x in args.gemm.split(","))
+    lib = E.Library()
+    lib.lib.evslcu_fp64_probe.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    dfma, dmma = C.c_double(), C.c_double()
+    lib._check(lib.lib.evslcu_fp64_probe(C.byref(dfma), C.byref(dmma)), "evslcu_fp64_probe")
+    peak = max(dfma.value, dmma.value)
+    g = torch.Generator(device="cuda").manual_seed(SEED)
+    W0 = torch.randn(m, n, dtype=torch.float64, device="cuda", generator=g)  # column-major n x m
+    W = torch.empty_like(W0)
+    H = torch.empty(m * b, dtype=torch.float64, device="cuda")
+    nrm = torch.empty(1, dtype=torch.float64, device="cuda")
+    lib.lib.evslcu_cgs_work_size.restype = C.c_size_t
+    lib.lib.evslcu_cgs_work_size.argtypes = [C.c_int, C.c_int]
+    work = torch.empty(int(lib.lib.evslcu_cgs_work_size(n, b)), dtype=torch.float64, device="cuda")
+    fn = lib.lib.evslcu_block_cgs2
+    fn.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    lstream = torch.cuda.ExternalStream(lib.stream_handle())
+
+    def once():
+        W.copy_(W0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lstream)
+        lib._check(fn(n, m, C.c_void_p(W.data_ptr()), b, C.c_void_p(H.data_ptr()), C.c_void_p(nrm.data_ptr()),
+                      C.c_void_p(work.data_ptr())), "evslcu_block_cgs2")
+        e1.record(lstream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    for _ in range(args.warmup):
+        once()
+    sampler = ClockSampler(rank_info()[2])
+    sampler.start()
+    times = [once() for _ in range(args.steps)]
+    clocks = sampler.stop()
+    t = statistics.median(times)
+    flops = sum(8.0 * n * c0 * min(b, m - c0) for c0 in range(0, m, b))
+    print(json.dumps({
+        "metric": "blocked CGS2 FP64 TFLOP/s", "value": flops / t / 1e12, "unit": "TFLOP/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded normal block)",
+        "config": {"workload": "block-cgs: n=%d m=%d block %d" % (n, m, b), "gemm_flops": flops},
+        "roofline": {"bound": "fp64", "achieved": flops / t / 1e12, "peak": peak, "unit": "TFLOP/s",
+                     "frac": flops / t / 1e12 / peak,
+                     "peak_kind": "measured on this GPU (FMA %.1f, mma.sync f64 %.1f TFLOP/s)" % (dfma.value,
+                                                                                               dmma.value)},
+        "clocks": clocks}))
+
+
 def run_multifilter(args):
     """lap3d-multifilter: the multi-column filter kernel alone on the 3-D
     Laplacian 100^3, `--ncols` columns with the slice request's polynomial
@@ -1521,6 +1671,10 @@ def main():
         run_dgemm(args)
     elif args.workload == "batch-uneven":
         run_batch_uneven(args)
+    elif args.workload == "lap3d-pipeline":
+        run_pipeline(args)
+    elif args.workload == "block-cgs":
+        run_block_cgs(args)
     elif args.workload == "rspd-kpm":
         run_rspd_kpm(args)
     else:

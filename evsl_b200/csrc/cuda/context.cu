@@ -153,6 +153,7 @@ int evslcu_finish(void) {
   evslcu_kpm_release();
   evslcu_trid_release();
   evslcu_lz_release();
+  evslcu_gemm_release();
   cudaFree(g_ctx.partials);
   cudaFree(g_ctx.counters);
   cudaFree(g_ctx.scalars);

@@ -18,6 +18,7 @@ using namespace evslcu;
 namespace {
 
 constexpr double kEta = 0.70710678118654752440;  // 1/sqrt(2), SRC/misc_la.c:226
+constexpr int EVSL_NGS_MAX_CU = 2;                 // Gram-Schmidt passes, INC/internal_header.h:24
 
 __global__ void k_dot(int n, const double *x, const double *y, double *part, unsigned int *ctr, double *out,
                       int sqrt_result) {
@@ -813,6 +814,33 @@ size_t evslcu_cgs_work_size(int n, int k) {
   return nchunks * (size_t)std::max(k, 1) + (size_t)std::max(k, 1) + 8;
 }
 
+// Block classical Gram-Schmidt, twice (BCGS2), on the m columns of W (ld
+// n): each block of b columns is first projected against every earlier
+// column by two passes of two GEMMs (H = W_prev^T W_b, W_b -= W_prev H: the
+// earlier columns are read once per block, not once per column), then its
+// columns are orthonormalised among themselves by classical Gram-Schmidt
+// with the DGKS test (SRC/misc_la.c:221-261) and scaled to unit norm.
+// H: (m - b) x b doubles of device scratch; norm_dev: one device double;
+// cgsw: evslcu_cgs_work_size(n, b) doubles.
+int evslcu_block_cgs2(int n, int m, double *W, int b, double *H, double *norm_dev, double *cgsw) {
+  if (n < 1 || m < 1 || b < 1 || !W || !H || !norm_dev || !cgsw) return fail(EVSLCU_ERR_ARG, "block_cgs2: bad arguments");
+  int rc = 0;
+  for (int c0 = 0; !rc && c0 < m; c0 += b) {
+    const int nb = std::min(b, m - c0);
+    double *Wb = W + (size_t)c0 * n;
+    for (int pass = 0; !rc && c0 > 0 && pass < 2; ++pass) {
+      rc = evslcu_dgemm('T', 'N', c0, nb, n, 1.0, W, n, Wb, n, 0.0, H, c0);
+      if (!rc) rc = evslcu_dgemm('N', 'N', n, nb, c0, -1.0, W, n, H, c0, 1.0, Wb, n);
+    }
+    for (int j = 0; !rc && j < nb; ++j) {
+      double *wj = Wb + (size_t)j * n;
+      rc = (j == 0) ? evslcu_nrm2(n, wj, norm_dev) : evslcu_cgs_dgks(n, j, EVSL_NGS_MAX_CU, Wb, n, wj, norm_dev, cgsw);
+      if (!rc) rc = evslcu_scal_inv_ds(n, norm_dev, wj);
+    }
+  }
+  return rc;
+}
+
 int evslcu_cgs_dgks(int n, int k, int imax, const double *Q, long long ldq, double *v, double *nrm_out_dev,
                     double *work) {
   if (k < 1 || n < 1) return fail(EVSLCU_ERR_ARG, "cgs: bad sizes n=%d k=%d", n, k);
@@ -949,6 +977,9 @@ int evslcu_set_dgemm_tiled(int on) {
   return 0;
 }
 
+static double *g_splitk = nullptr;  // split-K partial products (cached)
+static size_t g_splitk_cap = 0;
+
 int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const double *A, long long lda,
                  const double *B, long long ldb, double beta, double *C, long long ldc) {
   if (m <= 0 || n <= 0) return 0;
@@ -979,10 +1010,12 @@ int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const doub
   }
   const int gm = (m + BM - 1) / BM, gn = (n + BN - 1) / BN;
   // Long inner dimension with few output tiles (V^T W): split K into slabs
+  // (at least 2048 deep) so that the blocks fill the GPU about four times,
   // computed in parallel, then summed in slab order (deterministic).
   int slabs = 1, kchunk = 0;
-  if ((long long)k >= 32768 && (long long)gm * gn < 512) {
-    slabs = (int)std::min<long long>((k + 16383) / 16384, std::max(1, 2048 / (gm * gn)));
+  const long long tiles = (long long)gm * gn, fill = 4LL * sm_count();
+  if ((long long)k >= 8192 && tiles < fill) {
+    slabs = (int)std::min<long long>((fill + tiles - 1) / tiles, (k + 2047) / 2048);
     kchunk = (int)(((k + slabs - 1) / slabs + BK - 1) / BK * BK);
     slabs = (k + kchunk - 1) / kchunk;
   }
@@ -991,8 +1024,19 @@ int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const doub
   long long ldo = ldc, cstride = 0;
   double a = alpha, b = beta;
   if (slabs > 1) {
-    part = (double *)evslcu_malloc(sizeof(double) * (size_t)slabs * m * n);
-    if (!part) return EVSLCU_ERR_NOMEM;
+    // the slabs' partial products live in a cached buffer (grown, never
+    // shrunk until finish): no allocation per call
+    const size_t need = (size_t)slabs * m * n;
+    if (need > g_splitk_cap) {
+      if (g_splitk) {
+        cudaStreamSynchronize(st);
+        evslcu_free(g_splitk);
+      }
+      g_splitk = (double *)evslcu_malloc(sizeof(double) * need);
+      g_splitk_cap = g_splitk ? need : 0;
+      if (!g_splitk) return EVSLCU_ERR_NOMEM;
+    }
+    part = g_splitk;
     Cout = part;
     ldo = m;
     cstride = (long long)m * n;
@@ -1015,8 +1059,13 @@ int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const doub
     count_launch();
     rc = check_launch("k_splitk_reduce");
   }
-  if (part) evslcu_free(part);
   return rc;
+}
+
+void evslcu_gemm_release(void) {
+  evslcu_free(g_splitk);
+  g_splitk = nullptr;
+  g_splitk_cap = 0;
 }
 
 int evslcu_ritz_eval(const evslcu_op *op, int n, int m, double *U, double *W, double *norm, double *lam,

@@ -327,10 +327,17 @@ typedef struct {
 size_t evslcu_lz_scratch_doubles(void);
 size_t evslcu_lanczos_batch_table_bytes(int ns);
 int evslcu_lanczos_batch(int ns, const evslcu_lz_col *cols, int imax, void *table, size_t table_bytes);
+/* Block Gram-Schmidt, twice, on the m columns of W (n x m, ld n), blocks of
+ * b columns: GEMM projections against the earlier columns, then CGS with the
+ * DGKS test and unit norms inside the block.  H: (m - b) x b device doubles;
+ * norm_dev: 1 device double; cgsw: evslcu_cgs_work_size(n, b) doubles. */
+int evslcu_block_cgs2(int n, int m, double *W, int b, double *H, double *norm_dev, double *cgsw);
 /* x_i *= a_i (evslcu_scal) for ns vectors in one launch. */
 size_t evslcu_scal_batch_table_bytes(int ns);
 int evslcu_scal_batch(int ns, const int *n, double *const *x, const double *a, void *table, size_t table_bytes);
 void evslcu_lz_release(void);
+/* Free the cached split-K partial products of evslcu_dgemm. */
+void evslcu_gemm_release(void);
 /* Free the cached KPM and tridiagonal workspaces (evslcu_finish calls them). */
 void evslcu_kpm_release(void);
 void evslcu_trid_release(void);

@@ -51,6 +51,7 @@
 #define ENG_MAX_SWEEPS 4
 #define ENG_NSCAL 4
 #define ENG_MIN_GUARDS 16
+#define ENG_CGS_BLOCK 32 /* columns per block of the refinement's Gram-Schmidt */
 
 enum { PH_START = 0, PH_LANCZOS = 1, PH_RESTART = 2 };
 
@@ -694,16 +695,10 @@ static int refine_fp64(evslx_engine *E, slot_t *s, int m, double *U, double *W, 
       cols[j].y = W + (size_t)j * n_l;
     }
     CU(evslcu_filter_columns(r->M->mat, 0, m, cols, fw, need));
-    /* orthonormalise W in place: CGS + DGKS column by column */
+    /* orthonormalise W in place: block Gram-Schmidt twice (GEMM projections
+     * against the earlier blocks), CGS + DGKS inside each block */
     double *ds = E->ds + ENG_NSCAL * (size_t)(s - E->slots);
-    CU(evslcu_nrm2(n, W, ds + 3));
-    CU(evslcu_scal_inv_ds(n, ds + 3, W));
-    for (int j = 1; j < m && !rc; j++) {
-      double *wj = W + (size_t)j * n_l;
-      rc = evslcu_cgs_dgks(n, j, EVSL_NGS_MAX, W, (long long)n, wj, ds + 3, cgsw);
-      if (!rc) rc = evslcu_scal_inv_ds(n, ds + 3, wj);
-    }
-    CU(rc);
+    CU(evslcu_block_cgs2(n, m, W, ENG_CGS_BLOCK, dH, ds + 3, cgsw));
     /* U = A W; H = W' A W (symmetrised on the host); eigenpairs; U = W Q */
     for (int j = 0; j < m && !rc; j++) rc = evslcu_spmv(r->M->mat, W + (size_t)j * n_l, U + (size_t)j * n_l);
     CU(rc);

@@ -47,3 +47,30 @@ def test_tiled_gemm_matches(gpu_lib, m, n, k, pad, beta):
     assert np.max(np.abs(got[:, :m].T - ref)) <= 1e-13 * np.max(np.abs(ref))
     # the padding rows of C are untouched
     assert np.array_equal(got[:, m:], C0[:, m:])
+
+
+@pytest.mark.parametrize("n, m, b", [(20000, 100, 32), (5003, 45, 16), (40000, 33, 32)])
+def test_block_cgs2_orthonormalises(gpu_lib, n, m, b):
+    """Block Gram-Schmidt twice (the mixed-precision refinement's
+    orthonormalisation; GEMM projections between blocks, CGS + DGKS as in
+    SRC/misc_la.c:221-261 inside a block): the columns come out orthonormal to
+    1e-13 and span the input columns (every input column is reproduced by its
+    projection to 1e-12 of its norm), on well and badly conditioned inputs."""
+    rng = np.random.default_rng(n + m)
+    W0 = rng.standard_normal((m, n))  # row j = column j of the n x m block
+    # a badly conditioned half: columns nearly dependent on the first ones
+    W0[m // 2:] = W0[: m - m // 2] + 1e-6 * rng.standard_normal((m - m // 2, n))
+    dW = evsl_b200.DeviceBuffer.from_host(gpu_lib.lib, W0)
+    dH = evsl_b200.DeviceBuffer(gpu_lib.lib, 8 * m * m)
+    dn = evsl_b200.DeviceBuffer(gpu_lib.lib, 8)
+    gpu_lib.lib.evslcu_cgs_work_size.restype = C.c_size_t
+    gpu_lib.lib.evslcu_cgs_work_size.argtypes = [C.c_int, C.c_int]
+    work = evsl_b200.DeviceBuffer(gpu_lib.lib, 8 * int(gpu_lib.lib.evslcu_cgs_work_size(n, b)))
+    fn = gpu_lib.lib.evslcu_block_cgs2
+    fn.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    assert fn(n, m, dW.ptr, b, dH.ptr, dn.ptr, work.ptr) == 0
+    Q = dW.to_host(shape=(m, n))
+    G = Q @ Q.T
+    assert np.max(np.abs(G - np.eye(m))) <= 1e-13
+    P = (W0 @ Q.T) @ Q
+    assert np.max(np.linalg.norm(W0 - P, axis=1) / np.linalg.norm(W0, axis=1)) <= 1e-12
