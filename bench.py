@@ -78,6 +78,8 @@ def parse():
     p.add_argument("--rspd-n", type=int, default=RSPD_N, help="rspd-filter: rows of the random SPD matrix")
     p.add_argument("--grid", type=int, default=50,
                    help="lap3d-pipeline: the 3-D Laplacian's grid points per side")
+    p.add_argument("--kpm-prefetch", type=int, choices=[-1, 0, 1], default=-1,
+                   help="lap3d-kpm / rspd-kpm: the KPM step's own-row prefetch form (-1: library default)")
     p.add_argument("--kpm-split", type=int, choices=[-1, 0, 1], default=-1,
                    help="rspd-kpm: KPM block step on the column-split copy: -1 automatic, 0 off, 1 on")
     p.add_argument("--split-range-mb", type=float, default=0.0,
@@ -1233,6 +1235,8 @@ def run_kpm(args):
     lib = evsl_b200.Library()
     lib.lib.evslx_last_kpm_seconds.restype = C.c_double
     lib.lib.evslcu_set_kpm_doubling(0 if args.kpm_direct else 1)
+    if args.kpm_prefetch >= 0:
+        lib.lib.evslcu_set_kpm_prefetch(args.kpm_prefetch)
     ia, ja, a = W.laplacian_csr(NX, NY, NZ)
     lib.set_csr(ia, ja, a)
     n, nnz = NX * NY * NZ, int(ia[-1])

@@ -251,6 +251,7 @@ def load():
         "evslx_rand_device_draws": ([C.c_int, C.c_int, C.c_uint64, C.c_void_p], C.c_int),
         "evslx_get_spmv_kernel": ([], C.c_int),
         "evslx_matvec": ([C.c_void_p, C.c_void_p], C.c_int),
+        "evslx_matvec_cols": ([C.c_int, C.c_void_p, C.c_void_p], C.c_int),
         "evslx_problem_info": ([_ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
         "evslx_launch_count": ([], C.c_uint64),
         "evslx_last_kpm_seconds": ([], C.c_double),
@@ -661,6 +662,14 @@ class Library:
         dy = DeviceBuffer(self.lib, dx.nbytes)
         self._check(self.lib.evslx_matvec(dx.ptr, dy.ptr), "evslx_matvec")
         return dy.to_host()
+
+    def matvec_cols(self, X):
+        """Rows of X (m x n) each multiplied by A, in one launch."""
+        X = np.ascontiguousarray(np.atleast_2d(X), dtype=np.float64)
+        dx = DeviceBuffer.from_host(self.lib, X)
+        dy = DeviceBuffer(self.lib, dx.nbytes)
+        self._check(self.lib.evslx_matvec_cols(X.shape[0], dx.ptr, dy.ptr), "evslx_matvec_cols")
+        return dy.to_host().reshape(X.shape)
 
     # -- filter --------------------------------------------------------------
     def find_pol(self, intv, *, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=None, deg=0):

@@ -1081,14 +1081,11 @@ int evslcu_ritz_eval(const evslcu_op *op, int n, int m, double *U, double *W, do
     count_launch();
     rc = check_launch("k_colscale_inv");
   }
-  for (int c = 0; !rc && c < m; ++c) {
-    if (op->A) {
-      rc = evslcu_spmv(op->A, U + (size_t)c * n, W + (size_t)c * n);
-    } else {
-      cudaError_t e = cudaStreamSynchronize(stream());
-      if (e != cudaSuccess) rc = fail(EVSLCU_ERR_CUDA, "sync before matvec: %s", cudaGetErrorString(e));
-      if (!rc) op->func(U + (size_t)c * n, W + (size_t)c * n, op->data);
-    }
+  if (!rc && op->A) rc = evslcu_spmv_cols(op->A, U, W, m);  // all m products in one launch
+  for (int c = 0; !rc && !op->A && c < m; ++c) {
+    cudaError_t e = cudaStreamSynchronize(stream());
+    if (e != cudaSuccess) rc = fail(EVSLCU_ERR_CUDA, "sync before matvec: %s", cudaGetErrorString(e));
+    if (!rc) op->func(U + (size_t)c * n, W + (size_t)c * n, op->data);
   }
   if (!rc) rc = colred(n, m, 1, U, W, nullptr, dl);
   if (!rc) rc = colred(n, m, 2, U, W, dl, dr);

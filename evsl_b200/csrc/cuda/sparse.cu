@@ -293,6 +293,18 @@ __global__ void __launch_bounds__(kThreads) k_spmv(M A, const double *__restrict
     y[row_of(A, s)] = row_dot<false>(A, s, x);
 }
 
+// Y(:, c) = A X(:, c) for the m columns of column-major X, Y (leading
+// dimension ld), column c in blockIdx.y: each row is k_spmv's row product,
+// so every column equals evslcu_spmv of that column bit for bit.
+template <class M>
+__global__ void __launch_bounds__(kThreads)
+    k_spmv_cols(M A, const double *__restrict__ X, double *__restrict__ Y, long long ld) {
+  const double *x = X + (long long)blockIdx.y * ld;
+  double *y = Y + (long long)blockIdx.y * ld;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < A.n; s += gridDim.x * blockDim.x)
+    y[row_of(A, s)] = row_dot<false>(A, s, x);
+}
+
 // One Chebyshev degree step k (FIRST: k == 1; EPI: k == deg, Lanczos epilogue).
 //   out may alias vkm1 (each thread reads vkm1[r] before writing out[r]).
 //   WMAX > 0: rows have at most WMAX stored entries (unrolled row products);
@@ -623,8 +635,11 @@ __global__ void __launch_bounds__(kThreads)
 // only -- not on B, nb or VEC -- so probe shards reproduce the full block.
 constexpr int kKpmHalfRows = 4;  // rows per half-warp and iteration
 
-template <bool FIRST, bool VEC>
-__global__ void __launch_bounds__(kThreads, 4)
+// PRE: the rows' own v_k and v_k-1 values are loaded before the gathers (so
+// their DRAM latency overlaps the gathers') and the new vector is stored with
+// 16-byte stores; same arithmetic, more registers (3 blocks per SM).
+template <bool FIRST, bool VEC, bool PRE>
+__global__ void __launch_bounds__(kThreads, PRE ? 3 : 4)
     k_kpm_dbl(CsrView A, int B, int p0, int nb, const double *__restrict__ vk, const double *vkm1, double *out,
               double scal, double nctr, double *part) {
   constexpr int NS = FIRST ? 3 : 2;
@@ -649,6 +664,37 @@ __global__ void __launch_bounds__(kThreads, 4)
       mymax = max(mymax, len[i]);
     }
     const int maxlen = __reduce_max_sync(0xffffffffu, mymax);
+    double px[kKpmHalfRows][2], pm[kKpmHalfRows][2];
+    if constexpr (PRE) {
+#pragma unroll
+      for (int i = 0; i < kKpmHalfRows; ++i) {
+        const int r = r0 + i;
+        px[i][0] = px[i][1] = pm[i][0] = pm[i][1] = 0.0;
+        if (r < A.n) {
+          const long long idx = (long long)r * B + pa;
+          if (VEC && onB) {
+            const double2 t = __ldg(reinterpret_cast<const double2 *>(vk + idx));
+            px[i][0] = t.x;
+            px[i][1] = t.y;
+            if (!FIRST) {
+              // v_k-1 is overwritten by this step's output: plain loads
+              const double2 u = *reinterpret_cast<const double2 *>(vkm1 + idx);
+              pm[i][0] = u.x;
+              pm[i][1] = u.y;
+            }
+          } else {
+            if (onA) {
+              px[i][0] = vk[idx];
+              if (!FIRST) pm[i][0] = vkm1[idx];
+            }
+            if (onB) {
+              px[i][1] = vk[idx + 1];
+              if (!FIRST) pm[i][1] = vkm1[idx + 1];
+            }
+          }
+        }
+      }
+    }
     double acc[kKpmHalfRows][2];
 #pragma unroll
     for (int i = 0; i < kKpmHalfRows; ++i) acc[i][0] = acc[i][1] = 0.0;
@@ -717,18 +763,21 @@ __global__ void __launch_bounds__(kThreads, 4)
     for (int i = 0; i < kKpmHalfRows; ++i) {
       const int r = r0 + i;
       if (r >= A.n) continue;
+      double wv[2] = {0.0, 0.0};
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         if (!(c == 0 ? onA : onB)) continue;
         const long long idx = (long long)r * B + pa + c;
-        const double x = vk[idx];
+        const double x = PRE ? px[i][c] : vk[idx];
         double w = __dmul_rn(scal, __dadd_rn(acc[i][c], __dmul_rn(nctr, x)));
-        if (!FIRST) w = __dadd_rn(w, -vkm1[idx]);
-        out[idx] = w;
+        if (!FIRST) w = __dadd_rn(w, -(PRE ? pm[i][c] : vkm1[idx]));
+        if (!PRE || !(VEC && onB)) out[idx] = w;
+        wv[c] = w;
         sum[0][c] += w * w;
         sum[1][c] += w * x;
         if (FIRST) sum[NS - 1][c] += x * x;
       }
+      if (PRE && VEC && onB) *reinterpret_cast<double2 *>(out + (long long)r * B + pa) = make_double2(wv[0], wv[1]);
     }
   }
 #pragma unroll
@@ -1429,6 +1478,40 @@ int evslcu_spmv(const evslcu_mat *A, const double *x, double *y) {
 }
 
 
+int evslcu_spmv_cols(const evslcu_mat *A, const double *X, double *Y, int m) {
+  if (!A) return fail(EVSLCU_ERR_ARG, "null matrix");
+  if (m <= 0) return 0;
+  const long long ld = A->n;
+  for (int c0 = 0; c0 < m; c0 += 65535) {  // grid.y limit
+    const int mc = std::min(65535, m - c0);
+    // enough blocks in all to fill the GPU a few times; the row products do
+    // not depend on the grid
+    const int gx = std::max(1, std::min(grid_for(A->n), (16 * sm_count() + mc - 1) / mc));
+    const dim3 g(gx, mc);
+    const double *Xc = X + (size_t)c0 * ld;
+    double *Yc = Y + (size_t)c0 * ld;
+    if (evslcu_mat_uses_patterns(A)) {
+      if (A->pat_chdr >= 0 && g_pattern_const && A->pat_f32)
+        k_spmv_cols<PatCPView><<<g, kThreads, 0, stream()>>>(PatCPView{A->n, A->pat_id, A->pat_chdr}, Xc, Yc, ld);
+      else if (A->pat_chdr >= 0 && g_pattern_const)
+        k_spmv_cols<PatCView><<<g, kThreads, 0, stream()>>>(PatCView{A->n, A->pat_id, A->pat_chdr}, Xc, Yc, ld);
+      else if (A->pat_f32)
+        k_spmv_cols<PatPView><<<g, kThreads, 0, stream()>>>(pat_pview(A), Xc, Yc, ld);
+      else
+        k_spmv_cols<PatView><<<g, kThreads, 0, stream()>>>(pat_view(A), Xc, Yc, ld);
+      EVSLCU_LAUNCH_CHECK("k_spmv_cols");
+      continue;
+    }
+    int rc = with_view(A, [&](auto view) {
+      k_spmv_cols<decltype(view)><<<g, kThreads, 0, stream()>>>(view, Xc, Yc, ld);
+      EVSLCU_LAUNCH_CHECK("k_spmv_cols");
+      return 0;
+    });
+    if (rc) return rc;
+  }
+  return 0;
+}
+
 int evslcu_cheb_update(int n, int k, double t, double s, double cc, double *vkp1, const double *vk,
                        const double *vkm1, double *y) {
   k_cheb_update<<<grid_for(n), kThreads, 0, stream()>>>(n, k, t, s, -cc, vkp1, vk, vkm1, y);
@@ -1438,6 +1521,7 @@ int evslcu_cheb_update(int n, int k, double t, double s, double cc, double *vkp1
 
 static int g_kpm_doubling = 1;
 static int g_kpm_split = -1;  // -1: automatic, 0: never, 1: whenever the matrix has a column-split copy
+static int g_kpm_pre = 0;     // 1: the k_kpm_dbl form that loads the rows' own values before the gathers
 
 // The column-split copy the KPM block step runs on, or null for k_kpm_dbl:
 // automatically for matrices whose columns reach far from the diagonal (the
@@ -1519,6 +1603,11 @@ int evslcu_set_kpm_doubling(int on) {
   return 0;
 }
 
+int evslcu_set_kpm_prefetch(int on) {
+  g_kpm_pre = on ? 1 : 0;
+  return 0;
+}
+
 int evslcu_set_kpm_split(int mode) {
   if (mode < -1 || mode > 1) return fail(EVSLCU_ERR_ARG, "KPM split mode must be -1, 0 or 1");
   g_kpm_split = mode;
@@ -1577,14 +1666,23 @@ static int kpm_dots_doubling(const evslcu_op *op, int n, int Mdeg, int nvec, con
     for (int p0 = 0; !X && !rc && p0 < B; p0 += 32) {
       const int nb = std::min(32, B - p0);
       const bool vec = (B % 2 == 0);  // two probes per 16-byte access
-      if (k == 0 && vec)
-        k_kpm_dbl<true, true><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+      if (g_kpm_pre) {
+        if (k == 0 && vec)
+          k_kpm_dbl<true, true, true><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+        else if (k == 0)
+          k_kpm_dbl<true, false, true><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+        else if (vec)
+          k_kpm_dbl<false, true, true><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+        else
+          k_kpm_dbl<false, false, true><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+      } else if (k == 0 && vec)
+        k_kpm_dbl<true, true, false><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
       else if (k == 0)
-        k_kpm_dbl<true, false><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+        k_kpm_dbl<true, false, false><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
       else if (vec)
-        k_kpm_dbl<false, true><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+        k_kpm_dbl<false, true, false><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
       else
-        k_kpm_dbl<false, false><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
+        k_kpm_dbl<false, false, false><<<grid, kThreads, 0, stream()>>>(A, B, p0, nb, vk, vkm1, o, scal, nctr, part);
       count_launch();
       rc = check_launch("k_kpm_dbl");
     }

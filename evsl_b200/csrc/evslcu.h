@@ -81,6 +81,9 @@ int evslcu_mat_set_kernel(evslcu_mat *A, int which);
 int evslcu_mat_get_kernel(const evslcu_mat *A);
 /* y = A x, rows summed left to right. */
 int evslcu_spmv(const evslcu_mat *A, const double *x, double *y);
+/* Y(:,c) = A X(:,c) for the m columns of column-major X, Y (n rows each) in
+ * one launch; each column bitwise evslcu_spmv's. */
+int evslcu_spmv_cols(const evslcu_mat *A, const double *X, double *Y, int m);
 
 /* User matvec callback (SetAMatvec): y = A x on device vectors. */
 typedef void (*evslcu_mvfunc)(double *x, double *y, void *data);
@@ -306,6 +309,10 @@ int evslcu_set_kpm_doubling(int on);
  * 0 never, 1 whenever the matrix can have a copy.  The moments agree to
  * rounding. */
 int evslcu_set_kpm_split(int mode);
+/* 1: the KPM block step loads each row's own v_k and v_k-1 before its
+ * gathers and stores the new vector 16 bytes at a time; 0: after them.
+ * Same arithmetic. */
+int evslcu_set_kpm_prefetch(int on);
 /* The request engine's Lanczos step for many slots in a dozen launches:
  * per slot, z = V(:,k+1) (the filtered vector) gets z -= beta V(:,k-1)
  * (k > 0), alpha = z.V(:,k) into ds[0], z -= alpha V(:,k), then classical

@@ -700,8 +700,7 @@ static int refine_fp64(evslx_engine *E, slot_t *s, int m, double *U, double *W, 
     double *ds = E->ds + ENG_NSCAL * (size_t)(s - E->slots);
     CU(evslcu_block_cgs2(n, m, W, ENG_CGS_BLOCK, dH, ds + 3, cgsw));
     /* U = A W; H = W' A W (symmetrised on the host); eigenpairs; U = W Q */
-    for (int j = 0; j < m && !rc; j++) rc = evslcu_spmv(r->M->mat, W + (size_t)j * n_l, U + (size_t)j * n_l);
-    CU(rc);
+    CU(evslcu_spmv_cols(r->M->mat, W, U, m));
     CU(evslcu_dgemm('T', 'N', m, m, n, 1.0, W, n, U, n, 0.0, dH, m));
     CU(evslcu_d2h(H, dH, sizeof(double) * (size_t)m * m));
     for (int i = 0; i < m; i++)

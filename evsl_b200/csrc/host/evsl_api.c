@@ -555,6 +555,21 @@ int evslx_matvec(const double *x, double *y) {
   return 0;
 }
 
+int evslx_matvec_cols(int m, const double *X, double *Y) {
+  int rc = evsl_require_operator();
+  if (rc) return rc;
+  if (m < 0 || (m > 0 && (!X || !Y))) return evsl_seterr(EVSLX_ERR_ARG, "evslx_matvec_cols: bad arguments");
+  if (evslh.op.A) {
+    rc = evslcu_spmv_cols(evslh.op.A, X, Y, m);
+    if (!rc) rc = evslcu_sync();
+    return from_cu(rc);
+  }
+  evslcu_sync();
+  const size_t n = (size_t)evslh.op.n;
+  for (int c = 0; c < m; c++) evslh.op.func((double *)X + (size_t)c * n, Y + (size_t)c * n, evslh.op.data);
+  return 0;
+}
+
 int evslx_problem_info(int *n, long long *nnz, long long *stored) {
   if (n) *n = evslh.op.n;
   if (nnz) *nnz = evslh.op.A ? evslcu_mat_nnz(evslh.op.A) : 0;

@@ -209,6 +209,11 @@ int evslx_matrix_storage(int *value_bytes, int *index_bytes);
 /* y = A x for the registered matrix on device vectors (rows summed left to
  * right, like the reference CPU matvec SRC/spmat.c:257-298). */
 int evslx_matvec(const double *x, double *y);
+/* Y(:,c) = A X(:,c) for the m columns of the column-major device blocks X,
+ * Y (n x m) in one launch, each column bitwise evslx_matvec's (a registered
+ * CSR matrix; with a SetAMatvec operator, the callback once per column).
+ * The Ritz pairs of the solvers use it for their residuals. */
+int evslx_matvec_cols(int m, const double *X, double *Y);
 
 /* Y = p(A) V for ncols device vectors at once (V, Y: column-major n x ncols;
  * work: 2 n ncols doubles).  One pass over A per degree serves every group

@@ -555,3 +555,41 @@ def test_filter_kernels_on_nine_entry_rows(gpu_lib, variant):
         assert np.array_equal(gpu_lib.matvec(v), O.csr_matvec(ia, ja, a, v))
     finally:
         gpu_lib.set_filter_kernel(-1)
+
+
+@pytest.mark.parametrize("nvec", [20, 13])
+def test_kpm_prefetch_form_is_bitwise(gpu_lib, nvec):
+    """The KPM block step that loads each row's own v_k, v_k-1 before its
+    gathers (and stores 16 bytes at a time) performs the same operations:
+    its raw dot products equal the default form's bit for bit, even and odd
+    probe counts (paired and single loads)."""
+    import evsl_b200
+
+    ia, ja, a = _lap(gpu_lib, 14, 12, 5)
+    n = len(ia) - 1
+    iv = [0.7, 2.9, 0.0, 12.0]
+    probes = evsl_b200.DeviceBuffer.from_host(gpu_lib.lib, O.seeded_rademacher(nvec, n, 5))
+    ref = gpu_lib.kpm_dots(40, iv, probes, nvec)
+    try:
+        gpu_lib.lib.evslcu_set_kpm_prefetch(1)
+        got = gpu_lib.kpm_dots(40, iv, probes, nvec)
+    finally:
+        gpu_lib.lib.evslcu_set_kpm_prefetch(0)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("case", ["lap3d", "rspd"])
+def test_matvec_cols_bitwise(gpu_lib, case):
+    """The block matvec the Ritz residuals use (all columns in one launch)
+    equals the reference CPU CSR matvec (SRC/spmat.c:257-298) column by
+    column bit for bit: on the row-pattern dictionary of a Laplacian and on
+    the SELL-C-sigma copy of a random SPD matrix."""
+    from evsl_b200 import workloads as W
+
+    ia, ja, a = O.lap_csr(23, 19, 17) if case == "lap3d" else W.random_spd_csr(7001, 16, 41)
+    gpu_lib.set_csr(ia, ja, a)
+    n = len(ia) - 1
+    X = np.stack([O.seeded_normal(n, 60 + c) for c in range(37)])
+    Y = gpu_lib.matvec_cols(X)
+    for c in range(X.shape[0]):
+        assert np.array_equal(Y[c], O.csr_matvec(ia, ja, a, X[c])), c
