@@ -34,6 +34,10 @@ struct MMItem {
   const int *cw;
   const void *scol, *sval;
   const int *perm;
+  // row-pattern dictionary (fmt 4: double2 entries, 5: packed entries)
+  const unsigned short *pid;
+  const int2 *phdr;
+  const void *pent;
   const double *mu;  // device, deg + 1
   const double *x;
   double *y;
@@ -48,6 +52,12 @@ __device__ __forceinline__ double mm_row(const MMItem &I, int s, const double *x
   return row_dot<false>(A, s, x);
 }
 __device__ __forceinline__ int mm_row_of(const MMItem &I, int s) { return I.perm ? __ldg(I.perm + s) : s; }
+
+// A row of a matrix read through its row-pattern dictionary (slot = row).
+__device__ __forceinline__ double mm_row_pat(const MMItem &I, int r, const double *x) {
+  if (I.fmt == 4) return row_dot<false>(PatView{I.n, I.pid, I.phdr, (const double2 *)I.pent}, r, x);
+  return row_dot<false>(PatPView{I.n, I.pid, I.phdr, (const unsigned long long *)I.pent}, r, x);
+}
 
 constexpr int kMMThreads = 256;
 
@@ -75,7 +85,8 @@ __global__ void __launch_bounds__(kMMThreads) k_mm_cheb(const MMItem *__restrict
     case 0: acc = mm_row<double, int>(I, sl, vk); break;
     case 1: acc = mm_row<double, short>(I, sl, vk); break;
     case 2: acc = mm_row<float, int>(I, sl, vk); break;
-    default: acc = mm_row<float, short>(I, sl, vk); break;
+    case 3: acc = mm_row<float, short>(I, sl, vk); break;
+    default: acc = mm_row_pat(I, r, vk); break;
   }
   const double x = vk[r];
   double w = __dmul_rn(t, __dadd_rn(acc, __dmul_rn(I.ncc, x)));
@@ -209,6 +220,7 @@ __global__ void __launch_bounds__(kMMThreads) k_mm_persistent(MMPersist P) {
 }
 
 unsigned g_mm_polls = 1u << 22;  // polls per dependency wait of the persistent form
+int g_mm_patterns = 1;           // 1: matrices with a row-pattern dictionary are read through it
 int g_mm_persistent = 0;         // 1: the persistent form
 
 template <class F>
@@ -270,6 +282,26 @@ int evslcu_filter_batch(int ncols, const evslcu_batch_col *cols, void *table, si
     I.sval = c.A->sval;
     I.perm = c.A->perm;
     I.fmt = 2 * (c.A->vfmt ? 1 : 0) + (c.A->ifmt ? 1 : 0);
+    I.pid = nullptr;
+    I.phdr = nullptr;
+    I.pent = nullptr;
+    if (g_mm_patterns && !g_mm_persistent && evslcu_mat_uses_patterns(c.A) && !c.A->perm) {
+      // the dictionary in global memory (PatView / PatPView): the same
+      // rounded row products as the SELL copy
+      if (c.A->pat_f32) {
+        const PatPView v = pat_pview(c.A);
+        I.pid = v.pid;
+        I.phdr = v.hdr;
+        I.pent = v.pk;
+        I.fmt = 5;
+      } else {
+        const PatView v = pat_view(c.A);
+        I.pid = v.pid;
+        I.phdr = v.hdr;
+        I.pent = v.ent;
+        I.fmt = 4;
+      }
+    }
     I.ellw = c.A->ellw;
     I.mu = c.mu;
     I.x = c.x;
