@@ -43,7 +43,7 @@ struct MMItem {
   double *y;
   double *w;  // 2n
   double t1, t2, ncc;
-  int n, deg, block0, fmt, ellw, pad;
+  int n, deg, block0, fmt, ellw, pmax;  // pmax: longest row pattern (fmt 4, 5)
 };
 
 template <class VT, class IT>
@@ -54,9 +54,16 @@ __device__ __forceinline__ double mm_row(const MMItem &I, int s, const double *x
 __device__ __forceinline__ int mm_row_of(const MMItem &I, int s) { return I.perm ? __ldg(I.perm + s) : s; }
 
 // A row of a matrix read through its row-pattern dictionary (slot = row).
+// Patterns of at most 8 entries (stencils) take the unrolled row product:
+// every load of the row in flight before the first add, same rounded
+// operations in the same order.
 __device__ __forceinline__ double mm_row_pat(const MMItem &I, int r, const double *x) {
-  if (I.fmt == 4) return row_dot<false>(PatView{I.n, I.pid, I.phdr, (const double2 *)I.pent}, r, x);
-  return row_dot<false>(PatPView{I.n, I.pid, I.phdr, (const unsigned long long *)I.pent}, r, x);
+  if (I.fmt == 4) {
+    const PatView v{I.n, I.pid, I.phdr, (const double2 *)I.pent};
+    return I.pmax <= 8 ? row_dot_w<8, false>(v, r, x) : row_dot<false>(v, r, x);
+  }
+  const PatPView v{I.n, I.pid, I.phdr, (const unsigned long long *)I.pent};
+  return I.pmax <= 8 ? row_dot_w<8, false>(v, r, x) : row_dot<false>(v, r, x);
 }
 
 constexpr int kMMThreads = 256;
@@ -313,7 +320,7 @@ int evslcu_filter_batch(int ncols, const evslcu_batch_col *cols, void *table, si
     I.n = n;
     I.deg = c.deg;
     I.block0 = prefix[i];
-    I.pad = 0;
+    I.pmax = c.A->pat_maxlen;
     prefix[i + 1] = prefix[i] + (n + kMMThreads - 1) / kMMThreads;
     rows += n;
   }
