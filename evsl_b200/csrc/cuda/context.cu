@@ -74,6 +74,36 @@ int evslcu_device_count(void) {
   return n;
 }
 
+// Device memory of the library comes from a stream-ordered pool on the
+// library stream (cudaMallocFromPoolAsync / cudaFreeAsync): a free does not
+// wait for the device -- work already queued on the stream that still uses
+// the memory runs first -- and freed memory is reused by later allocations
+// without a trip to the driver.  Freed memory stays in the pool (up to
+// kPoolKeep bytes) for later allocations; EVSLFinish trims it.  The pool outlives EVSLFinish, so that
+// buffers handed to the caller (eigenvectors) can be freed afterwards.
+static cudaMemPool_t g_pool = nullptr;
+static int g_pool_dev = -1;
+constexpr unsigned long long kPoolKeep = ~0ull;  // keep freed memory for reuse until EVSLFinish
+
+static void pool_init(int dev) {
+  if (g_pool && g_pool_dev == dev) return;
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t p = nullptr;
+  if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+    cudaGetLastError();  // plain cudaMalloc / cudaFree then
+    return;
+  }
+  unsigned long long keep = kPoolKeep;
+  cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+  g_pool = p;
+  g_pool_dev = dev;
+}
+
+static bool pool_ready() { return g_ctx.ready && g_pool && g_pool_dev == g_ctx.device; }
+
 int evslcu_init(void) {
   if (g_ctx.ready) return 0;
   if (evslcu_device_count() < 1) return fail(EVSLCU_ERR_NODEV, "no CUDA device is visible");
@@ -94,6 +124,7 @@ int evslcu_init(void) {
   EVSLCU_CUDA(cudaMalloc(&g_ctx.barrier, sizeof(unsigned int) * kBarrierWords));
   EVSLCU_CUDA(cudaMemset(g_ctx.barrier, 0, sizeof(unsigned int) * kBarrierWords));
   EVSLCU_CUDA(cudaMemset(g_ctx.scalars, 0, sizeof(double) * 64));
+  pool_init(g_ctx.device);
   g_ctx.ready = true;
   return 0;
 }
@@ -158,6 +189,8 @@ int evslcu_finish(void) {
   cudaFree(g_ctx.counters);
   cudaFree(g_ctx.scalars);
   cudaFree(g_ctx.barrier);
+  cudaStreamSynchronize(g_ctx.stream);
+  if (g_pool) cudaMemPoolTrimTo(g_pool, 0);
   cudaStreamDestroy(g_ctx.stream);
   g_ctx = Context();
   cudaError_t e = cudaGetLastError();
@@ -189,7 +222,7 @@ int evslcu_last_cuda_error(char *buf, int len) {
 void *evslcu_malloc(size_t nbytes) {
   void *p = nullptr;
   if (nbytes == 0) nbytes = 1;
-  cudaError_t e = cudaMalloc(&p, nbytes);
+  cudaError_t e = pool_ready() ? cudaMallocFromPoolAsync(&p, nbytes, g_pool, g_ctx.stream) : cudaMalloc(&p, nbytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     fail(EVSLCU_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", nbytes, cudaGetErrorString(e));
@@ -200,7 +233,12 @@ void *evslcu_malloc(size_t nbytes) {
 
 int evslcu_free(void *p) {
   if (!p) return 0;
-  // Memory may still be in use by queued work on the library stream.
+  // Memory may still be in use by work queued on the library stream: a
+  // stream-ordered free runs after it; otherwise wait for the stream.
+  if (pool_ready()) {
+    EVSLCU_CUDA(cudaFreeAsync(p, g_ctx.stream));
+    return 0;
+  }
   if (g_ctx.ready) cudaStreamSynchronize(g_ctx.stream);
   EVSLCU_CUDA(cudaFree(p));
   return 0;
