@@ -427,8 +427,13 @@ inline const evslcu_xsplit *xs_of(const evslcu_mat *M, int fp32, int B) {
   const int P = xs_ranges(M, fp32, B);
   if (!P) return nullptr;
   const evslcu_xsplit *X = M->xs[xs_slot(P)];
-  if (!X || (fp32 && !X->val32[0])) return nullptr;
-  return X;
+  if (X && (!fp32 || X->val32[0])) return X;
+  // the range budget changed since this width was tuned: every copy holds the
+  // whole matrix, so any built one serves (its ranges are just sized for
+  // another budget)
+  for (const evslcu_xsplit *Y : M->xs)
+    if (Y && (!fp32 || Y->val32[0])) return Y;
+  return nullptr;
 }
 
 template <class VT, int B, bool PF, bool PL>
@@ -605,7 +610,8 @@ int mf_step(const evslcu_mat *M, const SellT<AV, IT> &A, int variant, int k, con
 // Kernel launches of one degree step: one, or one per column range
 // (variant 7).
 inline int launches_per_step(const evslcu_mat *M, int fp32, int B, int variant) {
-  return (variant == 7) ? std::max(1, xs_ranges(M, fp32, B)) : 1;
+  const evslcu_xsplit *X = (variant == 7) ? xs_of(M, fp32, B) : nullptr;
+  return X ? X->P : 1;
 }
 
 // Number of VT values of the coefficient table of one group.
