@@ -76,6 +76,9 @@ def parse():
     p.add_argument("--serve-mix", choices=["default", "small"], default="default",
                    help="serve: 'small' draws the large-matrix requests on the 2-D 100x100 Laplacian only")
     p.add_argument("--rspd-n", type=int, default=RSPD_N, help="rspd-filter: rows of the random SPD matrix")
+    p.add_argument("--dgemm-kernel", type=int, choices=[-1, 0, 1, 2], default=-1,
+                   help="dgemm: 0 the 64x64 kernel, 1 the 128x128 DFMA kernel, 2 the mma.sync f64 kernel "
+                        "(-1: library default)")
     p.add_argument("--grid", type=int, default=50,
                    help="lap3d-pipeline: the 3-D Laplacian's grid points per side")
     p.add_argument("--kpm-prefetch", type=int, choices=[-1, 0, 1], default=-1,
@@ -844,6 +847,8 @@ def run_dgemm(args):
 
     n, K, m = (int(x) for x in args.gemm.split(","))
     lib = E.Library()
+    if args.dgemm_kernel >= 0:
+        lib.lib.evslcu_set_dgemm_tiled(args.dgemm_kernel)
     lib.lib.evslcu_fp64_probe.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
     dfma, dmma = C.c_double(), C.c_double()
     lib._check(lib.lib.evslcu_fp64_probe(C.byref(dfma), C.byref(dmma)), "evslcu_fp64_probe")
@@ -885,7 +890,9 @@ def run_dgemm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded normal operands)",
         "config": {"workload": "dgemm: U = V(:,1:K) Y, n=%d K=%d m=%d" % (n, K, m), "check_rel_err": err},
-        "roofline": {"bound": "fp64", "kernel": "k_dgemm_nn128", "achieved": tf, "peak": peak,
+        "roofline": {"bound": "fp64", "kernel": {0: "k_dgemm", 1: "k_dgemm_nn128"}.get(args.dgemm_kernel,
+                                                                                   "k_dgemm_mma"),
+                     "achieved": tf, "peak": peak,
                      "peak_kind": "measured on this GPU (FMA %.1f, mma.sync f64 %.1f TFLOP/s)" % (dfma.value,
                                                                                                dmma.value),
                      "unit": "TFLOP/s", "frac": tf / peak},
@@ -943,12 +950,13 @@ def run_pipeline(args):
             iv = [float(sli[i]), float(sli[i + 1]), 0.0, 12.0]
             exact = int(np.count_nonzero((ev >= iv[0]) & (ev <= iv[1])))
             pol = lib.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2)
-            maxit = max(2000, 8 * exact)
+            maxit = max(2000, 5 * exact)  # about 4 Lanczos steps per eigenvalue are needed
             (lam, _, res), t = timed(lambda: lib.cheblan_nr(iv, maxit, TOL, v0, pol, want_vectors=False))
             kdim, ncand = lib.last_solve_info()
             slices.append({"interval": iv[:2], "degree": int(pol.deg), "found": int(len(lam)), "exact": exact,
                            "max_res": float(np.max(res)) if len(res) else 0.0, "seconds": t,
                            "lanczos_steps": int(kdim), "ritz_candidates": int(ncand)})
+            print("slice %d: %s" % (i, json.dumps(slices[-1])), file=sys.stderr, flush=True)
             lib.free_pol(pol)
         return {"kpm_s": t_kpm, "ecount": float(ecnt), "slicer_s": t_sli, "slices": slices}
 

@@ -547,6 +547,102 @@ __global__ void __launch_bounds__(256, 1)
   }
 }
 
+// The same tall GEMM on the FP64 tensor instruction mma.sync m8n8k4: the
+// staging is k_dgemm_nn128's (A slices padded to GTA doubles per k row so the
+// fragment loads of a warp spread over the banks); each warp's 64 x 32 tile
+// is 8 x 4 accumulator fragments of 8 x 8, and a 16-deep k slice is four
+// steps of (8 A + 4 B fragment loads, 32 mma).  One mma does 256 multiply-adds
+// of a warp, so the k loop issues about a fifth of the shared loads and an
+// eighth of the arithmetic instructions of the DFMA kernel.  The products are
+// summed in the instruction's order, not the FMA chain's: results agree with
+// k_dgemm_nn128 to rounding, not bit for bit.
+constexpr int GTA = GT + 4;
+constexpr size_t kGemmMmaSmem = 2 * (size_t)(GK * GTA + GT * GKP) * sizeof(double);
+
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <bool A16, bool B16>
+__global__ void __launch_bounds__(256, 1)
+    k_dgemm_mma(int m, int n, int k, double alpha, const double *__restrict__ A, long long lda,
+                const double *__restrict__ B, long long ldb, double beta, double *C, long long ldc) {
+  extern __shared__ __align__(16) double gsm[];
+  double *const sA0 = gsm;                 // 2 stages of [GK][GTA]
+  double *const sB0 = gsm + 2 * GK * GTA;  // 2 stages of [GT][GKP]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int m0 = blockIdx.x * GT, n0 = blockIdx.y * GT;
+  const int wm = 64 * (warp & 1), wn = 32 * (warp >> 1);
+  const int fr = lane >> 2, fc = lane & 3;  // fragment row / column of this lane
+  auto load = [&](int st, int k0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = tid + 256 * i;
+      const int kk = c >> 6, pa = c & 63;
+      const int gr = m0 + 2 * pa, gk = k0 + kk;
+      int bytes = 0;
+      if (gk < k) bytes = (gr + 1 < m) ? 16 : ((gr < m) ? 8 : 0);
+      cp_pair<A16>(sA0 + st * (GK * GTA) + kk * GTA + 2 * pa, A + (long long)gk * lda + gr, A, bytes);
+      const int nn = c >> 3, q = c & 7;
+      const int gc = n0 + nn, gk2 = k0 + 2 * q;
+      int bb = 0;
+      if (gc < n) bb = (gk2 + 1 < k) ? 16 : ((gk2 < k) ? 8 : 0);
+      cp_pair<B16>(sB0 + st * (GT * GKP) + nn * GKP + 2 * q, B + (long long)gc * ldb + gk2, B, bb);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  double acc[8][4][2];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  const int nk = (k + GK - 1) / GK;
+  load(0, 0);
+  for (int t = 0; t < nk; ++t) {
+    const int st = t & 1;
+    if (t + 1 < nk) {
+      load(st ^ 1, (t + 1) * GK);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    const double *a_s = sA0 + st * (GK * GTA) + fc * GTA + wm + fr;
+    const double *b_s = sB0 + st * (GT * GKP) + (wn + fr) * GKP + fc;
+#pragma unroll
+    for (int k4 = 0; k4 < GK; k4 += 4) {
+      double a[8], b[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) a[i] = a_s[k4 * GTA + 8 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = b_s[8 * j * GKP + k4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int gn = n0 + wn + 8 * j + 2 * fc + h;
+      if (gn >= n) continue;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int gm = m0 + wm + 8 * i + fr;
+        if (gm < m) {
+          double *c = C + (long long)gn * ldc + gm;
+          *c = (beta == 0.0) ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*c);
+        }
+      }
+    }
+  }
+}
+
 // C = sum over slabs of part (slab stride m*n, ld m) scaled: C = S + beta C
 __global__ void k_splitk_reduce(int m, int n, int slabs, const double *part, double beta, double *C, long long ldc) {
   const long long total = (long long)m * n;
@@ -938,7 +1034,7 @@ __global__ void __launch_bounds__(256) k_probe_dmma(int iters, double seed, doub
   out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
-static int g_dgemm_tiled = 1;
+static int g_dgemm_tiled = 2;
 
 int evslcu_fp64_probe(double *dfma_tflops, double *dmma_tflops) {
   const int blocks = 4 * sm_count(), iters = 1 << 14;
@@ -973,8 +1069,9 @@ int evslcu_fp64_probe(double *dfma_tflops, double *dmma_tflops) {
 }
 
 int evslcu_set_dgemm_tiled(int on) {
-  g_dgemm_tiled = on ? 1 : 0;
-  return 0;
+  const int prev = g_dgemm_tiled;
+  g_dgemm_tiled = (on == 2) ? 2 : (on ? 1 : 0);
+  return prev;
 }
 
 static double *g_splitk = nullptr;  // split-K partial products (cached)
@@ -990,6 +1087,25 @@ int evslcu_dgemm(char ta, char tb, int m, int n, int k, double alpha, const doub
       ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 7) == 0) {
     const bool a16 = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (lda & 1) == 0;
     const bool b16 = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (ldb & 1) == 0;
+    if (g_dgemm_tiled == 2) {
+      auto gom = [&](auto fn) -> int {
+        static bool smem_set[4] = {false, false, false, false};
+        const int idx = (a16 ? 2 : 0) + (b16 ? 1 : 0);
+        if (!smem_set[idx]) {
+          cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmMmaSmem);
+          if (e != cudaSuccess) return fail(EVSLCU_ERR_CUDA, "dgemm: shared memory limit: %s", cudaGetErrorString(e));
+          smem_set[idx] = true;
+        }
+        dim3 g((m + GT - 1) / GT, (n + GT - 1) / GT);
+        fn<<<g, 256, kGemmMmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        count_launch();
+        return check_launch("k_dgemm_mma");
+      };
+      if (a16 && b16) return gom(k_dgemm_mma<true, true>);
+      if (a16) return gom(k_dgemm_mma<true, false>);
+      if (b16) return gom(k_dgemm_mma<false, true>);
+      return gom(k_dgemm_mma<false, false>);
+    }
     auto go = [&](auto fn) -> int {
       static bool smem_set[4] = {false, false, false, false};
       const int idx = (a16 ? 2 : 0) + (b16 ? 1 : 0);

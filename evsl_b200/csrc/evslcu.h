@@ -155,8 +155,10 @@ int evslcu_cgs_dgks(int n, int k, int imax, const double *Q, long long ldq, doub
 int evslcu_dgemv(char trans, int m, int n, double alpha, const double *A, long long lda,
                  const double *x, double beta, double *y);
 /* C = alpha * op(A) op(B) + beta * C, column-major; op = 'N' or 'T'. */
-/* 1 (default): tall no-transpose products with 16-byte aligned operands use
- * the 128 x 128 tiled GEMM; 0: always the 64 x 64 kernel (same results). */
+/* Tall no-transpose products: 2 (default) use the 128 x 128 tile kernel on
+ * the FP64 tensor instruction (mma.sync m8n8k4), 1 the same tiles on DFMA
+ * (bitwise equal to 0), 0 always the 64 x 64 kernel.  Returns the previous
+ * setting. */
 int evslcu_set_dgemm_tiled(int on);
 /* FP64 throughput of this GPU (TFLOP/s): FMA chains per thread and
  * mma.sync m8n8k4 f64 chains per warp, registers only (the FP64 roofline). */

@@ -1,10 +1,11 @@
 """FP64 GEMM of the Ritz step (SRC/cheblanNr.c:333-399 forms the Ritz vectors
 V(:,1:K) Y; evsl_dgemm_device is the reference's device BLAS entry point)
-through the C ABI: the 128 x 128 tiled kernel (cp.async double buffering,
-8 x 8 accumulators per thread) against the 64 x 64 kernel -- both form each
-entry as the FMA chain over k in order, so they agree bit for bit -- and
-against numpy (1e-13 of the largest |C| entry): aligned and unaligned
-operands (odd leading dimensions), ragged edges, beta 0 and 0.5.
+through the C ABI: the 128 x 128 tiled DFMA kernel (cp.async double
+buffering, 8 x 8 accumulators per thread) against the 64 x 64 kernel -- both
+form each entry as the FMA chain over k in order, so they agree bit for bit
+-- and the default kernel on the FP64 tensor instruction against both and
+numpy (1e-13 of the largest |C| entry): aligned and unaligned operands (odd
+leading dimensions), ragged edges, beta 0 and 0.5.
 """
 import ctypes as C
 
@@ -17,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _gemm(lib, m, n, k, A, lda, B, ldb, Cm, ldc, alpha, beta, tiled):
-    lib.lib.evslcu_set_dgemm_tiled(1 if tiled else 0)
+    prev = lib.lib.evslcu_set_dgemm_tiled(int(tiled))
     dA = evsl_b200.DeviceBuffer.from_host(lib.lib, A)
     dB = evsl_b200.DeviceBuffer.from_host(lib.lib, B)
     dC = evsl_b200.DeviceBuffer.from_host(lib.lib, Cm)
@@ -26,7 +27,7 @@ def _gemm(lib, m, n, k, A, lda, B, ldb, Cm, ldc, alpha, beta, tiled):
     lib.lib.evsl_dgemm_device(b"N", b"N", ci(m), ci(n), ci(k), cd(alpha), C.c_void_p(dA.ptr), ci(lda),
                               C.c_void_p(dB.ptr), ci(ldb), cd(beta), C.c_void_p(dC.ptr), ci(ldc))
     out = dC.to_host(shape=Cm.shape)
-    lib.lib.evslcu_set_dgemm_tiled(1)
+    lib.lib.evslcu_set_dgemm_tiled(prev)
     return out
 
 
@@ -74,3 +75,27 @@ def test_block_cgs2_orthonormalises(gpu_lib, n, m, b):
     assert np.max(np.abs(G - np.eye(m))) <= 1e-13
     P = (W0 @ Q.T) @ Q
     assert np.max(np.linalg.norm(W0 - P, axis=1) / np.linalg.norm(W0, axis=1)) <= 1e-12
+
+
+@pytest.mark.parametrize("m, n, k, pad", [(1000, 70, 333, 0), (1001, 64, 257, 0), (4096, 300, 1000, 0),
+                                         (777, 129, 33, 3), (2048, 32, 16, 1), (513, 40, 1, 0)])
+@pytest.mark.parametrize("beta", [0.0, 0.5])
+def test_mma_gemm_matches(gpu_lib, m, n, k, pad, beta):
+    """The tall GEMM on the FP64 tensor instruction (mma.sync m8n8k4, same
+    tiles and staging as the DFMA kernel, products summed in the
+    instruction's order): within 1e-13 of numpy and of the DFMA kernel,
+    aligned and unaligned operands, ragged edges, beta 0 and 0.5; the padding
+    rows of C untouched."""
+    rng = np.random.default_rng(m + 2 * n + k)
+    lda, ldb, ldc = m + pad, k + pad, m + pad
+    A = rng.standard_normal((k, lda))
+    B = rng.standard_normal((n, ldb))
+    C0 = rng.standard_normal((n, ldc))
+    alpha = 1.0 if beta == 0.0 else -0.75
+    got = _gemm(gpu_lib, m, n, k, A, lda, B, ldb, C0, ldc, alpha, beta, 2)
+    dfma = _gemm(gpu_lib, m, n, k, A, lda, B, ldb, C0, ldc, alpha, beta, 1)
+    ref = alpha * (A[:, :m].T @ B[:, :k].T) + beta * C0[:, :m].T
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(got[:, :m].T - ref)) <= 1e-13 * scale
+    assert np.max(np.abs(got - dfma)) <= 1e-13 * scale
+    assert np.array_equal(got[:, m:], C0[:, m:])
