@@ -903,14 +903,16 @@ def run_pipeline(args):
     """lap3d-pipeline: the drop-in slicing pipeline of the reference's
     Laplacian driver (TESTS/PLanN/LapPLanN.c:10-283) with the drop-in slicing
     configuration's settings on a `--grid`^3 3-D Laplacian (default 50^3 =
-    125,000 rows; the configuration's 100^3 takes hours per step): kpmdos over
+    125,000 rows; the configuration's 100^3 takes about half an hour): kpmdos over
     [0.6, 1.2] (300 moments, Jackson damping, 30 seeded Rademacher probes),
     spslicer into 8 slices (npts = 10 ecount), then per slice find_pol
     (damping 2, thresholds 0.8 / 0.2) and ChebLanNr (tol 1e-8) from a seeded
     normal start vector.  One step = the whole pipeline; every slice's count
     is checked against the analytic spectrum and every residual against tol.
-    Device time per phase from CUDA events on the library stream (the
-    slicer's host time by the wall clock)."""
+    Device time per stage from CUDA events on the library stream (the
+    slicer's host time by the wall clock); within a slice, the filter's
+    device time (events around each filter call) and the solver's own
+    timers for the tridiagonal eigenproblems and the Ritz step."""
     import torch
 
     import evsl_b200 as E
@@ -951,11 +953,24 @@ def run_pipeline(args):
             exact = int(np.count_nonzero((ev >= iv[0]) & (ev <= iv[1])))
             pol = lib.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2)
             maxit = max(2000, 5 * exact)  # about 4 Lanczos steps per eigenvalue are needed
+            lib.stats_reset()
+            lib.filter_profile(True)
             (lam, _, res), t = timed(lambda: lib.cheblan_nr(iv, maxit, TOL, v0, pol, want_vectors=False))
+            t_filter, _, _, _ = lib.filter_stats()
+            lib.filter_profile(False)
+            st = lib.stats()
             kdim, ncand = lib.last_solve_info()
+            # phases: filter (CUDA events around every filter call), the
+            # tridiagonal eigenproblems (convergence tests and Ritz), the Ritz
+            # step (GEMM V(:,1:K) Y, residuals, gather), and the rest of the
+            # Lanczos loop (reorthogonalisation, norms, scalar reads)
+            t_rest = st["t_iter"] - t_filter - st["t_eig"] - st["t_ritz"]
             slices.append({"interval": iv[:2], "degree": int(pol.deg), "found": int(len(lam)), "exact": exact,
                            "max_res": float(np.max(res)) if len(res) else 0.0, "seconds": t,
-                           "lanczos_steps": int(kdim), "ritz_candidates": int(ncand)})
+                           "lanczos_steps": int(kdim), "ritz_candidates": int(ncand),
+                           "phase_s": {"filter": t_filter, "tridiag_eig": st["t_eig"], "ritz": st["t_ritz"],
+                                       "reorth_and_rest": t_rest},
+                           "ritz_gemm_tflop": 2e-12 * n * kdim * ncand})
             print("slice %d: %s" % (i, json.dumps(slices[-1])), file=sys.stderr, flush=True)
             lib.free_pol(pol)
         return {"kpm_s": t_kpm, "ecount": float(ecnt), "slicer_s": t_sli, "slices": slices}

@@ -328,6 +328,16 @@ def load():
     return lib
 
 
+class EvslStat(C.Structure):
+    """Layout of the reference's timing statistics (INC/struct.h:223-253),
+    the library's exported `evslstat`."""
+    _fields_ = ([(f, C.c_double) for f in ("t_setBsv", "t_setASigBsv", "t_iter", "t_polAv", "t_reorth",
+                                           "t_siorth", "t_ritz", "t_eig", "t_mvA", "t_mvB", "t_svB", "t_svLT",
+                                           "t_svASigB", "t_blas", "t_ratAv")] +
+                [(f, C.c_size_t) for f in ("n_mvA", "n_mvB", "n_svB", "n_svLT", "n_svASigB", "n_polAv", "n_ratAv",
+                                           "alloced", "alloced_total", "alloced_max")])
+
+
 class DeviceBuffer:
     """A block of device memory owned by the library allocator."""
 
@@ -887,6 +897,15 @@ class Library:
     def stream_handle(self):
         """cudaStream_t of the library (for recording CUDA events on it)."""
         return int(self.lib.evslx_stream() or 0)
+
+    def stats(self):
+        """The timing statistics of the last solves (`evslstat`, reset by
+        StatsReset) as a dict of its fields."""
+        st = EvslStat.in_dll(self.lib, "evslstat")
+        return {f: getattr(st, f) for f, _ in EvslStat._fields_}
+
+    def stats_reset(self):
+        self.lib.StatsReset()
 
     def filter_profile(self, enable=True):
         self._check(self.lib.evslx_filter_profile(1 if enable else 0), "evslx_filter_profile")

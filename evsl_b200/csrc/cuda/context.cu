@@ -223,6 +223,15 @@ void *evslcu_malloc(size_t nbytes) {
   void *p = nullptr;
   if (nbytes == 0) nbytes = 1;
   cudaError_t e = pool_ready() ? cudaMallocFromPoolAsync(&p, nbytes, g_pool, g_ctx.stream) : cudaMalloc(&p, nbytes);
+  if (e == cudaErrorMemoryAllocation && pool_ready()) {
+    // the pool keeps freed blocks; blocks of other sizes (an earlier
+    // solve's basis) may hold the memory this request needs: return them
+    // to the device once the stream has finished with them, then retry
+    cudaGetLastError();
+    cudaStreamSynchronize(g_ctx.stream);
+    cudaMemPoolTrimTo(g_pool, 0);
+    e = cudaMallocFromPoolAsync(&p, nbytes, g_pool, g_ctx.stream);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     fail(EVSLCU_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", nbytes, cudaGetErrorString(e));

@@ -29,10 +29,10 @@ constexpr int kRounds = 12;               // 129^12 > 2e25
 constexpr int kTridThreads = 256;
 
 __global__ void __launch_bounds__(kTridThreads)
-    k_trid_bisect(int k, const double *__restrict__ d, const double *__restrict__ e2, double glo, double ghi,
-                  double pivmin, double *__restrict__ w) {
+    k_trid_bisect(int k, int i0, const double *__restrict__ d, const double *__restrict__ e2, double glo,
+                  double ghi, double pivmin, double *__restrict__ w) {
   const int lane = threadIdx.x & 31;
-  const int i = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int i = i0 + (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (i >= k) return;  // uniform over the warp
   double lo = glo, hi = ghi;
   for (int round = 0; round < kRounds; ++round) {
@@ -86,7 +86,7 @@ void evslcu_trid_release(void) {
   g_trid_cap = 0;
 }
 
-int evslcu_trid_eigvals(int k, const double *d, const double *e, double *w) {
+int evslcu_trid_eigvals_above(int k, const double *d, const double *e, double xmin, double *w) {
   if (k <= 0) return 0;
   if (!d || !w || (k > 1 && !e)) return fail(EVSLCU_ERR_ARG, "evslcu_trid_eigvals: bad arguments");
   if (k > g_trid_cap) {
@@ -115,18 +115,43 @@ int evslcu_trid_eigvals(int k, const double *d, const double *e, double *w) {
   const double fudge = 2.0 * DBL_EPSILON * std::max(fabs(glo), fabs(ghi)) * k + 2.0 * pivmin;
   glo -= fudge;
   ghi += fudge;
+  // Indices below i0 are skipped: their eigenvalues lie below xc, far
+  // enough under xmin (1e-8 of the spectral scale, four orders above the
+  // counts' rounding) that none of them can reach xmin.  One index of slack
+  // on top.  The others are bisected from the same bracket as in the full
+  // computation, so they come out bit for bit the same.
+  int i0 = 0;
+  if (xmin > glo) {
+    const double xc = xmin - 1e-8 * std::max(1.0, std::max(fabs(glo), fabs(ghi)));
+    double q = d[0] - xc;
+    if (fabs(q) < pivmin) q = -pivmin;
+    int cnt = q < 0.0;
+    for (int j = 1; j < k; ++j) {
+      q = (d[j] - xc) - e2[j - 1] / q;
+      if (fabs(q) < pivmin) q = -pivmin;
+      cnt += q < 0.0;
+    }
+    i0 = std::max(0, cnt - 1);
+  }
   double *dd = g_trid_buf, *de2 = g_trid_buf + g_trid_cap, *dw = g_trid_buf + 2 * (size_t)g_trid_cap;
   int rc = evslcu_h2d_async(dd, d, sizeof(double) * (size_t)k);
   if (!rc && k > 1) rc = evslcu_h2d_async(de2, e2.data(), sizeof(double) * (size_t)(k - 1));
   if (rc) return rc;
-  const long long threads = 32LL * k;
-  const int grid = (int)((threads + kTridThreads - 1) / kTridThreads);
-  k_trid_bisect<<<grid, kTridThreads, 0, stream()>>>(k, dd, de2, glo, ghi, pivmin, dw);
-  count_launch();
-  if ((rc = check_launch("k_trid_bisect"))) return rc;
-  if ((rc = evslcu_d2h(w, dw, sizeof(double) * (size_t)k))) return rc;
+  if (i0 < k) {
+    const long long threads = 32LL * (k - i0);
+    const int grid = (int)((threads + kTridThreads - 1) / kTridThreads);
+    k_trid_bisect<<<grid, kTridThreads, 0, stream()>>>(k, i0, dd, de2, glo, ghi, pivmin, dw);
+    count_launch();
+    if ((rc = check_launch("k_trid_bisect"))) return rc;
+    if ((rc = evslcu_d2h(w + i0, dw + i0, sizeof(double) * (size_t)(k - i0)))) return rc;
+  }
+  for (int i = 0; i < i0; ++i) w[i] = glo;  // below every computed eigenvalue and below xmin
   std::sort(w, w + k);
   return 0;
+}
+
+int evslcu_trid_eigvals(int k, const double *d, const double *e, double *w) {
+  return evslcu_trid_eigvals_above(k, d, e, -HUGE_VAL, w);
 }
 
 }  // extern "C"

@@ -355,6 +355,10 @@ void evslcu_trid_release(void);
  * the GPU by multisection on Sturm counts (one warp per eigenvalue);
  * synchronous. */
 int evslcu_trid_eigvals(int k, const double *d, const double *e, double *w);
+/* The same, computing only the eigenvalues that may be >= xmin (bit for bit
+ * those of evslcu_trid_eigvals); the entries of the eigenvalues well below
+ * xmin hold a value below xmin instead.  Ascending. */
+int evslcu_trid_eigvals_above(int k, const double *d, const double *e, double xmin, double *w);
 /* Pattern tables read from the constant-memory pool when they fit there (1,
  * default) or always from global memory (0).  Same arithmetic either way. */
 int evslcu_set_pattern_const(int on);

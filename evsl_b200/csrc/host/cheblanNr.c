@@ -117,7 +117,7 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
     if ((k < NR_NTEST || (k - NR_NTEST) % NR_CYCLE != 0) && k != maxit - 1) continue;
     kdim = k + 1;
     const double te = evsl_timer();
-    if ((rc = evsl_trid_eigvals_test(kdim, dT, eT, EvalT))) goto done;
+    if ((rc = evsl_trid_eigvals_test(kdim, dT, eT, bar - EVSL_DBL_EPS_MULT * DBL_EPSILON, EvalT))) goto done;
     evslstat.t_eig += evsl_timer() - te;
     count = kdim;
     tr1 = 0.0;
@@ -141,7 +141,8 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
   /* ---- Ritz pairs ---- */
   {
     const double te = evsl_timer();
-    if ((rc = evsl_trid_eigvals(kdim, dT, eT, EvalT))) goto done;
+    /* EvalT holds the eigenvalues of T_kdim from the last convergence test
+     * (the loop ends right after one): the ones >= bar are selected */
     int msel = 0;
     sel = (int *)malloc(sizeof(int) * (size_t)(kdim > 0 ? kdim : 1));
     for (int i = 0; i < count; i++)

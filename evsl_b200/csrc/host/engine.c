@@ -740,7 +740,10 @@ static int finalize(evslx_engine *E, slot_t *s, int kdim, evslx_result *out) {
     rc = evsl_seterr(EVSLX_ERR_NOMEM, "engine: out of memory");
     goto done;
   }
-  if ((rc = evsl_trid_eigvals(kdim, s->dT, s->eT, s->EvalT))) goto done;
+  /* s->EvalT holds the eigenvalues of T_kdim from the convergence test that
+   * ended the solve, those below bar only where they may reach it; the
+   * FP32 path's guard vectors need the ones below bar: all of them again */
+  if (slot_fp32(E, r->M) && (rc = evsl_trid_eigvals(kdim, s->dT, s->eT, s->EvalT))) goto done;
   for (int i = 0; i < kdim; i++)
     if (s->EvalT[i] >= bar) {
       wsel[msel] = s->EvalT[i];
@@ -1112,7 +1115,9 @@ int evslx_engine_step(evslx_engine *E) {
     const int k = s->k;
     int finished = 0, kdim = k + 1;
     if (!((k < ENG_NTEST || (k - ENG_NTEST) % ENG_NCYCLE != 0) && k != r->maxit - 1)) {
-      if ((rc = evsl_trid_eigvals_test(kdim, s->dT, s->eT, s->EvalT))) return rc;
+      if ((rc = evsl_trid_eigvals_test(kdim, s->dT, s->eT, r->pol.bar - EVSL_DBL_EPS_MULT * DBL_EPSILON,
+                                        s->EvalT)))
+        return rc;
       double tr1 = 0.0;
       for (int j = 0; j < kdim; j++)
         if (s->EvalT[j] + EVSL_DBL_EPS_MULT * DBL_EPSILON >= r->pol.bar) tr1 += s->EvalT[j];

@@ -51,7 +51,7 @@ int evsl_check_intv(const double *intv, FILE *fstats);
 /* tridiagonal / dense symmetric eigensolvers (host, FP64; tridiag.c) */
 int evsl_trid_eig_first(int n, const double *d, const double *e, double *w, double *z1);
 int evsl_trid_eigvals(int n, const double *d, const double *e, double *w);
-int evsl_trid_eigvals_test(int n, const double *d, const double *e, double *w);
+int evsl_trid_eigvals_test(int n, const double *d, const double *e, double xmin, double *w);
 int evsl_trid_eigvecs(int n, const double *d, const double *e, int m, const double *w, double *Z, int ldz);
 int evsl_sym_eig(int n, const double *A, int lda, double *Q, int ldq, double *w);
 int evsl_tr_eig(int k, int m, const double *T, int ldt, double thresh, double *w, double *Z, int ldz);

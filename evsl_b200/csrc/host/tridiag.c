@@ -32,6 +32,9 @@
  */
 #include "internal.h"
 
+#include <pthread.h>
+#include <unistd.h>
+
 #define QL_MAX_ITER 60
 #define INVIT_ITERS 3
 #define CLUSTER_TOL 1e-7
@@ -140,13 +143,15 @@ int evsl_trid_eigvals(int n, const double *d, const double *e, double *w) {
 }
 
 /* Eigenvalues for the Lanczos convergence tests: on the GPU (multisection,
- * evslcu_trid_eigvals) from TRID_GPU_MIN rows on, where the host QL's
+ * evslcu_trid_eigvals_above) from TRID_GPU_MIN rows on, where the host QL's
  * O(k^2) work per test would dominate small-matrix solves; the host QL below
- * that.  Both are backward stable; they agree to a few ulps. */
+ * that.  Both are backward stable; they agree to a few ulps.  The trace test
+ * reads only the eigenvalues >= xmin: on the GPU the others are not
+ * computed (their entries hold values below xmin). */
 #define TRID_GPU_MIN 64
-int evsl_trid_eigvals_test(int n, const double *d, const double *e, double *w) {
+int evsl_trid_eigvals_test(int n, const double *d, const double *e, double xmin, double *w) {
   if (n < TRID_GPU_MIN) return evsl_trid_eigvals(n, d, e, w);
-  const int rc = evslcu_trid_eigvals(n, d, e, w);
+  const int rc = evslcu_trid_eigvals_above(n, d, e, xmin, w);
   if (rc) return evsl_seterr(EVSLX_ERR_CUDA, "%s", evslcu_errstr());
   return 0;
 }
@@ -179,41 +184,33 @@ static uint64_t mix64(uint64_t z) {
   return z ^ (z >> 31);
 }
 
-int evsl_trid_eigvecs(int n, const double *d, const double *e, int m, const double *w, double *Z, int ldz) {
-  if (m <= 0 || n <= 0) return 0;
-  if (n == 1) {
-    for (int j = 0; j < m; j++) Z[(size_t)j * ldz] = 1.0;
-    return 0;
-  }
-  double tnorm = 0.0;
-  for (int i = 0; i < n; i++) {
-    double r = fabs(d[i]);
-    if (i > 0) r += fabs(e[i - 1]);
-    if (i < n - 1) r += fabs(e[i]);
-    tnorm = evsl_max(tnorm, r);
-  }
-  if (tnorm == 0.0) tnorm = 1.0;
-  const double pert = 10.0 * DBL_EPSILON * tnorm;
-  const double tiny = DBL_EPSILON * tnorm;
-  const double clus = CLUSTER_TOL * tnorm;
+/* Inverse iteration for the vectors j0 <= j < j1 (shifts and cluster starts
+ * precomputed); a vector depends only on its shift and the earlier vectors of
+ * its cluster, so ranges that start at a cluster start run independently. */
+typedef struct {
+  int n, ldz, j0, j1, rc;
+  const double *d, *e, *shift;
+  const int *cst;
+  double *Z, tiny;
+} invit_job;
+
+static int invit_range(invit_job *jb) {
+  const int n = jb->n, ldz = jb->ldz;
+  const double *d = jb->d, *e = jb->e;
+  const double tiny = jb->tiny;
+  double *Z = jb->Z;
   double *buf = (double *)malloc(sizeof(double) * (size_t)n * 8);
   unsigned char *swp = (unsigned char *)malloc((size_t)n);
   if (!buf || !swp) {
     free(buf);
     free(swp);
-    return evsl_seterr(EVSLX_ERR_NOMEM, "inverse iteration: out of memory");
+    return EVSLX_ERR_NOMEM;
   }
   double *dg = buf, *du = buf + n, *u0 = buf + 2 * n, *u1 = buf + 3 * n, *u2 = buf + 4 * n, *ml = buf + 5 * n,
          *x = buf + 6 * n;
-  int cstart = 0;
-  double lam_prev = 0.0;
-  for (int j = 0; j < m; j++) {
-    double lam = w[j];
-    if (j > 0) {
-      if (w[j] - w[j - 1] > clus) cstart = j;
-      if (lam - lam_prev < pert) lam = lam_prev + pert;
-    }
-    lam_prev = lam;
+  for (int j = jb->j0; j < jb->j1; j++) {
+    const double lam = jb->shift[j];
+    const int cstart = jb->cst[j];
     /* LU with partial pivoting of T - lam I */
     for (int i = 0; i < n; i++) {
       dg[i] = d[i] - lam;
@@ -293,6 +290,83 @@ int evsl_trid_eigvecs(int n, const double *d, const double *e, int m, const doub
   }
   free(buf);
   free(swp);
+  return 0;
+}
+
+static void *invit_thread(void *arg) {
+  invit_job *jb = (invit_job *)arg;
+  jb->rc = invit_range(jb);
+  return NULL;
+}
+
+#define INVIT_MAX_THREADS 16
+#define INVIT_MIN_WORK (1L << 21) /* vectors x rows per thread */
+
+int evsl_trid_eigvecs(int n, const double *d, const double *e, int m, const double *w, double *Z, int ldz) {
+  if (m <= 0 || n <= 0) return 0;
+  if (n == 1) {
+    for (int j = 0; j < m; j++) Z[(size_t)j * ldz] = 1.0;
+    return 0;
+  }
+  double tnorm = 0.0;
+  for (int i = 0; i < n; i++) {
+    double r = fabs(d[i]);
+    if (i > 0) r += fabs(e[i - 1]);
+    if (i < n - 1) r += fabs(e[i]);
+    tnorm = evsl_max(tnorm, r);
+  }
+  if (tnorm == 0.0) tnorm = 1.0;
+  const double pert = 10.0 * DBL_EPSILON * tnorm;
+  const double clus = CLUSTER_TOL * tnorm;
+  /* shifts (separated by at least pert) and cluster starts, in order */
+  double *shift = (double *)malloc(sizeof(double) * (size_t)m);
+  int *cst = (int *)malloc(sizeof(int) * (size_t)m);
+  if (!shift || !cst) {
+    free(shift);
+    free(cst);
+    return evsl_seterr(EVSLX_ERR_NOMEM, "inverse iteration: out of memory");
+  }
+  int cstart = 0;
+  double lam_prev = 0.0;
+  for (int j = 0; j < m; j++) {
+    double lam = w[j];
+    if (j > 0) {
+      if (w[j] - w[j - 1] > clus) cstart = j;
+      if (lam - lam_prev < pert) lam = lam_prev + pert;
+    }
+    lam_prev = lam;
+    shift[j] = lam;
+    cst[j] = cstart;
+  }
+  /* ranges split at cluster starts over host threads; every vector is
+   * computed the same way whatever the split */
+  long nth = sysconf(_SC_NPROCESSORS_ONLN);
+  nth = evsl_min(evsl_min(nth, (long)INVIT_MAX_THREADS), ((long)m * n) / INVIT_MIN_WORK);
+  invit_job jobs[INVIT_MAX_THREADS];
+  pthread_t tid[INVIT_MAX_THREADS];
+  int nj = 0, j0 = 0;
+  for (int t = 0; t < (nth > 1 ? nth : 1) && j0 < m; t++) {
+    int j1 = (t == nth - 1 || nth <= 1) ? m : (int)(((long)m * (t + 1)) / nth);
+    if (j1 < j0 + 1) j1 = j0 + 1;
+    while (j1 < m && cst[j1] != j1) j1++;
+    jobs[nj] = (invit_job){n, ldz, j0, j1, 0, d, e, shift, cst, Z, DBL_EPSILON * tnorm};
+    nj++;
+    j0 = j1;
+  }
+  int started = 0;
+  for (int t = 1; t < nj; t++) {
+    if (pthread_create(&tid[t], NULL, invit_thread, &jobs[t]) != 0) break;
+    started = t;
+  }
+  jobs[0].rc = invit_range(&jobs[0]);
+  for (int t = 1; t <= started; t++) pthread_join(tid[t], NULL);
+  for (int t = started + 1; t < nj; t++) jobs[t].rc = invit_range(&jobs[t]); /* threads that did not start */
+  int rc = 0;
+  for (int t = 0; t < nj; t++)
+    if (jobs[t].rc) rc = jobs[t].rc;
+  free(shift);
+  free(cst);
+  if (rc) return evsl_seterr(EVSLX_ERR_NOMEM, "inverse iteration: out of memory");
   return 0;
 }
 

@@ -126,3 +126,38 @@ def test_start_fails_loudly_without_gpu():
         pytest.skip("a GPU is present")
     with pytest.raises(EvslError):
         evsl_b200.Library()
+
+
+@pytest.mark.parametrize("k, m, kind", [(3000, 1500, "random"), (3000, 1500, "repeated"), (200, 50, "random")])
+def test_tridiagonal_eigenvectors_host(k, m, kind):
+    """Inverse iteration for the Ritz step's tridiagonal eigenvectors (host,
+    split over threads at cluster starts when the work is large): each
+    vector solves T z = lambda z to 1e-12 of ||T||, the vectors are
+    orthonormal to 1e-12 (also inside clusters of exactly repeated
+    eigenvalues, where only the span is defined), and a second call gives
+    the same bits.  3000 x 1500 runs on two threads."""
+    lib = evsl_b200.load()
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    lib.evsl_trid_eigvecs.restype = C.c_int
+    lib.evsl_trid_eigvecs.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+    lib.evsl_trid_eigvals.restype = C.c_int
+    lib.evsl_trid_eigvals.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(k + m)
+    if kind == "random":
+        d, e = rng.uniform(-0.1, 1.0, k), rng.uniform(0.01, 0.3, k - 1)
+    else:  # four identical blocks: every eigenvalue four times
+        b = k // 4
+        d = np.tile(rng.uniform(-0.1, 1.0, b), 4)
+        e = np.tile(np.r_[rng.uniform(0.01, 0.3, b - 1), 0.0], 4)[: k - 1]
+    w = np.zeros(k)
+    assert lib.evsl_trid_eigvals(k, vp(d), vp(e), vp(w)) == 0
+    sel = np.ascontiguousarray(w[-m:])
+    Z = np.zeros((m, k))
+    assert lib.evsl_trid_eigvecs(k, vp(d), vp(e), m, vp(sel), vp(Z), k) == 0
+    Z2 = np.zeros((m, k))
+    assert lib.evsl_trid_eigvecs(k, vp(d), vp(e), m, vp(sel), vp(Z2), k) == 0
+    assert np.array_equal(Z, Z2)
+    tn = np.max(np.abs(d) + np.r_[np.abs(e), 0] + np.r_[0, np.abs(e)])
+    TZ = d * Z + np.c_[Z[:, 1:] * e, np.zeros(m)] + np.c_[np.zeros(m), Z[:, :-1] * e]
+    assert np.max(np.abs(TZ - sel[:, None] * Z)) <= 1e-12 * tn
+    assert np.max(np.abs(Z @ Z.T - np.eye(m))) <= 1e-12

@@ -460,6 +460,61 @@ def test_tridiagonal_eigenvalues_on_gpu(gpu_lib):
         assert np.max(np.abs(w - ref)) <= 1e-13 * scale, (k, np.max(np.abs(w - ref)) / scale)
 
 
+def test_tridiagonal_eigenvalues_above_a_bar(gpu_lib):
+    """The trace test's restricted form (only the eigenvalues that may reach
+    the bar are computed): every eigenvalue >= xmin is bit for bit the full
+    computation's, the entries of the skipped ones lie below xmin, the
+    array stays ascending; bars below, inside and above the spectrum, on a
+    Lanczos-like spectrum (a cluster of filtered values near 1 over a wide
+    bulk) and on repeated eigenvalues."""
+    import ctypes as C
+
+    full = gpu_lib.lib.evslcu_trid_eigvals
+    full.restype = C.c_int
+    full.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    above = gpu_lib.lib.evslcu_trid_eigvals_above
+    above.restype = C.c_int
+    above.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
+    rng = np.random.default_rng(21)
+    cases = []
+    for k in (64, 300, 3000):
+        cases.append((rng.standard_normal(k), rng.standard_normal(k - 1)))
+    # tridiagonal with a prescribed spectrum: Lanczos (full reorthogonalisation)
+    # on diag(lam), lam = 20% in [0.8, 1], the rest in [-0.1, 0.3]
+    n, k = 1500, 400
+    lam = np.concatenate([rng.uniform(0.8, 1.0, n // 5), rng.uniform(-0.1, 0.3, n - n // 5)])
+    Q = np.zeros((k, n))
+    q = rng.standard_normal(n)
+    Q[0] = q / np.linalg.norm(q)
+    al, be = np.zeros(k), np.zeros(k - 1)
+    for j in range(k):
+        z = lam * Q[j]
+        for _ in range(2):
+            z -= Q[: j + 1].T @ (Q[: j + 1] @ z)
+        al[j] = Q[j] @ (lam * Q[j])
+        if j + 1 < k:
+            be[j] = np.linalg.norm(z)
+            Q[j + 1] = z / be[j]
+    cases.append((al, be))
+    d = np.tile([2.0, -1.0, 0.5], 40)
+    e = np.ones(119)
+    e[2::3] = 0.0
+    cases.append((d, e))
+    for d, e in cases:
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        k = len(d)
+        ref = np.zeros(k)
+        assert full(k, d.ctypes.data, e.ctypes.data, ref.ctypes.data) == 0
+        for xmin in (ref[0] - 1.0, ref[k // 2], ref[(4 * k) // 5] - 1e-3, 0.8, ref[-1], ref[-1] + 1.0):
+            w = np.zeros(k)
+            assert above(k, d.ctypes.data, e.ctypes.data, float(xmin), w.ctypes.data) == 0
+            keep = ref >= xmin
+            assert np.array_equal(w[keep], ref[keep]), (k, xmin)
+            assert np.all(w[~keep] < xmin)
+            assert np.all(np.diff(w) >= 0)
+
+
 def test_long_rows_on_the_dictionary(gpu_lib):
     """A banded matrix with 261 entries per interior row keeps a row-pattern
     dictionary (261 row forms, 51,091 table entries) but has rows too long
