@@ -557,7 +557,10 @@ __global__ void __launch_bounds__(256, 1)
 // summed in the instruction's order, not the FMA chain's: results agree with
 // k_dgemm_nn128 to rounding, not bit for bit.
 constexpr int GTA = GT + 4;
-constexpr size_t kGemmMmaSmem = 2 * (size_t)(GK * GTA + GT * GKP) * sizeof(double);
+// B rows padded to 20 doubles: the B fragment loads (row = lane/4, k =
+// lane%4) then fall on 4 row + k distinct bank pairs in each half-warp
+constexpr int GKM = GK + 4;
+constexpr size_t kGemmMmaSmem = 2 * (size_t)(GK * GTA + GT * GKM) * sizeof(double);
 
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -571,7 +574,7 @@ __global__ void __launch_bounds__(256, 1)
                 const double *__restrict__ B, long long ldb, double beta, double *C, long long ldc) {
   extern __shared__ __align__(16) double gsm[];
   double *const sA0 = gsm;                 // 2 stages of [GK][GTA]
-  double *const sB0 = gsm + 2 * GK * GTA;  // 2 stages of [GT][GKP]
+  double *const sB0 = gsm + 2 * GK * GTA;  // 2 stages of [GT][GKM]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int m0 = blockIdx.x * GT, n0 = blockIdx.y * GT;
   const int wm = 64 * (warp & 1), wn = 32 * (warp >> 1);
@@ -589,7 +592,7 @@ __global__ void __launch_bounds__(256, 1)
       const int gc = n0 + nn, gk2 = k0 + 2 * q;
       int bb = 0;
       if (gc < n) bb = (gk2 + 1 < k) ? 16 : ((gk2 < k) ? 8 : 0);
-      cp_pair<B16>(sB0 + st * (GT * GKP) + nn * GKP + 2 * q, B + (long long)gc * ldb + gk2, B, bb);
+      cp_pair<B16>(sB0 + st * (GT * GKM) + nn * GKM + 2 * q, B + (long long)gc * ldb + gk2, B, bb);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
@@ -610,14 +613,14 @@ __global__ void __launch_bounds__(256, 1)
     }
     __syncthreads();
     const double *a_s = sA0 + st * (GK * GTA) + fc * GTA + wm + fr;
-    const double *b_s = sB0 + st * (GT * GKP) + (wn + fr) * GKP + fc;
+    const double *b_s = sB0 + st * (GT * GKM) + (wn + fr) * GKM + fc;
 #pragma unroll
     for (int k4 = 0; k4 < GK; k4 += 4) {
       double a[8], b[4];
 #pragma unroll
       for (int i = 0; i < 8; ++i) a[i] = a_s[k4 * GTA + 8 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = b_s[8 * j * GKP + k4];
+      for (int j = 0; j < 4; ++j) b[j] = b_s[8 * j * GKM + k4];
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
