@@ -301,6 +301,41 @@ evslcu_timer *evslcu_timer_start(void) {
   return t;
 }
 
+struct evslcu_marks {
+  int count;
+  cudaEvent_t *ev;
+};
+
+evslcu_marks *evslcu_marks_create(int count) {
+  if (count <= 0) return nullptr;
+  evslcu_marks *m = new evslcu_marks;
+  m->count = count;
+  m->ev = new cudaEvent_t[count];
+  for (int i = 0; i < count; ++i) cudaEventCreate(&m->ev[i]);
+  return m;
+}
+
+void evslcu_marks_record(evslcu_marks *m, int i) {
+  if (m && i >= 0 && i < m->count) cudaEventRecord(m->ev[i], g_ctx.stream);
+}
+
+double evslcu_marks_elapsed(evslcu_marks *m, int i, int j) {
+  if (!m || i < 0 || j < 0 || i >= m->count || j >= m->count) return 0.0;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, m->ev[i], m->ev[j]) != cudaSuccess) {
+    cudaGetLastError();
+    return 0.0;
+  }
+  return 1e-3 * (double)ms;
+}
+
+void evslcu_marks_destroy(evslcu_marks *m) {
+  if (!m) return;
+  for (int i = 0; i < m->count; ++i) cudaEventDestroy(m->ev[i]);
+  delete[] m->ev;
+  delete m;
+}
+
 double evslcu_timer_stop(evslcu_timer *t) {
   if (!t) return 0.0;
   float ms = 0.f;

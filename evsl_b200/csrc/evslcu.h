@@ -63,6 +63,14 @@ int evslcu_h2d_async(void *dst, const void *src, size_t nbytes);
 typedef struct evslcu_timer evslcu_timer;
 evslcu_timer *evslcu_timer_start(void);
 double evslcu_timer_stop(evslcu_timer *t); /* seconds; synchronises on the stop event */
+/* A reusable set of timing marks on the library stream: record mark i,
+ * then, once the stream has passed both, read the device seconds between
+ * two marks (0 when either has not completed). */
+typedef struct evslcu_marks evslcu_marks;
+evslcu_marks *evslcu_marks_create(int count);
+void evslcu_marks_record(evslcu_marks *m, int i);
+double evslcu_marks_elapsed(evslcu_marks *m, int i, int j);
+void evslcu_marks_destroy(evslcu_marks *m);
 
 /* ---- prepared sparse matrix --------------------------------------------- */
 typedef struct evslcu_mat evslcu_mat;

@@ -63,6 +63,7 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
   int *sel = NULL;
   int kdim = 0, count = 0, nev = 0;
   double tt_ritz = 0.0;
+  evslcu_marks *marks = NULL;
   if (!V || !wk || !vrand || !cgsw || !ds || !dT || !eT || !EvalT) {
     rc = evsl_seterr(EVSLX_ERR_NOMEM, "ChebLanNr: out of memory for a basis of %d x %d", n, maxit + 1);
     goto done;
@@ -78,6 +79,10 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
   double t = 1.0 / h[0];
   if ((rc = evslcu_scal(n, t, V))) goto cuda_fail;
 
+  /* with a stats stream, the filter and reorthogonalisation device times of
+   * every step go to evslstat.t_polAv / t_reorth (events read after the
+   * step's scalar read has synchronised) */
+  marks = fstats ? evslcu_marks_create(3) : NULL;
   double wn = 0.0, tr0 = 0.0, tr1 = 0.0, beta = 0.0;
   int nwn = 0, k;
   for (k = 0; k < maxit; k++) {
@@ -86,13 +91,20 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
     double *vnew = v + n_l;
     /* znew = p(A) v - beta zold; alpha = v . znew */
     evslcu_cheb_epi epi = {zold, -beta, v, d_alpha};
+    evslcu_marks_record(marks, 0);
     if ((rc = evslcu_chebav(op, pol->mu, deg, pol->cc, pol->dd, v, vnew, wk, &epi))) goto cuda_fail;
     evslstat.n_polAv++;
+    evslcu_marks_record(marks, 1);
     /* znew -= alpha v */
     if ((rc = evslcu_axpy_ds(n, d_alpha, -1.0, v, vnew))) goto cuda_fail;
     /* full reorthogonalisation, beta = ||vnew|| */
     if ((rc = evslcu_cgs_dgks(n, k + 1, EVSL_NGS_MAX, V, (long long)n, vnew, d_beta, cgsw))) goto cuda_fail;
+    evslcu_marks_record(marks, 2);
     if ((rc = evslcu_get_scalars(ds, h, 2))) goto cuda_fail;
+    if (marks) {
+      evslstat.t_polAv += evslcu_marks_elapsed(marks, 0, 1);
+      evslstat.t_reorth += evslcu_marks_elapsed(marks, 1, 2);
+    }
     const double alpha = h[0];
     beta = h[1];
     dT[k] = alpha;
@@ -216,6 +228,7 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
 cuda_fail:
   rc = evsl_seterr(rc, "%s", evslcu_errstr());
 done:
+  evslcu_marks_destroy(marks);
   evslcu_free(V);
   evslcu_free(wk);
   evslcu_free(vrand);
