@@ -19,7 +19,7 @@ ecnt 1e-10 relative.  Both errors are printed.
 For the Rademacher probes on 10^6 rows the reference's own moments are off
 by ~1.5e-12 of max |mu|: every probe entry has the same magnitude, so the
 rounding of its sequential FP64 dot over 10^6 terms is systematic.  That
-case is therefore judged against the moments of the reference's own FP64
+case is therefore checked against the moments of the reference's own FP64
 recurrence with every dot accumulated in extended precision (the
 `exactdot` fixture): the library must be within the bars of those, and its
 distance to the reference's printed moments must not exceed the reference's
