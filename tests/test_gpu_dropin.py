@@ -43,3 +43,36 @@ def test_reference_driver_runs_unchanged_on_this_library(tmp_path, args, nslices
     assert len(rows) >= sum(min(int(a), 52) for a, _ in counts) - nslices
     assert max(abs(float(r[3])) for r in rows) <= 1e-10 * width
     assert max(float(r[1]) for r in rows) <= 1e-6
+
+
+REF_CUDA_DRIVER = os.path.join(ROOT, "oracle", "_ref", "cuda", "LapPLanN_refcuda.ex")
+
+
+def test_reference_cuda_build_under_the_same_driver(tmp_path):
+    """The same driver on the reference's own CUDA build (cuSPARSE / cuBLAS,
+    `make -C oracle cuda`) and on this library, on one problem: both find
+    every eigenvalue of every slice (counts from the driver's own check
+    against the analytic spectrum), and this library's run reports the
+    filter and reorthogonalisation times the reference's StatsPrint
+    reports."""
+    if not os.path.exists(REF_CUDA_DRIVER):
+        pytest.skip("the reference CUDA build is not built (make -C oracle cuda)")
+    args = ["-nx", "30", "-ny", "30", "-nz", "30", "-a", "0.5", "-b", "0.9", "-nslices", "2"]
+    found = {}
+    for name, exe in (("ref", REF_CUDA_DRIVER), ("b200", DRIVER)):
+        d = tmp_path / name
+        d.mkdir()
+        p = subprocess.run([exe] + args, cwd=d, capture_output=True, text=True, timeout=600)
+        assert p.returncode == 0, p.stdout + p.stderr
+        counts = re.findall(r"number of eigenvalues: (\d+), found: (\d+)", p.stdout)
+        assert len(counts) == 2 and all(int(a) == int(b) > 0 for a, b in counts), (name, counts)
+        found[name] = sum(int(a) for a, _ in counts)
+        out = open(os.path.join(d, "OUT", "LapPLanN.out")).read()
+        if name == "b200":
+            pol = re.findall(r"Pol\(A\)\*v\s+:\s+([0-9.]+)", out)
+            reo = re.findall(r"Reorthogonalization\s+:\s+([0-9.]+)", out)
+            assert len(pol) == 2 and all(float(t) > 0 for t in pol), out[-800:]
+            assert len(reo) == 2 and all(float(t) > 0 for t in reo), out[-800:]
+    # the slices come from each library's own random probes, so their end
+    # points differ; the eigenvalues of [a, b] are the same set
+    assert found["ref"] == found["b200"]
