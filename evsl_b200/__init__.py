@@ -262,6 +262,7 @@ def load():
         "StatsReset": ([], None),
         "evslx_last_solve_info": ([_ip, _ip], C.c_int),
         "evslx_set_filter_persistent": ([C.c_int], C.c_int),
+        "evslx_set_async_tests": ([C.c_int], C.c_int),
         "evslx_set_filter_block": ([C.c_int], C.c_int),
         "evslx_set_filter_rows_per_thread": ([C.c_int], C.c_int),
         "evslx_set_matrix_compression": ([C.c_int], C.c_int),
@@ -617,6 +618,10 @@ class Library:
 
     def set_l2_resident(self, on):
         self._check(self.lib.evslx_set_l2_resident(1 if on else 0), "evslx_set_l2_resident")
+
+    def set_async_tests(self, on):
+        """ChebLanNr's convergence tests on a side stream (default) or waited for."""
+        self._check(self.lib.evslx_set_async_tests(1 if on else 0), "evslx_set_async_tests")
 
     def set_filter_persistent(self, on):
         self._check(self.lib.evslx_set_filter_persistent(1 if on else 0), "evslx_set_filter_persistent")

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
@@ -73,33 +74,27 @@ __global__ void __launch_bounds__(kTridThreads)
 double *g_trid_buf = nullptr;
 int g_trid_cap = 0;
 
-}  // namespace
-}  // namespace evslcu
+// Side-stream form for the convergence tests: inputs staged in pinned host
+// memory, the bisection on its own stream, the result copied back
+// asynchronously; the solver reads it when it needs it.
+cudaStream_t g_side = nullptr;
+cudaEvent_t g_main_mark = nullptr, g_side_done = nullptr;
+double *g_pin = nullptr;  // pinned: d | e2 | w, g_pin_cap each
+int g_pin_cap = 0;
+struct {
+  bool pending;
+  int k, i0;
+  double glo;
+} g_async = {false, 0, 0, 0.0};
 
-using namespace evslcu;
+// Gershgorin interval (widened), pivot floor, squared off-diagonals (into
+// e2[0..k-1)) and the first index that may reach xmin (see below).
+struct TridPrep {
+  double glo, ghi, pivmin;
+  int i0;
+};
 
-extern "C" {
-
-void evslcu_trid_release(void) {
-  evslcu_free(g_trid_buf);
-  g_trid_buf = nullptr;
-  g_trid_cap = 0;
-}
-
-int evslcu_trid_eigvals_above(int k, const double *d, const double *e, double xmin, double *w) {
-  if (k <= 0) return 0;
-  if (!d || !w || (k > 1 && !e)) return fail(EVSLCU_ERR_ARG, "evslcu_trid_eigvals: bad arguments");
-  if (k > g_trid_cap) {
-    evslcu_free(g_trid_buf);
-    g_trid_cap = std::max(k, 1024);
-    g_trid_buf = (double *)evslcu_malloc(sizeof(double) * 3 * (size_t)g_trid_cap);
-    if (!g_trid_buf) {
-      g_trid_cap = 0;
-      return fail(EVSLCU_ERR_NOMEM, "tridiagonal eigenvalues: out of device memory");
-    }
-  }
-  // squared off-diagonals, Gershgorin interval and the pivot floor
-  std::vector<double> e2((size_t)std::max(k - 1, 1), 0.0);
+TridPrep trid_prep(int k, const double *d, const double *e, double xmin, double *e2) {
   double emax = 0.0, glo = d[0], ghi = d[0];
   for (int j = 0; j < k; ++j) {
     const double ej = (j + 1 < k) ? fabs(e[j]) : 0.0;
@@ -133,19 +128,129 @@ int evslcu_trid_eigvals_above(int k, const double *d, const double *e, double xm
     }
     i0 = std::max(0, cnt - 1);
   }
-  double *dd = g_trid_buf, *de2 = g_trid_buf + g_trid_cap, *dw = g_trid_buf + 2 * (size_t)g_trid_cap;
-  int rc = evslcu_h2d_async(dd, d, sizeof(double) * (size_t)k);
-  if (!rc && k > 1) rc = evslcu_h2d_async(de2, e2.data(), sizeof(double) * (size_t)(k - 1));
-  if (rc) return rc;
-  if (i0 < k) {
-    const long long threads = 32LL * (k - i0);
-    const int grid = (int)((threads + kTridThreads - 1) / kTridThreads);
-    k_trid_bisect<<<grid, kTridThreads, 0, stream()>>>(k, i0, dd, de2, glo, ghi, pivmin, dw);
-    count_launch();
-    if ((rc = check_launch("k_trid_bisect"))) return rc;
-    if ((rc = evslcu_d2h(w + i0, dw + i0, sizeof(double) * (size_t)(k - i0)))) return rc;
+  return {glo, ghi, pivmin, i0};
+}
+
+int trid_device_buffers(int k) {
+  if (k <= g_trid_cap) return 0;
+  evslcu_free(g_trid_buf);
+  g_trid_cap = std::max(k, 1024);
+  g_trid_buf = (double *)evslcu_malloc(sizeof(double) * 3 * (size_t)g_trid_cap);
+  if (!g_trid_buf) {
+    g_trid_cap = 0;
+    return fail(EVSLCU_ERR_NOMEM, "tridiagonal eigenvalues: out of device memory");
   }
-  for (int i = 0; i < i0; ++i) w[i] = glo;  // below every computed eigenvalue and below xmin
+  return 0;
+}
+
+int trid_launch(int k, const TridPrep &p, cudaStream_t st) {
+  if (p.i0 >= k) return 0;
+  double *dd = g_trid_buf, *de2 = g_trid_buf + g_trid_cap, *dw = g_trid_buf + 2 * (size_t)g_trid_cap;
+  const long long threads = 32LL * (k - p.i0);
+  const int grid = (int)((threads + kTridThreads - 1) / kTridThreads);
+  k_trid_bisect<<<grid, kTridThreads, 0, st>>>(k, p.i0, dd, de2, p.glo, p.ghi, p.pivmin, dw);
+  count_launch();
+  return check_launch("k_trid_bisect");
+}
+
+}  // namespace
+}  // namespace evslcu
+
+using namespace evslcu;
+
+extern "C" {
+
+void evslcu_trid_release(void) {
+  if (g_async.pending) {
+    cudaEventSynchronize(g_side_done);
+    g_async.pending = false;
+  }
+  evslcu_free(g_trid_buf);
+  g_trid_buf = nullptr;
+  g_trid_cap = 0;
+  if (g_pin) cudaFreeHost(g_pin);
+  g_pin = nullptr;
+  g_pin_cap = 0;
+  if (g_side) {
+    cudaStreamDestroy(g_side);
+    cudaEventDestroy(g_main_mark);
+    cudaEventDestroy(g_side_done);
+    g_side = nullptr;
+    g_main_mark = g_side_done = nullptr;
+  }
+}
+
+int evslcu_trid_eigvals_above(int k, const double *d, const double *e, double xmin, double *w) {
+  if (k <= 0) return 0;
+  if (!d || !w || (k > 1 && !e)) return fail(EVSLCU_ERR_ARG, "evslcu_trid_eigvals: bad arguments");
+  // a side-stream test still reading the device buffers goes first
+  if (g_async.pending) EVSLCU_CUDA(cudaStreamWaitEvent(stream(), g_side_done, 0));
+  int rc = trid_device_buffers(k);
+  if (rc) return rc;
+  std::vector<double> e2((size_t)std::max(k - 1, 1), 0.0);
+  const TridPrep p = trid_prep(k, d, e, xmin, e2.data());
+  double *dd = g_trid_buf, *de2 = g_trid_buf + g_trid_cap, *dw = g_trid_buf + 2 * (size_t)g_trid_cap;
+  rc = evslcu_h2d_async(dd, d, sizeof(double) * (size_t)k);
+  if (!rc && k > 1) rc = evslcu_h2d_async(de2, e2.data(), sizeof(double) * (size_t)(k - 1));
+  if (!rc) rc = trid_launch(k, p, stream());
+  if (!rc && p.i0 < k) rc = evslcu_d2h(w + p.i0, dw + p.i0, sizeof(double) * (size_t)(k - p.i0));
+  if (rc) return rc;
+  for (int i = 0; i < p.i0; ++i) w[i] = p.glo;  // below every computed eigenvalue and below xmin
+  std::sort(w, w + k);
+  return 0;
+}
+
+int evslcu_trid_eigvals_async(int k, const double *d, const double *e, double xmin) {
+  if (k <= 0 || !d || (k > 1 && !e)) return fail(EVSLCU_ERR_ARG, "evslcu_trid_eigvals_async: bad arguments");
+  if (g_async.pending) return fail(EVSLCU_ERR_ARG, "evslcu_trid_eigvals_async: a test is still in flight");
+  if (!g_side) {
+    EVSLCU_CUDA(cudaStreamCreateWithFlags(&g_side, cudaStreamNonBlocking));
+    EVSLCU_CUDA(cudaEventCreateWithFlags(&g_main_mark, cudaEventDisableTiming));
+    EVSLCU_CUDA(cudaEventCreateWithFlags(&g_side_done, cudaEventDisableTiming));
+  }
+  if (k > g_pin_cap) {
+    if (g_pin) cudaFreeHost(g_pin);
+    g_pin = nullptr;
+    const int cap = std::max(k, 2 * g_pin_cap);
+    EVSLCU_CUDA(cudaMallocHost(&g_pin, sizeof(double) * 3 * (size_t)cap));
+    g_pin_cap = cap;
+  }
+  int rc = trid_device_buffers(k);
+  if (rc) return rc;
+  double *pd = g_pin, *pe2 = g_pin + g_pin_cap, *pw = g_pin + 2 * (size_t)g_pin_cap;
+  memcpy(pd, d, sizeof(double) * (size_t)k);
+  const TridPrep p = trid_prep(k, d, e, xmin, pe2);
+  double *dd = g_trid_buf, *de2 = g_trid_buf + g_trid_cap, *dw = g_trid_buf + 2 * (size_t)g_trid_cap;
+  // the device buffers come from the library stream's pool: order the side
+  // stream after it
+  EVSLCU_CUDA(cudaEventRecord(g_main_mark, stream()));
+  EVSLCU_CUDA(cudaStreamWaitEvent(g_side, g_main_mark, 0));
+  EVSLCU_CUDA(cudaMemcpyAsync(dd, pd, sizeof(double) * (size_t)k, cudaMemcpyHostToDevice, g_side));
+  if (k > 1) EVSLCU_CUDA(cudaMemcpyAsync(de2, pe2, sizeof(double) * (size_t)(k - 1), cudaMemcpyHostToDevice, g_side));
+  if ((rc = trid_launch(k, p, g_side))) return rc;
+  if (p.i0 < k)
+    EVSLCU_CUDA(cudaMemcpyAsync(pw + p.i0, dw + p.i0, sizeof(double) * (size_t)(k - p.i0), cudaMemcpyDeviceToHost,
+                                g_side));
+  EVSLCU_CUDA(cudaEventRecord(g_side_done, g_side));
+  g_async = {true, k, p.i0, p.glo};
+  return 0;
+}
+
+int evslcu_trid_eigvals_async_ready(void) {
+  if (!g_async.pending) return 1;
+  const cudaError_t e = cudaEventQuery(g_side_done);
+  if (e == cudaErrorNotReady) return 0;
+  return 1;  // finished, or failed: the wait reports the error
+}
+
+int evslcu_trid_eigvals_async_wait(double *w) {
+  if (!g_async.pending) return fail(EVSLCU_ERR_ARG, "evslcu_trid_eigvals_async_wait: no test in flight");
+  g_async.pending = false;
+  EVSLCU_CUDA(cudaEventSynchronize(g_side_done));
+  const int k = g_async.k, i0 = g_async.i0;
+  const double *pw = g_pin + 2 * (size_t)g_pin_cap;
+  if (i0 < k) memcpy(w + i0, pw + i0, sizeof(double) * (size_t)(k - i0));
+  for (int i = 0; i < i0; ++i) w[i] = g_async.glo;
   std::sort(w, w + k);
   return 0;
 }

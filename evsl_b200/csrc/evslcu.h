@@ -367,6 +367,13 @@ int evslcu_trid_eigvals(int k, const double *d, const double *e, double *w);
  * those of evslcu_trid_eigvals); the entries of the eigenvalues well below
  * xmin hold a value below xmin instead.  Ascending. */
 int evslcu_trid_eigvals_above(int k, const double *d, const double *e, double xmin, double *w);
+/* The same computation started on a side stream (inputs copied at the call;
+ * one test in flight at a time): _ready returns 1 once it has finished (or
+ * when none is in flight), _wait blocks for it and writes w as
+ * evslcu_trid_eigvals_above would (same values). */
+int evslcu_trid_eigvals_async(int k, const double *d, const double *e, double xmin);
+int evslcu_trid_eigvals_async_ready(void);
+int evslcu_trid_eigvals_async_wait(double *w);
 /* Pattern tables read from the constant-memory pool when they fit there (1,
  * default) or always from global memory (0).  Same arithmetic either way. */
 int evslcu_set_pattern_const(int on);

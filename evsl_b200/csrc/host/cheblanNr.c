@@ -23,6 +23,35 @@
 #define NR_NTEST 30
 #define NR_CYCLE 20
 
+/* Restricted-trace convergence test on the eigenvalues of T_kdim
+ * (SRC/cheblanNr.c:269-309): 1 when converged; *tr0 carries the previous
+ * trace. */
+static int trace_converged(int kdim, const double *EvalT, double bar, double *tr0, int do_print, FILE *fstats) {
+  double tr1 = 0.0;
+  int nconv = 0;
+  for (int i = 0; i < kdim; i++) {
+    const double flami = EvalT[i];
+    if (flami + EVSL_DBL_EPS_MULT * DBL_EPSILON >= bar) {
+      tr1 += flami;
+      nconv++;
+    }
+  }
+  if (do_print) fprintf(fstats, "k %4d: nconv %4d  tr1 %21.15e\n", kdim - 1, nconv, tr1);
+  if ((fabs(tr1 - *tr0) < 2e-12) || (fabs(tr1) + fabs(*tr0) < 1e-10)) return 1;
+  *tr0 = tr1;
+  return 0;
+}
+
+/* Read the side-stream test of T_kd into EvalT and apply the trace test. */
+static int read_pending(int kd, double *EvalT, double bar, double *tr0, int do_print, FILE *fstats, int *conv) {
+  const double te = evsl_timer();
+  const int rc = evsl_trid_test_wait(EvalT);
+  evslstat.t_eig += evsl_timer() - te;
+  if (rc) return rc;
+  *conv = trace_converged(kd, EvalT, bar, tr0, do_print, fstats);
+  return 0;
+}
+
 int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol, int *nevOut, double **lamo,
               double **Wo, double **reso, FILE *fstats) {
   const double tall = evsl_timer();
@@ -64,6 +93,7 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
   int kdim = 0, count = 0, nev = 0;
   double tt_ritz = 0.0;
   evslcu_marks *marks = NULL;
+  int pend_k = 0; /* Lanczos dimension of the test running on the side stream */
   if (!V || !wk || !vrand || !cgsw || !ds || !dT || !eT || !EvalT) {
     rc = evsl_seterr(EVSLX_ERR_NOMEM, "ChebLanNr: out of memory for a basis of %d x %d", n, maxit + 1);
     goto done;
@@ -83,7 +113,14 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
    * every step go to evslstat.t_polAv / t_reorth (events read after the
    * step's scalar read has synchronised) */
   marks = fstats ? evslcu_marks_create(3) : NULL;
-  double wn = 0.0, tr0 = 0.0, tr1 = 0.0, beta = 0.0;
+  /* Convergence tests run on a side stream while the next steps proceed;
+   * each is read at the next test point, at the last step, before a lucky
+   * breakdown draws random numbers, or as soon as it has finished.  Steps
+   * taken past a test that reports convergence are discarded, so the result
+   * is that of waiting for every test. */
+  const int async_tests = !evslh.sync_tests;
+  const double xmin = bar - EVSL_DBL_EPS_MULT * DBL_EPSILON;
+  double wn = 0.0, tr0 = 0.0, beta = 0.0;
   int nwn = 0, k;
   for (k = 0; k < maxit; k++) {
     const double *zold = (k > 0) ? V + (size_t)(k - 1) * n_l : NULL;
@@ -112,6 +149,16 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
     wn += 2.0 * beta;
     nwn += 3;
     if (beta * nwn < EVSL_ORTH_TOL * wn) {
+      if (pend_k) {
+        const int kd = pend_k;
+        int conv = 0;
+        pend_k = 0;
+        if ((rc = read_pending(kd, EvalT, bar, &tr0, do_print, fstats, &conv))) goto done;
+        if (conv) {
+          kdim = count = kd;
+          break;
+        }
+      }
       if (do_print) fprintf(fstats, "it %4d: Lucky breakdown, beta = %.15e\n", k, beta);
       /* restart from a new filtered random vector */
       if ((rc = evsl_rand_device(n, 1, vrand))) goto done;
@@ -126,24 +173,35 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
       if ((rc = evslcu_scal(n, t, vnew))) goto cuda_fail;
     }
     eT[k] = beta;
-    if ((k < NR_NTEST || (k - NR_NTEST) % NR_CYCLE != 0) && k != maxit - 1) continue;
-    kdim = k + 1;
-    const double te = evsl_timer();
-    if ((rc = evsl_trid_eigvals_test(kdim, dT, eT, bar - EVSL_DBL_EPS_MULT * DBL_EPSILON, EvalT))) goto done;
-    evslstat.t_eig += evsl_timer() - te;
-    count = kdim;
-    tr1 = 0.0;
-    int nconv = 0;
-    for (int i = 0; i < count; i++) {
-      const double flami = EvalT[i];
-      if (flami + EVSL_DBL_EPS_MULT * DBL_EPSILON >= bar) {
-        tr1 += flami;
-        nconv++;
+    const int test_here = !((k < NR_NTEST || (k - NR_NTEST) % NR_CYCLE != 0) && k != maxit - 1);
+    if (pend_k && (test_here || evsl_trid_test_ready())) {
+      const int kd = pend_k;
+      int conv = 0;
+      pend_k = 0;
+      if ((rc = read_pending(kd, EvalT, bar, &tr0, do_print, fstats, &conv))) goto done;
+      if (conv) {
+        kdim = count = kd;
+        break;
       }
     }
-    if (do_print) fprintf(fstats, "k %4d: nconv %4d  tr1 %21.15e\n", k, nconv, tr1);
-    if ((fabs(tr1 - tr0) < 2e-12) || (fabs(tr1) + fabs(tr0) < 1e-10)) break;
-    tr0 = tr1;
+    if (!test_here) continue;
+    kdim = k + 1;
+    if (async_tests && k != maxit - 1) {
+      const int st = evsl_trid_test_start(kdim, dT, eT, xmin);
+      if (st < 0) {
+        rc = st;
+        goto done;
+      }
+      if (st == 1) {
+        pend_k = kdim;
+        continue;
+      }
+    }
+    const double te = evsl_timer();
+    if ((rc = evsl_trid_eigvals_test(kdim, dT, eT, xmin, EvalT))) goto done;
+    evslstat.t_eig += evsl_timer() - te;
+    count = kdim;
+    if (trace_converged(kdim, EvalT, bar, &tr0, do_print, fstats)) break;
   }
   if (k >= maxit && do_print)
     fprintf(fstats,
@@ -228,6 +286,7 @@ int ChebLanNr(double *intv, int maxit, double tol, double *vinit, polparams *pol
 cuda_fail:
   rc = evsl_seterr(rc, "%s", evslcu_errstr());
 done:
+  if (pend_k) evsl_trid_test_wait(EvalT); /* an error left a test in flight */
   evslcu_marks_destroy(marks);
   evslcu_free(V);
   evslcu_free(wk);

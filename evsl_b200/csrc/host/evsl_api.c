@@ -609,6 +609,11 @@ int evslx_set_filter_persistent(int on) {
 
 int evslx_set_matrix_compression(int on) { return from_cu(evslcu_set_compression(on)); }
 
+int evslx_set_async_tests(int on) {
+  evslh.sync_tests = on ? 0 : 1;
+  return 0;
+}
+
 int evslx_set_sell_sigma(int sigma) { return from_cu(evslcu_set_sell_sigma(sigma)); }
 
 int evslx_set_wait_limit(unsigned long long polls) { return from_cu(evslcu_set_wait_limit(polls)); }

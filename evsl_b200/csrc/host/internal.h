@@ -36,6 +36,7 @@ typedef struct {
   int last_kdim;             /* Lanczos dimension of the last ChebLanNr/ChebLanTr */
   int last_candidates;       /* Ritz values >= bar examined at the end */
   double last_filter_seconds;
+  int sync_tests;            /* 1: ChebLanNr waits for each convergence test */
 } evsl_host_state;
 
 extern evsl_host_state evslh;
@@ -52,6 +53,11 @@ int evsl_check_intv(const double *intv, FILE *fstats);
 int evsl_trid_eig_first(int n, const double *d, const double *e, double *w, double *z1);
 int evsl_trid_eigvals(int n, const double *d, const double *e, double *w);
 int evsl_trid_eigvals_test(int n, const double *d, const double *e, double xmin, double *w);
+/* the same test on a side stream: 1 when started, 0 when the size is below
+ * the GPU threshold (the caller runs it directly), a negative error code */
+int evsl_trid_test_start(int n, const double *d, const double *e, double xmin);
+int evsl_trid_test_ready(void);
+int evsl_trid_test_wait(double *w);
 int evsl_trid_eigvecs(int n, const double *d, const double *e, int m, const double *w, double *Z, int ldz);
 int evsl_sym_eig(int n, const double *A, int lda, double *Q, int ldq, double *w);
 int evsl_tr_eig(int k, int m, const double *T, int ldt, double thresh, double *w, double *Z, int ldz);

@@ -156,6 +156,21 @@ int evsl_trid_eigvals_test(int n, const double *d, const double *e, double xmin,
   return 0;
 }
 
+int evsl_trid_test_start(int n, const double *d, const double *e, double xmin) {
+  if (n < TRID_GPU_MIN) return 0;
+  const int rc = evslcu_trid_eigvals_async(n, d, e, xmin);
+  if (rc) return evsl_seterr(EVSLX_ERR_CUDA, "%s", evslcu_errstr());
+  return 1;
+}
+
+int evsl_trid_test_ready(void) { return evslcu_trid_eigvals_async_ready(); }
+
+int evsl_trid_test_wait(double *w) {
+  const int rc = evslcu_trid_eigvals_async_wait(w);
+  if (rc) return evsl_seterr(EVSLX_ERR_CUDA, "%s", evslcu_errstr());
+  return 0;
+}
+
 /* Eigenvalues (ascending) of the symmetric tridiagonal (d, e) and the first
  * component of each normalised eigenvector (the Lanczos quadrature weights
  * come from their squares): the QL rotations are applied to e_1^T only. */

@@ -106,6 +106,13 @@ int evslx_get_spmv_kernel(void);
  * cooperative kernel (bounded grid barriers between degrees, per-row state in
  * shared memory).  Results are identical bit for bit. */
 int evslx_set_filter_persistent(int on);
+
+/* ChebLanNr's convergence tests (the eigenvalues of T_k every 20 steps):
+ * 1 (default) runs each on a side stream while the next Lanczos steps
+ * proceed and reads it at the next test point or when it finishes (steps
+ * taken past a converged test are discarded); 0 waits for each test.  The
+ * results are identical bit for bit. */
+int evslx_set_async_tests(int on);
 /* Rows each thread of the per-degree filter kernel handles (1 or 2, default
  * 1; 2 gives each thread two independent load chains, measured slower on
  * the 3-D Laplacian).  Results are identical. */

@@ -239,6 +239,35 @@ def test_cheblan_nr_config1(gpu_lib, golden):
     gpu_lib.free_pol(pol)
 
 
+@pytest.mark.parametrize("grid, iv, maxit", [
+    ((100, 100, 1), [0.6, 0.9, 0.0, 8.0], 2000),         # config 1
+    ((40, 40, 40), [0.6, 0.8, 0.0, 12.0], 3000),         # tests overlap steps of a larger basis
+    ((12, 12, 1), [0.2, 7.8, 0.0, 8.0], 140),            # nearly the whole spectrum, basis near n
+    ((40, 40, 1), [0.6, 1.2, 0.0, 8.0], 95),             # maxit reached with a test in flight
+])
+def test_cheblan_nr_side_stream_tests_bitwise(gpu_lib, grid, iv, maxit):
+    """ChebLanNr with its convergence tests on a side stream (the default)
+    gives bit for bit what waiting for every test gives: eigenvalues,
+    residuals, eigenvectors and the Lanczos dimension."""
+    _lap(gpu_lib, *grid)
+    n = grid[0] * grid[1] * grid[2]
+    pol = gpu_lib.find_pol(iv, damping=2, thresh_int=0.8, thresh_ext=0.2, max_deg=3000)
+    v = O.seeded_normal(n, 77)
+    out = {}
+    try:
+        for on in (False, True):
+            gpu_lib.set_async_tests(on)
+            gpu_lib.set_seed(2024)  # lucky breakdowns draw restart vectors from the device RNG
+            lam, Y, res = gpu_lib.cheblan_nr(iv, maxit, 1e-8, v, pol, want_vectors=True)
+            out[on] = (lam, Y, res, gpu_lib.last_solve_info())
+    finally:
+        gpu_lib.set_async_tests(True)
+        gpu_lib.free_pol(pol)
+    a, b = out[False], out[True]
+    assert a[3] == b[3]
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+
+
 def test_cheblan_tr_small_matches_reference(gpu_lib, golden):
     _lap(gpu_lib, 20, 20, 1)
     pol = gpu_lib.find_pol([0.6, 1.2, 0.0, 8.0])
