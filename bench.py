@@ -77,7 +77,7 @@ def parse():
                    help="serve: 'small' draws the large-matrix requests on the 2-D 100x100 Laplacian only")
     p.add_argument("--rspd-n", type=int, default=RSPD_N, help="rspd-filter: rows of the random SPD matrix")
     p.add_argument("--dgemm-kernel", type=int, choices=[-1, 0, 1, 2], default=-1,
-                   help="dgemm: 0 the 64x64 kernel, 1 the 128x128 DFMA kernel, 2 the mma.sync f64 kernel "
+                   help="dgemm, block-cgs: 0 the 64x64 kernel, 1 the 128x128 DFMA kernel, 2 the mma.sync f64 kernel "
                         "(-1: library default)")
     p.add_argument("--grid", type=int, default=50,
                    help="lap3d-pipeline: the 3-D Laplacian's grid points per side")
@@ -1014,6 +1014,8 @@ def run_block_cgs(args):
 
     n, m, b = (int(x) for x in args.gemm.split(","))
     lib = E.Library()
+    if args.dgemm_kernel >= 0:
+        lib.lib.evslcu_set_dgemm_tiled(args.dgemm_kernel)
     lib.lib.evslcu_fp64_probe.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
     dfma, dmma = C.c_double(), C.c_double()
     lib._check(lib.lib.evslcu_fp64_probe(C.byref(dfma), C.byref(dmma)), "evslcu_fp64_probe")
