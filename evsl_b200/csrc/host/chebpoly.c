@@ -18,6 +18,9 @@
  */
 #include "internal.h"
 
+#include <pthread.h>
+#include <unistd.h>
+
 void set_pol_def(polparams *pol) {
   pol->max_deg = 10000;
   pol->min_deg = 2;
@@ -171,6 +174,104 @@ static int rootchb(int m, const double *v, const double *jac, double tha, double
   return 0;
 }
 
+/* One candidate degree m of the mid-interval design: damping, balance,
+ * peak and end values (each candidate is independent of the others). */
+typedef struct {
+  int skip, pass;
+} fp_result;
+
+static fp_result fp_candidate(int m, int damping, const double *v, double tha, double thb, int nitv,
+                              const double *itv, double thresh, double *jac, double *mu, double *gam, double *t,
+                              double *vals) {
+  fp_result r = {0, 0};
+  double thc = 0.0;
+  dampcf(m, damping, jac);
+  if (rootchb(m, v, jac, tha, thb, mu, &thc)) {
+    r.skip = 1;
+    return r;
+  }
+  *gam = cos(thc);
+  cheb_series(m, mu, 1, gam, t);
+  cheb_series(m, mu, nitv, itv, vals);
+  r.pass = (vals[0] <= *t * thresh && vals[1] <= *t * thresh);
+  return r;
+}
+
+/* The degree search over host threads: candidates are taken in increasing
+ * order from a shared counter; a worker stops taking them once a passing
+ * degree below its next candidate is known.  Every degree below the
+ * smallest passing one is evaluated, so the first passing degree (or, with
+ * none, the last degree that balances) is the sequential search's. */
+typedef struct {
+  int next, best; /* next candidate; smallest passing degree so far */
+  int min_deg, max_deg, damping, nitv;
+  const double *v, *itv;
+  double tha, thb, thresh;
+  unsigned char *state; /* per candidate: 1 skipped, 2 balanced, 3 passed */
+} fp_search;
+
+typedef struct {
+  fp_search *S;
+  double *jac, *mu;
+} fp_worker;
+
+static void *fp_worker_run(void *arg) {
+  fp_worker *w = (fp_worker *)arg;
+  fp_search *S = w->S;
+  for (;;) {
+    const int m = __atomic_fetch_add(&S->next, 1, __ATOMIC_RELAXED);
+    if (m >= S->max_deg || m > __atomic_load_n(&S->best, __ATOMIC_RELAXED)) break;
+    double gam = 0.0, t = 0.0, vals[2] = {0.0, 0.0};
+    const fp_result r = fp_candidate(m, S->damping, S->v, S->tha, S->thb, S->nitv, S->itv, S->thresh, w->jac, w->mu,
+                                     &gam, &t, vals);
+    __atomic_store_n(&S->state[m - S->min_deg], (unsigned char)(r.skip ? 1 : (r.pass ? 3 : 2)), __ATOMIC_RELAXED);
+    if (r.pass) {
+      int cur = __atomic_load_n(&S->best, __ATOMIC_RELAXED);
+      while (m < cur && !__atomic_compare_exchange_n(&S->best, &cur, m, 0, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+      }
+    }
+  }
+  return NULL;
+}
+
+#define FP_MAX_THREADS 16
+#define FP_THREAD_MIN_DEG 100 /* below this the candidates are too cheap to share out */
+
+/* Runs the search on threads; returns the degree whose design the
+ * sequential loop ends with (first passing, else the last balanced one, or
+ * -1 when none balanced) and *mend, the loop's final counter. */
+static int fp_search_threads(fp_search *S, int nth, int *mend) {
+  const int ncand = S->max_deg - S->min_deg;
+  fp_worker wk[FP_MAX_THREADS];
+  pthread_t tid[FP_MAX_THREADS];
+  double *buf = (double *)malloc(sizeof(double) * 2 * (size_t)(S->max_deg + 1) * (size_t)nth);
+  if (!buf || !S->state) {
+    free(buf);
+    return -2;
+  }
+  for (int i = 0; i < nth; i++) {
+    wk[i].S = S;
+    wk[i].jac = buf + (size_t)2 * i * (size_t)(S->max_deg + 1);
+    wk[i].mu = wk[i].jac + (S->max_deg + 1);
+  }
+  int started = 0;
+  for (int i = 1; i < nth; i++) {
+    if (pthread_create(&tid[i], NULL, fp_worker_run, &wk[i]) != 0) break;
+    started = i;
+  }
+  fp_worker_run(&wk[0]);
+  for (int i = 1; i <= started; i++) pthread_join(tid[i], NULL);
+  free(buf);
+  if (S->best < S->max_deg) {
+    *mend = S->best + 1;
+    return S->best;
+  }
+  *mend = S->max_deg;
+  for (int c = ncand - 1; c >= 0; c--)
+    if (S->state[c] == 2) return S->min_deg + c;
+  return -1;
+}
+
 int find_pol(double *intv, polparams *pol) {
   int max_deg = pol->max_deg, min_deg = pol->min_deg;
   const int damping = pol->damping;
@@ -238,17 +339,34 @@ int find_pol(double *intv, polparams *pol) {
       max_deg = pol->deg;
     }
     for (int j = 0; j < min_deg; j++) v[j] = cos(j * thb) - cos(j * tha);
-    int m;
-    for (m = min_deg; m < max_deg; m++) {
-      dampcf(m, damping, jac);
-      v[m] = cos(m * thb) - cos(m * tha);
-      if (rootchb(m, v, jac, tha, thb, mu, &thc)) continue;
-      gam = cos(thc);
-      cheb_series(m, mu, 1, &gam, &t);
-      cheb_series(m, mu, nitv, itv, vals);
-      if (vals[0] <= t * thresh && vals[1] <= t * thresh) {
-        m++;
-        break;
+    int m = min_deg;
+    long nth = (min_deg >= FP_THREAD_MIN_DEG && max_deg - min_deg >= 2) ? sysconf(_SC_NPROCESSORS_ONLN) : 1;
+    nth = evsl_min(evsl_min(nth, (long)FP_MAX_THREADS), (long)(max_deg - min_deg));
+    int done = 0;
+    if (nth > 1) {
+      /* v[j] for every candidate first (the same values the loop forms) */
+      for (int j = min_deg; j < max_deg; j++) v[j] = cos(j * thb) - cos(j * tha);
+      fp_search S = {min_deg, max_deg, min_deg, max_deg, damping, nitv, v, itv, tha, thb, thresh,
+                     (unsigned char *)calloc((size_t)(max_deg - min_deg), 1)};
+      int mend = max_deg;
+      const int mres = fp_search_threads(&S, (int)nth, &mend);
+      free(S.state);
+      if (mres >= -1) {
+        /* the chosen degree's design again, as the loop leaves it */
+        if (mres >= 0) fp_candidate(mres, damping, v, tha, thb, nitv, itv, thresh, jac, mu, &gam, &t, vals);
+        m = mend;
+        done = 1;
+      }
+    }
+    if (!done) {
+      for (m = min_deg; m < max_deg; m++) {
+        v[m] = cos(m * thb) - cos(m * tha);
+        const fp_result r = fp_candidate(m, damping, v, tha, thb, nitv, itv, thresh, jac, mu, &gam, &t, vals);
+        if (r.skip) continue;
+        if (r.pass) {
+          m++;
+          break;
+        }
       }
     }
     const int mbest = m - 1;

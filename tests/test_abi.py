@@ -161,3 +161,37 @@ def test_tridiagonal_eigenvectors_host(k, m, kind):
     TZ = d * Z + np.c_[Z[:, 1:] * e, np.zeros(m)] + np.c_[np.zeros(m), Z[:, :-1] * e]
     assert np.max(np.abs(TZ - sel[:, None] * Z)) <= 1e-12 * tn
     assert np.max(np.abs(Z @ Z.T - np.eye(m))) <= 1e-12
+
+
+@pytest.mark.skipif(not os.path.exists(O.REF_LIB_PATH), reason="reference build oracle/_ref not present")
+def test_find_pol_threaded_search_matches_reference_bitwise():
+    """The library's filter design on narrow mid-spectrum intervals, where
+    the degree search runs over host threads (starting degree >= 100),
+    designed and forced degrees and all three dampings: degree, type,
+    coefficients, gam and bar equal the reference build's bit for bit."""
+    lib = evsl_b200.load()
+    R = O.RefLib()
+    rng = np.random.default_rng(23)
+    for i in range(18):
+        lo, hi = 0.0, 12.0 + rng.uniform()
+        c = lo + rng.uniform(0.1, 0.9) * (hi - lo)
+        w = (hi - lo) * 10.0 ** rng.uniform(-4.0, -2.5)
+        iv = [c - w / 2, c + w / 2, lo, hi]
+        damping = i % 3
+        # start of the design loop: 2 + 0.5 / (width in [-1, 1])
+        dmin = int(2 + 0.5 / (w / ((hi - lo) / 2))) + 1
+        forced = 0 if i % 2 else int(rng.integers(dmin, dmin + 300))
+        rc_r, pol_r = R.find_pol(iv, damping=damping, thresh_int=0.8, thresh_ext=0.2, max_deg=6000, deg=forced)
+        ref = R.pol_dict(pol_r)
+        R.free_pol(pol_r)
+        pol = evsl_b200.PolParams()
+        lib.set_pol_def(C.byref(pol))
+        pol.damping, pol.thresh_int, pol.thresh_ext, pol.max_deg, pol.deg = damping, 0.8, 0.2, 6000, forced
+        arr = np.ascontiguousarray(iv, dtype=np.float64)
+        rc = lib.find_pol(arr.ctypes.data_as(C.POINTER(C.c_double)), C.byref(pol))
+        assert rc == rc_r == 0, (i, iv)
+        assert pol.deg == ref["deg"] and pol.type == ref["type"], (i, iv, forced, pol.deg, ref["deg"])
+        mu = np.ctypeslib.as_array(pol.mu, (pol.deg + 1,)).copy()
+        assert np.array_equal(mu, ref["mu"]), (i, iv, forced)
+        assert pol.gam == ref["gam"] and pol.bar == ref["bar"], (i, iv, forced)
+        lib.free_pol(C.byref(pol))
